@@ -1,0 +1,390 @@
+#!/usr/bin/env python
+"""Throughput of pp-sketchlib's all-vs-all core/accessory distance path on B200.
+
+Workload (one "step"): the plain all-vs-all of 4,096 bin-level synthetic
+samples (seeded random tree, k = 15, 17, ..., 29, sketchsize64 = 156 x 14 bit
+planes, i.e. 8 k-mer lengths x 10,000 bins): 8,386,560 pairs written as float32
+core/accessory in long form.  Inputs (573 MB of sketches) are larger than L2.
+
+Arms:
+  default            our CUDA path; `value` is device-timed with inputs resident
+                     in HBM, `e2e` goes through the C ABI with pinned host
+                     buffers (upload + pack + distances + result copy per step)
+  --impl reference   the reference's CPU path (oracle/_ref: the reference's own
+                     calc_intersize inside the query_db OpenMP loop) on this
+                     host's cores, on bounded row samples of the same workload
+
+Multi-GPU (torchrun): every rank runs its own replica of the workload (the path
+has no exchange step); value = pairs of all ranks / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "pp-sketchlib_b200"))
+
+METRIC = ("distances/sec @ 8 k × 10k bins (plain vs batched) on 1 B200; "
+          "p50/p99 query latency")
+UNIT = "distances/s"
+N_SAMPLES = 4096
+KMERS = list(range(15, 31, 2))
+S64 = 156
+BBITS = 14
+SEED = 0x5EED0002
+LOP3_PER_PAIR = len(KMERS) * 2 * S64 * BBITS        # one LOP3 per 32 bins per plane
+POPC_PER_PAIR = len(KMERS) * 2 * S64
+PUBLISHED_GPU = 6.0e6   # README.md:137,140 -- RTX 2080 Ti, 8 k x 10,000 bins
+PROFILE_SUMMARY = ROOT / "profiles" / "dist_tiles_kernel_4096.md"
+
+
+def n_pairs(n: int) -> int:
+    return n * (n - 1) // 2
+
+
+def workload_config(extra=None):
+    cfg = {
+        "workload": "plain all-vs-all, 4,096 bin-level synthetic samples (seeded random tree), "
+                    "8 k-mer lengths x 10,000 bins (sketchsize64 156 x 14 planes), float32 "
+                    "core/accessory long form",
+        "n_samples": N_SAMPLES, "kmers": KMERS, "sketchsize64": S64, "bbits": BBITS,
+        "pairs": n_pairs(N_SAMPLES), "seed": SEED,
+        "l2": "inputs larger than L2 (573 MB of packed sketches vs 126 MB L2)",
+    }
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+# ------------------------------------------------------------------ ranks
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def init_dist(world: int, backend: str = "nccl"):
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+
+
+def barrier(world: int, device=None):
+    if world > 1:
+        import torch.distributed as dist
+        if device is not None and dist.get_backend() == "nccl":
+            dist.barrier(device_ids=[device])
+        else:
+            dist.barrier()
+
+
+def reduce_max(value: float, world: int, device: str = "cpu") -> float:
+    """Max of a float over ranks (identity for one rank)."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ----------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples every 200 ms while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in getattr(self, "lines", []):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# -------------------------------------------------------------- baselines
+
+def cpu_reference_rate(target_s: float = 15.0, threads: int | None = None):
+    """The reference's CPU path (oracle/_ref) on a bounded row sample of the
+    workload; falls back to the oracle port when _ref was not built."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import numpy as np
+    import oracle
+    from sketchlib_b200 import capi, synth
+    threads = threads or os.cpu_count() or 1
+    parent, thresh = synth.random_tree(N_SAMPLES, kmers=KMERS, seed=SEED)
+    words = capi.synth_host(parent, thresh, S64, seed=SEED, threads=threads)
+    out = np.zeros((n_pairs(N_SAMPLES), 2), np.float32)
+    if oracle.ref_available():
+        kind = "reference"
+        ref = oracle.RefQueryDb()
+        prep = ref.prepare(words, KMERS, S64)
+
+        def run(r0, r1):
+            return ref.run_rows(prep, r0, r1, out, threads)
+    else:
+        kind = "port"
+
+        def run(r0, r1):
+            return oracle.dists_self_rows(words, KMERS, S64, r0, r1, out, threads)
+    return kind, threads, run, words
+
+
+def sample_rate(run, target_s: float):
+    """Runs row blocks of the all-vs-all until ~target_s of CPU work is done."""
+    row, pairs, elapsed, rows_per = 0, 0, 0.0, 2
+    while elapsed < target_s and row < N_SAMPLES - 1:
+        r1 = min(N_SAMPLES - 1, row + rows_per)
+        t0 = time.perf_counter()
+        done = run(row, r1)
+        dt = time.perf_counter() - t0
+        pairs += done
+        elapsed += dt
+        row = r1
+        if dt < target_s / 8:
+            rows_per *= 2
+    return pairs, elapsed, row
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    kind, threads, run, _ = cpu_reference_rate()
+    # calibrate the step size: ~2 s of CPU work per step
+    pairs, elapsed, _ = sample_rate(run, 1.0)
+    rate = pairs / elapsed
+    rows_per_step = 1
+    while rows_per_step < N_SAMPLES // 4 and rate * 2.0 > (N_SAMPLES - 1) * rows_per_step:
+        rows_per_step *= 2
+    total_pairs, total_t, row = 0, 0.0, 0
+    for step in range(args.warmup + args.steps):
+        r0 = row % (N_SAMPLES - rows_per_step)
+        t0 = time.perf_counter()
+        done = run(r0, r0 + rows_per_step)
+        dt = time.perf_counter() - t0
+        row += rows_per_step
+        if step >= args.warmup:
+            total_pairs += done
+            total_t += dt
+    value = total_pairs / total_t
+    sample = (f"{rows_per_step} consecutive all-vs-all rows of the 4,096-sample workload per step "
+              f"({total_pairs} pairs over {args.steps} steps)")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total_t / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded bin-level tree)",
+        "config": workload_config({"threads": threads}),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- our arm
+
+def profiled_traffic():
+    """DRAM bytes per launch of the distance kernel from the committed ncu
+    summary (line `dram_bytes_per_launch: N`), or None."""
+    try:
+        m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", PROFILE_SUMMARY.read_text())
+        return float(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
+def run_ours(args, rank, world, local):
+    import numpy as np
+    import torch
+    from sketchlib_b200 import capi, synth
+
+    torch.cuda.set_device(local)
+    dev = f"cuda:{local}"
+    ctx = capi.Context(local)
+    stream = torch.cuda.Stream(device=dev)
+    ctx.set_stream(stream.cuda_stream)
+    if args.tile_config:
+        ctx.set_tile_config(args.tile_config)
+
+    seed = SEED + rank
+    parent, thresh = synth.random_tree(N_SAMPLES, kmers=KMERS, seed=seed)
+    words_dev = torch.empty(N_SAMPLES * len(KMERS) * S64 * BBITS, dtype=torch.int64, device=dev)
+    capi.synth_device(ctx, parent, thresh, S64, seed=seed, d_words=words_dev.data_ptr())
+    db = capi.Database(ctx, words_dev.data_ptr(), KMERS, S64, n_samples=N_SAMPLES)
+    pairs = n_pairs(N_SAMPLES)
+    out = torch.empty((pairs, 2), dtype=torch.float32, device=dev)
+
+    lop3_peak, popc_peak = capi.probe_alu_peak(ctx)
+
+    # ---- device-timed, inputs resident in HBM
+    for _ in range(args.warmup):
+        capi.dists_dense(ctx, db, out=out.data_ptr())
+    ctx.synchronize()
+    barrier(world, local)
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with ClockSampler(local) as clocks:
+        with torch.cuda.stream(stream):
+            for s in range(args.steps):
+                starts[s].record(stream)
+                capi.dists_dense(ctx, db, out=out.data_ptr())
+                ends[s].record(stream)
+        ctx.synchronize()
+        torch.cuda.synchronize()
+    barrier(world, local)
+    step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
+    total_s = starts[0].elapsed_time(ends[-1]) / 1e3
+    total_s = reduce_max(total_s, world, dev)
+    value = pairs * world / total_s
+    launch_s = statistics.mean(step_ms) / 1e3
+
+    # ---- end to end through the C ABI with pinned host buffers
+    host_words = torch.empty(words_dev.numel(), dtype=torch.int64, pin_memory=True)
+    host_words.copy_(words_dev.cpu())
+    host_out = torch.empty((pairs, 2), dtype=torch.float32, pin_memory=True)
+    hw = host_words.numpy().view(np.uint64).reshape(N_SAMPLES, len(KMERS), S64 * BBITS)
+    ho = host_out.numpy()
+
+    def e2e_step():
+        d = capi.Database(ctx, hw, KMERS, S64)
+        capi.dists_dense(ctx, d, out=ho)
+        d.close()
+
+    for _ in range(min(args.warmup, 3)):
+        e2e_step()
+    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    barrier(world, local)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    e2e_s = reduce_max(time.perf_counter() - t0, world, dev)
+    e2e_value = pairs * world * e2e_steps / e2e_s
+    # the e2e result must be the resident run's result
+    ok = bool(torch.equal(host_out, out.cpu()))
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        kind, threads, run, _ = cpu_reference_rate()
+        cp, ct, rows = sample_rate(run, args.cpu_seconds)
+        cpu = {"value": cp / ct, "unit": UNIT, "cores": threads, "kind": kind,
+               "sample": f"rows 0..{rows - 1} of the 4,096-sample all-vs-all ({cp} pairs, "
+                         f"{ct:.1f} s)"}
+
+    achieved = pairs * LOP3_PER_PAIR / launch_s
+    traffic = profiled_traffic()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps,
+        "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": value / PUBLISHED_GPU,
+        "dtype": "u32", "data": "synthetic (seeded bin-level tree, generated on device)",
+        "config": workload_config({"tile_config": args.tile_config or "auto",
+                                   "vs_baseline_ref": "reference README.md:137,140 GPU figure, "
+                                                      "6.0e6 distances/s (RTX 2080 Ti)"}),
+        "roofline": {"bound": "alu", "achieved": achieved / 1e12, "peak": lop3_peak / 1e12,
+                     "unit": "T LOP3/s", "frac": achieved / lop3_peak,
+                     "traffic": traffic,
+                     "peak_source": "sk_probe_alu_peak, measured in this run (LOP3 chains on "
+                                    "every SM); popc peak %.3g/s" % popc_peak,
+                     "algorithmic": f"{LOP3_PER_PAIR} LOP3 + {POPC_PER_PAIR} POPC per pair x "
+                                    f"{pairs} pairs per launch",
+                     "popc_frac": pairs * POPC_PER_PAIR / launch_s / popc_peak},
+        "e2e": {"value": e2e_value, "unit": UNIT,
+                "h2d_bytes_per_step": int(host_words.numel() * 8),
+                "d2h_bytes_per_step": int(host_out.numel() * 4),
+                "steps": e2e_steps, "matches_resident_result": ok},
+        "gpu_launches": args.steps,
+        "clocks": clocks.summary(),
+        "kernel_ms": {"mean": statistics.mean(step_ms), "min": min(step_ms),
+                      "max": max(step_ms)},
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    db.close()
+    ctx.close()
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--tile-config", type=int, default=0)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+    init_dist(world)
+    try:
+        run_ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,241 @@
+/*
+ * sketchlib_b200.h -- C ABI of the B200 core/accessory distance library.
+ *
+ * This is the drop-in boundary for pp-sketchlib's GPU distance path.  Every
+ * entry point takes plain pointers and sizes; nothing here names a CUDA,
+ * torch or C++ type, so the library can be bound from C, ctypes, cgo or a
+ * pybind11 module alike.  No entry point throws: each returns an sk_status and
+ * leaves a message readable through sk_last_error().
+ *
+ * Sketch words are passed in the reference's own word layout: for sample s and
+ * k-mer index ki, sketchsize64 * bbits uint64 words, where word
+ * (blk * bbits + plane) holds bit `plane` of the 64 bins 64*blk .. 64*blk+63
+ * (bin i of the block is bit i of the word).  The host buffer is
+ * [n_samples][n_kmers][sketchsize64 * bbits], which is what
+ * Reference::get_sketch (src/reference.cpp:143-150) hands out per k, laid end to
+ * end per sample; src/sketch/sketch.cpp:82-92 (fillusigs) writes this layout.
+ *
+ * Reference interfaces replaced (paths are within bacpop/pp-sketchlib):
+ *   sk_db_create            <- flatten_by_bins / flatten_by_samples + DeviceMemory
+ *                              (src/gpu/gpu_api.cpp:232-305, src/gpu/device_memory.cu:7-65)
+ *   sk_random_create        <- RandomMC::flattened_random / lookup_array / csrs
+ *                              (src/random/random_match.cpp:254-310, 318-336)
+ *   sk_dists_dense          <- query_db_cuda / dispatchDists / calculate_dists
+ *                              (src/gpu/gpu_api.cpp:352-494, src/gpu/dist.cu:164-317, 408-489)
+ *                              and, for SK_OUT_JACCARD, the CPU-only jaccard branch of
+ *                              query_db (src/api.cpp:206-211, 256-260)
+ *   sk_dists_knn            <- query_db_sparse_cuda / sparseDists
+ *                              (src/gpu/gpu_api.cpp:496-531, src/gpu/dist.cu:495-791) and
+ *                              query_db_sparse (src/api.cpp:332-432)
+ *   sk_sparse_threshold     <- sparsify_dists_by_threshold (src/dist/matrix_ops.cpp:38-69)
+ *   sk_long_to_square       <- long_to_square (src/dist/matrix_ops.cpp:71-126)
+ *   sk_square_to_long       <- square_to_long (src/dist/matrix_ops.cpp:130-150)
+ *   sk_cancel               <- progress_atomics::set_kill (src/gpu/cuda.cuh:41-87),
+ *                              without the reference's __trap()
+ */
+#ifndef SKETCHLIB_B200_H
+#define SKETCHLIB_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SK_ABI_VERSION 1
+
+typedef enum sk_status {
+  SK_OK = 0,
+  SK_EINVAL = 1,      /* bad argument; the reference throws std::runtime_error */
+  SK_ENOMEM = 2,      /* device or pinned-host allocation failed */
+  SK_ECUDA = 3,       /* CUDA runtime error (the reference's CUDA_CALL throw) */
+  SK_EMISMATCH = 4,   /* bbits / sketchsize64 / k-mer lists differ between sketches */
+  SK_ECANCELLED = 5,  /* sk_cancel() was observed by the running kernels */
+  SK_ETIMEDOUT = 6,   /* a bounded wait (host or device) ran out */
+  SK_ENOTSUP = 7,     /* a parameter value this build does not implement */
+  SK_EKERNEL = 8,     /* a kernel raised its device-side error flag */
+  SK_ERANGE = 9       /* a size beyond a stated maximum */
+} sk_status;
+
+typedef struct sk_ctx sk_ctx;       /* one device + one stream + error state */
+typedef struct sk_db sk_db;         /* sketches resident in HBM, packed layout */
+typedef struct sk_random sk_random; /* random-match correction model */
+typedef struct sk_sparse sk_sparse; /* variable-length sparse (i, j, d) result */
+
+/* Random-match correction modes (RandomType, src/random/random_match.hpp:25). */
+enum {
+  SK_RANDOM_NONE = 0,       /* RandomType::NoAdjust: r = 0 */
+  SK_RANDOM_EQUAL_BASE = 1, /* RandomType::EqualBase: r = csrs(k, use_rc, len_a, len_b) */
+  SK_RANDOM_TABLE = 2       /* RandomType::MonteCarlo: r = table[k][cluster_ref][cluster_query] */
+};
+
+/* Dense output modes. */
+enum {
+  SK_OUT_CORE_ACC = 0, /* float32 (n_pairs, 2) row-major: core, accessory */
+  SK_OUT_JACCARD = 1,  /* float32 (n_pairs, n_kmers) row-major: corrected Jaccard */
+  SK_OUT_COUNTS = 2    /* uint32 (n_pairs, n_kmers) row-major: raw intersection counts */
+};
+
+/* ---- library / context ------------------------------------------------- */
+
+int32_t sk_abi_version(void);
+
+/* Binds a context to device_id (cudaSetDevice, src/gpu/dist.cu:373-384) and
+ * creates its own non-blocking stream. */
+sk_status sk_ctx_create(int32_t device_id, sk_ctx **out);
+sk_status sk_ctx_destroy(sk_ctx *ctx);
+/* Last error message of this context ("" if none).  Valid until the next call. */
+const char *sk_last_error(const sk_ctx *ctx);
+/* Runs all of this context's work on `stream` (a cudaStream_t) instead of its own. */
+sk_status sk_ctx_set_stream(sk_ctx *ctx, void *stream);
+/* Asks running kernels of this context to stop at their next tile boundary;
+ * the interrupted call returns SK_ECANCELLED.  Cleared when a call starts. */
+sk_status sk_cancel(sk_ctx *ctx);
+sk_status sk_device_info(sk_ctx *ctx, int64_t *mem_free, int64_t *mem_total,
+                         int32_t *sm_count);
+/* Waits for all work queued on the context's stream (calls made with
+ * out_on_device = 1 return before their kernels finish) and reports any
+ * device-side error or cancellation they raised. */
+sk_status sk_ctx_synchronize(sk_ctx *ctx);
+/* Chooses the dense kernel's tile shape (0 = automatic, from the tuning table
+ * or the built-in default; >0 = a shape id from sk_tile_config_count()). */
+sk_status sk_ctx_set_tile_config(sk_ctx *ctx, int32_t config_id);
+int32_t sk_tile_config_count(void);
+/* Describes shape `config_id`: rows x cols of the CTA tile and per-thread block. */
+sk_status sk_tile_config_info(int32_t config_id, int32_t *tile_rows,
+                              int32_t *tile_cols, int32_t *thread_rows,
+                              int32_t *thread_cols, int32_t *max_kmers);
+/* Loads a tuning table written by the autotuner: lines "n_kmers sketchsize64 config_id". */
+sk_status sk_ctx_load_tuning(sk_ctx *ctx, const char *path);
+
+/* ---- sketch databases --------------------------------------------------- */
+
+/* Uploads sketches from HOST memory in the reference word layout (see top of
+ * file) and packs them on the device.  kmers: the n_kmers k-mer lengths, in
+ * the order the words are stored (ascending in the reference).  bbits must
+ * be 14 (def_bbits, src/reference.hpp:18). */
+sk_status sk_db_create(sk_ctx *ctx, const uint64_t *words, int64_t n_samples,
+                       const int32_t *kmers, int32_t n_kmers,
+                       int32_t sketchsize64, int32_t bbits, sk_db **out);
+/* Same, with `d_words` already in this context's device memory. */
+sk_status sk_db_create_device(sk_ctx *ctx, const uint64_t *d_words,
+                              int64_t n_samples, const int32_t *kmers,
+                              int32_t n_kmers, int32_t sketchsize64,
+                              int32_t bbits, sk_db **out);
+sk_status sk_db_destroy(sk_db *db);
+sk_status sk_db_info(const sk_db *db, int64_t *n_samples, int32_t *n_kmers,
+                     int32_t *sketchsize64, int32_t *bbits);
+/* Per-sample random-match inputs: cluster ids (RandomMC::lookup_array,
+ * src/random/random_match.cpp:254-273) and sequence lengths
+ * (Reference::seq_length).  Either may be NULL (all zero). */
+sk_status sk_db_set_sample_info(sk_db *db, const uint16_t *cluster,
+                                const uint64_t *seq_len);
+/* Copies the packed device layout back out in the reference word layout
+ * (host buffer of n_samples * n_kmers * sketchsize64 * bbits words). */
+sk_status sk_db_download(sk_ctx *ctx, const sk_db *db, uint64_t *words);
+
+/* ---- random-match model ------------------------------------------------- */
+
+/* mode SK_RANDOM_TABLE: `table` is float [n_kmers][n_clusters][n_clusters],
+ *   indexed [k][cluster of the reference-side sample][cluster of the
+ *   query-side sample] (RandomMC::random_match, random_match.cpp:185-206); the
+ *   caller writes 0 for k >= max_k as the reference CPU path does.
+ * mode SK_RANDOM_EQUAL_BASE: per-pair csrs(k, use_rc, len_a, len_b)
+ *   (random_match.cpp:318-336) from the databases' seq_len.
+ * mode SK_RANDOM_NONE: no correction.  `kmers` must equal the databases'. */
+sk_status sk_random_create(sk_ctx *ctx, int32_t mode, int32_t use_rc,
+                           const int32_t *kmers, int32_t n_kmers,
+                           int32_t n_clusters, const float *table,
+                           sk_random **out);
+sk_status sk_random_destroy(sk_random *random);
+
+/* ---- dense distances ---------------------------------------------------- */
+
+/* Number of output rows: n*(n-1)/2 when query is NULL (all-vs-all of `ref`),
+ * else n_query * n_ref.  Row order follows square_to_condensed
+ * (src/dist/matrix_idx.hpp:46-50) for self, q * n_ref + r for query mode
+ * (src/api.cpp:251). */
+int64_t sk_dists_rows(const sk_db *ref, const sk_db *query);
+
+/* All-vs-all (query == NULL) or query-vs-reference distances.
+ * out: host pointer (out_on_device = 0: the call copies the result back and
+ * returns after it is complete) or device pointer (out_on_device = 1: the
+ * call returns once the kernels are queued on the context's stream).
+ * random may be NULL (no correction). */
+sk_status sk_dists_dense(sk_ctx *ctx, const sk_db *ref, const sk_db *query,
+                         const sk_random *random, int32_t out_mode, void *out,
+                         int32_t out_on_device);
+
+/* Self kNN (querySelfSparse with kNN > 0, src/sketchlib_bindings.cpp:136-187):
+ * for every sample i, the kNN smallest distances d(i, j), j != i, of column
+ * dist_col (0 = core, 1 = accessory; jaccard != 0 sorts on 1 - J at k-mer
+ * index dist_col and reports J).  Outputs have n_samples * kNN entries,
+ * ascending per row, ties broken by the smaller j.  Host pointers. */
+sk_status sk_dists_knn(sk_ctx *ctx, const sk_db *db, const sk_random *random,
+                       int32_t kNN, int32_t dist_col, int32_t jaccard,
+                       int64_t *i_out, int64_t *j_out, float *d_out);
+
+/* Query kNN: for each query q, the kNN smallest column-dist_col distances to
+ * the references (query-vs-reference rows), ascending, ties by smaller r. */
+sk_status sk_query_knn(sk_ctx *ctx, const sk_db *ref, const sk_db *query,
+                       const sk_random *random, int32_t kNN, int32_t dist_col,
+                       int64_t *r_out, float *d_out);
+
+/* ---- sparse / matrix transforms (device kernels over long-form data) ---- */
+
+/* Entries (i, j > i) of the square form of a long-form column with value
+ * < cutoff, row-major (src/dist/matrix_ops.cpp:38-69).  long_form: float
+ * (n_pairs, n_cols) row-major, host memory. */
+sk_status sk_sparse_threshold(sk_ctx *ctx, const float *long_form,
+                              int64_t n_samples, int32_t n_cols, int32_t col,
+                              float cutoff, sk_sparse **out);
+/* Threshold sparsification straight from sketches: dense distances stay on
+ * the device and only the sparse entries come back. */
+sk_status sk_dists_threshold(sk_ctx *ctx, const sk_db *db,
+                             const sk_random *random, int32_t dist_col,
+                             float cutoff, sk_sparse **out);
+int64_t sk_sparse_size(const sk_sparse *sp);
+sk_status sk_sparse_copy(const sk_sparse *sp, int64_t *i_out, int64_t *j_out,
+                         float *d_out);
+sk_status sk_sparse_destroy(sk_sparse *sp);
+
+/* long_to_square (matrix_ops.cpp:71-126): rr has n_rr*(n_rr-1)/2 values,
+ * qr n_rr*n_qq (ref index fastest) and qq n_qq*(n_qq-1)/2; qr/qq may be NULL
+ * with n_qq = 0.  square: float (n_rr+n_qq)^2 row-major.  Host pointers. */
+sk_status sk_long_to_square(sk_ctx *ctx, const float *rr, int64_t n_rr,
+                            const float *qr, const float *qq, int64_t n_qq,
+                            float *square);
+/* square_to_long (matrix_ops.cpp:130-150): upper triangle of an n x n
+ * row-major matrix into n*(n-1)/2 values.  Host pointers. */
+sk_status sk_square_to_long(sk_ctx *ctx, const float *square, int64_t n,
+                            float *long_out);
+
+/* ---- synthetic sketches (seeded generators for tests and benchmarks) ---- */
+
+/* Bin-level tree generator.  parent[s] < s (or -1 for a root); thresh[s][k]
+ * is the probability, scaled by 2^32, that sample s resamples a bin at
+ * k-mer index k instead of inheriting it from its parent.  Writes the
+ * reference word layout.  _host runs on the CPU (threads), _device writes a
+ * device buffer; both produce identical words. */
+sk_status sk_synth_host(const int32_t *parent, const uint32_t *thresh,
+                        int64_t n_samples, int32_t n_kmers,
+                        int32_t sketchsize64, uint64_t seed, int32_t threads,
+                        uint64_t *words);
+sk_status sk_synth_device(sk_ctx *ctx, const int32_t *parent,
+                          const uint32_t *thresh, int64_t n_samples,
+                          int32_t n_kmers, int32_t sketchsize64, uint64_t seed,
+                          uint64_t *d_words);
+
+/* ---- measurement ---------------------------------------------------------- */
+
+/* Measured integer-ALU peaks of the context's device, in operations per
+ * second: 32-bit LOP3 (the distance kernel's bound) and POPC.  Each is one
+ * ~20 ms saturating kernel on the context's stream. */
+sk_status sk_probe_alu_peak(sk_ctx *ctx, double *lop3_per_s, double *popc_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SKETCHLIB_B200_H */

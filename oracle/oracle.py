@@ -1,0 +1,244 @@
+"""ctypes wrapper of the CPU oracle (sk_oracle.c) and of the reference
+harness built from the reference sources (_ref/libref_querydb.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline / --impl reference legs of bench.py, as the checker and the CPU
+baseline.  The product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle.so"
+REF_PATH = HERE / "_ref" / "libref_querydb.so"
+
+
+class _Random(C.Structure):
+    _fields_ = [("mode", C.c_int), ("use_rc", C.c_int), ("n_clusters", C.c_int),
+                ("table", C.c_void_p), ("cl_rows", C.c_void_p), ("cl_cols", C.c_void_p),
+                ("len_rows", C.c_void_p), ("len_cols", C.c_void_p)]
+
+
+def build():
+    """Compiles the oracle (and the reference harness where the reference
+    sources are present) with oracle/Makefile."""
+    import subprocess
+    subprocess.run(["make", "-s", "-f", str(HERE / "Makefile")], check=True)
+
+
+def _load():
+    if not LIB_PATH.exists():
+        build()
+    lib = C.CDLL(str(LIB_PATH))
+    vp, i32, i64 = C.c_void_p, C.c_int, C.c_int64
+    lib.sko_intersize.restype = C.c_uint32
+    lib.sko_intersize.argtypes = [vp, vp, i32, i32]
+    lib.sko_csrs.restype = C.c_double
+    lib.sko_csrs.argtypes = [i32, i32, C.c_uint64, C.c_uint64]
+    lib.sko_jaccard.restype = C.c_double
+    lib.sko_jaccard.argtypes = [C.c_uint32, i32, C.c_double]
+    for f in (lib.sko_fit_slope_f64, lib.sko_fit_slope_f32):
+        f.restype = None
+        f.argtypes = [vp, vp, i32, i32, vp, vp]
+    lib.sko_dists.restype = None
+    lib.sko_dists.argtypes = [vp, i64, vp, i64, i32, i32, vp, i32, i32, C.POINTER(_Random), i32,
+                              i32, vp, i32]
+    lib.sko_dists_self_rows.restype = i64
+    lib.sko_dists_self_rows.argtypes = [vp, i64, i32, vp, i32, i32, i64, i64, vp, i32]
+    lib.sko_knn_self.restype = None
+    lib.sko_knn_self.argtypes = [vp, i64, i32, i32, i32, i32, vp, vp, vp]
+    lib.sko_sparsify.restype = i64
+    lib.sko_sparsify.argtypes = [vp, i64, i32, i32, C.c_float, vp, vp, vp]
+    lib.sko_long_to_square.restype = None
+    lib.sko_long_to_square.argtypes = [vp, i64, vp, vp, i64, vp]
+    lib.sko_square_to_long.restype = None
+    lib.sko_square_to_long.argtypes = [vp, i64, vp]
+    return lib
+
+
+lib = _load()
+NTHREADS = os.cpu_count() or 1
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+class RandomSpec:
+    """mode 0 none, 1 equal base (per-sample lengths), 2 table [K][C][C] + clusters."""
+
+    def __init__(self, mode=0, use_rc=True, table=None, cl_rows=None, cl_cols=None,
+                 len_rows=None, len_cols=None):
+        self.mode = mode
+        self.use_rc = use_rc
+        self.table = None if table is None else np.ascontiguousarray(table, np.float32)
+        self.cl_rows = None if cl_rows is None else np.ascontiguousarray(cl_rows, np.uint16)
+        self.cl_cols = None if cl_cols is None else np.ascontiguousarray(cl_cols, np.uint16)
+        self.len_rows = None if len_rows is None else np.ascontiguousarray(len_rows, np.uint64)
+        self.len_cols = None if len_cols is None else np.ascontiguousarray(len_cols, np.uint64)
+
+    def struct(self):
+        return _Random(self.mode, int(self.use_rc),
+                       0 if self.table is None else self.table.shape[-1],
+                       _p(self.table), _p(self.cl_rows), _p(self.cl_cols), _p(self.len_rows),
+                       _p(self.len_cols))
+
+
+def dists(ref_words, kmers, s64, query_words=None, random: RandomSpec | None = None,
+          out_mode=0, regress=0, threads=NTHREADS, bbits=14):
+    """Dense distances (self when query_words is None), reference long-form order."""
+    cols = np.ascontiguousarray(ref_words, dtype=np.uint64)
+    self_ = query_words is None
+    rows = cols if self_ else np.ascontiguousarray(query_words, dtype=np.uint64)
+    n_cols, n_rows = cols.shape[0], rows.shape[0]
+    K = len(kmers)
+    km = np.ascontiguousarray(kmers, dtype=np.int32)
+    pairs = n_cols * (n_cols - 1) // 2 if self_ else n_rows * n_cols
+    if out_mode == 0:
+        out = np.zeros((pairs, 2), np.float32)
+    elif out_mode == 1:
+        out = np.zeros((pairs, K), np.float32)
+    else:
+        out = np.zeros((pairs, K), np.uint32)
+    rs = (random or RandomSpec()).struct()
+    lib.sko_dists(rows.ctypes.data, n_rows, cols.ctypes.data, n_cols, int(self_), K,
+                  km.ctypes.data, s64, bbits, C.byref(rs), out_mode, regress, out.ctypes.data,
+                  threads)
+    return out
+
+
+def dists_self_rows(words, kmers, s64, row_begin, row_end, out, threads=NTHREADS, bbits=14):
+    """Core/accessory of all-vs-all rows [row_begin, row_end) into the full
+    long-form `out`; returns the number of pairs computed."""
+    w = np.ascontiguousarray(words, np.uint64)
+    km = np.ascontiguousarray(kmers, np.int32)
+    return lib.sko_dists_self_rows(w.ctypes.data, w.shape[0], len(km), km.ctypes.data, s64, bbits,
+                                   row_begin, row_end, out.ctypes.data, threads)
+
+
+def intersize(a, b, s64, bbits=14):
+    a = np.ascontiguousarray(a, np.uint64)
+    b = np.ascontiguousarray(b, np.uint64)
+    return lib.sko_intersize(a.ctypes.data, b.ctypes.data, s64, bbits)
+
+
+def csrs(k, use_rc, l1, l2):
+    return lib.sko_csrs(k, int(use_rc), l1, l2)
+
+
+def jaccard(intersize_, s64, random_jaccard=0.0):
+    return lib.sko_jaccard(intersize_, s64, random_jaccard)
+
+
+def fit_slope(J, kmers, s64, f32=False):
+    J = np.ascontiguousarray(J, np.float32)
+    km = np.ascontiguousarray(kmers, np.int32)
+    core, acc = C.c_float(), C.c_float()
+    fn = lib.sko_fit_slope_f32 if f32 else lib.sko_fit_slope_f64
+    fn(J.ctypes.data, km.ctypes.data, len(km), s64, C.byref(core), C.byref(acc))
+    return core.value, acc.value
+
+
+def knn_self(long_form, n, col, kNN, jaccard_=False):
+    lf = np.ascontiguousarray(long_form, np.float32)
+    if lf.ndim == 1:
+        lf = lf.reshape(-1, 1)
+    i = np.empty(n * kNN, np.int64)
+    j = np.empty(n * kNN, np.int64)
+    d = np.empty(n * kNN, np.float32)
+    lib.sko_knn_self(lf.ctypes.data, n, lf.shape[1], col, int(jaccard_), kNN, i.ctypes.data,
+                     j.ctypes.data, d.ctypes.data)
+    return i, j, d
+
+
+def sparsify(long_form, n, col, cutoff):
+    lf = np.ascontiguousarray(long_form, np.float32)
+    if lf.ndim == 1:
+        lf = lf.reshape(-1, 1)
+    m = lib.sko_sparsify(lf.ctypes.data, n, lf.shape[1], col, cutoff, None, None, None)
+    i = np.empty(m, np.int64)
+    j = np.empty(m, np.int64)
+    d = np.empty(m, np.float32)
+    lib.sko_sparsify(lf.ctypes.data, n, lf.shape[1], col, cutoff, i.ctypes.data, j.ctypes.data,
+                     d.ctypes.data)
+    return i, j, d
+
+
+def long_to_square(rr, n_rr, qr=None, qq=None, n_qq=0):
+    rr = np.ascontiguousarray(rr, np.float32)
+    qr = None if qr is None else np.ascontiguousarray(qr, np.float32)
+    qq = None if qq is None else np.ascontiguousarray(qq, np.float32)
+    n = n_rr + n_qq
+    out = np.zeros((n, n), np.float32)
+    lib.sko_long_to_square(rr.ctypes.data, n_rr, _p(qr), _p(qq), n_qq, out.ctypes.data)
+    return out
+
+
+def square_to_long(sq):
+    sq = np.ascontiguousarray(sq, np.float32)
+    n = sq.shape[0]
+    out = np.zeros(n * (n - 1) // 2, np.float32)
+    lib.sko_square_to_long(sq.ctypes.data, n, out.ctypes.data)
+    return out
+
+
+# ----------------------------------------------------- reference harness
+
+class RefQueryDb:
+    """query_db's all-vs-all loop around the reference's compiled
+    calc_intersize (oracle/_ref).  Available when it was built."""
+
+    def __init__(self):
+        if not REF_PATH.exists():
+            raise FileNotFoundError(f"{REF_PATH} not built (needs the reference sources)")
+        lib_ = C.CDLL(str(REF_PATH))
+        vp, i32, i64 = C.c_void_p, C.c_int, C.c_int64
+        lib_.ref_sketches_create.restype = vp
+        lib_.ref_sketches_create.argtypes = [vp, i64, i32, i32, i32]
+        lib_.ref_sketches_destroy.restype = None
+        lib_.ref_sketches_destroy.argtypes = [vp]
+        lib_.ref_query_db_self.restype = i64
+        lib_.ref_query_db_self.argtypes = [vp, i64, i32, vp, i32, i32, i64, i64, vp, i32]
+        lib_.ref_intersize.restype = C.c_uint32
+        lib_.ref_intersize.argtypes = [vp, vp, i32, i32]
+        self.lib = lib_
+
+    def intersize(self, a, b, s64, bbits=14):
+        a = np.ascontiguousarray(a, np.uint64)
+        b = np.ascontiguousarray(b, np.uint64)
+        return self.lib.ref_intersize(a.ctypes.data, b.ctypes.data, s64, bbits)
+
+    def prepare(self, words, kmers, s64, bbits=14):
+        """Holds the sketches as per-sample, per-k std::vector<uint64_t>."""
+        w = np.ascontiguousarray(words, np.uint64)
+        return (self.lib.ref_sketches_create(w.ctypes.data, w.shape[0], len(kmers), s64, bbits),
+                w.shape[0], np.ascontiguousarray(kmers, np.int32), s64, bbits)
+
+    def release(self, prepared):
+        self.lib.ref_sketches_destroy(prepared[0])
+
+    def run_rows(self, prepared, row_begin, row_end, out, threads=NTHREADS):
+        h, n, km, s64, bbits = prepared
+        return self.lib.ref_query_db_self(h, n, len(km), km.ctypes.data, s64, bbits, row_begin,
+                                          row_end, out.ctypes.data, threads)
+
+    def self_dists(self, words, kmers, s64, row_begin=0, row_end=None, threads=NTHREADS,
+                   bbits=14, out=None):
+        n = np.asarray(words).shape[0]
+        if out is None:
+            out = np.zeros((n * (n - 1) // 2, 2), np.float32)
+        prep = self.prepare(words, kmers, s64, bbits)
+        try:
+            done = self.run_rows(prep, row_begin, n if row_end is None else row_end, out, threads)
+        finally:
+            self.release(prep)
+        return out, done
+
+
+def ref_available() -> bool:
+    return REF_PATH.exists()

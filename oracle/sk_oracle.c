@@ -1,0 +1,328 @@
+/*
+ * sk_oracle.c -- CPU restatement of pp-sketchlib's distance path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the checker the CUDA path is compared
+ * against (and the CPU baseline bench.py times); the product library never
+ * links, loads or calls it.
+ *
+ * Every function restates one piece of the reference (paths within
+ * bacpop/pp-sketchlib):
+ *   sko_intersize      calc_intersize            src/dist/dist.cpp:50-78
+ *   sko_csrs           csrs                      src/random/random_match.cpp:318-336
+ *   sko_jaccard        Reference::jaccard_dist   src/reference.cpp:86-96
+ *                      observed_excess           src/dist/dist.hpp:14-24
+ *   sko_fit_slope_f64  fit_slope (semantics)     src/dist/linear_regression.cpp:16-60
+ *   sko_fit_slope_f32  fit_slope (float LDLT arithmetic of Eigen's pivoted LDLT)
+ *   sko_dists          query_db loops            src/api.cpp:195-283
+ *   sko_knn_self       query_db_sparse           src/api.cpp:332-432
+ *   sko_sparsify       sparsify_dists_by_threshold src/dist/matrix_ops.cpp:38-69
+ *   sko_long_to_square long_to_square            src/dist/matrix_ops.cpp:71-126
+ *   sko_square_to_long square_to_long            src/dist/matrix_ops.cpp:130-150
+ *
+ * Pinning: the golden vectors of the reference's own regression test
+ * (test/ppsketch_ref*.npy, checked by test/test-dists.py) pin the Jaccard,
+ * random-correction and fit semantics; tests/test_oracle_golden.py holds the
+ * checks.  Built with -ffp-contract=off so no multiply-add is fused.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* ---------------------------------------------------------- intersection */
+
+/* Number of the 64*s64 bins whose bbits-bit values are equal in both sketches.
+ * The reference returns raw samebits in both of its branches: observed_excess
+ * with expected 0 is samebits * max / max. */
+uint32_t sko_intersize(const uint64_t *s1, const uint64_t *s2, int s64, int bbits) {
+  uint64_t samebits = 0;
+  for (int i = 0; i < s64; i++) {
+    uint64_t bits = ~(uint64_t)0;
+    for (int j = 0; j < bbits; j++) bits &= ~(s1[i * bbits + j] ^ s2[i * bbits + j]);
+    samebits += (uint64_t)__builtin_popcountll(bits);
+  }
+  return (uint32_t)samebits;
+}
+
+/* ----------------------------------------------------------- random match */
+
+double sko_csrs(int k, int use_rc, uint64_t l1, uint64_t l2) {
+  double random_chance = 0;
+  const double match_chance = ldexp(1.0, (k - 1) * 2 + (use_rc ? 1 : 0));
+  const double j1 = 1 - pow(1 - (double)1 / match_chance, (double)l1);
+  const double j2 = 1 - pow(1 - (double)1 / match_chance, (double)l2);
+  if (j1 > 0 && j2 > 0) random_chance = (j1 * j2) / (j1 + j2 - j1 * j2);
+  return random_chance;
+}
+
+typedef struct {
+  int mode;               /* 0 none, 1 equal base, 2 table */
+  int use_rc;
+  int n_clusters;
+  const float *table;     /* [K][C][C] */
+  const uint16_t *cl_rows, *cl_cols;
+  const uint64_t *len_rows, *len_cols;
+} sko_random;
+
+/* Self: rows are "this" (r1 = i); query mode: rows are queries and the table
+ * is indexed [k][cluster(ref = col)][cluster(query = row)] (src/api.cpp:264-266). */
+static double random_for(const sko_random *r, int self, int k_idx, int kmer, int64_t i,
+                         int64_t j) {
+  if (!r || r->mode == 0) return 0.0;
+  if (r->mode == 1) {
+    const uint64_t li = r->len_rows ? r->len_rows[i] : 0, lj = r->len_cols ? r->len_cols[j] : 0;
+    return self ? sko_csrs(kmer, r->use_rc, li, lj) : sko_csrs(kmer, r->use_rc, lj, li);
+  }
+  const int C = r->n_clusters;
+  const int ci = r->cl_rows ? r->cl_rows[i] : 0, cj = r->cl_cols ? r->cl_cols[j] : 0;
+  const int a = self ? ci : cj, b = self ? cj : ci;
+  return (double)r->table[(int64_t)k_idx * C * C + a * C + b];
+}
+
+/* Reference::jaccard_dist + observed_excess(obs, r, 1), as a double. */
+double sko_jaccard(uint32_t intersize, int s64, double random_jaccard) {
+  const double jaccard_obs = intersize / (double)(64 * (uint64_t)s64);
+  const double diff = jaccard_obs > random_jaccard ? jaccard_obs - random_jaccard : 0;
+  return diff * 1 / (1 - random_jaccard);
+}
+
+/* ------------------------------------------------------------ regression */
+
+/* Range of the fit: first..last index with J > tolerance (the reference's
+ * `valid` vector).  Returns the range length, 0 when no J passes. */
+static int fit_range(const float *J, int K, int s64, int *first) {
+  const double tolerance = 5.0 / (s64 * 64);
+  int f = -1, l = -1;
+  for (int i = 0; i < K; i++) {
+    if (J[i] > tolerance) {
+      if (f < 0) f = i;
+      l = i;
+    }
+  }
+  *first = f;
+  return f < 0 ? 0 : l - f + 1;
+}
+
+/* Exact-arithmetic semantics of fit_slope: least squares of log J on k over
+ * the range, centred sums in double.  Fewer than 2 points in the range gives
+ * (0, 0) (the reference CPU calls exit(1) there, its GPU writes 0, 0). */
+void sko_fit_slope_f64(const float *J, const int *kmers, int K, int s64, float *core, float *acc) {
+  int f;
+  const int n = fit_range(J, K, s64, &f);
+  *core = 0.0f;
+  *acc = 0.0f;
+  if (n < 2) return;
+  double y[64];
+  double sx = 0.0, sy = 0.0;
+  for (int i = f; i < f + n; i++) {
+    y[i - f] = log((double)J[i]);
+    sx = sx + (double)kmers[i];
+    sy = sy + y[i - f];
+  }
+  const double xm = sx / n, ym = sy / n;
+  double sxx = 0.0, sxy = 0.0;
+  for (int i = f; i < f + n; i++) {
+    const double dx = (double)kmers[i] - xm, dy = y[i - f] - ym;
+    sxx = sxx + dx * dx;
+    sxy = sxy + dx * dy;
+  }
+  const double slope = sxy / sxx;
+  const double icpt = ym - slope * xm;
+  if (slope < 0.0) *core = (float)(1.0 - exp(slope));
+  if (icpt < 0.0) *acc = (float)(1.0 - exp(icpt));
+}
+
+/* The reference's float arithmetic: normal equations X'X b = X'y with
+ * X = [1, k] solved by Eigen's pivoted LDLT in float.  The larger diagonal
+ * (sum k^2) is pivoted first, so with c = sum k^2, b = sum k, a = n:
+ *   l = b / c, d1 = a - l * (c * l),
+ *   z0 = sum k*y, z1 = sum y - l * z0, z0 /= c, z1 /= d1, z0 -= l * z1,
+ *   slope = z0, intercept = z1; then 1 - expf() of each when negative. */
+void sko_fit_slope_f32(const float *J, const int *kmers, int K, int s64, float *core, float *acc) {
+  int f;
+  const int n = fit_range(J, K, s64, &f);
+  *core = 0.0f;
+  *acc = 0.0f;
+  if (n < 2) return;
+  float a = (float)n, b = 0.0f, c = 0.0f, sy = 0.0f, sxy = 0.0f;
+  for (int i = f; i < f + n; i++) {
+    const float x = (float)kmers[i], y = logf(J[i]);
+    b = b + x;
+    c = c + x * x;
+    sy = sy + y;
+    sxy = sxy + x * y;
+  }
+  const float l = b / c;
+  const float d1 = a - l * (c * l);
+  float z0 = sxy;
+  float z1 = sy - l * z0;
+  z0 = z0 / c;
+  z1 = (fabsf(d1) > 1.17549435e-38f) ? z1 / d1 : 0.0f;
+  z0 = z0 - l * z1;
+  if (z0 < 0.0f) *core = 1.0f - expf(z0);
+  if (z1 < 0.0f) *acc = 1.0f - expf(z1);
+}
+
+/* --------------------------------------------------------------- dists */
+
+static int64_t condensed(int64_t i, int64_t j, int64_t n) {
+  return n * i - ((i * (i + 1)) >> 1) + j - 1 - i;
+}
+
+/* Dense distances, rows x cols, in the reference's long-form order.
+ * Sketches in the reference word layout [n][K][s64 * bbits].
+ * out_mode 0: float (pairs, 2) core/acc; 1: float (pairs, K) Jaccard;
+ *          2: uint32 (pairs, K) intersection counts.
+ * regress 0: sko_fit_slope_f64, 1: sko_fit_slope_f32. */
+void sko_dists(const uint64_t *rows, int64_t n_rows, const uint64_t *cols, int64_t n_cols, int self,
+               int K, const int *kmers, int s64, int bbits, const sko_random *random, int out_mode,
+               int regress, void *out, int threads) {
+  const int64_t W = (int64_t)s64 * bbits;
+  const int64_t outer = self ? n_cols : n_rows;
+#ifdef _OPENMP
+  if (threads < 1) threads = 1;
+#pragma omp parallel for schedule(dynamic, 5) num_threads(threads)
+#endif
+  for (int64_t i = 0; i < outer; i++) {
+    float J[64];
+    const int64_t j0 = self ? i + 1 : 0;
+    for (int64_t j = j0; j < n_cols; j++) {
+      const int64_t pos = self ? condensed(i, j, n_cols) : i * n_cols + j;
+      const uint64_t *si = (self ? cols : rows) + i * K * W;
+      const uint64_t *sj = cols + j * K * W;
+      for (int k = 0; k < K; k++) {
+        const uint32_t c = sko_intersize(si + k * W, sj + k * W, s64, bbits);
+        if (out_mode == 2) {
+          ((uint32_t *)out)[pos * K + k] = c;
+          continue;
+        }
+        J[k] = (float)sko_jaccard(c, s64, random_for(random, self, k, kmers[k], i, j));
+      }
+      if (out_mode == 1) {
+        memcpy((float *)out + pos * K, J, sizeof(float) * K);
+      } else if (out_mode == 0) {
+        float core, acc;
+        if (regress) sko_fit_slope_f32(J, kmers, K, s64, &core, &acc);
+        else sko_fit_slope_f64(J, kmers, K, s64, &core, &acc);
+        ((float *)out)[pos * 2] = core;
+        ((float *)out)[pos * 2 + 1] = acc;
+      }
+    }
+  }
+}
+
+/* All-vs-all core/accessory (double fit) for rows [row_begin, row_end) only;
+ * out is the full (n(n-1)/2, 2) long form.  Returns the pairs computed. */
+int64_t sko_dists_self_rows(const uint64_t *words, int64_t n, int K, const int *kmers, int s64,
+                            int bbits, int64_t row_begin, int64_t row_end, float *out,
+                            int threads) {
+  const int64_t W = (int64_t)s64 * bbits;
+  int64_t done = 0;
+#ifdef _OPENMP
+  if (threads < 1) threads = 1;
+#pragma omp parallel for schedule(dynamic, 5) num_threads(threads) reduction(+ : done)
+#endif
+  for (int64_t i = row_begin; i < row_end; i++) {
+    float J[64];
+    for (int64_t j = i + 1; j < n; j++) {
+      for (int k = 0; k < K; k++)
+        J[k] = (float)sko_jaccard(sko_intersize(words + (i * K + k) * W, words + (j * K + k) * W,
+                                                s64, bbits), s64, 0.0);
+      const int64_t pos = condensed(i, j, n);
+      sko_fit_slope_f64(J, kmers, K, s64, &out[pos * 2], &out[pos * 2 + 1]);
+      done++;
+    }
+  }
+  return done;
+}
+
+/* ------------------------------------------------------------------ kNN */
+
+/* Self kNN from a dense long-form matrix (pairs, n_cols), column `col`:
+ * per row the kNN smallest d(i, j), j != i, with self as +inf; ascending by
+ * (d, j).  jaccard != 0 ranks 1 - J and reports 1 - (1 - J) as the reference
+ * does (src/api.cpp:370-371, 424-429). */
+void sko_knn_self(const float *long_form, int64_t n, int n_cols, int col, int jaccard, int knn,
+                  int64_t *i_out, int64_t *j_out, float *d_out) {
+  float *key = (float *)malloc(sizeof(float) * (size_t)knn);
+  int64_t *idx = (int64_t *)malloc(sizeof(int64_t) * (size_t)knn);
+  for (int64_t i = 0; i < n; i++) {
+    int count = 0;
+    for (int64_t j = 0; j < n; j++) {
+      float d;
+      if (j == i) {
+        d = INFINITY;
+      } else {
+        const int64_t a = j < i ? j : i, b = j < i ? i : j;
+        d = long_form[condensed(a, b, n) * n_cols + col];
+        if (jaccard) d = 1.0f - d;
+      }
+      if (count < knn || d < key[knn - 1]) {
+        int pos = count < knn ? count++ : knn - 1;
+        while (pos > 0 && key[pos - 1] > d) {
+          key[pos] = key[pos - 1];
+          idx[pos] = idx[pos - 1];
+          pos--;
+        }
+        key[pos] = d;
+        idx[pos] = j;
+      }
+    }
+    for (int e = 0; e < knn; e++) {
+      i_out[i * knn + e] = i;
+      j_out[i * knn + e] = idx[e];
+      d_out[i * knn + e] = jaccard ? 1.0f - key[e] : key[e];
+    }
+  }
+  free(key);
+  free(idx);
+}
+
+/* ----------------------------------------------------- matrix transforms */
+
+/* Upper-triangle entries of the square form with value < cutoff, row-major.
+ * Returns the count; outputs may be NULL to count only. */
+int64_t sko_sparsify(const float *long_form, int64_t n, int n_cols, int col, float cutoff,
+                     int64_t *i_out, int64_t *j_out, float *d_out) {
+  int64_t m = 0;
+  for (int64_t i = 0; i < n; i++) {
+    for (int64_t j = i + 1; j < n; j++) {
+      const float v = long_form[condensed(i, j, n) * n_cols + col];
+      if (v < cutoff) {
+        if (i_out) {
+          i_out[m] = i;
+          j_out[m] = j;
+          d_out[m] = v;
+        }
+        m++;
+      }
+    }
+  }
+  return m;
+}
+
+void sko_long_to_square(const float *rr, int64_t n_rr, const float *qr, const float *qq,
+                        int64_t n_qq, float *square) {
+  const int64_t n = n_rr + n_qq;
+  for (int64_t i = 0; i < n; i++) square[i * n + i] = 0.0f;
+  for (int64_t i = 0; i < n_rr; i++)
+    for (int64_t j = i + 1; j < n_rr; j++)
+      square[i * n + j] = square[j * n + i] = rr[condensed(i, j, n_rr)];
+  for (int64_t i = 0; i < n_qq; i++)
+    for (int64_t j = i + 1; j < n_qq; j++)
+      square[(i + n_rr) * n + j + n_rr] = square[(j + n_rr) * n + i + n_rr] =
+          qq[condensed(i, j, n_qq)];
+  for (int64_t d = 0; d < n_rr * n_qq; d++) {
+    const int64_t i = d % n_rr, j = d / n_rr + n_rr;
+    square[i * n + j] = square[j * n + i] = qr[d];
+  }
+}
+
+void sko_square_to_long(const float *square, int64_t n, float *long_out) {
+  for (int64_t i = 0; i < n; i++)
+    for (int64_t j = i + 1; j < n; j++) long_out[condensed(i, j, n)] = square[i * n + j];
+}

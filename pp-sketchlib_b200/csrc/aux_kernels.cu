@@ -1,0 +1,387 @@
+// aux_kernels.cu -- the kernels around the distance kernel: packing sketches
+// into device stripes, the synthetic sketch generator, kNN selection,
+// threshold sparsification and long <-> square conversion.  All are
+// memory-bound; each keeps its global accesses coalesced along the
+// contiguous dimension of the long-form / stripe layouts.
+#include <cuda_runtime.h>
+#include <cub/device/device_scan.cuh>
+
+#include <cfloat>
+#include <cstdint>
+
+#include "sk_common.h"
+#include "sk_launch.h"
+
+namespace sk {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+inline int grid_for(int64_t work, int per_block, int cap = 148 * 32) {
+  int64_t g = (work + per_block - 1) / per_block;
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return static_cast<int>(g);
+}
+
+__device__ __forceinline__ int64_t condensed(int64_t i, int64_t j, int64_t n) {
+  return n * i - ((i * (i + 1)) >> 1) + j - 1 - i;
+}
+
+// ------------------------------------------------------------------- packing
+
+// One CTA per (k, 64-bin block, granule): reads the 64 samples' 14 words of
+// the block (112 contiguous bytes per sample) into shared memory and writes
+// the two 32-bin stripes (3584 contiguous bytes each).
+__global__ void pack_kernel(const uint64_t *__restrict__ words, int64_t n, int n_kmers, int s64,
+                            int ng, uint32_t *__restrict__ packed) {
+  __shared__ uint64_t tile[kGranule * kBbits];
+  const int64_t nblocks = static_cast<int64_t>(n_kmers) * s64 * ng;
+  const int nb = 2 * s64;
+  for (int64_t item = blockIdx.x; item < nblocks; item += gridDim.x) {
+    const int g = static_cast<int>(item % ng);
+    const int64_t rest = item / ng;
+    const int b64 = static_cast<int>(rest % s64);
+    const int k = static_cast<int>(rest / s64);
+    for (int e = threadIdx.x; e < kGranule * kBbits; e += blockDim.x) {
+      const int lane = e / kBbits, plane = e % kBbits;
+      const int64_t s = static_cast<int64_t>(g) * kGranule + lane;
+      tile[plane * kGranule + lane] =
+          s < n ? words[((s * n_kmers + k) * s64 + b64) * kBbits + plane] : 0ull;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < 2 * kStripeWords; e += blockDim.x) {
+      const int h = e / kStripeWords, w = e % kStripeWords;
+      const uint64_t v = tile[w];
+      const int64_t blk = static_cast<int64_t>(k) * nb + 2 * b64 + h;
+      packed[(blk * ng + g) * kStripeWords + w] = static_cast<uint32_t>(h ? (v >> 32) : v);
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void unpack_kernel(const uint32_t *__restrict__ packed, int64_t n, int n_kmers,
+                              int s64, int ng, uint64_t *__restrict__ words) {
+  const int64_t total = n * n_kmers * s64 * kBbits;
+  const int nb = 2 * s64;
+  for (int64_t o = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; o < total;
+       o += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int plane = static_cast<int>(o % kBbits);
+    int64_t r = o / kBbits;
+    const int b64 = static_cast<int>(r % s64);
+    r /= s64;
+    const int k = static_cast<int>(r % n_kmers);
+    const int64_t s = r / n_kmers;
+    const int64_t g = s / kGranule, lane = s % kGranule;
+    const int64_t base = ((static_cast<int64_t>(k) * nb + 2 * b64) * ng + g) * kStripeWords +
+                         plane * kGranule + lane;
+    const uint64_t lo = packed[base];
+    const uint64_t hi = packed[base + static_cast<int64_t>(ng) * kStripeWords];
+    words[o] = lo | (hi << 32);
+  }
+}
+
+// ----------------------------------------------------------------- synthetic
+
+// One warp per (sample, k, 64-bin block): each lane draws bins lane and
+// lane+32, the 14 bit planes are gathered with ballots into reference words.
+__global__ void synth_kernel(const int32_t *__restrict__ parent, const uint32_t *__restrict__ thresh,
+                             int64_t n, int n_kmers, int s64, uint64_t seed,
+                             uint64_t *__restrict__ words) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps_total = n * n_kmers * s64;
+  const int64_t warp0 = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5;
+  const int64_t wstride = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t w = warp0; w < warps_total; w += wstride) {
+    const int b64 = static_cast<int>(w % s64);
+    const int64_t rest = w / s64;
+    const int k = static_cast<int>(rest % n_kmers);
+    const int64_t s = rest / n_kmers;
+    const uint32_t bin = static_cast<uint32_t>(b64) * 64u + lane;
+    const uint32_t vlo = synth_bin(parent, thresh, n_kmers, s, k, bin, seed);
+    const uint32_t vhi = synth_bin(parent, thresh, n_kmers, s, k, bin + 32u, seed);
+    uint64_t mine = 0;
+#pragma unroll
+    for (int p = 0; p < kBbits; ++p) {
+      const uint32_t lo = __ballot_sync(0xffffffffu, (vlo >> p) & 1u);
+      const uint32_t hi = __ballot_sync(0xffffffffu, (vhi >> p) & 1u);
+      if (lane == p) mine = static_cast<uint64_t>(lo) | (static_cast<uint64_t>(hi) << 32);
+    }
+    if (lane < kBbits) words[w * kBbits + lane] = mine;
+  }
+}
+
+// ----------------------------------------------------------------------- kNN
+
+// Self kNN over a condensed single column: lane = row i of a 32-row block.
+// Each lane keeps its kNN best (key, j) in shared memory, sorted ascending;
+// j is visited in increasing order, so equal keys keep the smaller j first.
+// Keys are the distances, or 1 - J for Jaccard (src/api.cpp:370-371).
+__global__ void knn_self_kernel(const float *__restrict__ vals, int64_t n, int knn, int jaccard,
+                                int64_t *__restrict__ j_out, float *__restrict__ d_out) {
+  extern __shared__ unsigned char smem[];
+  float *key = reinterpret_cast<float *>(smem);
+  int32_t *idx = reinterpret_cast<int32_t *>(key + 32 * knn);
+  const int lane = threadIdx.x;
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * 32 + lane;
+  const bool active = i < n;
+  int count = 0;
+  float worst = FLT_MAX;
+  for (int64_t j = 0; j < n; ++j) {
+    if (!active) break;
+    float d;
+    if (j == i) {
+      d = INFINITY;  // the diagonal (src/api.cpp:365)
+    } else {
+      const int64_t a = j < i ? j : i, b = j < i ? i : j;
+      d = vals[condensed(a, b, n)];
+      if (jaccard) d = 1.0f - d;
+    }
+    if (count < knn || d < worst) {
+      int pos = count < knn ? count++ : knn - 1;
+      while (pos > 0 && key[(pos - 1) * 32 + lane] > d) {
+        key[pos * 32 + lane] = key[(pos - 1) * 32 + lane];
+        idx[pos * 32 + lane] = idx[(pos - 1) * 32 + lane];
+        --pos;
+      }
+      key[pos * 32 + lane] = d;
+      idx[pos * 32 + lane] = static_cast<int32_t>(j);
+      worst = key[(count - 1) * 32 + lane];
+    }
+  }
+  if (active) {
+    for (int e = 0; e < knn; ++e) {
+      const float k = key[e * 32 + lane];
+      j_out[i * knn + e] = idx[e * 32 + lane];
+      d_out[i * knn + e] = jaccard ? 1.0f - k : k;
+    }
+  }
+}
+
+// Row kNN over a dense (n_rows, n_cols) column: one warp per row, lanes take
+// every 32nd column, then lane 0 merges the 32 sorted lists by (key, col).
+__global__ void knn_rows_kernel(const float *__restrict__ vals, int64_t n_rows, int64_t n_cols,
+                                int knn, int64_t *__restrict__ j_out, float *__restrict__ d_out) {
+  extern __shared__ unsigned char smem[];
+  float *key = reinterpret_cast<float *>(smem);
+  int32_t *idx = reinterpret_cast<int32_t *>(key + 32 * knn);
+  __shared__ int counts[32];
+  const int lane = threadIdx.x;
+  for (int64_t row = blockIdx.x; row < n_rows; row += gridDim.x) {
+    const float *v = vals + row * n_cols;
+    int count = 0;
+    float worst = FLT_MAX;
+    for (int64_t c = lane; c < n_cols; c += 32) {
+      const float d = v[c];
+      if (count < knn || d < worst) {
+        int pos = count < knn ? count++ : knn - 1;
+        while (pos > 0 && key[(pos - 1) * 32 + lane] > d) {
+          key[pos * 32 + lane] = key[(pos - 1) * 32 + lane];
+          idx[pos * 32 + lane] = idx[(pos - 1) * 32 + lane];
+          --pos;
+        }
+        key[pos * 32 + lane] = d;
+        idx[pos * 32 + lane] = static_cast<int32_t>(c);
+        worst = key[(count - 1) * 32 + lane];
+      }
+    }
+    counts[lane] = count;
+    __syncwarp();
+    if (lane == 0) {
+      int head[32];
+      for (int l = 0; l < 32; ++l) head[l] = 0;
+      for (int e = 0; e < knn; ++e) {
+        int best = -1;
+        float bk = 0.0f;
+        int32_t bj = 0;
+        for (int l = 0; l < 32; ++l) {
+          if (head[l] >= counts[l]) continue;
+          const float k = key[head[l] * 32 + l];
+          const int32_t j = idx[head[l] * 32 + l];
+          if (best < 0 || k < bk || (k == bk && j < bj)) { best = l; bk = k; bj = j; }
+        }
+        if (best < 0) { j_out[row * knn + e] = -1; d_out[row * knn + e] = INFINITY; continue; }
+        ++head[best];
+        j_out[row * knn + e] = bj;
+        d_out[row * knn + e] = bk;
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------- threshold sparse
+
+// Row i of the square form above the diagonal is condensed entries
+// [condensed(i, i+1), +n-i-1): contiguous, read by one warp per row.
+__global__ void threshold_count_kernel(const float *__restrict__ vals, int64_t n, int stride,
+                                       int col, float cutoff, int64_t *__restrict__ counts) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp0 = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5;
+  const int64_t wstride = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t i = warp0; i < n; i += wstride) {
+    const int64_t base = i + 1 < n ? condensed(i, i + 1, n) : 0;
+    const int64_t len = n - i - 1;
+    int64_t c = 0;
+    for (int64_t e0 = 0; e0 < len; e0 += 32) {
+      const int64_t e = e0 + lane;
+      const bool hit = e < len && vals[(base + e) * stride + col] < cutoff;
+      c += __popc(__ballot_sync(0xffffffffu, hit));
+    }
+    if (lane == 0) counts[i] = c;
+  }
+}
+
+__global__ void threshold_fill_kernel(const float *__restrict__ vals, int64_t n, int stride,
+                                      int col, float cutoff, const int64_t *__restrict__ offsets,
+                                      int64_t *__restrict__ i_out, int64_t *__restrict__ j_out,
+                                      float *__restrict__ d_out) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp0 = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5;
+  const int64_t wstride = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t i = warp0; i < n; i += wstride) {
+    const int64_t base = i + 1 < n ? condensed(i, i + 1, n) : 0;
+    const int64_t len = n - i - 1;
+    int64_t out = offsets[i];
+    for (int64_t e0 = 0; e0 < len; e0 += 32) {
+      const int64_t e = e0 + lane;
+      float v = 0.0f;
+      const bool hit = e < len && (v = vals[(base + e) * stride + col]) < cutoff;
+      const uint32_t mask = __ballot_sync(0xffffffffu, hit);
+      if (hit) {
+        const int64_t o = out + __popc(mask & ((1u << lane) - 1u));
+        i_out[o] = i;
+        j_out[o] = i + 1 + e;
+        d_out[o] = v;
+      }
+      out += __popc(mask);
+    }
+  }
+}
+
+// ------------------------------------------------------- long <-> square
+
+__global__ void long_to_square_kernel(const float *__restrict__ rr, int64_t n_rr,
+                                      const float *__restrict__ qr, const float *__restrict__ qq,
+                                      int64_t n_qq, float *__restrict__ square) {
+  const int64_t n = n_rr + n_qq;
+  const int64_t total = n * n;
+  for (int64_t o = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; o < total;
+       o += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t i = o / n, j = o % n;
+    float v = 0.0f;
+    if (i != j) {
+      const int64_t a = i < j ? i : j, b = i < j ? j : i;
+      if (b < n_rr) {
+        v = rr[condensed(a, b, n_rr)];
+      } else if (a >= n_rr) {
+        v = qq[condensed(a - n_rr, b - n_rr, n_qq)];
+      } else {
+        v = qr[(b - n_rr) * n_rr + a];  // ref index fastest (src/dist/matrix_ops.cpp:115-123)
+      }
+    }
+    square[o] = v;
+  }
+}
+
+__global__ void square_to_long_kernel(const float *__restrict__ square, int64_t n,
+                                      float *__restrict__ long_out) {
+  for (int64_t i = blockIdx.x; i < n - 1; i += gridDim.x) {
+    const int64_t base = condensed(i, i + 1, n);
+    for (int64_t j = i + 1 + threadIdx.x; j < n; j += blockDim.x) {
+      long_out[base + (j - i - 1)] = square[i * n + j];
+    }
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_pack(const uint64_t *words, int64_t n, int32_t n_kmers, int32_t s64, int32_t ng,
+                        uint32_t *packed, cudaStream_t stream) {
+  const int64_t items = static_cast<int64_t>(n_kmers) * s64 * ng;
+  pack_kernel<<<grid_for(items, 1, 148 * 64), kThreads, 0, stream>>>(words, n, n_kmers, s64, ng,
+                                                                     packed);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_unpack(const uint32_t *packed, int64_t n, int32_t n_kmers, int32_t s64,
+                          int32_t ng, uint64_t *words, cudaStream_t stream) {
+  const int64_t total = n * n_kmers * s64 * kBbits;
+  unpack_kernel<<<grid_for(total, kThreads), kThreads, 0, stream>>>(packed, n, n_kmers, s64, ng,
+                                                                    words);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_synth(const int32_t *parent, const uint32_t *thresh, int64_t n,
+                         int32_t n_kmers, int32_t s64, uint64_t seed, uint64_t *words,
+                         cudaStream_t stream) {
+  const int64_t warps = n * n_kmers * s64;
+  synth_kernel<<<grid_for(warps, kThreads / 32, 148 * 64), kThreads, 0, stream>>>(
+      parent, thresh, n, n_kmers, s64, seed, words);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_knn_self(const float *col_vals, int64_t n, int32_t knn, int32_t jaccard,
+                            int64_t *j_out, float *d_out, cudaStream_t stream) {
+  const int smem = 32 * knn * 8;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(knn_self_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+  }
+  const int blocks = static_cast<int>((n + 31) / 32);
+  knn_self_kernel<<<blocks, 32, smem, stream>>>(col_vals, n, knn, jaccard, j_out, d_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_knn_rows(const float *vals, int64_t n_rows, int64_t n_cols, int32_t knn,
+                            int64_t *j_out, float *d_out, cudaStream_t stream) {
+  const int smem = 32 * knn * 8;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(knn_rows_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+  }
+  const int blocks = static_cast<int>(n_rows < 148 * 64 ? n_rows : 148 * 64);
+  knn_rows_kernel<<<blocks > 0 ? blocks : 1, 32, smem, stream>>>(vals, n_rows, n_cols, knn, j_out,
+                                                                 d_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_threshold_count(const float *vals, int64_t n, int32_t stride, int32_t col,
+                                   float cutoff, int64_t *row_counts, cudaStream_t stream) {
+  threshold_count_kernel<<<grid_for(n, kThreads / 32), kThreads, 0, stream>>>(
+      vals, n, stride, col, cutoff, row_counts);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_threshold_fill(const float *vals, int64_t n, int32_t stride, int32_t col,
+                                  float cutoff, const int64_t *row_offsets, int64_t *i_out,
+                                  int64_t *j_out, float *d_out, cudaStream_t stream) {
+  threshold_fill_kernel<<<grid_for(n, kThreads / 32), kThreads, 0, stream>>>(
+      vals, n, stride, col, cutoff, row_offsets, i_out, j_out, d_out);
+  return cudaGetLastError();
+}
+
+cudaError_t exclusive_scan_i64(const int64_t *in, int64_t *out, int64_t n, void *tmp,
+                               size_t *tmp_bytes, cudaStream_t stream) {
+  return cub::DeviceScan::ExclusiveSum(tmp, *tmp_bytes, in, out, n, stream);
+}
+
+cudaError_t launch_long_to_square(const float *rr, int64_t n_rr, const float *qr, const float *qq,
+                                  int64_t n_qq, float *square, cudaStream_t stream) {
+  const int64_t n = n_rr + n_qq;
+  long_to_square_kernel<<<grid_for(n * n, kThreads), kThreads, 0, stream>>>(rr, n_rr, qr, qq,
+                                                                           n_qq, square);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_square_to_long(const float *square, int64_t n, float *long_out,
+                                  cudaStream_t stream) {
+  if (n < 2) return cudaSuccess;
+  square_to_long_kernel<<<grid_for(n, 1), kThreads, 0, stream>>>(square, n, long_out);
+  return cudaGetLastError();
+}
+
+}  // namespace sk

@@ -1,0 +1,855 @@
+// capi.cu -- the C ABI (include/sketchlib_b200.h): contexts, resident sketch
+// databases, random-match models and the dense / kNN / sparse entry points.
+//
+// Host responsibilities mirror the reference's GPU host driver
+// (src/gpu/gpu_api.cpp:166-531, src/gpu/dist.cu:326-489): parameter checks
+// with the reference's messages, device selection, layout packing (here on the
+// device instead of OpenMP flattening on the host), launch planning and result
+// copies.  No C++ exception crosses the ABI; errors become sk_status codes.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "sk_common.h"
+#include "sk_launch.h"
+#include "sketchlib_b200.h"
+#include "sk_runtime.h"
+
+using namespace sk;
+
+// ------------------------------------------------------------------ helpers
+
+namespace sk {
+
+sk_status fail(sk_ctx *ctx, sk_status st, const char *fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (ctx) ctx->err = buf;
+  return st;
+}
+
+sk_status cuda_fail(sk_ctx *ctx, cudaError_t e, const char *what) {
+  const sk_status st = (e == cudaErrorMemoryAllocation) ? SK_ENOMEM : SK_ECUDA;
+  return fail(ctx, st, "CUDA error in %s: %s", what, cudaGetErrorString(e));
+}
+
+DeviceGuard::DeviceGuard(int dev) {
+  cudaGetDevice(&prev_);
+  if (prev_ != dev) cudaSetDevice(dev);
+}
+DeviceGuard::~DeviceGuard() { cudaSetDevice(prev_); }
+
+// Grows the context's device scratch buffer `slot` to at least `bytes`.
+sk_status scratch(sk_ctx *ctx, int slot, size_t bytes, void **out) {
+  Scratch &s = ctx->scratch[slot];
+  if (s.bytes < bytes) {
+    if (s.ptr) {
+      cudaStreamSynchronize(ctx->stream);
+      cudaFree(s.ptr);
+      s.ptr = nullptr;
+      s.bytes = 0;
+    }
+    cudaError_t e = cudaMalloc(&s.ptr, bytes);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "scratch allocation");
+    s.bytes = bytes;
+  }
+  *out = s.ptr;
+  return SK_OK;
+}
+
+// Begins a public call: the context's device becomes current and the cancel
+// word and device status are cleared.
+sk_status begin_call(sk_ctx *ctx) {
+  ctx->err.clear();
+  *ctx->cancel_host = 0;
+  cudaError_t e = cudaMemsetAsync(ctx->status_dev, 0, sizeof(DevStatus), ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "status reset");
+  return SK_OK;
+}
+
+// Waits for the context's stream and turns the device status into a code.
+sk_status finish_call(sk_ctx *ctx) {
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel execution");
+  DevStatus st{};
+  e = cudaMemcpy(&st, ctx->status_dev, sizeof(st), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "status readback");
+  ctx->last_tiles = st.tiles_done;
+  if (st.error & 2u) return fail(ctx, SK_ECANCELLED, "Distance calculation cancelled");
+  if (st.error & 1u)
+    return fail(ctx, SK_ETIMEDOUT, "A device-side bounded wait timed out (site %u)", st.where);
+  if (st.error) return fail(ctx, SK_EKERNEL, "Device error flag 0x%x", st.error);
+  return SK_OK;
+}
+
+const TileConfig *choose_config(sk_ctx *ctx, int K, int s64) {
+  if (ctx->tile_cfg > 0) {
+    const TileConfig *c = tile_config(ctx->tile_cfg);
+    if (c && c->max_kmers >= K) return c;
+  }
+  auto it = ctx->tuning.find({K, s64});
+  if (it != ctx->tuning.end()) {
+    const TileConfig *c = tile_config(it->second);
+    if (c && c->max_kmers >= K) return c;
+  }
+  if (K <= 8) return tile_config(1);
+  return tile_config(2);
+}
+
+// Upper-triangle / rectangle tile counts for a tile shape.
+void plan_tiles(JobParams &jp, const TileConfig &cfg) {
+  jp.tile_rows = cfg.tile_rows;
+  jp.tile_cols = cfg.tile_cols;
+  if (jp.self) {
+    const int64_t n = jp.n_rows;
+    jp.n_row_tiles = static_cast<int32_t>(n > 1 ? (n - 1 + cfg.tile_rows - 1) / cfg.tile_rows : 0);
+    jp.n_col_tiles = static_cast<int32_t>((n + cfg.tile_cols - 1) / cfg.tile_cols);
+    const int64_t m = cfg.tile_rows / cfg.tile_cols;
+    int64_t tiles = 0;
+    for (int64_t ti = 0; ti < jp.n_row_tiles; ++ti) tiles += jp.n_col_tiles - ti * m;
+    jp.n_tiles = tiles;
+  } else {
+    jp.n_row_tiles = static_cast<int32_t>((jp.n_rows + cfg.tile_rows - 1) / cfg.tile_rows);
+    jp.n_col_tiles = static_cast<int32_t>((jp.n_cols + cfg.tile_cols - 1) / cfg.tile_cols);
+    jp.n_tiles = static_cast<int64_t>(jp.n_row_tiles) * jp.n_col_tiles;
+  }
+}
+
+// Equal-base random-match factors j(k, len) = 1 - (1 - 4^-k')^len per sample
+// (csrs, src/random/random_match.cpp:318-336), computed with std::pow on the
+// host exactly as the reference does and cached on the database.
+sk_status ensure_jv(sk_ctx *ctx, sk_db *db, int use_rc) {
+  if (db->jv && db->jv_rc == use_rc) return SK_OK;
+  const int64_t ld = static_cast<int64_t>(db->ng) * kGranule;
+  std::vector<double> jv(static_cast<size_t>(db->K) * ld, 0.0);
+  for (int k = 0; k < db->K; ++k) {
+    const int shift = (db->kmers[k] - 1) * 2 + (use_rc ? 1 : 0);
+    const double match_chance = std::ldexp(1.0, shift);
+    for (int64_t s = 0; s < db->n; ++s) {
+      const double len = static_cast<double>(db->seq_len.empty() ? 0 : db->seq_len[s]);
+      jv[k * ld + s] = 1 - std::pow(1 - (double)1 / match_chance, len);
+    }
+  }
+  if (!db->jv) {
+    cudaError_t e = cudaMalloc(&db->jv, jv.size() * sizeof(double));
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "random-match factors");
+  }
+  cudaError_t e = cudaMemcpy(db->jv, jv.data(), jv.size() * sizeof(double), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "random-match factors");
+  db->jv_rc = use_rc;
+  return SK_OK;
+}
+
+sk_status check_compatible(sk_ctx *ctx, const sk_db *a, const sk_db *b) {
+  if (a->bbits != b->bbits) return fail(ctx, SK_EMISMATCH, "Mismatching bbits in sketches");
+  if (a->s64 != b->s64) return fail(ctx, SK_EMISMATCH, "Mismatching sketchsize64 in sketches");
+  if (a->kmers != b->kmers) return fail(ctx, SK_EMISMATCH, "Mismatching k-mer lengths in sketches");
+  return SK_OK;
+}
+
+// Fills a JobParams for ref (columns) vs query (rows; NULL = all-vs-all).
+sk_status build_job(sk_ctx *ctx, const sk_db *ref, const sk_db *query, const sk_random *random,
+                    int out_mode, int out_col, void *d_out, const TileConfig **cfg_out,
+                    JobParams *jp) {
+  if (!ref) return fail(ctx, SK_EINVAL, "No reference database");
+  if (ref->n < 1 || (query && query->n < 1))
+    return fail(ctx, SK_EINVAL, "Query with empty ref or query list!");
+  if (query) {
+    sk_status st = check_compatible(ctx, ref, query);
+    if (st != SK_OK) return st;
+  }
+  if (random && random->kmers != ref->kmers)
+    return fail(ctx, SK_EMISMATCH, "Random match table k-mer lengths differ from the sketches");
+  const TileConfig *cfg = choose_config(ctx, ref->K, ref->s64);
+  if (!cfg || cfg->max_kmers < ref->K)
+    return fail(ctx, SK_ENOTSUP, "No tile configuration holds %d k-mer lengths (at most 16)",
+                ref->K);
+  std::memset(jp, 0, sizeof(*jp));
+  const sk_db *rows = query ? query : ref;
+  jp->self = query ? 0 : 1;
+  jp->row_words = rows->packed;
+  jp->col_words = ref->packed;
+  jp->n_rows = rows->n;
+  jp->n_cols = ref->n;
+  jp->ng_rows = rows->ng;
+  jp->ng_cols = ref->ng;
+  jp->n_kmers = ref->K;
+  jp->nb = 2 * ref->s64;
+  jp->out_mode = out_mode;
+  jp->out_col = out_col;
+  jp->out = d_out;
+  jp->tol = 5.0 / (ref->s64 * 64);
+  jp->union_bits = static_cast<double>(64 * ref->s64);
+  for (int k = 0; k < ref->K; ++k) jp->kmers[k] = ref->kmers[k];
+  jp->rmode = random ? random->mode : kRandNone;
+  if (jp->rmode == kRandTable) {
+    const int C = random->n_clusters;
+    jp->rtable = random->table;
+    jp->rs_k = C * C;
+    // self: [k][cluster(i = row)][cluster(j = col)]  (random_match(r1=i, r2=j))
+    // query: [k][cluster(ref = col)][cluster(query = row)]  (src/api.cpp:264-266)
+    jp->rs_row = query ? 1 : C;
+    jp->rs_col = query ? C : 1;
+    jp->cl_rows = rows->cluster;
+    jp->cl_cols = ref->cluster;
+  } else if (jp->rmode == kRandEqualBase) {
+    sk_status st = ensure_jv(ctx, const_cast<sk_db *>(ref), random->use_rc);
+    if (st != SK_OK) return st;
+    if (query) {
+      st = ensure_jv(ctx, const_cast<sk_db *>(query), random->use_rc);
+      if (st != SK_OK) return st;
+    }
+    jp->jv_rows = rows->jv;
+    jp->jv_cols = ref->jv;
+    jp->jv_rows_ld = static_cast<int64_t>(rows->ng) * kGranule;
+    jp->jv_cols_ld = static_cast<int64_t>(ref->ng) * kGranule;
+  }
+  plan_tiles(*jp, *cfg);
+  *cfg_out = cfg;
+  return SK_OK;
+}
+
+sk_status launch_job(sk_ctx *ctx, const JobParams &jp, const TileConfig &cfg) {
+  if (jp.n_tiles == 0) return SK_OK;
+  int per_sm = cfg.blocks_per_sm();
+  if (per_sm < 1) return fail(ctx, SK_ECUDA, "Tile configuration %d does not fit the device", cfg.id);
+  int64_t grid = static_cast<int64_t>(per_sm) * ctx->sm_count;
+  if (grid > jp.n_tiles) grid = jp.n_tiles;
+  cudaError_t e = cfg.launch(jp, ctx->status_dev, ctx->cancel_dev, static_cast<int>(grid), ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "distance kernel launch");
+  return SK_OK;
+}
+
+int64_t n_pairs(const sk_db *ref, const sk_db *query) {
+  if (!ref) return 0;
+  if (query) return query->n * ref->n;
+  return ref->n * (ref->n - 1) / 2;
+}
+
+size_t out_bytes(int out_mode, int64_t pairs, int K) {
+  switch (out_mode) {
+    case kOutCoreAcc: return static_cast<size_t>(pairs) * 8;
+    case kOutJaccard:
+    case kOutCounts: return static_cast<size_t>(pairs) * 4 * K;
+    default: return static_cast<size_t>(pairs) * 4;
+  }
+}
+
+// Dense distances into device memory `d_out` (queued on the context stream).
+sk_status dense_to_device(sk_ctx *ctx, const sk_db *ref, const sk_db *query,
+                          const sk_random *random, int out_mode, int out_col, void *d_out) {
+  JobParams jp;
+  const TileConfig *cfg = nullptr;
+  sk_status st = build_job(ctx, ref, query, random, out_mode, out_col, d_out, &cfg, &jp);
+  if (st != SK_OK) return st;
+  return launch_job(ctx, jp, *cfg);
+}
+
+}  // namespace sk
+
+// ------------------------------------------------------------------ context
+
+#define SK_GUARD(ctx)                                      \
+  if (!(ctx)) return SK_EINVAL;                            \
+  std::lock_guard<std::recursive_mutex> lock_((ctx)->mu);  \
+  DeviceGuard dev_guard_((ctx)->device)
+
+extern "C" {
+
+int32_t sk_abi_version(void) { return SK_ABI_VERSION; }
+
+sk_status sk_ctx_create(int32_t device_id, sk_ctx **out) {
+  if (!out) return SK_EINVAL;
+  *out = nullptr;
+  int n_dev = 0;
+  if (cudaGetDeviceCount(&n_dev) != cudaSuccess || n_dev < 1) return SK_ECUDA;
+  if (device_id < 0 || device_id >= n_dev) return SK_EINVAL;
+  sk_ctx *ctx = new sk_ctx();
+  ctx->device = device_id;
+  DeviceGuard g(device_id);
+  cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device_id);
+  if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void **>(&ctx->cancel_host), sizeof(int), cudaHostAllocMapped);
+  if (e == cudaSuccess) e = cudaHostGetDevicePointer(reinterpret_cast<void **>(&ctx->cancel_dev), ctx->cancel_host, 0);
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->status_dev, sizeof(DevStatus));
+  if (e != cudaSuccess) {
+    sk_ctx_destroy(ctx);
+    return e == cudaErrorMemoryAllocation ? SK_ENOMEM : SK_ECUDA;
+  }
+  *ctx->cancel_host = 0;
+  cudaMemset(ctx->status_dev, 0, sizeof(DevStatus));
+  *out = ctx;
+  return SK_OK;
+}
+
+sk_status sk_ctx_destroy(sk_ctx *ctx) {
+  if (!ctx) return SK_EINVAL;
+  {
+    DeviceGuard g(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (auto &s : ctx->scratch)
+      if (s.ptr) cudaFree(s.ptr);
+    if (ctx->status_dev) cudaFree(ctx->status_dev);
+    if (ctx->cancel_host) cudaFreeHost(ctx->cancel_host);
+    if (ctx->stream && ctx->own_stream) cudaStreamDestroy(ctx->stream);
+  }
+  delete ctx;
+  return SK_OK;
+}
+
+const char *sk_last_error(const sk_ctx *ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+sk_status sk_ctx_set_stream(sk_ctx *ctx, void *stream) {
+  SK_GUARD(ctx);
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+  ctx->stream = static_cast<cudaStream_t>(stream);
+  ctx->own_stream = false;
+  return SK_OK;
+}
+
+sk_status sk_cancel(sk_ctx *ctx) {
+  if (!ctx) return SK_EINVAL;
+  // deliberately no lock: called from another thread while a call runs
+  reinterpret_cast<volatile int *>(ctx->cancel_host)[0] = 1;
+  return SK_OK;
+}
+
+sk_status sk_device_info(sk_ctx *ctx, int64_t *mem_free, int64_t *mem_total, int32_t *sm_count) {
+  SK_GUARD(ctx);
+  size_t f = 0, t = 0;
+  cudaError_t e = cudaMemGetInfo(&f, &t);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemGetInfo");
+  if (mem_free) *mem_free = static_cast<int64_t>(f);
+  if (mem_total) *mem_total = static_cast<int64_t>(t);
+  if (sm_count) *sm_count = ctx->sm_count;
+  return SK_OK;
+}
+
+sk_status sk_ctx_synchronize(sk_ctx *ctx) {
+  SK_GUARD(ctx);
+  return finish_call(ctx);
+}
+
+sk_status sk_ctx_set_tile_config(sk_ctx *ctx, int32_t config_id) {
+  SK_GUARD(ctx);
+  if (config_id != 0 && !tile_config(config_id))
+    return fail(ctx, SK_EINVAL, "Unknown tile configuration %d", config_id);
+  ctx->tile_cfg = config_id;
+  return SK_OK;
+}
+
+int32_t sk_tile_config_count(void) { return tile_config_count(); }
+
+sk_status sk_tile_config_info(int32_t config_id, int32_t *tile_rows, int32_t *tile_cols,
+                              int32_t *thread_rows, int32_t *thread_cols, int32_t *max_kmers) {
+  const TileConfig *c = tile_config(config_id);
+  if (!c) return SK_EINVAL;
+  if (tile_rows) *tile_rows = c->tile_rows;
+  if (tile_cols) *tile_cols = c->tile_cols;
+  if (thread_rows) *thread_rows = c->thread_rows;
+  if (thread_cols) *thread_cols = c->thread_cols;
+  if (max_kmers) *max_kmers = c->max_kmers;
+  return SK_OK;
+}
+
+sk_status sk_ctx_load_tuning(sk_ctx *ctx, const char *path) {
+  SK_GUARD(ctx);
+  std::ifstream in(path ? path : "");
+  if (!in) return fail(ctx, SK_EINVAL, "Cannot open tuning table %s", path ? path : "(null)");
+  std::string line;
+  while (std::getline(in, line)) {
+    if (line.empty() || line[0] == '#') continue;
+    std::istringstream ls(line);
+    int K = 0, s64 = 0, id = 0;
+    if (!(ls >> K >> s64 >> id)) continue;
+    if (tile_config(id)) ctx->tuning[{K, s64}] = id;
+  }
+  return SK_OK;
+}
+
+// ------------------------------------------------------------------ databases
+
+static sk_status db_create_impl(sk_ctx *ctx, const uint64_t *words, bool on_device, int64_t n,
+                                const int32_t *kmers, int32_t K, int32_t s64, int32_t bbits,
+                                sk_db **out) {
+  if (!out) return fail(ctx, SK_EINVAL, "null output handle");
+  *out = nullptr;
+  if (n < 0) return fail(ctx, SK_EINVAL, "negative sample count");
+  if (n > 0 && !words) return fail(ctx, SK_EINVAL, "null sketch words");
+  if (bbits != kBbits)
+    return fail(ctx, SK_ENOTSUP, "bbits %d not supported (sketches use %d bit planes)", bbits, kBbits);
+  if (s64 < 1 || s64 > kMaxSketch64)
+    return fail(ctx, SK_ERANGE, "sketchsize64 %d outside [1, %d]", s64, kMaxSketch64);
+  if (K < 1 || K > kMaxKmers || !kmers)
+    return fail(ctx, SK_ERANGE, "n_kmers %d outside [1, %d]", K, kMaxKmers);
+  for (int k = 0; k < K; ++k)
+    if (kmers[k] < 1 || kmers[k] > 64) return fail(ctx, SK_EINVAL, "bad k-mer length %d", kmers[k]);
+  sk_db *db = new sk_db();
+  db->ctx = ctx;
+  db->n = n;
+  db->K = K;
+  db->s64 = s64;
+  db->bbits = bbits;
+  db->kmers.assign(kmers, kmers + K);
+  const int64_t npad = ((n + kSamplePad - 1) / kSamplePad) * kSamplePad;
+  db->ng = static_cast<int32_t>(std::max<int64_t>(npad, kSamplePad) / kGranule);
+  const size_t packed_words = static_cast<size_t>(K) * 2 * s64 * db->ng * kStripeWords;
+  cudaError_t e = cudaMalloc(&db->packed, packed_words * 4);
+  if (e != cudaSuccess) {
+    delete db;
+    return cuda_fail(ctx, e, "sketch database allocation");
+  }
+  const size_t in_words = static_cast<size_t>(n) * K * s64 * kBbits;
+  const uint64_t *d_words = words;
+  uint64_t *tmp = nullptr;
+  if (!on_device && n > 0) {
+    e = cudaMalloc(&tmp, in_words * 8);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(tmp, words, in_words * 8, cudaMemcpyHostToDevice, ctx->stream);
+    d_words = tmp;
+  }
+  if (e == cudaSuccess) e = launch_pack(d_words, n, K, s64, db->ng, db->packed, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (tmp) cudaFree(tmp);
+  if (e != cudaSuccess) {
+    cudaFree(db->packed);
+    delete db;
+    return cuda_fail(ctx, e, "sketch upload");
+  }
+  *out = db;
+  return SK_OK;
+}
+
+sk_status sk_db_create(sk_ctx *ctx, const uint64_t *words, int64_t n_samples, const int32_t *kmers,
+                       int32_t n_kmers, int32_t sketchsize64, int32_t bbits, sk_db **out) {
+  SK_GUARD(ctx);
+  ctx->err.clear();
+  return db_create_impl(ctx, words, false, n_samples, kmers, n_kmers, sketchsize64, bbits, out);
+}
+
+sk_status sk_db_create_device(sk_ctx *ctx, const uint64_t *d_words, int64_t n_samples,
+                              const int32_t *kmers, int32_t n_kmers, int32_t sketchsize64,
+                              int32_t bbits, sk_db **out) {
+  SK_GUARD(ctx);
+  ctx->err.clear();
+  return db_create_impl(ctx, d_words, true, n_samples, kmers, n_kmers, sketchsize64, bbits, out);
+}
+
+sk_status sk_db_destroy(sk_db *db) {
+  if (!db) return SK_EINVAL;
+  DeviceGuard g(db->ctx->device);
+  cudaStreamSynchronize(db->ctx->stream);
+  if (db->packed) cudaFree(db->packed);
+  if (db->cluster) cudaFree(db->cluster);
+  if (db->jv) cudaFree(db->jv);
+  delete db;
+  return SK_OK;
+}
+
+sk_status sk_db_info(const sk_db *db, int64_t *n_samples, int32_t *n_kmers, int32_t *sketchsize64,
+                     int32_t *bbits) {
+  if (!db) return SK_EINVAL;
+  if (n_samples) *n_samples = db->n;
+  if (n_kmers) *n_kmers = db->K;
+  if (sketchsize64) *sketchsize64 = db->s64;
+  if (bbits) *bbits = db->bbits;
+  return SK_OK;
+}
+
+sk_status sk_db_set_sample_info(sk_db *db, const uint16_t *cluster, const uint64_t *seq_len) {
+  if (!db) return SK_EINVAL;
+  sk_ctx *ctx = db->ctx;
+  SK_GUARD(ctx);
+  const int64_t npad = static_cast<int64_t>(db->ng) * kGranule;
+  if (cluster) {
+    std::vector<uint16_t> cl(npad, 0);
+    std::copy(cluster, cluster + db->n, cl.begin());
+    if (!db->cluster) {
+      cudaError_t e = cudaMalloc(&db->cluster, npad * sizeof(uint16_t));
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "cluster ids");
+    }
+    cudaError_t e = cudaMemcpy(db->cluster, cl.data(), npad * sizeof(uint16_t), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cluster ids");
+  }
+  if (seq_len) {
+    db->seq_len.assign(seq_len, seq_len + db->n);
+    db->jv_rc = -1;  // factors depend on lengths
+  }
+  return SK_OK;
+}
+
+sk_status sk_db_download(sk_ctx *ctx, const sk_db *db, uint64_t *words) {
+  SK_GUARD(ctx);
+  if (!db || (!words && db->n > 0)) return fail(ctx, SK_EINVAL, "null argument");
+  const size_t n_words = static_cast<size_t>(db->n) * db->K * db->s64 * kBbits;
+  if (n_words == 0) return SK_OK;
+  void *tmp = nullptr;
+  sk_status st = scratch(ctx, 0, n_words * 8, &tmp);
+  if (st != SK_OK) return st;
+  cudaError_t e = launch_unpack(db->packed, db->n, db->K, db->s64, db->ng, static_cast<uint64_t *>(tmp), ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(words, tmp, n_words * 8, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "sketch download");
+  return SK_OK;
+}
+
+// ------------------------------------------------------------------- random
+
+sk_status sk_random_create(sk_ctx *ctx, int32_t mode, int32_t use_rc, const int32_t *kmers,
+                           int32_t n_kmers, int32_t n_clusters, const float *table,
+                           sk_random **out) {
+  SK_GUARD(ctx);
+  ctx->err.clear();
+  if (!out) return fail(ctx, SK_EINVAL, "null output handle");
+  *out = nullptr;
+  if (mode != kRandNone && mode != kRandEqualBase && mode != kRandTable)
+    return fail(ctx, SK_EINVAL, "Unknown random-match mode %d", mode);
+  if (n_kmers < 1 || n_kmers > kMaxKmers || !kmers)
+    return fail(ctx, SK_EINVAL, "bad k-mer list for random matches");
+  sk_random *r = new sk_random();
+  r->ctx = ctx;
+  r->mode = mode;
+  r->use_rc = use_rc ? 1 : 0;
+  r->kmers.assign(kmers, kmers + n_kmers);
+  if (mode == kRandTable) {
+    if (n_clusters < 1 || !table) {
+      delete r;
+      return fail(ctx, SK_EINVAL, "Random match table needs n_clusters >= 1 and a table");
+    }
+    r->n_clusters = n_clusters;
+    const size_t sz = static_cast<size_t>(n_kmers) * n_clusters * n_clusters * sizeof(float);
+    cudaError_t e = cudaMalloc(&r->table, sz);
+    if (e == cudaSuccess) e = cudaMemcpy(r->table, table, sz, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      if (r->table) cudaFree(r->table);
+      delete r;
+      return cuda_fail(ctx, e, "random match table");
+    }
+  }
+  *out = r;
+  return SK_OK;
+}
+
+sk_status sk_random_destroy(sk_random *random) {
+  if (!random) return SK_EINVAL;
+  DeviceGuard g(random->ctx->device);
+  if (random->table) cudaFree(random->table);
+  delete random;
+  return SK_OK;
+}
+
+// ------------------------------------------------------------------- dense
+
+int64_t sk_dists_rows(const sk_db *ref, const sk_db *query) { return n_pairs(ref, query); }
+
+sk_status sk_dists_dense(sk_ctx *ctx, const sk_db *ref, const sk_db *query, const sk_random *random,
+                         int32_t out_mode, void *out, int32_t out_on_device) {
+  SK_GUARD(ctx);
+  sk_status st = begin_call(ctx);
+  if (st != SK_OK) return st;
+  if (out_mode != kOutCoreAcc && out_mode != kOutJaccard && out_mode != kOutCounts)
+    return fail(ctx, SK_EINVAL, "Unknown output mode %d", out_mode);
+  const int64_t pairs = n_pairs(ref, query);
+  if (pairs > 0 && !out) return fail(ctx, SK_EINVAL, "null output buffer");
+  const size_t bytes = ref ? out_bytes(out_mode, pairs, ref->K) : 0;
+  void *d_out = out;
+  if (!out_on_device && bytes > 0) {
+    st = scratch(ctx, 1, bytes, &d_out);
+    if (st != SK_OK) return st;
+  }
+  st = dense_to_device(ctx, ref, query, random, out_mode, 0, d_out);
+  if (st != SK_OK) return st;
+  if (out_on_device) return SK_OK;
+  if (bytes > 0) {
+    cudaError_t e = cudaMemcpyAsync(out, d_out, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "result copy");
+  }
+  return finish_call(ctx);
+}
+
+// --------------------------------------------------------------------- kNN
+
+sk_status sk_dists_knn(sk_ctx *ctx, const sk_db *db, const sk_random *random, int32_t kNN,
+                       int32_t dist_col, int32_t jaccard, int64_t *i_out, int64_t *j_out,
+                       float *d_out) {
+  SK_GUARD(ctx);
+  sk_status st = begin_call(ctx);
+  if (st != SK_OK) return st;
+  if (!db || db->n < 1) return fail(ctx, SK_EINVAL, "Query with empty ref or query list!");
+  // check_sparse_inputs (src/api.cpp:293-313)
+  if ((jaccard && dist_col >= db->K) || (dist_col != 0 && dist_col != 1))
+    return fail(ctx, SK_EINVAL, "dist_col out of range");
+  if (kNN < 0 || kNN > db->n) return fail(ctx, SK_EINVAL, "kNN must be between 0 and the number of samples");
+  if (kNN > 800) return fail(ctx, SK_ENOTSUP, "kNN above 800 is not supported");
+  if (kNN == 0) return SK_OK;
+  const int64_t n = db->n, pairs = n_pairs(db, nullptr);
+  void *d_vals = nullptr, *d_res = nullptr;
+  st = scratch(ctx, 1, std::max<size_t>(pairs, 1) * 4, &d_vals);
+  if (st != SK_OK) return st;
+  const size_t res_elems = static_cast<size_t>(n) * kNN;
+  st = scratch(ctx, 2, res_elems * 12, &d_res);
+  if (st != SK_OK) return st;
+  int64_t *d_j = static_cast<int64_t *>(d_res);
+  float *d_d = reinterpret_cast<float *>(d_j + res_elems);
+  if (pairs > 0) {
+    st = dense_to_device(ctx, db, nullptr, random, kOutColumn, jaccard ? 2 + dist_col : dist_col, d_vals);
+    if (st != SK_OK) return st;
+  }
+  cudaError_t e = launch_knn_self(static_cast<float *>(d_vals), n, kNN, jaccard, d_j, d_d, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(j_out, d_j, res_elems * 8, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_out, d_d, res_elems * 4, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "kNN");
+  st = finish_call(ctx);
+  if (st != SK_OK) return st;
+  for (int64_t i = 0; i < n; ++i) std::fill_n(i_out + i * kNN, kNN, i);
+  return SK_OK;
+}
+
+sk_status sk_query_knn(sk_ctx *ctx, const sk_db *ref, const sk_db *query, const sk_random *random,
+                       int32_t kNN, int32_t dist_col, int64_t *r_out, float *d_out) {
+  SK_GUARD(ctx);
+  sk_status st = begin_call(ctx);
+  if (st != SK_OK) return st;
+  if (!ref || !query || ref->n < 1 || query->n < 1)
+    return fail(ctx, SK_EINVAL, "Query with empty ref or query list!");
+  if (dist_col != 0 && dist_col != 1) return fail(ctx, SK_EINVAL, "dist_col out of range");
+  if (kNN < 0 || kNN > ref->n) return fail(ctx, SK_EINVAL, "kNN must be between 0 and the number of references");
+  if (kNN > 800) return fail(ctx, SK_ENOTSUP, "kNN above 800 is not supported");
+  if (kNN == 0) return SK_OK;
+  const int64_t pairs = n_pairs(ref, query);
+  void *d_vals = nullptr, *d_res = nullptr;
+  st = scratch(ctx, 1, pairs * 4, &d_vals);
+  if (st != SK_OK) return st;
+  const size_t res_elems = static_cast<size_t>(query->n) * kNN;
+  st = scratch(ctx, 2, res_elems * 12, &d_res);
+  if (st != SK_OK) return st;
+  int64_t *d_j = static_cast<int64_t *>(d_res);
+  float *d_d = reinterpret_cast<float *>(d_j + res_elems);
+  st = dense_to_device(ctx, ref, query, random, kOutColumn, dist_col, d_vals);
+  if (st != SK_OK) return st;
+  cudaError_t e = launch_knn_rows(static_cast<float *>(d_vals), query->n, ref->n, kNN, d_j, d_d, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(r_out, d_j, res_elems * 8, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_out, d_d, res_elems * 4, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "query kNN");
+  return finish_call(ctx);
+}
+
+// ---------------------------------------------------------- threshold sparse
+
+static sk_status threshold_device(sk_ctx *ctx, const float *d_vals, int64_t n, int stride, int col,
+                                  float cutoff, sk_sparse **out) {
+  void *d_cnt = nullptr;
+  sk_status st = scratch(ctx, 2, static_cast<size_t>(n + 1) * 16, &d_cnt);
+  if (st != SK_OK) return st;
+  int64_t *counts = static_cast<int64_t *>(d_cnt);
+  int64_t *offsets = counts + (n + 1);
+  cudaError_t e = cudaMemsetAsync(counts, 0, (n + 1) * 8, ctx->stream);
+  if (e == cudaSuccess) e = launch_threshold_count(d_vals, n, stride, col, cutoff, counts, ctx->stream);
+  size_t tmp_bytes = 0;
+  if (e == cudaSuccess) e = exclusive_scan_i64(counts, offsets, n + 1, nullptr, &tmp_bytes, ctx->stream);
+  void *tmp = nullptr;
+  if (e == cudaSuccess) {
+    st = scratch(ctx, 3, std::max<size_t>(tmp_bytes, 16), &tmp);
+    if (st != SK_OK) return st;
+    e = exclusive_scan_i64(counts, offsets, n + 1, tmp, &tmp_bytes, ctx->stream);
+  }
+  int64_t total = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&total, offsets + n, 8, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "threshold count");
+  sk_sparse *sp = new sk_sparse();
+  sp->i.resize(total);
+  sp->j.resize(total);
+  sp->d.resize(total);
+  if (total > 0) {
+    void *d_res = nullptr;
+    st = scratch(ctx, 3, static_cast<size_t>(total) * 20, &d_res);
+    if (st != SK_OK) { delete sp; return st; }
+    int64_t *di = static_cast<int64_t *>(d_res);
+    int64_t *dj = di + total;
+    float *dd = reinterpret_cast<float *>(dj + total);
+    e = launch_threshold_fill(d_vals, n, stride, col, cutoff, offsets, di, dj, dd, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(sp->i.data(), di, total * 8, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(sp->j.data(), dj, total * 8, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(sp->d.data(), dd, total * 4, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e != cudaSuccess) { delete sp; return cuda_fail(ctx, e, "threshold fill"); }
+  }
+  st = finish_call(ctx);
+  if (st != SK_OK) { delete sp; return st; }
+  *out = sp;
+  return SK_OK;
+}
+
+sk_status sk_sparse_threshold(sk_ctx *ctx, const float *long_form, int64_t n_samples, int32_t n_cols,
+                              int32_t col, float cutoff, sk_sparse **out) {
+  SK_GUARD(ctx);
+  sk_status st = begin_call(ctx);
+  if (st != SK_OK) return st;
+  if (!out) return fail(ctx, SK_EINVAL, "null output handle");
+  *out = nullptr;
+  if (cutoff < 0) return fail(ctx, SK_EINVAL, "Distance threshold must be at least 0");
+  if (n_samples < 0 || n_cols < 1 || col < 0 || col >= n_cols)
+    return fail(ctx, SK_EINVAL, "bad long-form shape");
+  const int64_t pairs = n_samples * (n_samples - 1) / 2;
+  void *d_vals = nullptr;
+  st = scratch(ctx, 1, std::max<int64_t>(pairs, 1) * n_cols * 4, &d_vals);
+  if (st != SK_OK) return st;
+  if (pairs > 0) {
+    cudaError_t e = cudaMemcpyAsync(d_vals, long_form, pairs * n_cols * 4, cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "long-form upload");
+  }
+  return threshold_device(ctx, static_cast<float *>(d_vals), n_samples, n_cols, col, cutoff, out);
+}
+
+sk_status sk_dists_threshold(sk_ctx *ctx, const sk_db *db, const sk_random *random, int32_t dist_col,
+                             float cutoff, sk_sparse **out) {
+  SK_GUARD(ctx);
+  sk_status st = begin_call(ctx);
+  if (st != SK_OK) return st;
+  if (!out) return fail(ctx, SK_EINVAL, "null output handle");
+  *out = nullptr;
+  if (cutoff < 0) return fail(ctx, SK_EINVAL, "Distance threshold must be at least 0");
+  if (!db || db->n < 1) return fail(ctx, SK_EINVAL, "Query with empty ref or query list!");
+  if (dist_col != 0 && dist_col != 1) return fail(ctx, SK_EINVAL, "dist_col out of range");
+  const int64_t pairs = n_pairs(db, nullptr);
+  void *d_vals = nullptr;
+  st = scratch(ctx, 1, std::max<int64_t>(pairs, 1) * 4, &d_vals);
+  if (st != SK_OK) return st;
+  if (pairs > 0) {
+    st = dense_to_device(ctx, db, nullptr, random, kOutColumn, dist_col, d_vals);
+    if (st != SK_OK) return st;
+  }
+  return threshold_device(ctx, static_cast<float *>(d_vals), db->n, 1, 0, cutoff, out);
+}
+
+int64_t sk_sparse_size(const sk_sparse *sp) { return sp ? static_cast<int64_t>(sp->d.size()) : 0; }
+
+sk_status sk_sparse_copy(const sk_sparse *sp, int64_t *i_out, int64_t *j_out, float *d_out) {
+  if (!sp) return SK_EINVAL;
+  if (i_out) std::copy(sp->i.begin(), sp->i.end(), i_out);
+  if (j_out) std::copy(sp->j.begin(), sp->j.end(), j_out);
+  if (d_out) std::copy(sp->d.begin(), sp->d.end(), d_out);
+  return SK_OK;
+}
+
+sk_status sk_sparse_destroy(sk_sparse *sp) {
+  if (!sp) return SK_EINVAL;
+  delete sp;
+  return SK_OK;
+}
+
+// ------------------------------------------------------------ long / square
+
+sk_status sk_long_to_square(sk_ctx *ctx, const float *rr, int64_t n_rr, const float *qr,
+                            const float *qq, int64_t n_qq, float *square) {
+  SK_GUARD(ctx);
+  sk_status st = begin_call(ctx);
+  if (st != SK_OK) return st;
+  if (n_rr < 0 || n_qq < 0 || (n_qq > 0 && !qr)) return fail(ctx, SK_EINVAL, "bad long-form shape");
+  const int64_t n = n_rr + n_qq;
+  if (n == 0) return SK_OK;
+  const int64_t n_rr_long = n_rr * (n_rr - 1) / 2, n_qq_long = n_qq * (n_qq - 1) / 2;
+  const int64_t n_qr = n_rr * n_qq;
+  void *d = nullptr;
+  const size_t bytes = (n_rr_long + n_qr + n_qq_long + n * n) * 4;
+  st = scratch(ctx, 1, std::max<size_t>(bytes, 16), &d);
+  if (st != SK_OK) return st;
+  float *drr = static_cast<float *>(d), *dqr = drr + n_rr_long, *dqq = dqr + n_qr, *dsq = dqq + n_qq_long;
+  cudaError_t e = cudaSuccess;
+  if (n_rr_long) e = cudaMemcpyAsync(drr, rr, n_rr_long * 4, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess && n_qr) e = cudaMemcpyAsync(dqr, qr, n_qr * 4, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess && n_qq_long && qq) e = cudaMemcpyAsync(dqq, qq, n_qq_long * 4, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = launch_long_to_square(drr, n_rr, dqr, dqq, n_qq, dsq, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(square, dsq, n * n * 4, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "long_to_square");
+  return finish_call(ctx);
+}
+
+sk_status sk_square_to_long(sk_ctx *ctx, const float *square, int64_t n, float *long_out) {
+  SK_GUARD(ctx);
+  sk_status st = begin_call(ctx);
+  if (st != SK_OK) return st;
+  if (n < 0) return fail(ctx, SK_EINVAL, "square_to_long input must be a square matrix");
+  if (n < 2) return SK_OK;
+  const int64_t n_long = n * (n - 1) / 2;
+  void *d = nullptr;
+  st = scratch(ctx, 1, (n * n + n_long) * 4, &d);
+  if (st != SK_OK) return st;
+  float *dsq = static_cast<float *>(d), *dl = dsq + n * n;
+  cudaError_t e = cudaMemcpyAsync(dsq, square, n * n * 4, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = launch_square_to_long(dsq, n, dl, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(long_out, dl, n_long * 4, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "square_to_long");
+  return finish_call(ctx);
+}
+
+// ---------------------------------------------------------------- synthetic
+
+sk_status sk_synth_host(const int32_t *parent, const uint32_t *thresh, int64_t n_samples,
+                        int32_t n_kmers, int32_t sketchsize64, uint64_t seed, int32_t threads,
+                        uint64_t *words) {
+  if (!parent || !thresh || !words || n_samples < 0 || n_kmers < 1 || sketchsize64 < 1)
+    return SK_EINVAL;
+  for (int64_t s = 0; s < n_samples; ++s)
+    if (parent[s] >= s) return SK_EINVAL;  // parents precede children
+  const int nt = std::max(1, threads);
+  auto work = [&](int tid) {
+    for (int64_t s = tid; s < n_samples; s += nt) {
+      for (int k = 0; k < n_kmers; ++k) {
+        for (int b = 0; b < sketchsize64; ++b) {
+          uint64_t w[kBbits] = {0};
+          for (int i = 0; i < 64; ++i) {
+            const uint32_t v = synth_bin(parent, thresh, n_kmers, s, k, b * 64u + i, seed);
+            for (int p = 0; p < kBbits; ++p) w[p] |= static_cast<uint64_t>((v >> p) & 1u) << i;
+          }
+          uint64_t *o = words + ((s * n_kmers + k) * static_cast<int64_t>(sketchsize64) + b) * kBbits;
+          for (int p = 0; p < kBbits; ++p) o[p] = w[p];
+        }
+      }
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nt; ++t) pool.emplace_back(work, t);
+  work(0);
+  for (auto &t : pool) t.join();
+  return SK_OK;
+}
+
+sk_status sk_synth_device(sk_ctx *ctx, const int32_t *parent, const uint32_t *thresh, int64_t n_samples,
+                          int32_t n_kmers, int32_t sketchsize64, uint64_t seed, uint64_t *d_words) {
+  SK_GUARD(ctx);
+  sk_status st = begin_call(ctx);
+  if (st != SK_OK) return st;
+  if (!parent || !thresh || !d_words || n_samples < 1 || n_kmers < 1 || sketchsize64 < 1)
+    return fail(ctx, SK_EINVAL, "bad synthetic generator arguments");
+  for (int64_t s = 0; s < n_samples; ++s)
+    if (parent[s] >= s) return fail(ctx, SK_EINVAL, "parents must precede their children");
+  int32_t *d_parent = nullptr;
+  uint32_t *d_thresh = nullptr;
+  cudaError_t e = cudaMalloc(&d_parent, n_samples * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&d_thresh, n_samples * n_kmers * 4);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_parent, parent, n_samples * 4, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_thresh, thresh, n_samples * n_kmers * 4, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = launch_synth(d_parent, d_thresh, n_samples, n_kmers, sketchsize64, seed, d_words, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (d_parent) cudaFree(d_parent);
+  if (d_thresh) cudaFree(d_thresh);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "synthetic sketches");
+  return SK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,109 @@
+// sk_common.h -- types shared by the host runtime and the device kernels.
+//
+// Packed device layout of a sketch database ("stripes"):
+//   uint32 words[n_kmers][nb][n_granules][kBbits][kGranule]
+// with nb = 2 * sketchsize64 32-bin blocks, kGranule = 64 samples per granule.
+// Element (k, b, g, plane, lane) is bit-plane `plane` of bins 32*b .. 32*b+31 of
+// sample g*64+lane at k-mer index k: the low (b even) or high (b odd) half of
+// reference word (b/2)*bbits + plane (src/sketch/sketch.cpp:82-92).  One
+// (k, b, g) stripe is 14*64*4 = 3584 contiguous bytes, so a tile of samples for
+// one block is a single bulk copy, and the 64 samples of a plane are one
+// 256-byte row read with 128-bit shared-memory loads.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+namespace sk {
+
+constexpr int kBbits = 14;              // def_bbits (src/reference.hpp:18)
+constexpr int kGranule = 64;            // samples per packed granule
+constexpr int kStripeWords = kBbits * kGranule;       // 896 uint32
+constexpr int kStripeBytes = kStripeWords * 4;        // 3584 bytes
+constexpr int kSamplePad = 256;         // databases are padded to this many samples
+constexpr int kMaxKmers = 32;           // k-mer lengths per database
+constexpr int kMaxSketch64 = 1023;      // 64 * s64 must fit the uint16 tile counters
+
+// Output modes (public values in sketchlib_b200.h) plus internal single-column modes.
+enum OutMode : int {
+  kOutCoreAcc = 0,   // float2 per pair
+  kOutJaccard = 1,   // float[K] per pair
+  kOutCounts = 2,    // uint32[K] per pair
+  kOutColumn = 3     // float per pair: core (col 0) / accessory (col 1)
+};
+enum RandMode : int { kRandNone = 0, kRandEqualBase = 1, kRandTable = 2 };
+
+// Device-side status word of a context.  error != 0 makes the host call fail.
+struct DevStatus {
+  unsigned int error;      // bit 0: bounded wait timed out, bit 1: cancelled
+  unsigned int where;      // last site that raised an error
+  unsigned long long tiles_done;
+};
+
+// Everything one distance launch (one job) needs.  Rows are the "this"/query
+// side of a pair, columns the reference side; for all-vs-all both are the
+// same database and only pairs with col > row are produced.
+struct JobParams {
+  const uint32_t *row_words;   // packed stripes of the row database
+  const uint32_t *col_words;   // packed stripes of the column database
+  int64_t n_rows, n_cols;      // real sample counts
+  int32_t ng_rows, ng_cols;    // granules in each packed array
+  int32_t n_kmers;             // K
+  int32_t nb;                  // 2 * sketchsize64
+  int32_t self;                // 1: all-vs-all upper triangle
+  int32_t out_mode;            // OutMode
+  int32_t out_col;             // column for kOutColumn
+  int32_t tile_rows, tile_cols;  // CTA tile (must match the kernel instance)
+  int64_t n_tiles;
+  int32_t n_row_tiles, n_col_tiles;
+  void *out;                   // device output
+  double tol;                  // 5 / (64 * s64) (src/dist/linear_regression.cpp:22)
+  double union_bits;           // 64 * s64 (src/reference.cpp:91)
+  // random-match correction
+  int32_t rmode;
+  const float *rtable;         // kRandTable: [K][C][C]
+  int32_t rs_k, rs_row, rs_col;  // strides into rtable for (k, row cluster, col cluster)
+  const uint16_t *cl_rows, *cl_cols;   // per-sample cluster ids (may be null)
+  const double *jv_rows, *jv_cols;     // kRandEqualBase: [K][n_pad] 1-(1-4^-k')^len
+  int64_t jv_rows_ld, jv_cols_ld;      // leading dimension (padded samples)
+  int32_t kmers[kMaxKmers];
+};
+
+// splitmix64 finaliser: the counter-based hash of the synthetic generator.
+// Identical on host and device (pure integer arithmetic).
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+inline uint64_t synth_mix(uint64_t x) {
+  x ^= x >> 30;
+  x *= 0xBF58476D1CE4E5B9ULL;
+  x ^= x >> 27;
+  x *= 0x94D049BB133111EBULL;
+  x ^= x >> 31;
+  return x;
+}
+
+// 14-bit bin value of sample s at k-mer index k, bin `bin`.  A sample copies
+// its parent's bin unless the hash's high word falls below thresh[s][k]
+// (probability 1-(1-c)^k(1-a) for its branch), in which case it draws a fresh
+// uniform value; roots always draw.  Walking up the lineage makes every bin
+// independent of the order samples are generated in.
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+inline uint32_t synth_bin(const int32_t *parent, const uint32_t *thresh,
+                          int32_t n_kmers, int64_t s, int32_t k, uint32_t bin,
+                          uint64_t seed) {
+  int64_t node = s;
+  for (;;) {
+    uint64_t h = synth_mix(seed ^ (static_cast<uint64_t>(node) * 0x9E3779B97F4A7C15ULL) ^
+                           ((static_cast<uint64_t>(k) << 32 | bin) * 0xC2B2AE3D27D4EB4FULL));
+    int32_t par = parent[node];
+    if (par < 0 || static_cast<uint32_t>(h >> 32) < thresh[node * n_kmers + k]) {
+      return static_cast<uint32_t>(h) & ((1u << kBbits) - 1u);
+    }
+    node = par;
+  }
+}
+
+}  // namespace sk

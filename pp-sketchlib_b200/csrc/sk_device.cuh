@@ -1,0 +1,243 @@
+// sk_device.cuh -- device helpers shared by the distance kernels: bulk-copy /
+// mbarrier wrappers with bounded waits, the bit-plane intersect primitive, the
+// triangular tile map and the per-pair epilogue (random-match correction,
+// k-range truncation and the log-linear fit).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "sk_common.h"
+
+namespace sk {
+
+// ---------------------------------------------------------------- PTX wrappers
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+               : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+// One bulk (TMA engine) copy global -> shared, completing on `bar`.
+// dst, src and bytes must be multiples of 16.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes,
+                                         uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Waits for phase `parity` of `bar` for at most `limit_ns`.  Returns false on
+// timeout; the caller records the error and unwinds instead of spinning on.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity,
+                                                  uint64_t limit_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (;;) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (global_ns() - t0 > limit_ns) return false;
+  }
+}
+
+// acc & ~(a ^ b): one 3-input LOP3 per 32 bins per bit plane.
+__device__ __forceinline__ uint32_t lop_eq_and(uint32_t acc, uint32_t a, uint32_t b) {
+  uint32_t d;
+  asm("lop3.b32 %0, %1, %2, %3, 0x82;" : "=r"(d) : "r"(a), "r"(b), "r"(acc));
+  return d;
+}
+// ~(a ^ b): the first plane of a block.
+__device__ __forceinline__ uint32_t lop_eq(uint32_t a, uint32_t b) {
+  uint32_t d;
+  asm("lop3.b32 %0, %1, %2, %1, 0xC3;" : "=r"(d) : "r"(a), "r"(b));
+  return d;
+}
+
+// ------------------------------------------------------------------ tile map
+
+// All-vs-all: row tile ti (rows ti*tr .. ti*tr+tr-1) needs column tiles
+// tj >= ti*m (m = tile_rows / tile_cols), the first one holding a column
+// greater than the tile's first row.  Tiles are numbered row-tile-major.
+__device__ __forceinline__ int64_t tri_tiles_before(int64_t ti, int64_t n_col_tiles, int64_t m) {
+  return ti * n_col_tiles - m * ti * (ti - 1) / 2;
+}
+
+__device__ __forceinline__ void tile_coords(const JobParams &p, int64_t tile, int32_t &ti,
+                                            int32_t &tj) {
+  if (p.self) {
+    const int64_t m = p.tile_rows / p.tile_cols;
+    int64_t lo = 0, hi = p.n_row_tiles - 1;
+    while (lo < hi) {  // largest ti with tiles_before(ti) <= tile
+      const int64_t mid = (lo + hi + 1) >> 1;
+      if (tri_tiles_before(mid, p.n_col_tiles, m) <= tile) lo = mid; else hi = mid - 1;
+    }
+    ti = static_cast<int32_t>(lo);
+    tj = static_cast<int32_t>(lo * m + (tile - tri_tiles_before(lo, p.n_col_tiles, m)));
+  } else {
+    ti = static_cast<int32_t>(tile / p.n_col_tiles);
+    tj = static_cast<int32_t>(tile % p.n_col_tiles);
+  }
+}
+
+// -------------------------------------------------------------- pair epilogue
+
+// Random match chance for (row gi, col gj) at k-mer index k
+// (RandomMC::random_match, src/random/random_match.cpp:185-206; csrs :318-336).
+__device__ __forceinline__ double random_match(const JobParams &p, int k, int64_t gi, int64_t gj) {
+  if (p.rmode == kRandTable) {
+    const int cr = p.cl_rows ? p.cl_rows[gi] : 0;
+    const int cc = p.cl_cols ? p.cl_cols[gj] : 0;
+    return static_cast<double>(p.rtable[k * p.rs_k + cr * p.rs_row + cc * p.rs_col]);
+  }
+  if (p.rmode == kRandEqualBase) {
+    const double j1 = p.jv_rows[k * p.jv_rows_ld + gi];
+    const double j2 = p.jv_cols[k * p.jv_cols_ld + gj];
+    if (j1 > 0.0 && j2 > 0.0) {
+      const double num = __dmul_rn(j1, j2);
+      return __ddiv_rn(num, __dsub_rn(__dadd_rn(j1, j2), num));
+    }
+  }
+  return 0.0;
+}
+
+// Random-corrected Jaccard as the float the reference regresses on:
+// J = max(obs - r, 0) / (1 - r), obs = count / (64 * s64) in double
+// (Reference::jaccard_dist, src/reference.cpp:86-96; observed_excess,
+// src/dist/dist.hpp:19-24), then narrowed to float (regress_kmers,
+// src/dist/linear_regression.cpp:66-69).
+__device__ __forceinline__ float corrected_jaccard(uint32_t count, double union_bits, double r) {
+  const double obs = __ddiv_rn(static_cast<double>(count), union_bits);
+  const double diff = obs > r ? __dsub_rn(obs, r) : 0.0;
+  return __double2float_rn(__ddiv_rn(diff, __dsub_rn(1.0, r)));
+}
+
+// Log-linear fit log J_k = log(1-acc) + k log(1-core) over the contiguous
+// k-range from the first to the last J above tolerance (fit_slope,
+// src/dist/linear_regression.cpp:16-60).  Fewer than 2 points in the range
+// gives (0, 0), the reference GPU's result (src/gpu/dist.cu:95-97); the
+// reference CPU exits the process there.  Solved in double with centred sums
+// and no fused multiply-adds, identical operation order to the oracle.
+template <int KMAX>
+__device__ __forceinline__ float2 fit_core_acc(const float (&jf)[KMAX], const JobParams &p) {
+  int first = -1, last = -1;
+#pragma unroll
+  for (int k = 0; k < KMAX; ++k) {
+    if (k < p.n_kmers && static_cast<double>(jf[k]) > p.tol) {
+      if (first < 0) first = k;
+      last = k;
+    }
+  }
+  float2 res = make_float2(0.0f, 0.0f);
+  if (first < 0 || last - first + 1 < 2) return res;
+  const double n = static_cast<double>(last - first + 1);
+  double y[KMAX];
+  double sx = 0.0, sy = 0.0;
+#pragma unroll
+  for (int k = 0; k < KMAX; ++k) {
+    if (k >= first && k <= last) {
+      y[k] = log(static_cast<double>(jf[k]));
+      sx = __dadd_rn(sx, static_cast<double>(p.kmers[k]));
+      sy = __dadd_rn(sy, y[k]);
+    }
+  }
+  const double xm = __ddiv_rn(sx, n);
+  const double ym = __ddiv_rn(sy, n);
+  double sxx = 0.0, sxy = 0.0;
+#pragma unroll
+  for (int k = 0; k < KMAX; ++k) {
+    if (k >= first && k <= last) {
+      const double dx = __dsub_rn(static_cast<double>(p.kmers[k]), xm);
+      const double dy = __dsub_rn(y[k], ym);
+      sxx = __dadd_rn(sxx, __dmul_rn(dx, dx));
+      sxy = __dadd_rn(sxy, __dmul_rn(dx, dy));
+    }
+  }
+  const double slope = __ddiv_rn(sxy, sxx);
+  const double icpt = __dsub_rn(ym, __dmul_rn(slope, xm));
+  if (slope < 0.0) res.x = __double2float_rn(__dsub_rn(1.0, exp(slope)));
+  if (icpt < 0.0) res.y = __double2float_rn(__dsub_rn(1.0, exp(icpt)));
+  return res;
+}
+
+// Long-form row of pair (gi, gj): square_to_condensed (src/dist/matrix_idx.hpp:46-50)
+// for all-vs-all, gi * n_cols + gj for query-vs-reference (src/api.cpp:251).
+__device__ __forceinline__ int64_t pair_row(const JobParams &p, int64_t gi, int64_t gj) {
+  if (p.self) return p.n_rows * gi - ((gi * (gi + 1)) >> 1) + gj - 1 - gi;
+  return gi * p.n_cols + gj;
+}
+
+// Finishes one pair from its K intersection counts and writes it out.
+template <int KMAX>
+__device__ __forceinline__ void finish_pair(const JobParams &p, int64_t gi, int64_t gj,
+                                            const uint16_t *counts, int count_stride) {
+  const int64_t row = pair_row(p, gi, gj);
+  const int K = p.n_kmers;
+  if (p.out_mode == kOutCounts) {
+    uint32_t *o = static_cast<uint32_t *>(p.out) + row * K;
+    for (int k = 0; k < K; ++k) o[k] = counts[k * count_stride];
+    return;
+  }
+  float jf[KMAX];
+#pragma unroll
+  for (int k = 0; k < KMAX; ++k) {
+    jf[k] = 0.0f;
+    if (k < K) jf[k] = corrected_jaccard(counts[k * count_stride], p.union_bits,
+                                         random_match(p, k, gi, gj));
+  }
+  if (p.out_mode == kOutJaccard) {
+    float *o = static_cast<float *>(p.out) + row * K;
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k)
+      if (k < K) o[k] = jf[k];
+    return;
+  }
+  if (p.out_mode == kOutColumn && p.out_col >= 2) {  // Jaccard at k index out_col - 2
+    float v = 0.0f;
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k)
+      if (k == p.out_col - 2) v = jf[k];
+    static_cast<float *>(p.out)[row] = v;
+    return;
+  }
+  const float2 ca = fit_core_acc<KMAX>(jf, p);
+  if (p.out_mode == kOutCoreAcc) {
+    static_cast<float2 *>(p.out)[row] = ca;
+  } else {
+    static_cast<float *>(p.out)[row] = p.out_col == 0 ? ca.x : ca.y;
+  }
+}
+
+}  // namespace sk

@@ -1,0 +1,60 @@
+// sk_launch.h -- host-side declarations of the kernel launchers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "sk_common.h"
+
+namespace sk {
+
+// One compiled instance of the tiled distance kernel.
+struct TileConfig {
+  int id;
+  int tile_rows, tile_cols;      // CTA tile (rows x cols of pairs)
+  int thread_rows, thread_cols;  // per-thread register block
+  int max_kmers;                 // K the shared count buffer holds
+  int stages;                    // pipeline depth
+  int threads;
+  int smem_bytes;
+  cudaError_t (*launch)(const JobParams &, DevStatus *, const volatile int *, int grid,
+                        cudaStream_t);
+  int (*blocks_per_sm)();        // resident CTAs per SM at this shape's shared memory
+};
+
+int tile_config_count();
+const TileConfig *tile_config(int id);
+
+// Batched persistent launch over many jobs (batch_kernel.cu).
+struct BatchJob;  // device-side job descriptor
+cudaError_t launch_batch(const TileConfig &cfg, const void *d_jobs, int n_jobs,
+                         const int64_t *d_tile_prefix, int64_t total_tiles, DevStatus *status,
+                         const volatile int *cancel, int grid, cudaStream_t stream);
+
+// aux_kernels.cu
+cudaError_t launch_pack(const uint64_t *words, int64_t n, int32_t n_kmers, int32_t s64,
+                        int32_t ng, uint32_t *packed, cudaStream_t stream);
+cudaError_t launch_unpack(const uint32_t *packed, int64_t n, int32_t n_kmers, int32_t s64,
+                          int32_t ng, uint64_t *words, cudaStream_t stream);
+cudaError_t launch_synth(const int32_t *parent, const uint32_t *thresh, int64_t n,
+                         int32_t n_kmers, int32_t s64, uint64_t seed, uint64_t *words,
+                         cudaStream_t stream);
+cudaError_t launch_knn_self(const float *col_vals, int64_t n, int32_t knn, int32_t jaccard,
+                            int64_t *j_out, float *d_out, cudaStream_t stream);
+cudaError_t launch_knn_rows(const float *vals, int64_t n_rows, int64_t n_cols, int32_t knn,
+                            int64_t *j_out, float *d_out, cudaStream_t stream);
+cudaError_t launch_threshold_count(const float *vals, int64_t n, int32_t stride, int32_t col,
+                                   float cutoff, int64_t *row_counts, cudaStream_t stream);
+cudaError_t launch_threshold_fill(const float *vals, int64_t n, int32_t stride, int32_t col,
+                                  float cutoff, const int64_t *row_offsets, int64_t *i_out,
+                                  int64_t *j_out, float *d_out, cudaStream_t stream);
+cudaError_t exclusive_scan_i64(const int64_t *in, int64_t *out, int64_t n, void *tmp,
+                               size_t *tmp_bytes, cudaStream_t stream);
+cudaError_t launch_long_to_square(const float *rr, int64_t n_rr, const float *qr,
+                                  const float *qq, int64_t n_qq, float *square,
+                                  cudaStream_t stream);
+cudaError_t launch_square_to_long(const float *square, int64_t n, float *long_out,
+                                  cudaStream_t stream);
+
+}  // namespace sk

@@ -1,0 +1,94 @@
+// sk_runtime.h -- host-side state behind the opaque C ABI handles.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <mutex>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "sk_common.h"
+#include "sk_launch.h"
+#include "sketchlib_b200.h"
+
+struct Scratch {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+};
+
+struct sk_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = true;
+  int sm_count = 0;
+  std::string err;
+  int *cancel_host = nullptr;   // mapped pinned word polled by the kernels
+  int *cancel_dev = nullptr;
+  sk::DevStatus *status_dev = nullptr;
+  unsigned long long last_tiles = 0;
+  int tile_cfg = 0;                               // forced tile shape (0 = automatic)
+  std::map<std::pair<int, int>, int> tuning;      // (K, s64) -> shape id
+  Scratch scratch[4];                             // reusable device buffers
+  std::recursive_mutex mu;
+};
+
+struct sk_db {
+  sk_ctx *ctx = nullptr;
+  int64_t n = 0;
+  int32_t K = 0, s64 = 0, bbits = 0;
+  std::vector<int32_t> kmers;
+  int32_t ng = 0;                 // granules in the packed array (padded samples / 64)
+  uint32_t *packed = nullptr;     // [K][2*s64][ng][14][64]
+  uint16_t *cluster = nullptr;    // [ng*64] random-match cluster ids
+  std::vector<uint64_t> seq_len;  // per-sample sequence lengths
+  double *jv = nullptr;           // [K][ng*64] equal-base factors
+  int jv_rc = -1;
+};
+
+struct sk_random {
+  sk_ctx *ctx = nullptr;
+  int mode = 0;
+  int use_rc = 1;
+  std::vector<int32_t> kmers;
+  int n_clusters = 0;
+  float *table = nullptr;         // [K][C][C]
+};
+
+struct sk_sparse {
+  std::vector<int64_t> i, j;
+  std::vector<float> d;
+};
+
+namespace sk {
+
+class DeviceGuard {
+ public:
+  explicit DeviceGuard(int dev);
+  ~DeviceGuard();
+  DeviceGuard(const DeviceGuard &) = delete;
+  DeviceGuard &operator=(const DeviceGuard &) = delete;
+
+ private:
+  int prev_ = 0;
+};
+
+sk_status fail(sk_ctx *ctx, sk_status st, const char *fmt, ...);
+sk_status cuda_fail(sk_ctx *ctx, cudaError_t e, const char *what);
+sk_status scratch(sk_ctx *ctx, int slot, size_t bytes, void **out);
+sk_status begin_call(sk_ctx *ctx);
+sk_status finish_call(sk_ctx *ctx);
+const TileConfig *choose_config(sk_ctx *ctx, int K, int s64);
+void plan_tiles(JobParams &jp, const TileConfig &cfg);
+sk_status build_job(sk_ctx *ctx, const sk_db *ref, const sk_db *query, const sk_random *random,
+                    int out_mode, int out_col, void *d_out, const TileConfig **cfg_out,
+                    JobParams *jp);
+sk_status launch_job(sk_ctx *ctx, const JobParams &jp, const TileConfig &cfg);
+sk_status dense_to_device(sk_ctx *ctx, const sk_db *ref, const sk_db *query,
+                          const sk_random *random, int out_mode, int out_col, void *d_out);
+int64_t n_pairs(const sk_db *ref, const sk_db *query);
+size_t out_bytes(int out_mode, int64_t pairs, int K);
+
+}  // namespace sk
