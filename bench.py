@@ -291,7 +291,7 @@ def run_ours(args, rank, world, local):
     step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
     total_s = starts[0].elapsed_time(ends[-1]) / 1e3
     total_s = reduce_max(total_s, world, dev)
-    value = pairs * world / total_s
+    value = pairs * args.steps * world / total_s
     launch_s = statistics.mean(step_ms) / 1e3
 
     # ---- end to end through the C ABI with pinned host buffers
@@ -362,6 +362,24 @@ def run_ours(args, rank, world, local):
     ctx.close()
 
 
+def run_profile_case(n: int, launches: int):
+    """A small case for ncu: n samples, `launches` dense launches, nothing else."""
+    import torch
+    from sketchlib_b200 import capi, synth
+    ctx = capi.Context(0)
+    parent, thresh = synth.random_tree(n, kmers=KMERS, seed=SEED)
+    words = torch.empty(n * len(KMERS) * S64 * BBITS, dtype=torch.int64, device="cuda")
+    capi.synth_device(ctx, parent, thresh, S64, seed=SEED, d_words=words.data_ptr())
+    db = capi.Database(ctx, words.data_ptr(), KMERS, S64, n_samples=n)
+    out = torch.empty((n_pairs(n), 2), dtype=torch.float32, device="cuda")
+    for _ in range(launches):
+        capi.dists_dense(ctx, db, out=out.data_ptr())
+    ctx.synchronize()
+    print(json.dumps({"profile_case": n, "pairs": n_pairs(n), "launches": launches}))
+    db.close()
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -372,7 +390,13 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", type=int, default=0,
+                    help="run only N-sample dense launches (a small case for ncu)")
+    ap.add_argument("--profile-launches", type=int, default=2)
     args = ap.parse_args()
+    if args.profile:
+        run_profile_case(args.profile, args.profile_launches)
+        return
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference_arm(args, rank, world)

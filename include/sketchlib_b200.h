@@ -84,6 +84,8 @@ int32_t sk_abi_version(void);
 /* Binds a context to device_id (cudaSetDevice, src/gpu/dist.cu:373-384) and
  * creates its own non-blocking stream. */
 sk_status sk_ctx_create(int32_t device_id, sk_ctx **out);
+/* Releases the caller's handle.  Databases and random models created on the
+ * context keep it alive; its device resources go with the last of them. */
 sk_status sk_ctx_destroy(sk_ctx *ctx);
 /* Last error message of this context ("" if none).  Valid until the next call. */
 const char *sk_last_error(const sk_ctx *ctx);

@@ -108,28 +108,29 @@ static int fit_range(const float *J, int K, int s64, int *first) {
 }
 
 /* Exact-arithmetic semantics of fit_slope: least squares of log J on k over
- * the range, centred sums in double.  Fewer than 2 points in the range gives
- * (0, 0) (the reference CPU calls exit(1) there, its GPU writes 0, 0). */
+ * the range in double,
+ *   xm = sum x / n, ym = sum y / n,
+ *   slope = sum (x - xm) y / sum (x - xm)^2, intercept = ym - slope xm.
+ * Fewer than 2 points in the range gives (0, 0) (the reference CPU calls
+ * exit(1) there, its GPU writes 0, 0). */
 void sko_fit_slope_f64(const float *J, const int *kmers, int K, int s64, float *core, float *acc) {
   int f;
   const int n = fit_range(J, K, s64, &f);
   *core = 0.0f;
   *acc = 0.0f;
   if (n < 2) return;
-  double y[64];
-  double sx = 0.0, sy = 0.0;
+  double sx = 0.0;
+  for (int i = f; i < f + n; i++) sx = sx + (double)kmers[i];
+  const double xm = sx / n;
+  double sy = 0.0, sxx = 0.0, sxy = 0.0;
   for (int i = f; i < f + n; i++) {
-    y[i - f] = log((double)J[i]);
-    sx = sx + (double)kmers[i];
-    sy = sy + y[i - f];
-  }
-  const double xm = sx / n, ym = sy / n;
-  double sxx = 0.0, sxy = 0.0;
-  for (int i = f; i < f + n; i++) {
-    const double dx = (double)kmers[i] - xm, dy = y[i - f] - ym;
+    const double y = log((double)J[i]);
+    const double dx = (double)kmers[i] - xm;
+    sy = sy + y;
     sxx = sxx + dx * dx;
-    sxy = sxy + dx * dy;
+    sxy = sxy + dx * y;
   }
+  const double ym = sy / n;
   const double slope = sxy / sxx;
   const double icpt = ym - slope * xm;
   if (slope < 0.0) *core = (float)(1.0 - exp(slope));

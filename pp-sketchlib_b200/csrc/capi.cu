@@ -47,6 +47,35 @@ sk_status cuda_fail(sk_ctx *ctx, cudaError_t e, const char *what) {
   return fail(ctx, st, "CUDA error in %s: %s", what, cudaGetErrorString(e));
 }
 
+static std::mutex g_ctx_refs_mu;
+
+static void ctx_free(sk_ctx *ctx) {
+  {
+    DeviceGuard g(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (auto &s : ctx->scratch)
+      if (s.ptr) cudaFree(s.ptr);
+    if (ctx->status_dev) cudaFree(ctx->status_dev);
+    if (ctx->cancel_host) cudaFreeHost(ctx->cancel_host);
+    if (ctx->stream && ctx->own_stream) cudaStreamDestroy(ctx->stream);
+  }
+  delete ctx;
+}
+
+void ctx_retain(sk_ctx *ctx) {
+  std::lock_guard<std::mutex> g(g_ctx_refs_mu);
+  ++ctx->refs;
+}
+
+void ctx_release(sk_ctx *ctx) {
+  bool last = false;
+  {
+    std::lock_guard<std::mutex> g(g_ctx_refs_mu);
+    last = --ctx->refs == 0;
+  }
+  if (last) ctx_free(ctx);
+}
+
 DeviceGuard::DeviceGuard(int dev) {
   cudaGetDevice(&prev_);
   if (prev_ != dev) cudaSetDevice(dev);
@@ -106,8 +135,7 @@ const TileConfig *choose_config(sk_ctx *ctx, int K, int s64) {
     const TileConfig *c = tile_config(it->second);
     if (c && c->max_kmers >= K) return c;
   }
-  if (K <= 8) return tile_config(1);
-  return tile_config(2);
+  return tile_config(1);
 }
 
 // Upper-triangle / rectangle tile counts for a tile shape.
@@ -194,6 +222,7 @@ sk_status build_job(sk_ctx *ctx, const sk_db *ref, const sk_db *query, const sk_
   jp->out = d_out;
   jp->tol = 5.0 / (ref->s64 * 64);
   jp->union_bits = static_cast<double>(64 * ref->s64);
+  jp->one = 1;
   for (int k = 0; k < ref->K; ++k) jp->kmers[k] = ref->kmers[k];
   jp->rmode = random ? random->mode : kRandNone;
   if (jp->rmode == kRandTable) {
@@ -229,7 +258,11 @@ sk_status launch_job(sk_ctx *ctx, const JobParams &jp, const TileConfig &cfg) {
   if (per_sm < 1) return fail(ctx, SK_ECUDA, "Tile configuration %d does not fit the device", cfg.id);
   int64_t grid = static_cast<int64_t>(per_sm) * ctx->sm_count;
   if (grid > jp.n_tiles) grid = jp.n_tiles;
-  cudaError_t e = cfg.launch(jp, ctx->status_dev, ctx->cancel_dev, static_cast<int>(grid), ctx->stream);
+  void *counts = nullptr;
+  sk_status st = scratch(ctx, 0, count_scratch_bytes(cfg, static_cast<int>(grid), jp.n_kmers), &counts);
+  if (st != SK_OK) return st;
+  cudaError_t e = cfg.launch(jp, static_cast<uint16_t *>(counts), ctx->status_dev, ctx->cancel_dev,
+                             static_cast<int>(grid), ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "distance kernel launch");
   return SK_OK;
 }
@@ -299,15 +332,11 @@ sk_status sk_ctx_create(int32_t device_id, sk_ctx **out) {
 sk_status sk_ctx_destroy(sk_ctx *ctx) {
   if (!ctx) return SK_EINVAL;
   {
-    DeviceGuard g(ctx->device);
-    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    for (auto &s : ctx->scratch)
-      if (s.ptr) cudaFree(s.ptr);
-    if (ctx->status_dev) cudaFree(ctx->status_dev);
-    if (ctx->cancel_host) cudaFreeHost(ctx->cancel_host);
-    if (ctx->stream && ctx->own_stream) cudaStreamDestroy(ctx->stream);
+    std::lock_guard<std::mutex> g(g_ctx_refs_mu);
+    if (ctx->destroyed) return SK_EINVAL;
+    ctx->destroyed = true;
   }
-  delete ctx;
+  ctx_release(ctx);
   return SK_OK;
 }
 
@@ -401,6 +430,7 @@ static sk_status db_create_impl(sk_ctx *ctx, const uint64_t *words, bool on_devi
     if (kmers[k] < 1 || kmers[k] > 64) return fail(ctx, SK_EINVAL, "bad k-mer length %d", kmers[k]);
   sk_db *db = new sk_db();
   db->ctx = ctx;
+  ctx_retain(ctx);
   db->n = n;
   db->K = K;
   db->s64 = s64;
@@ -412,6 +442,7 @@ static sk_status db_create_impl(sk_ctx *ctx, const uint64_t *words, bool on_devi
   cudaError_t e = cudaMalloc(&db->packed, packed_words * 4);
   if (e != cudaSuccess) {
     delete db;
+    ctx_release(ctx);
     return cuda_fail(ctx, e, "sketch database allocation");
   }
   const size_t in_words = static_cast<size_t>(n) * K * s64 * kBbits;
@@ -428,7 +459,9 @@ static sk_status db_create_impl(sk_ctx *ctx, const uint64_t *words, bool on_devi
   if (e != cudaSuccess) {
     cudaFree(db->packed);
     delete db;
-    return cuda_fail(ctx, e, "sketch upload");
+    sk_status st = cuda_fail(ctx, e, "sketch upload");
+    ctx_release(ctx);
+    return st;
   }
   *out = db;
   return SK_OK;
@@ -451,12 +484,16 @@ sk_status sk_db_create_device(sk_ctx *ctx, const uint64_t *d_words, int64_t n_sa
 
 sk_status sk_db_destroy(sk_db *db) {
   if (!db) return SK_EINVAL;
-  DeviceGuard g(db->ctx->device);
-  cudaStreamSynchronize(db->ctx->stream);
-  if (db->packed) cudaFree(db->packed);
-  if (db->cluster) cudaFree(db->cluster);
-  if (db->jv) cudaFree(db->jv);
+  sk_ctx *ctx = db->ctx;
+  {
+    DeviceGuard g(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    if (db->packed) cudaFree(db->packed);
+    if (db->cluster) cudaFree(db->cluster);
+    if (db->jv) cudaFree(db->jv);
+  }
   delete db;
+  ctx_release(ctx);
   return SK_OK;
 }
 
@@ -522,12 +559,14 @@ sk_status sk_random_create(sk_ctx *ctx, int32_t mode, int32_t use_rc, const int3
     return fail(ctx, SK_EINVAL, "bad k-mer list for random matches");
   sk_random *r = new sk_random();
   r->ctx = ctx;
+  ctx_retain(ctx);
   r->mode = mode;
   r->use_rc = use_rc ? 1 : 0;
   r->kmers.assign(kmers, kmers + n_kmers);
   if (mode == kRandTable) {
     if (n_clusters < 1 || !table) {
       delete r;
+      ctx_release(ctx);
       return fail(ctx, SK_EINVAL, "Random match table needs n_clusters >= 1 and a table");
     }
     r->n_clusters = n_clusters;
@@ -537,7 +576,9 @@ sk_status sk_random_create(sk_ctx *ctx, int32_t mode, int32_t use_rc, const int3
     if (e != cudaSuccess) {
       if (r->table) cudaFree(r->table);
       delete r;
-      return cuda_fail(ctx, e, "random match table");
+      sk_status st = cuda_fail(ctx, e, "random match table");
+      ctx_release(ctx);
+      return st;
     }
   }
   *out = r;
@@ -546,9 +587,13 @@ sk_status sk_random_create(sk_ctx *ctx, int32_t mode, int32_t use_rc, const int3
 
 sk_status sk_random_destroy(sk_random *random) {
   if (!random) return SK_EINVAL;
-  DeviceGuard g(random->ctx->device);
-  if (random->table) cudaFree(random->table);
+  sk_ctx *ctx = random->ctx;
+  {
+    DeviceGuard g(ctx->device);
+    if (random->table) cudaFree(random->table);
+  }
   delete random;
+  ctx_release(ctx);
   return SK_OK;
 }
 

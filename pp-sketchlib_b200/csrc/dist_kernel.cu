@@ -28,33 +28,39 @@ namespace sk {
 constexpr int kBlocksPerStage = 2;   // 32-bin blocks per pipeline stage
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s bounded waits
 
-template <int QT, int RT, int TQ, int TR, int KMAX, int STAGES>
+template <int QT, int RT, int TQ, int TR, int STAGES>
 struct TileShape {
   static constexpr int kThreads = (QT / TQ) * (RT / TR);
+  static constexpr int kPairsPerThread = TQ * TR;
   static constexpr int kQG = QT / kGranule;
   static constexpr int kRG = RT / kGranule;
   static constexpr int kStageQWords = kBlocksPerStage * kQG * kStripeWords;
   static constexpr int kStageRWords = kBlocksPerStage * kRG * kStripeWords;
   static constexpr int kStageBytes = (kStageQWords + kStageRWords) * 4;
-  static constexpr int kCountBytes = KMAX * QT * RT * 2;
-  static constexpr int kSmemBytes = STAGES * kStageBytes + kCountBytes;
+  static constexpr int kSmemBytes = STAGES * kStageBytes;
   static_assert(QT % kGranule == 0 && RT % kGranule == 0, "tiles are whole granules");
   static_assert(kGranule % TQ == 0 && kGranule % TR == 0, "thread blocks stay in a granule");
   static_assert(TQ % 4 == 0 && TR % 4 == 0, "128-bit shared loads");
+  static_assert(kPairsPerThread % 8 == 0, "counts are stored as 16-byte groups");
   static_assert(QT % RT == 0, "triangular map needs tile_rows multiple of tile_cols");
 };
 
-template <int QT, int RT, int TQ, int TR, int KMAX, int STAGES>
-__global__ void __launch_bounds__((QT / TQ) * (RT / TR), 1)
-    dist_tiles_kernel(const JobParams p, DevStatus *status, const volatile int *cancel) {
-  using S = TileShape<QT, RT, TQ, TR, KMAX, STAGES>;
+// Per-k counts of a thread's TQ x TR pairs are parked in `scratch` (this CTA's
+// slot: [K][threads][TQ*TR] uint16, written and read back by the same thread,
+// so no barrier is needed; 38 MB for 296 CTAs at K = 8, resident in L2).  The
+// thread then finishes its own pairs, so a tile needs no CTA-wide epilogue.
+template <int QT, int RT, int TQ, int TR, int STAGES, int MINB>
+__global__ void __launch_bounds__((QT / TQ) * (RT / TR), MINB)
+    dist_tiles_kernel(const JobParams p, uint16_t *__restrict__ scratch, DevStatus *status,
+                      const volatile int *cancel) {
+  using S = TileShape<QT, RT, TQ, TR, STAGES>;
   constexpr int NT = S::kThreads;
+  constexpr int PT = S::kPairsPerThread;
   constexpr int TCOLS = RT / TR;
 
   extern __shared__ __align__(128) unsigned char smem[];
   uint32_t *sq = reinterpret_cast<uint32_t *>(smem);
   uint32_t *sr = sq + STAGES * S::kStageQWords;
-  uint16_t *scnt = reinterpret_cast<uint16_t *>(sr + STAGES * S::kStageRWords);
   __shared__ __align__(8) uint64_t full_bar[STAGES];
   __shared__ int s_abort;
 
@@ -69,6 +75,8 @@ __global__ void __launch_bounds__((QT / TQ) * (RT / TR), 1)
   const int64_t steps_per_k = p.nb / kBlocksPerStage;
   const int64_t spt = steps_per_k * p.n_kmers;
   const int64_t total = my_tiles * spt;
+  uint16_t *my_counts = scratch + (static_cast<int64_t>(blockIdx.x) * p.n_kmers * NT + tid) * PT;
+  const int64_t k_stride = static_cast<int64_t>(NT) * PT;   // uint16 between k slots
 
   if (tid == 0) {
     for (int s = 0; s < STAGES; ++s) mbar_init(&full_bar[s], 1);
@@ -105,6 +113,9 @@ __global__ void __launch_bounds__((QT / TQ) * (RT / TR), 1)
     while (next_issue < total && next_issue < STAGES) issue(next_issue++);
   }
 
+  // 1 at run time: makes the count accumulation a multiply-add, which runs on
+  // the otherwise idle FMA pipe instead of taking ALU slots from the LOP3s.
+  const uint32_t one = p.one;
   uint32_t cnt[TQ][TR];
 #pragma unroll
   for (int i = 0; i < TQ; ++i)
@@ -150,48 +161,54 @@ __global__ void __launch_bounds__((QT / TQ) * (RT / TR), 1)
 #pragma unroll
         for (int i = 0; i < TQ; ++i)
 #pragma unroll
-          for (int j = 0; j < TR; ++j) cnt[i][j] += __popc(acc[i][j]);
+          for (int j = 0; j < TR; ++j) cnt[i][j] = mad_u32(__popc(acc[i][j]), one, cnt[i][j]);
       }
     }
+    __syncthreads();  // stage s fully read by every warp
+    if (s_abort) break;
+    if (tid == 0 && next_issue < total) issue(next_issue++);
 
     const int64_t local = t % spt;
     const int64_t kidx = local / steps_per_k;
     if (local - kidx * steps_per_k == steps_per_k - 1) {
-      // all blocks of k-mer index kidx done: park the counts in shared memory
-      uint16_t *dst = scnt + kidx * (QT * RT);
+      // all blocks of k-mer index kidx done: park this thread's counts
+      uint4 *dst = reinterpret_cast<uint4 *>(my_counts + kidx * k_stride);
+#pragma unroll
+      for (int w = 0; w < PT / 8; ++w) {
+        uint32_t packed[4];
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+          const int q0 = w * 8 + 2 * h, q1 = q0 + 1;
+          packed[h] = cnt[q0 / TR][q0 % TR] | (cnt[q1 / TR][q1 % TR] << 16);
+        }
+        dst[w] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+      }
 #pragma unroll
       for (int i = 0; i < TQ; ++i)
 #pragma unroll
-        for (int j = 0; j < TR; ++j) {
-          dst[(row0 + i) * RT + col0 + j] = static_cast<uint16_t>(cnt[i][j]);
-          cnt[i][j] = 0;
-        }
-    }
-    __syncthreads();  // stage s fully read; counts of kidx visible
-    if (s_abort) break;
-    if (tid == 0 && next_issue < total) issue(next_issue++);
+        for (int j = 0; j < TR; ++j) cnt[i][j] = 0;
 
-    if (local == spt - 1) {
-      // tile complete: epilogue over all pairs of the tile
-      int32_t ti, tj;
-      tile_coords(p, blockIdx.x + (t / spt) * gridDim.x, ti, tj);
-      const int64_t gi0 = static_cast<int64_t>(ti) * QT;
-      const int64_t gj0 = static_cast<int64_t>(tj) * RT;
-      for (int pidx = tid; pidx < QT * RT; pidx += NT) {
-        const int64_t gi = gi0 + pidx / RT;
-        const int64_t gj = gj0 + pidx % RT;
-        const bool valid = p.self ? (gj > gi && gj < p.n_cols) : (gi < p.n_rows && gj < p.n_cols);
-        if (valid) finish_pair<KMAX>(p, gi, gj, scnt + pidx, QT * RT);
-      }
-      if (tid == 0) {
-        atomicAdd(&status->tiles_done, 1ull);
-        if (cancel != nullptr && *cancel != 0) {
-          s_abort = 1;
-          atomicOr(&status->error, 2u);
+      if (kidx == p.n_kmers - 1) {
+        // tile complete: this thread finishes its own TQ x TR pairs
+        int32_t ti, tj;
+        tile_coords(p, blockIdx.x + (t / spt) * gridDim.x, ti, tj);
+        const int64_t gi0 = static_cast<int64_t>(ti) * QT + row0;
+        const int64_t gj0 = static_cast<int64_t>(tj) * RT + col0;
+#pragma unroll 1
+        for (int q = 0; q < PT; ++q) {
+          const int64_t gi = gi0 + q / TR;
+          const int64_t gj = gj0 + q % TR;
+          const bool valid = p.self ? (gj > gi && gj < p.n_cols) : (gi < p.n_rows && gj < p.n_cols);
+          if (valid) finish_pair_any(p, gi, gj, my_counts + q, static_cast<int>(k_stride));
+        }
+        if (tid == 0) {
+          atomicAdd(&status->tiles_done, 1ull);
+          if (cancel != nullptr && *cancel != 0) {
+            s_abort = 1;   // seen by every thread after the next step's barrier
+            atomicOr(&status->error, 2u);
+          }
         }
       }
-      __syncthreads();  // counts consumed before the next tile overwrites them
-      if (s_abort) break;
     }
   }
 
@@ -207,11 +224,11 @@ __global__ void __launch_bounds__((QT / TQ) * (RT / TR), 1)
 
 namespace {
 
-template <int QT, int RT, int TQ, int TR, int KMAX, int STAGES>
-cudaError_t launch_cfg(const JobParams &p, DevStatus *status, const volatile int *cancel,
-                       int grid, cudaStream_t stream) {
-  using S = TileShape<QT, RT, TQ, TR, KMAX, STAGES>;
-  auto kern = dist_tiles_kernel<QT, RT, TQ, TR, KMAX, STAGES>;
+template <int QT, int RT, int TQ, int TR, int STAGES, int MINB>
+cudaError_t launch_cfg(const JobParams &p, uint16_t *scratch, DevStatus *status,
+                       const volatile int *cancel, int grid, cudaStream_t stream) {
+  using S = TileShape<QT, RT, TQ, TR, STAGES>;
+  auto kern = dist_tiles_kernel<QT, RT, TQ, TR, STAGES, MINB>;
   static bool attr_set = false;
   if (!attr_set) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -219,14 +236,14 @@ cudaError_t launch_cfg(const JobParams &p, DevStatus *status, const volatile int
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
-  kern<<<grid, S::kThreads, S::kSmemBytes, stream>>>(p, status, cancel);
+  kern<<<grid, S::kThreads, S::kSmemBytes, stream>>>(p, scratch, status, cancel);
   return cudaGetLastError();
 }
 
-template <int QT, int RT, int TQ, int TR, int KMAX, int STAGES>
+template <int QT, int RT, int TQ, int TR, int STAGES, int MINB>
 int occupancy_cfg() {
-  using S = TileShape<QT, RT, TQ, TR, KMAX, STAGES>;
-  auto kern = dist_tiles_kernel<QT, RT, TQ, TR, KMAX, STAGES>;
+  using S = TileShape<QT, RT, TQ, TR, STAGES>;
+  auto kern = dist_tiles_kernel<QT, RT, TQ, TR, STAGES, MINB>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, S::kSmemBytes) !=
       cudaSuccess)
     return 0;
@@ -237,28 +254,28 @@ int occupancy_cfg() {
   return blocks;
 }
 
-template <int QT, int RT, int TQ, int TR, int KMAX, int STAGES>
+template <int QT, int RT, int TQ, int TR, int STAGES, int MINB>
 constexpr TileConfig make_cfg(int id) {
   return TileConfig{id,
                     QT,
                     RT,
                     TQ,
                     TR,
-                    KMAX,
+                    kMaxKmers,
                     STAGES,
-                    TileShape<QT, RT, TQ, TR, KMAX, STAGES>::kThreads,
-                    TileShape<QT, RT, TQ, TR, KMAX, STAGES>::kSmemBytes,
-                    &launch_cfg<QT, RT, TQ, TR, KMAX, STAGES>,
-                    &occupancy_cfg<QT, RT, TQ, TR, KMAX, STAGES>};
+                    TileShape<QT, RT, TQ, TR, STAGES>::kThreads,
+                    TileShape<QT, RT, TQ, TR, STAGES>::kSmemBytes,
+                    &launch_cfg<QT, RT, TQ, TR, STAGES, MINB>,
+                    &occupancy_cfg<QT, RT, TQ, TR, STAGES, MINB>};
 }
 
 const TileConfig kConfigs[] = {
-    make_cfg<128, 64, 8, 4, 8, 3>(1),   // default for K <= 8
-    make_cfg<64, 64, 4, 4, 16, 3>(2),   // K <= 16
-    make_cfg<128, 128, 8, 8, 4, 3>(3),  // K <= 4, largest tile
-    make_cfg<64, 64, 8, 4, 16, 3>(4),   // K <= 16, 128 threads
-    make_cfg<128, 64, 4, 8, 8, 3>(5),   // K <= 8, transposed thread block
-    make_cfg<64, 64, 4, 4, 8, 4>(6),    // K <= 8, small tiles for small problems
+    make_cfg<128, 64, 8, 4, 3, 2>(1),   // default: 2 CTAs x 8 warps per SM
+    make_cfg<64, 64, 4, 4, 3, 2>(2),    // small tiles, 16 pairs per thread
+    make_cfg<128, 128, 8, 8, 3, 1>(3),  // large tiles, 64 pairs per thread, 1 CTA per SM
+    make_cfg<64, 64, 8, 4, 4, 3>(4),    // 128 threads, 3 CTAs per SM
+    make_cfg<128, 64, 4, 8, 3, 2>(5),   // transposed thread block
+    make_cfg<128, 128, 8, 4, 3, 1>(6),  // 512 threads, 16 warps in one CTA
 };
 
 }  // namespace

@@ -1,0 +1,200 @@
+// host_db.cpp -- see host_db.h.
+#include "host_db.h"
+
+#include <algorithm>
+#include <cmath>
+#include <limits>
+#include <numeric>
+#include <sstream>
+#include <stdexcept>
+
+#include "host_h5.h"
+
+namespace skhost {
+namespace {
+
+constexpr uint64_t kDefaultLength = 3000000;  // DEFAULT_LENGTH, database.hpp:22
+
+std::string h5_path(const std::string &db_name) {
+  // the reference appends ".h5" to the database prefix (api.cpp:458)
+  return db_name + ".h5";
+}
+
+std::string join(const std::vector<int32_t> &v) {
+  std::ostringstream o;
+  for (int32_t x : v) o << x << ",";
+  return o.str();
+}
+
+}  // namespace
+
+std::vector<std::string> list_samples(const std::string &db_name) {
+  h5::File f(h5_path(db_name));
+  return f.list(f.open("/sketches"));
+}
+
+SketchSet load_sketches(const std::string &db_name, const std::vector<std::string> &names,
+                        const std::vector<int32_t> &kmers) {
+  h5::File f(h5_path(db_name));
+  SketchSet out;
+  out.names = names;
+  out.kmers = kmers;
+  const size_t n = names.size();
+  out.seq_len.resize(n);
+  out.bases.resize(n);
+  size_t W = 0;
+  for (size_t i = 0; i < n; ++i) {
+    h5::Object g;
+    try {
+      g = f.open("/sketches/" + names[i]);
+    } catch (const h5::Error &e) {
+      throw h5::Error(std::string("Missing sketch: ") + e.what());
+    }
+    std::vector<int64_t> have = f.attr_ints(g, "kmers");
+    const int32_t s64 = static_cast<int32_t>(f.attr_ints(g, "sketchsize64").at(0));
+    const int32_t bbits = static_cast<int32_t>(f.attr_ints(g, "bbits").at(0));
+    if (i == 0) {
+      out.sketchsize64 = s64;
+      out.bbits = bbits;
+      W = static_cast<size_t>(s64) * bbits;
+      out.words.assign(n * kmers.size() * W, 0);
+    } else if (s64 != out.sketchsize64) {
+      throw std::runtime_error("Mismatching sketchsize64 in sketches");
+    } else if (bbits != out.bbits) {
+      throw std::runtime_error("Mismatching bbits in sketches");
+    }
+    // every requested k must be present (api.cpp:464-489)
+    std::vector<int32_t> have32(have.begin(), have.end());
+    std::sort(have32.begin(), have32.end());
+    for (int32_t k : kmers) {
+      if (!std::binary_search(have32.begin(), have32.end(), k)) {
+        std::vector<int32_t> req(kmers);
+        std::sort(req.begin(), req.end());
+        throw std::runtime_error("Mismatched data: k-mer lengths in old database (" + join(have32) +
+                                 ") do not match those requested (" + join(req) + ")");
+      }
+    }
+    out.seq_len[i] = h5::File::has_attr(g, "length")
+                         ? static_cast<uint64_t>(f.attr_ints(g, "length").at(0))
+                         : kDefaultLength;
+    out.bases[i] = h5::File::has_attr(g, "base_freq") ? f.attr_doubles(g, "base_freq")
+                                                      : std::vector<double>{0.25, 0.25, 0.25, 0.25};
+    if (h5::File::has_attr(g, "reads")) out.reads = out.reads || f.attr_ints(g, "reads").at(0) != 0;
+    for (size_t ki = 0; ki < kmers.size(); ++ki) {
+      h5::Object ds = f.open("/sketches/" + names[i] + "/" + std::to_string(kmers[ki]));
+      if (ds.space.count() != W)
+        throw std::runtime_error("Sketch " + names[i] + " at k = " + std::to_string(kmers[ki]) +
+                                 " has the wrong number of words");
+      f.read_u64(ds, out.words.data() + (i * kmers.size() + ki) * W);
+    }
+  }
+  return out;
+}
+
+uint16_t RandomModel::closest_cluster(const std::vector<double> &bases_in, bool rc) const {
+  if (mode != 2 || n_clusters == 0) return 0;
+  std::vector<double> b(bases_in);
+  if (rc) {  // apply_rc (random_match.cpp:338-348)
+    b[0] = 0.5 * (b[0] + b[3]);
+    b[1] = 0.5 * (b[1] + b[2]);
+    b[2] = b[1];
+    b[3] = b[0];
+  }
+  // nearest centroid by squared distance in float, first minimum wins
+  int best = 0;
+  float best_d = std::numeric_limits<float>::infinity();
+  for (int c = 0; c < n_clusters; ++c) {
+    float d = 0.0f;
+    for (int j = 0; j < 4; ++j) {
+      const float diff = centroids[c * 4 + j] - static_cast<float>(b[j]);
+      d += diff * diff;
+    }
+    if (d < best_d) {
+      best_d = d;
+      best = c;
+    }
+  }
+  return static_cast<uint16_t>(best);
+}
+
+std::vector<uint16_t> RandomModel::lookup(const SketchSet &s, bool queries_by_centroid) const {
+  std::vector<uint16_t> ids(s.size(), 0);
+  if (mode != 2) return ids;
+  for (size_t i = 0; i < s.size(); ++i) {
+    auto it = cluster_table.find(s.names[i]);
+    if (!queries_by_centroid && it != cluster_table.end()) {
+      ids[i] = it->second;
+    } else {
+      ids[i] = closest_cluster(s.bases[i], true);  // loaded references have rc() == true
+    }
+  }
+  return ids;
+}
+
+std::vector<float> RandomModel::flat_table(const std::vector<int32_t> &kmers) const {
+  const size_t C = static_cast<size_t>(std::max(1, n_clusters));
+  std::vector<float> t(kmers.size() * C * C, 0.0f);
+  if (mode != 2) return t;
+  for (size_t ki = 0; ki < kmers.size(); ++ki) {
+    const int64_t k = kmers[ki];
+    if (k >= static_cast<int64_t>(max_k)) continue;  // strict <, as the CPU path
+    auto it = matches.find(k);
+    if (it == matches.end())
+      throw std::runtime_error("Trying to choose a k-mer length below the minimum allowed\n");
+    std::copy(it->second.begin(), it->second.end(), t.begin() + ki * C * C);
+  }
+  return t;
+}
+
+size_t RandomModel::min_supported_k() const {
+  size_t min_k_signal = min_k;
+  if (mode == 2) {
+    for (size_t k = min_k; k < max_k; ++k) {
+      auto it = matches.find(static_cast<int64_t>(k));
+      if (it == matches.end()) continue;
+      const double mean =
+          std::accumulate(it->second.begin(), it->second.end(), 0.0) / it->second.size();
+      if (mean < 1) {
+        min_k_signal = k;
+        break;
+      }
+    }
+  }
+  return min_k_signal;
+}
+
+RandomModel get_random(const std::string &db_name, bool use_rc_default) {
+  RandomModel r;
+  r.mode = 1;
+  r.use_rc = use_rc_default;
+  r.min_k = 0;
+  r.max_k = 101;
+  h5::File f(h5_path(db_name));
+  if (!f.exists("/random")) return r;
+  h5::Object g = f.open("/random");
+  r.mode = 2;
+  r.min_k = static_cast<unsigned>(f.attr_ints(g, "k_min").at(0));
+  r.max_k = static_cast<unsigned>(f.attr_ints(g, "k_max").at(0));
+  r.use_rc = f.attr_ints(g, "use_rc").at(0) != 0;
+  const auto names = f.read_strings(f.open("/random/table_keys"));
+  const auto ids = f.read_ints(f.open("/random/table_values"));
+  for (size_t i = 0; i < names.size() && i < ids.size(); ++i)
+    r.cluster_table[names[i]] = static_cast<uint16_t>(ids[i]);
+  const auto keys = f.read_ints(f.open("/random/matches_keys"));
+  h5::Object mv = f.open("/random/matches_values");
+  const auto values = f.read_doubles(mv);
+  const auto dims = f.attr_ints(mv, "dims");
+  const size_t C = static_cast<size_t>(dims.at(0));
+  if (dims.at(1) != dims.at(0)) throw std::runtime_error("random match matrices are not square");
+  r.n_clusters = static_cast<int>(C);
+  for (size_t i = 0; i < keys.size(); ++i) {
+    if ((i + 1) * C * C > values.size()) throw std::runtime_error("truncated random match table");
+    r.matches[keys[i]] = std::vector<float>(values.begin() + i * C * C, values.begin() + (i + 1) * C * C);
+  }
+  h5::Object cen = f.open("/random/centroids");
+  const auto cvals = f.read_doubles(cen);
+  r.centroids.assign(cvals.begin(), cvals.end());
+  return r;
+}
+
+}  // namespace skhost

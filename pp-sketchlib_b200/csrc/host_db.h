@@ -1,0 +1,66 @@
+// host_db.h -- reads pp-sketchlib sketch databases (<name>.h5) into the flat
+// word layout of the C ABI, plus the random-match model stored beside them.
+//
+// Database layout (src/database/database.cpp:48-112, 195-227):
+//   /sketches                      attrs sketch_version, codon_phased, reverse_complement
+//   /sketches/<sample>             attrs kmers (int[]), sketchsize64, bbits, length,
+//                                  missing_bases, reads, base_freq (double[4])
+//   /sketches/<sample>/<k>         uint64[sketchsize64 * bbits]
+//   /random                        attrs k_min, k_max, use_rc
+//   /random/table_keys|_values     sample name -> cluster id (uint16)
+//   /random/matches_keys|_values   k -> C x C float matrix (attr dims = [C, C, n_k])
+//   /random/centroids              C x 4 float (attr dims), base composition centroids
+#pragma once
+
+#include <cstdint>
+#include <map>
+#include <string>
+#include <vector>
+
+namespace skhost {
+
+struct SketchSet {
+  std::vector<std::string> names;
+  std::vector<int32_t> kmers;           // in the order requested
+  int32_t sketchsize64 = 0, bbits = 0;
+  std::vector<uint64_t> words;          // [n][K][sketchsize64 * bbits]
+  std::vector<uint64_t> seq_len;        // Reference::seq_length
+  std::vector<std::vector<double>> bases;  // A, C, G, T frequencies
+  bool reads = false;
+  size_t size() const { return names.size(); }
+};
+
+// load_sketches (src/api.cpp:436-516): the named samples' sketches at the
+// requested k-mer lengths.  Throws std::runtime_error with the reference's
+// messages when a sample or k-mer length is missing.
+SketchSet load_sketches(const std::string &db_name, const std::vector<std::string> &names,
+                        const std::vector<int32_t> &kmers);
+
+// All sample names in a database, in the file's (sorted) order.
+std::vector<std::string> list_samples(const std::string &db_name);
+
+// RandomMC as loaded by Database::load_random (database.cpp:195-227).
+struct RandomModel {
+  int mode = 0;                 // 0 NoAdjust, 1 EqualBase, 2 MonteCarlo
+  bool use_rc = true;
+  unsigned min_k = 0, max_k = 101;
+  std::map<std::string, uint16_t> cluster_table;
+  std::map<int64_t, std::vector<float>> matches;   // k -> C*C row-major
+  int n_clusters = 0;
+  std::vector<float> centroids;                   // C x 4 row-major
+
+  // closest_cluster (random_match.cpp:222-229, nearest_neighbour :339-348)
+  uint16_t closest_cluster(const std::vector<double> &bases, bool rc) const;
+  // cluster ids for samples: table entry, else nearest centroid
+  std::vector<uint16_t> lookup(const SketchSet &s, bool queries_by_centroid) const;
+  // [K][C][C] table with zeros for k >= max_k (random_match.cpp:191)
+  std::vector<float> flat_table(const std::vector<int32_t> &kmers) const;
+  // min_supported_k (random_match.cpp:165-182)
+  size_t min_supported_k() const;
+};
+
+// get_random (src/api.cpp:531-535): MonteCarlo when the database holds
+// /random, else EqualBase (use_rc_default); random_correct = false gives NoAdjust.
+RandomModel get_random(const std::string &db_name, bool use_rc_default);
+
+}  // namespace skhost

@@ -67,6 +67,7 @@ struct JobParams {
   const double *jv_rows, *jv_cols;     // kRandEqualBase: [K][n_pad] 1-(1-4^-k')^len
   int64_t jv_rows_ld, jv_cols_ld;      // leading dimension (padded samples)
   int32_t kmers[kMaxKmers];
+  uint32_t one;                // 1 (a run-time operand for the count multiply-adds)
 };
 
 // splitmix64 finaliser: the counter-based hash of the synthetic generator.

@@ -86,6 +86,13 @@ __device__ __forceinline__ uint32_t lop_eq(uint32_t a, uint32_t b) {
   return d;
 }
 
+// d = a * b + c on 32-bit integers (an IMAD: FMA pipe).
+__device__ __forceinline__ uint32_t mad_u32(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t d;
+  asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+  return d;
+}
+
 // ------------------------------------------------------------------ tile map
 
 // All-vs-all: row tile ti (rows ti*tr .. ti*tr+tr-1) needs column tiles
@@ -148,8 +155,10 @@ __device__ __forceinline__ float corrected_jaccard(uint32_t count, double union_
 // k-range from the first to the last J above tolerance (fit_slope,
 // src/dist/linear_regression.cpp:16-60).  Fewer than 2 points in the range
 // gives (0, 0), the reference GPU's result (src/gpu/dist.cu:95-97); the
-// reference CPU exits the process there.  Solved in double with centred sums
-// and no fused multiply-adds, identical operation order to the oracle.
+// reference CPU exits the process there.  Least squares in double:
+//   xm = sum x / n, ym = sum y / n,
+//   slope = sum (x - xm) y / sum (x - xm)^2, intercept = ym - slope xm,
+// without fused multiply-adds, in the same operation order as the oracle.
 template <int KMAX>
 __device__ __forceinline__ float2 fit_core_acc(const float (&jf)[KMAX], const JobParams &p) {
   int first = -1, last = -1;
@@ -163,28 +172,23 @@ __device__ __forceinline__ float2 fit_core_acc(const float (&jf)[KMAX], const Jo
   float2 res = make_float2(0.0f, 0.0f);
   if (first < 0 || last - first + 1 < 2) return res;
   const double n = static_cast<double>(last - first + 1);
-  double y[KMAX];
-  double sx = 0.0, sy = 0.0;
+  double sx = 0.0;
 #pragma unroll
-  for (int k = 0; k < KMAX; ++k) {
-    if (k >= first && k <= last) {
-      y[k] = log(static_cast<double>(jf[k]));
-      sx = __dadd_rn(sx, static_cast<double>(p.kmers[k]));
-      sy = __dadd_rn(sy, y[k]);
-    }
-  }
+  for (int k = 0; k < KMAX; ++k)
+    if (k >= first && k <= last) sx = __dadd_rn(sx, static_cast<double>(p.kmers[k]));
   const double xm = __ddiv_rn(sx, n);
-  const double ym = __ddiv_rn(sy, n);
-  double sxx = 0.0, sxy = 0.0;
+  double sy = 0.0, sxx = 0.0, sxy = 0.0;
 #pragma unroll
   for (int k = 0; k < KMAX; ++k) {
     if (k >= first && k <= last) {
+      const double y = log(static_cast<double>(jf[k]));
       const double dx = __dsub_rn(static_cast<double>(p.kmers[k]), xm);
-      const double dy = __dsub_rn(y[k], ym);
+      sy = __dadd_rn(sy, y);
       sxx = __dadd_rn(sxx, __dmul_rn(dx, dx));
-      sxy = __dadd_rn(sxy, __dmul_rn(dx, dy));
+      sxy = __dadd_rn(sxy, __dmul_rn(dx, y));
     }
   }
+  const double ym = __ddiv_rn(sy, n);
   const double slope = __ddiv_rn(sxy, sxx);
   const double icpt = __dsub_rn(ym, __dmul_rn(slope, xm));
   if (slope < 0.0) res.x = __double2float_rn(__dsub_rn(1.0, exp(slope)));
@@ -199,22 +203,23 @@ __device__ __forceinline__ int64_t pair_row(const JobParams &p, int64_t gi, int6
   return gi * p.n_cols + gj;
 }
 
-// Finishes one pair from its K intersection counts and writes it out.
+// Finishes one pair from its K intersection counts (counts[k * stride]) and
+// writes its long-form row.
 template <int KMAX>
 __device__ __forceinline__ void finish_pair(const JobParams &p, int64_t gi, int64_t gj,
-                                            const uint16_t *counts, int count_stride) {
+                                            const uint16_t *counts, int stride) {
   const int64_t row = pair_row(p, gi, gj);
   const int K = p.n_kmers;
   if (p.out_mode == kOutCounts) {
     uint32_t *o = static_cast<uint32_t *>(p.out) + row * K;
-    for (int k = 0; k < K; ++k) o[k] = counts[k * count_stride];
+    for (int k = 0; k < K; ++k) o[k] = counts[k * stride];
     return;
   }
   float jf[KMAX];
 #pragma unroll
   for (int k = 0; k < KMAX; ++k) {
     jf[k] = 0.0f;
-    if (k < K) jf[k] = corrected_jaccard(counts[k * count_stride], p.union_bits,
+    if (k < K) jf[k] = corrected_jaccard(counts[k * stride], p.union_bits,
                                          random_match(p, k, gi, gj));
   }
   if (p.out_mode == kOutJaccard) {
@@ -238,6 +243,15 @@ __device__ __forceinline__ void finish_pair(const JobParams &p, int64_t gi, int6
   } else {
     static_cast<float *>(p.out)[row] = p.out_col == 0 ? ca.x : ca.y;
   }
+}
+
+// Dispatches on the number of k-mer lengths so the per-pair arrays stay in
+// registers for the common K <= 8 and K <= 16 cases.
+__device__ __forceinline__ void finish_pair_any(const JobParams &p, int64_t gi, int64_t gj,
+                                                const uint16_t *counts, int stride) {
+  if (p.n_kmers <= 8) finish_pair<8>(p, gi, gj, counts, stride);
+  else if (p.n_kmers <= 16) finish_pair<16>(p, gi, gj, counts, stride);
+  else finish_pair<kMaxKmers>(p, gi, gj, counts, stride);
 }
 
 }  // namespace sk

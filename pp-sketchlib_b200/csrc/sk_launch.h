@@ -14,17 +14,21 @@ struct TileConfig {
   int id;
   int tile_rows, tile_cols;      // CTA tile (rows x cols of pairs)
   int thread_rows, thread_cols;  // per-thread register block
-  int max_kmers;                 // K the shared count buffer holds
+  int max_kmers;                 // largest K the instance handles
   int stages;                    // pipeline depth
   int threads;
   int smem_bytes;
-  cudaError_t (*launch)(const JobParams &, DevStatus *, const volatile int *, int grid,
-                        cudaStream_t);
+  cudaError_t (*launch)(const JobParams &, uint16_t *scratch, DevStatus *,
+                        const volatile int *, int grid, cudaStream_t);
   int (*blocks_per_sm)();        // resident CTAs per SM at this shape's shared memory
 };
 
 int tile_config_count();
 const TileConfig *tile_config(int id);
+// Bytes of per-CTA count scratch a launch of `cfg` with `grid` CTAs needs.
+inline size_t count_scratch_bytes(const TileConfig &cfg, int grid, int n_kmers) {
+  return static_cast<size_t>(grid) * n_kmers * cfg.tile_rows * cfg.tile_cols * 2;
+}
 
 // Batched persistent launch over many jobs (batch_kernel.cu).
 struct BatchJob;  // device-side job descriptor

@@ -33,6 +33,10 @@ struct sk_ctx {
   std::map<std::pair<int, int>, int> tuning;      // (K, s64) -> shape id
   Scratch scratch[4];                             // reusable device buffers
   std::recursive_mutex mu;
+  // Databases and random models keep their context alive: sk_ctx_destroy only
+  // marks it, the last dependent handle to go frees it.
+  int refs = 1;
+  bool destroyed = false;
 };
 
 struct sk_db {
@@ -76,6 +80,8 @@ class DeviceGuard {
 };
 
 sk_status fail(sk_ctx *ctx, sk_status st, const char *fmt, ...);
+void ctx_retain(sk_ctx *ctx);
+void ctx_release(sk_ctx *ctx);
 sk_status cuda_fail(sk_ctx *ctx, cudaError_t e, const char *what);
 sk_status scratch(sk_ctx *ctx, int slot, size_t bytes, void **out);
 sk_status begin_call(sk_ctx *ctx);

@@ -15,7 +15,11 @@ from sketchlib_b200 import capi
 pytestmark = pytest.mark.gpu
 
 TOL_F64 = 1e-6   # GPU vs oracle, both double-precision fits
-TOL_REF = 1e-5   # GPU vs the reference's float arithmetic
+# GPU vs the float LDLT restatement of fit_slope: that arithmetic is itself off
+# the exact fit by up to ~3e-5 on short k ranges (the golden vectors, which
+# match the double fit to 2e-7, show the reference's shipped results do not
+# carry that error); the bar here bounds the float restatement's own error.
+TOL_REF = 1e-4
 
 SHAPES = [  # (n, K, s64)
     (1, 2, 16), (2, 2, 16), (31, 3, 1), (33, 8, 156), (65, 8, 156), (130, 4, 64),
@@ -102,6 +106,7 @@ def test_jaccard_and_coreacc(gpu_ctx, mode, self_):
     want32 = oracle.dists(rw, kmers, s64, query_words=qw, random=spec, regress=1)
     assert np.abs(ca - want64).max() <= TOL_F64
     assert np.abs(ca - want32).max() <= TOL_REF
+    assert np.quantile(np.abs(ca - want32), 0.99) <= 1e-5
     assert np.mean(ca == want64) > 0.99
 
 
@@ -258,3 +263,16 @@ def test_device_output_and_large_properties(gpu_ctx):
     qdb = capi.Database(gpu_ctx, host[rows], kmers, s64)
     q = capi.dists_dense(gpu_ctx, db, qdb)
     np.testing.assert_allclose(q, sub, atol=TOL_F64, rtol=0)
+
+
+def test_context_outlives_its_handles():
+    """Destroying a context before its databases is safe: the handles keep it
+    alive and the last one to go frees it."""
+    ctx = capi.Context(0)
+    w, kmers = random_sketches(20, 2, 16, seed=3)
+    db = capi.Database(ctx, w, kmers, 16)
+    rnd = capi.Random(ctx, capi.RANDOM_EQUAL_BASE, kmers)
+    capi.lib.sk_ctx_destroy(ctx.handle)
+    ctx.handle = None
+    rnd.close()
+    db.close()
