@@ -184,6 +184,48 @@ sk_status sk_query_knn(sk_ctx *ctx, const sk_db *ref, const sk_db *query,
                        const sk_random *random, int32_t kNN, int32_t dist_col,
                        int64_t *r_out, float *d_out);
 
+/* ---- batched persistent launch ------------------------------------------- */
+
+/* One distance job of a batch: all-vs-all of `ref` (query NULL) or query vs
+ * ref, written to `out` in DEVICE memory (sk_dists_rows(ref, query) rows of
+ * the out_mode's width).  Jobs of one batch may differ in sample counts, k-mer
+ * sets and sketch widths. */
+typedef struct sk_job {
+  const sk_db *ref;
+  const sk_db *query;
+  const sk_random *random;
+  int32_t out_mode;
+  void *out;
+} sk_job;
+
+typedef struct sk_batch sk_batch;
+
+enum { SK_BATCH_AUTOTUNE = 1 /* time every tile shape on this batch, keep the fastest */ };
+
+/* Plans all jobs as one work list for one persistent kernel launch (longest
+ * tiles first, the last wave split along k), and captures the launch in a
+ * CUDA graph on the context's stream.  The databases, random models and
+ * output buffers must outlive the batch.  No reference counterpart: the
+ * reference runs one dispatchDists per job (src/gpu/dist.cu:408-489). */
+sk_status sk_batch_create(sk_ctx *ctx, const sk_job *jobs, int32_t n_jobs, int32_t flags,
+                          sk_batch **out);
+/* Replays the graph and waits for it. */
+sk_status sk_batch_run(sk_batch *batch);
+/* Replays the graph and returns; sk_ctx_synchronize() waits. */
+sk_status sk_batch_launch(sk_batch *batch);
+sk_status sk_batch_info(const sk_batch *batch, int32_t *tile_config, int32_t *grid,
+                        int64_t *n_items, int64_t *n_pairs);
+sk_status sk_batch_destroy(sk_batch *batch);
+
+/* Autotuner: times every tile shape on one job (out_mode core/accessory into
+ * scratch), records the fastest for the job's (n_kmers, sketchsize64) class in
+ * the context's tuning table and returns it. */
+sk_status sk_autotune(sk_ctx *ctx, const sk_db *ref, const sk_db *query,
+                      const sk_random *random, int32_t repeats, int32_t *best_config);
+/* Writes the context's tuning table ("n_kmers sketchsize64 config_id" lines)
+ * for sk_ctx_load_tuning. */
+sk_status sk_ctx_save_tuning(sk_ctx *ctx, const char *path);
+
 /* ---- sparse / matrix transforms (device kernels over long-form data) ---- */
 
 /* Entries (i, j > i) of the square form of a long-form column with value

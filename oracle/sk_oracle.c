@@ -112,13 +112,19 @@ static int fit_range(const float *J, int K, int s64, int *first) {
  *   xm = sum x / n, ym = sum y / n,
  *   slope = sum (x - xm) y / sum (x - xm)^2, intercept = ym - slope xm.
  * Fewer than 2 points in the range gives (0, 0) (the reference CPU calls
- * exit(1) there, its GPU writes 0, 0). */
+ * exit(1) there, its GPU writes 0, 0); so does a zero J strictly inside the
+ * range (first and last are above tolerance by construction). */
 void sko_fit_slope_f64(const float *J, const int *kmers, int K, int s64, float *core, float *acc) {
   int f;
   const int n = fit_range(J, K, s64, &f);
   *core = 0.0f;
   *acc = 0.0f;
   if (n < 2) return;
+  /* a zero J inside the range has no logarithm; Eigen's float LDLT solve
+   * (the arithmetic of sko_fit_slope_f32) turns the -inf into NaN slopes,
+   * which fit_slope reports as (0, 0) */
+  for (int i = f + 1; i < f + n - 1; i++)
+    if (J[i] <= 0.0f) return;
   double sx = 0.0;
   for (int i = f; i < f + n; i++) sx = sx + (double)kmers[i];
   const double xm = sx / n;

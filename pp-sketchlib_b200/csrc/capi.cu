@@ -252,19 +252,156 @@ sk_status build_job(sk_ctx *ctx, const sk_db *ref, const sk_db *query, const sk_
   return SK_OK;
 }
 
-sk_status launch_job(sk_ctx *ctx, const JobParams &jp, const TileConfig &cfg) {
-  if (jp.n_tiles == 0) return SK_OK;
-  int per_sm = cfg.blocks_per_sm();
-  if (per_sm < 1) return fail(ctx, SK_ECUDA, "Tile configuration %d does not fit the device", cfg.id);
-  int64_t grid = static_cast<int64_t>(per_sm) * ctx->sm_count;
-  if (grid > jp.n_tiles) grid = jp.n_tiles;
-  void *counts = nullptr;
-  sk_status st = scratch(ctx, 0, count_scratch_bytes(cfg, static_cast<int>(grid), jp.n_kmers), &counts);
-  if (st != SK_OK) return st;
-  cudaError_t e = cfg.launch(jp, static_cast<uint16_t *>(counts), ctx->status_dev, ctx->cancel_dev,
-                             static_cast<int>(grid), ctx->stream);
+// Work list for one launch.  Jobs are visited in decreasing cost per tile
+// (K x blocks, longest first) so the dynamic queue ends on the cheapest items.
+// The tiles of the last, partial wave are cut into p parts along k (p chosen to
+// minimise ceil(r p / W) * ceil(K / p), r tail tiles on W resident CTAs); the
+// per-k counts are independent, so the parts need no reduction, only a shared
+// count slot and an arrival counter.
+void plan_items(const std::vector<JobParams> &jobs, int grid, Plan &plan) {
+  plan.items.clear();
+  plan.n_splits = 0;
+  plan.k_slots = 1;
+  std::vector<int> order(jobs.size());
+  for (size_t j = 0; j < jobs.size(); ++j) order[j] = static_cast<int>(j);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    return static_cast<int64_t>(jobs[a].n_kmers) * jobs[a].nb >
+           static_cast<int64_t>(jobs[b].n_kmers) * jobs[b].nb;
+  });
+  for (int j : order) {
+    plan.k_slots = std::max(plan.k_slots, jobs[j].n_kmers);
+    for (int64_t t = 0; t < jobs[j].n_tiles; ++t)
+      plan.items.push_back(WorkItem{t, j, 0, static_cast<int16_t>(jobs[j].n_kmers), -1, 1});
+  }
+  const int64_t T = static_cast<int64_t>(plan.items.size());
+  if (T == 0 || grid <= 0) return;
+  const int64_t r = T % grid == 0 ? 0 : T % grid;
+  if (r == 0) return;
+  // tail tiles: the last r items; k is split by the smallest K among them
+  int kmin = kMaxKmers;
+  for (int64_t i = T - r; i < T; ++i) kmin = std::min<int>(kmin, plan.items[i].k1);
+  int best_p = 1;
+  int64_t best = -1;
+  for (int p = 1; p <= kmin; ++p) {
+    const int64_t rounds = (r * p + grid - 1) / grid;
+    const int64_t cost = rounds * ((kmin + p - 1) / p);
+    if (best < 0 || cost < best) {
+      best = cost;
+      best_p = p;
+    }
+  }
+  if (best_p == 1) return;
+  std::vector<WorkItem> tail(plan.items.end() - r, plan.items.end());
+  plan.items.resize(T - r);
+  int32_t slot = 0;
+  for (const WorkItem &it : tail) {
+    const int K = it.k1;
+    const int parts = std::min(best_p, K);
+    for (int q = 0; q < parts; ++q) {
+      const int k0 = K * q / parts, k1 = K * (q + 1) / parts;
+      plan.items.push_back(WorkItem{it.tile, it.job, static_cast<int16_t>(k0),
+                                    static_cast<int16_t>(k1), slot, parts});
+    }
+    ++slot;
+  }
+  plan.n_splits = slot;
+}
+
+// Device buffers for a plan: job table, work list, control block (queue
+// counter + split arrival counters, zeroed per launch) and count scratch.
+sk_status upload_plan(sk_ctx *ctx, const std::vector<JobParams> &jobs, Plan &plan,
+                      LaunchBuffers &buf, bool owned) {
+  const TileConfig &cfg = *plan.cfg;
+  const size_t jobs_bytes = jobs.size() * sizeof(JobParams);
+  const size_t items_bytes = plan.items.size() * sizeof(WorkItem);
+  const size_t ctrl_bytes = 8 + static_cast<size_t>(plan.n_splits) * cfg.threads * 4;
+  const size_t jobs_off = 0;
+  const size_t items_off = (jobs_bytes + 255) & ~static_cast<size_t>(255);
+  const size_t ctrl_off = (items_off + items_bytes + 255) & ~static_cast<size_t>(255);
+  const size_t meta_bytes = ctrl_off + ctrl_bytes;
+  const size_t slot = count_slot_bytes(cfg, plan.k_slots);
+  const size_t cta_bytes = static_cast<size_t>(plan.grid) * slot;
+  const size_t split_bytes = std::max<size_t>(static_cast<size_t>(plan.n_splits) * slot, 16);
+  void *meta = nullptr, *cta = nullptr, *split = nullptr;
+  if (owned) {
+    cudaError_t e = cudaMalloc(&meta, meta_bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&cta, cta_bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&split, split_bytes);
+    if (e != cudaSuccess) {
+      if (meta) cudaFree(meta);
+      if (cta) cudaFree(cta);
+      if (split) cudaFree(split);
+      return cuda_fail(ctx, e, "batch buffers");
+    }
+  } else {
+    sk_status st = scratch(ctx, kSlotLaunchMeta, meta_bytes, &meta);
+    if (st == SK_OK) st = scratch(ctx, kSlotCounts, cta_bytes, &cta);
+    if (st == SK_OK) st = scratch(ctx, kSlotSplitCounts, split_bytes, &split);
+    if (st != SK_OK) return st;
+  }
+  char *m = static_cast<char *>(meta);
+  cudaError_t e = cudaMemcpyAsync(m + jobs_off, jobs.data(), jobs_bytes, cudaMemcpyHostToDevice,
+                                  ctx->stream);
+  if (e == cudaSuccess && items_bytes)
+    e = cudaMemcpyAsync(m + items_off, plan.items.data(), items_bytes, cudaMemcpyHostToDevice,
+                        ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "work list upload");
+  buf.meta = meta;
+  buf.cta = cta;
+  buf.split = split;
+  buf.ctrl = m + ctrl_off;
+  buf.ctrl_bytes = ctrl_bytes;
+  LaunchParams &lp = buf.lp;
+  lp.jobs = reinterpret_cast<const JobParams *>(m + jobs_off);
+  lp.items = reinterpret_cast<const WorkItem *>(m + items_off);
+  lp.n_items = static_cast<int64_t>(plan.items.size());
+  lp.item_counter = reinterpret_cast<unsigned long long *>(m + ctrl_off);
+  lp.split_done = reinterpret_cast<unsigned int *>(m + ctrl_off + 8);
+  lp.cta_scratch = static_cast<uint16_t *>(cta);
+  lp.split_scratch = static_cast<uint16_t *>(split);
+  lp.k_slots = plan.k_slots;
+  lp.status = ctx->status_dev;
+  lp.cancel = ctx->cancel_dev;
+  return SK_OK;
+}
+
+sk_status enqueue_plan(sk_ctx *ctx, const Plan &plan, const LaunchBuffers &buf) {
+  if (buf.lp.n_items == 0) return SK_OK;
+  cudaError_t e = cudaMemsetAsync(buf.ctrl, 0, buf.ctrl_bytes, ctx->stream);
+  if (e == cudaSuccess) e = plan.cfg->launch(buf.lp, plan.grid, ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "distance kernel launch");
   return SK_OK;
+}
+
+int resident_grid(sk_ctx *ctx, const TileConfig &cfg) {
+  const int per_sm = cfg.blocks_per_sm();
+  return per_sm < 1 ? 0 : per_sm * ctx->sm_count;
+}
+
+sk_status make_plan(sk_ctx *ctx, const std::vector<JobParams> &jobs, const TileConfig &cfg,
+                    Plan &plan) {
+  plan.cfg = &cfg;
+  const int resident = resident_grid(ctx, cfg);
+  if (resident < 1) return fail(ctx, SK_ECUDA, "Tile configuration %d does not fit the device", cfg.id);
+  int64_t tiles = 0;
+  for (const JobParams &j : jobs) tiles += j.n_tiles;
+  plan.grid = resident;
+  plan_items(jobs, resident, plan);
+  if (static_cast<int64_t>(plan.items.size()) < plan.grid)
+    plan.grid = static_cast<int>(std::max<int64_t>(1, plan.items.size()));
+  return SK_OK;
+}
+
+sk_status launch_job(sk_ctx *ctx, const JobParams &jp, const TileConfig &cfg) {
+  if (jp.n_tiles == 0) return SK_OK;
+  std::vector<JobParams> jobs{jp};
+  Plan plan;
+  sk_status st = make_plan(ctx, jobs, cfg, plan);
+  if (st != SK_OK) return st;
+  LaunchBuffers buf;
+  st = upload_plan(ctx, jobs, plan, buf, false);
+  if (st != SK_OK) return st;
+  return enqueue_plan(ctx, plan, buf);
 }
 
 int64_t n_pairs(const sk_db *ref, const sk_db *query) {
@@ -535,7 +672,7 @@ sk_status sk_db_download(sk_ctx *ctx, const sk_db *db, uint64_t *words) {
   const size_t n_words = static_cast<size_t>(db->n) * db->K * db->s64 * kBbits;
   if (n_words == 0) return SK_OK;
   void *tmp = nullptr;
-  sk_status st = scratch(ctx, 0, n_words * 8, &tmp);
+  sk_status st = scratch(ctx, kSlotTemp, n_words * 8, &tmp);
   if (st != SK_OK) return st;
   cudaError_t e = launch_unpack(db->packed, db->n, db->K, db->s64, db->ng, static_cast<uint64_t *>(tmp), ctx->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(words, tmp, n_words * 8, cudaMemcpyDeviceToHost, ctx->stream);
@@ -613,7 +750,7 @@ sk_status sk_dists_dense(sk_ctx *ctx, const sk_db *ref, const sk_db *query, cons
   const size_t bytes = ref ? out_bytes(out_mode, pairs, ref->K) : 0;
   void *d_out = out;
   if (!out_on_device && bytes > 0) {
-    st = scratch(ctx, 1, bytes, &d_out);
+    st = scratch(ctx, kSlotOut, bytes, &d_out);
     if (st != SK_OK) return st;
   }
   st = dense_to_device(ctx, ref, query, random, out_mode, 0, d_out);
@@ -643,10 +780,10 @@ sk_status sk_dists_knn(sk_ctx *ctx, const sk_db *db, const sk_random *random, in
   if (kNN == 0) return SK_OK;
   const int64_t n = db->n, pairs = n_pairs(db, nullptr);
   void *d_vals = nullptr, *d_res = nullptr;
-  st = scratch(ctx, 1, std::max<size_t>(pairs, 1) * 4, &d_vals);
+  st = scratch(ctx, kSlotOut, std::max<size_t>(pairs, 1) * 4, &d_vals);
   if (st != SK_OK) return st;
   const size_t res_elems = static_cast<size_t>(n) * kNN;
-  st = scratch(ctx, 2, res_elems * 12, &d_res);
+  st = scratch(ctx, kSlotResult, res_elems * 12, &d_res);
   if (st != SK_OK) return st;
   int64_t *d_j = static_cast<int64_t *>(d_res);
   float *d_d = reinterpret_cast<float *>(d_j + res_elems);
@@ -677,10 +814,10 @@ sk_status sk_query_knn(sk_ctx *ctx, const sk_db *ref, const sk_db *query, const 
   if (kNN == 0) return SK_OK;
   const int64_t pairs = n_pairs(ref, query);
   void *d_vals = nullptr, *d_res = nullptr;
-  st = scratch(ctx, 1, pairs * 4, &d_vals);
+  st = scratch(ctx, kSlotOut, pairs * 4, &d_vals);
   if (st != SK_OK) return st;
   const size_t res_elems = static_cast<size_t>(query->n) * kNN;
-  st = scratch(ctx, 2, res_elems * 12, &d_res);
+  st = scratch(ctx, kSlotResult, res_elems * 12, &d_res);
   if (st != SK_OK) return st;
   int64_t *d_j = static_cast<int64_t *>(d_res);
   float *d_d = reinterpret_cast<float *>(d_j + res_elems);
@@ -698,7 +835,7 @@ sk_status sk_query_knn(sk_ctx *ctx, const sk_db *ref, const sk_db *query, const 
 static sk_status threshold_device(sk_ctx *ctx, const float *d_vals, int64_t n, int stride, int col,
                                   float cutoff, sk_sparse **out) {
   void *d_cnt = nullptr;
-  sk_status st = scratch(ctx, 2, static_cast<size_t>(n + 1) * 16, &d_cnt);
+  sk_status st = scratch(ctx, kSlotResult, static_cast<size_t>(n + 1) * 16, &d_cnt);
   if (st != SK_OK) return st;
   int64_t *counts = static_cast<int64_t *>(d_cnt);
   int64_t *offsets = counts + (n + 1);
@@ -708,7 +845,7 @@ static sk_status threshold_device(sk_ctx *ctx, const float *d_vals, int64_t n, i
   if (e == cudaSuccess) e = exclusive_scan_i64(counts, offsets, n + 1, nullptr, &tmp_bytes, ctx->stream);
   void *tmp = nullptr;
   if (e == cudaSuccess) {
-    st = scratch(ctx, 3, std::max<size_t>(tmp_bytes, 16), &tmp);
+    st = scratch(ctx, kSlotTemp, std::max<size_t>(tmp_bytes, 16), &tmp);
     if (st != SK_OK) return st;
     e = exclusive_scan_i64(counts, offsets, n + 1, tmp, &tmp_bytes, ctx->stream);
   }
@@ -722,7 +859,7 @@ static sk_status threshold_device(sk_ctx *ctx, const float *d_vals, int64_t n, i
   sp->d.resize(total);
   if (total > 0) {
     void *d_res = nullptr;
-    st = scratch(ctx, 3, static_cast<size_t>(total) * 20, &d_res);
+    st = scratch(ctx, kSlotTemp, static_cast<size_t>(total) * 20, &d_res);
     if (st != SK_OK) { delete sp; return st; }
     int64_t *di = static_cast<int64_t *>(d_res);
     int64_t *dj = di + total;
@@ -751,7 +888,7 @@ sk_status sk_sparse_threshold(sk_ctx *ctx, const float *long_form, int64_t n_sam
     return fail(ctx, SK_EINVAL, "bad long-form shape");
   const int64_t pairs = n_samples * (n_samples - 1) / 2;
   void *d_vals = nullptr;
-  st = scratch(ctx, 1, std::max<int64_t>(pairs, 1) * n_cols * 4, &d_vals);
+  st = scratch(ctx, kSlotOut, std::max<int64_t>(pairs, 1) * n_cols * 4, &d_vals);
   if (st != SK_OK) return st;
   if (pairs > 0) {
     cudaError_t e = cudaMemcpyAsync(d_vals, long_form, pairs * n_cols * 4, cudaMemcpyHostToDevice, ctx->stream);
@@ -772,7 +909,7 @@ sk_status sk_dists_threshold(sk_ctx *ctx, const sk_db *db, const sk_random *rand
   if (dist_col != 0 && dist_col != 1) return fail(ctx, SK_EINVAL, "dist_col out of range");
   const int64_t pairs = n_pairs(db, nullptr);
   void *d_vals = nullptr;
-  st = scratch(ctx, 1, std::max<int64_t>(pairs, 1) * 4, &d_vals);
+  st = scratch(ctx, kSlotOut, std::max<int64_t>(pairs, 1) * 4, &d_vals);
   if (st != SK_OK) return st;
   if (pairs > 0) {
     st = dense_to_device(ctx, db, nullptr, random, kOutColumn, dist_col, d_vals);
@@ -811,7 +948,7 @@ sk_status sk_long_to_square(sk_ctx *ctx, const float *rr, int64_t n_rr, const fl
   const int64_t n_qr = n_rr * n_qq;
   void *d = nullptr;
   const size_t bytes = (n_rr_long + n_qr + n_qq_long + n * n) * 4;
-  st = scratch(ctx, 1, std::max<size_t>(bytes, 16), &d);
+  st = scratch(ctx, kSlotOut, std::max<size_t>(bytes, 16), &d);
   if (st != SK_OK) return st;
   float *drr = static_cast<float *>(d), *dqr = drr + n_rr_long, *dqq = dqr + n_qr, *dsq = dqq + n_qq_long;
   cudaError_t e = cudaSuccess;
@@ -832,7 +969,7 @@ sk_status sk_square_to_long(sk_ctx *ctx, const float *square, int64_t n, float *
   if (n < 2) return SK_OK;
   const int64_t n_long = n * (n - 1) / 2;
   void *d = nullptr;
-  st = scratch(ctx, 1, (n * n + n_long) * 4, &d);
+  st = scratch(ctx, kSlotOut, (n * n + n_long) * 4, &d);
   if (st != SK_OK) return st;
   float *dsq = static_cast<float *>(d), *dl = dsq + n * n;
   cudaError_t e = cudaMemcpyAsync(dsq, square, n * n * 4, cudaMemcpyHostToDevice, ctx->stream);

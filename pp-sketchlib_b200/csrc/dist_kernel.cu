@@ -1,16 +1,20 @@
 // dist_kernel.cu -- the fused bit-sliced MinHash distance kernel for sm_100a.
 //
-// One persistent CTA per SM walks its share of (row tile x column tile) work
-// items.  For every k-mer length and every 32-bin block it stages the 14 bit
-// planes of its row and column samples into shared memory with bulk copies
-// (TMA engine, one copy per 64-sample stripe, mbarrier completion), and each
-// thread intersects a TQ x TR register block of pairs:
+// A persistent kernel: every CTA pulls work items (job, tile, k range) from a
+// device queue, so one launch can serve one all-vs-all, one query batch or a
+// whole batch of unrelated databases of different sizes, k sets and sketch
+// widths.  Thread 0 is the producer: for every 2-block step of its current
+// item it stages the 14 bit planes of the tile's row and column samples into
+// shared memory with bulk copies (TMA engine, one copy per 64-sample stripe,
+// mbarrier completion) and records the step in a per-stage descriptor.  All
+// warps consume: each thread intersects a TQ x TR register block of pairs
 //     acc = AND over planes of ~(row_word ^ col_word)   (one LOP3 per plane)
-//     count += popc(acc)
-// which is calc_intersize (src/dist/dist.cpp:50-78) for 32 bins at a time.
-// Per-k counts of the tile go to shared memory as uint16; once all k are done
-// the CTA turns each pair's counts into random-corrected Jaccards and the
-// log-linear core/accessory fit and writes the long-form row directly.
+//     count += popc(acc)                                 (POPC + IMAD)
+// which is calc_intersize (src/dist/dist.cpp:50-78) for 32 bins at a time,
+// releases the stage with a per-stage named barrier (only warp 0, which
+// refills, waits on it), parks its per-k counts in L2-resident scratch, and
+// after an item's last k turns its own pairs into random-corrected Jaccards
+// and the log-linear core/accessory fit, written straight to the long form.
 //
 // Replaces calculate_dists (src/gpu/dist.cu:164-317): one thread per pair with
 // strided 8-byte global loads there; register-blocked tiles over staged
@@ -28,6 +32,18 @@ namespace sk {
 constexpr int kBlocksPerStage = 2;   // 32-bin blocks per pipeline stage
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s bounded waits
 
+// Per-stage step descriptor written by the producer before it arms the stage.
+struct StepMeta {
+  int32_t job;
+  int32_t ti, tj;     // tile coordinates within the job
+  int32_t kidx;       // k-mer index of this step
+  int32_t flags;      // kStepEnd / kStepLastOfK / kStepLastOfItem
+  int32_t split;      // split slot of the item, -1 for whole tiles
+  int32_t nparts;
+  int32_t pad;
+};
+constexpr int32_t kStepEnd = 1, kStepLastOfK = 2, kStepLastOfItem = 4;
+
 template <int QT, int RT, int TQ, int TR, int STAGES>
 struct TileShape {
   static constexpr int kThreads = (QT / TQ) * (RT / TR);
@@ -43,16 +59,39 @@ struct TileShape {
   static_assert(TQ % 4 == 0 && TR % 4 == 0, "128-bit shared loads");
   static_assert(kPairsPerThread % 8 == 0, "counts are stored as 16-byte groups");
   static_assert(QT % RT == 0, "triangular map needs tile_rows multiple of tile_cols");
+  static_assert(STAGES >= 2 && STAGES <= 4, "one named barrier (ids 1..4) per stage");
+  static_assert(kThreads % 32 == 0, "whole warps");
 };
 
-// Per-k counts of a thread's TQ x TR pairs are parked in `scratch` (this CTA's
-// slot: [K][threads][TQ*TR] uint16, written and read back by the same thread,
-// so no barrier is needed; 38 MB for 296 CTAs at K = 8, resident in L2).  The
-// thread then finishes its own pairs, so a tile needs no CTA-wide epilogue.
+// Per-stage named barriers 1..4 with literal ids (the hardware reserves only
+// the ids a kernel names).
+template <int NT>
+__device__ __forceinline__ void stage_sync(int s) {
+  switch (s) {
+    case 0: asm volatile("bar.sync 1, %0;" ::"n"(NT) : "memory"); break;
+    case 1: asm volatile("bar.sync 2, %0;" ::"n"(NT) : "memory"); break;
+    case 2: asm volatile("bar.sync 3, %0;" ::"n"(NT) : "memory"); break;
+    default: asm volatile("bar.sync 4, %0;" ::"n"(NT) : "memory"); break;
+  }
+}
+template <int NT>
+__device__ __forceinline__ void stage_arrive(int s) {
+  switch (s) {
+    case 0: asm volatile("bar.arrive 1, %0;" ::"n"(NT) : "memory"); break;
+    case 1: asm volatile("bar.arrive 2, %0;" ::"n"(NT) : "memory"); break;
+    case 2: asm volatile("bar.arrive 3, %0;" ::"n"(NT) : "memory"); break;
+    default: asm volatile("bar.arrive 4, %0;" ::"n"(NT) : "memory"); break;
+  }
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Count scratch layout (per CTA slot, and per split slot): [k][threads][pairs
+// per thread] uint16; a thread writes and reads back only its own entries.
 template <int QT, int RT, int TQ, int TR, int STAGES, int MINB>
 __global__ void __launch_bounds__((QT / TQ) * (RT / TR), MINB)
-    dist_tiles_kernel(const JobParams p, uint16_t *__restrict__ scratch, DevStatus *status,
-                      const volatile int *cancel) {
+    dist_items_kernel(const LaunchParams lp) {
   using S = TileShape<QT, RT, TQ, TR, STAGES>;
   constexpr int NT = S::kThreads;
   constexpr int PT = S::kPairsPerThread;
@@ -62,21 +101,18 @@ __global__ void __launch_bounds__((QT / TQ) * (RT / TR), MINB)
   uint32_t *sq = reinterpret_cast<uint32_t *>(smem);
   uint32_t *sr = sq + STAGES * S::kStageQWords;
   __shared__ __align__(8) uint64_t full_bar[STAGES];
+  __shared__ StepMeta meta[STAGES];
   __shared__ int s_abort;
 
   const int tid = threadIdx.x;
+  const int warp = tid >> 5;
   const int tq = tid / TCOLS;
   const int tr = tid % TCOLS;
   const int row0 = tq * TQ;   // first tile row of this thread
   const int col0 = tr * TR;   // first tile column of this thread
-
-  if (blockIdx.x >= p.n_tiles) return;
-  const int64_t my_tiles = (p.n_tiles - blockIdx.x + gridDim.x - 1) / gridDim.x;
-  const int64_t steps_per_k = p.nb / kBlocksPerStage;
-  const int64_t spt = steps_per_k * p.n_kmers;
-  const int64_t total = my_tiles * spt;
-  uint16_t *my_counts = scratch + (static_cast<int64_t>(blockIdx.x) * p.n_kmers * NT + tid) * PT;
-  const int64_t k_stride = static_cast<int64_t>(NT) * PT;   // uint16 between k slots
+  const int64_t slot_k_stride = static_cast<int64_t>(NT) * PT;      // uint16 between k slots
+  const int64_t slot_size = slot_k_stride * lp.k_slots;
+  uint16_t *my_counts = lp.cta_scratch + blockIdx.x * slot_size + static_cast<int64_t>(tid) * PT;
 
   if (tid == 0) {
     for (int s = 0; s < STAGES; ++s) mbar_init(&full_bar[s], 1);
@@ -85,94 +121,166 @@ __global__ void __launch_bounds__((QT / TQ) * (RT / TR), MINB)
   }
   __syncthreads();
 
-  // Producer (thread 0): stage step u into buffer u % STAGES.
-  int64_t next_issue = 0;
-  auto issue = [&](int64_t u) {
-    const int64_t tile_iter = u / spt;
-    const int64_t local = u - tile_iter * spt;
-    const int64_t kidx = local / steps_per_k;
-    const int64_t b0 = (local - kidx * steps_per_k) * kBlocksPerStage;
-    int32_t ti, tj;
-    tile_coords(p, blockIdx.x + tile_iter * gridDim.x, ti, tj);
+  // ---------------------------------------------------------------- producer
+  // (thread 0 only)  Its state lives in shared memory so the consumer loop
+  // keeps its registers for the pair block.
+  struct Producer {
+    const uint32_t *rows, *cols;
+    int32_t done, have, job, ti, tj, k, k1, split, nparts, b0, nb, ngr, ngc;
+  };
+  __shared__ Producer ps;
+  if (tid == 0) {
+    ps.done = 0;
+    ps.have = 0;
+  }
+
+  auto produce = [&](int64_t u) {
+    if (ps.done) return;
     const int s = static_cast<int>(u % STAGES);
+    if (s_abort != 0) {   // a consumer timed out: end the stream now
+      meta[s].flags = kStepEnd;
+      mbar_arrive(&full_bar[s]);
+      ps.done = 1;
+      return;
+    }
+    if (!ps.have) {
+      const bool cancelled = lp.cancel != nullptr && *lp.cancel != 0;
+      if (cancelled) atomicOr(&lp.status->error, 2u);
+      const unsigned long long idx = cancelled ? ~0ull : atomicAdd(lp.item_counter, 1ull);
+      if (idx >= static_cast<unsigned long long>(lp.n_items)) {
+        meta[s].flags = kStepEnd;
+        mbar_arrive(&full_bar[s]);   // completes the phase without data
+        ps.done = 1;
+        return;
+      }
+      const WorkItem it = lp.items[idx];
+      const JobParams &jp = lp.jobs[it.job];
+      ps.job = it.job;
+      int32_t ti, tj;
+      tile_coords(jp, it.tile, ti, tj);
+      ps.ti = ti;
+      ps.tj = tj;
+      ps.k = it.k0;
+      ps.k1 = it.k1;
+      ps.split = it.split;
+      ps.nparts = it.nparts;
+      ps.b0 = 0;
+      ps.nb = jp.nb;
+      ps.rows = jp.row_words;
+      ps.cols = jp.col_words;
+      ps.ngr = jp.ng_rows;
+      ps.ngc = jp.ng_cols;
+      ps.have = 1;
+      atomicAdd(&lp.status->tiles_done, 1ull);
+    }
+    const bool last_of_k = ps.b0 + kBlocksPerStage >= ps.nb;
+    const bool last_of_item = last_of_k && ps.k + 1 >= ps.k1;
+    StepMeta &m = meta[s];
+    m.job = ps.job;
+    m.ti = ps.ti;
+    m.tj = ps.tj;
+    m.kidx = ps.k;
+    m.flags = (last_of_k ? kStepLastOfK : 0) | (last_of_item ? kStepLastOfItem : 0);
+    m.split = ps.split;
+    m.nparts = ps.nparts;
     mbar_arrive_expect_tx(&full_bar[s], S::kStageBytes);
 #pragma unroll
     for (int b = 0; b < kBlocksPerStage; ++b) {
-      const int64_t blk = kidx * p.nb + b0 + b;
+      const int64_t blk = static_cast<int64_t>(ps.k) * ps.nb + ps.b0 + b;
       const uint32_t *src_q =
-          p.row_words + ((blk * p.ng_rows) + static_cast<int64_t>(ti) * S::kQG) * kStripeWords;
+          ps.rows + ((blk * ps.ngr) + static_cast<int64_t>(ps.ti) * S::kQG) * kStripeWords;
       const uint32_t *src_r =
-          p.col_words + ((blk * p.ng_cols) + static_cast<int64_t>(tj) * S::kRG) * kStripeWords;
+          ps.cols + ((blk * ps.ngc) + static_cast<int64_t>(ps.tj) * S::kRG) * kStripeWords;
       bulk_g2s(sq + (s * kBlocksPerStage + b) * S::kQG * kStripeWords, src_q,
                S::kQG * kStripeBytes, &full_bar[s]);
       bulk_g2s(sr + (s * kBlocksPerStage + b) * S::kRG * kStripeWords, src_r,
                S::kRG * kStripeBytes, &full_bar[s]);
     }
+    ps.b0 += kBlocksPerStage;
+    if (last_of_k) {
+      ps.b0 = 0;
+      ++ps.k;
+      if (last_of_item) ps.have = 0;
+    }
   };
+
   if (tid == 0) {
-    while (next_issue < total && next_issue < STAGES) issue(next_issue++);
+    for (int64_t u = 0; u < STAGES; ++u) produce(u);
   }
 
-  // 1 at run time: makes the count accumulation a multiply-add, which runs on
-  // the otherwise idle FMA pipe instead of taking ALU slots from the LOP3s.
-  const uint32_t one = p.one;
+  // ---------------------------------------------------------------- consumers
+  const uint32_t one = lp.jobs[0].one;   // 1 at run time (count multiply-adds on the FMA pipe)
   uint32_t cnt[TQ][TR];
 #pragma unroll
   for (int i = 0; i < TQ; ++i)
 #pragma unroll
     for (int j = 0; j < TR; ++j) cnt[i][j] = 0;
 
-  int64_t t = 0;
-  for (; t < total; ++t) {
+  for (int64_t t = 0;; ++t) {
     const int s = static_cast<int>(t % STAGES);
     const uint32_t parity = static_cast<uint32_t>((t / STAGES) & 1);
-    const bool ok = mbar_wait_bounded(&full_bar[s], parity, kWaitLimitNs);
-    if (!ok) {
-      s_abort = 1;
-      atomicOr(&status->error, 1u);
-      status->where = 1;
+    StepMeta m;
+    if (mbar_wait_bounded(&full_bar[s], parity, kWaitLimitNs)) {
+      m = meta[s];
+      if (m.flags & kStepEnd) break;
     } else {
+      // a stage never landed: record it and keep to the protocol without
+      // computing; the producer ends the stream at its next step, so every
+      // warp still arrives at every stage barrier and the loop ends
+      s_abort = 1;
+      atomicOr(&lp.status->error, 1u);
+      lp.status->where = 1;
+      m.flags = 0;
+      m.split = -1;
+    }
+
 #pragma unroll
-      for (int b = 0; b < kBlocksPerStage; ++b) {
-        const uint32_t *qb = sq + (s * kBlocksPerStage + b) * S::kQG * kStripeWords +
-                             (row0 / kGranule) * kStripeWords + (row0 % kGranule);
-        const uint32_t *rb = sr + (s * kBlocksPerStage + b) * S::kRG * kStripeWords +
-                             (col0 / kGranule) * kStripeWords + (col0 % kGranule);
-        uint32_t acc[TQ][TR];
+    for (int b = 0; b < kBlocksPerStage; ++b) {
+      const uint32_t *qb = sq + (s * kBlocksPerStage + b) * S::kQG * kStripeWords +
+                           (row0 / kGranule) * kStripeWords + (row0 % kGranule);
+      const uint32_t *rb = sr + (s * kBlocksPerStage + b) * S::kRG * kStripeWords +
+                           (col0 / kGranule) * kStripeWords + (col0 % kGranule);
+      uint32_t acc[TQ][TR];
 #pragma unroll
-        for (int pl = 0; pl < kBbits; ++pl) {
-          uint32_t qv[TQ], rv[TR];
+      for (int pl = 0; pl < kBbits; ++pl) {
+        uint32_t qv[TQ], rv[TR];
 #pragma unroll
-          for (int i = 0; i < TQ; i += 4) {
-            const uint4 v = *reinterpret_cast<const uint4 *>(qb + pl * kGranule + i);
-            qv[i] = v.x; qv[i + 1] = v.y; qv[i + 2] = v.z; qv[i + 3] = v.w;
-          }
+        for (int i = 0; i < TQ; i += 4) {
+          const uint4 v = *reinterpret_cast<const uint4 *>(qb + pl * kGranule + i);
+          qv[i] = v.x; qv[i + 1] = v.y; qv[i + 2] = v.z; qv[i + 3] = v.w;
+        }
 #pragma unroll
-          for (int j = 0; j < TR; j += 4) {
-            const uint4 v = *reinterpret_cast<const uint4 *>(rb + pl * kGranule + j);
-            rv[j] = v.x; rv[j + 1] = v.y; rv[j + 2] = v.z; rv[j + 3] = v.w;
-          }
-#pragma unroll
-          for (int i = 0; i < TQ; ++i)
-#pragma unroll
-            for (int j = 0; j < TR; ++j)
-              acc[i][j] = pl == 0 ? lop_eq(qv[i], rv[j]) : lop_eq_and(acc[i][j], qv[i], rv[j]);
+        for (int j = 0; j < TR; j += 4) {
+          const uint4 v = *reinterpret_cast<const uint4 *>(rb + pl * kGranule + j);
+          rv[j] = v.x; rv[j + 1] = v.y; rv[j + 2] = v.z; rv[j + 3] = v.w;
         }
 #pragma unroll
         for (int i = 0; i < TQ; ++i)
 #pragma unroll
-          for (int j = 0; j < TR; ++j) cnt[i][j] = mad_u32(__popc(acc[i][j]), one, cnt[i][j]);
+          for (int j = 0; j < TR; ++j)
+            acc[i][j] = pl == 0 ? lop_eq(qv[i], rv[j]) : lop_eq_and(acc[i][j], qv[i], rv[j]);
       }
+#pragma unroll
+      for (int i = 0; i < TQ; ++i)
+#pragma unroll
+        for (int j = 0; j < TR; ++j) cnt[i][j] = mad_u32(__popc(acc[i][j]), one, cnt[i][j]);
     }
-    __syncthreads();  // stage s fully read by every warp
-    if (s_abort) break;
-    if (tid == 0 && next_issue < total) issue(next_issue++);
 
-    const int64_t local = t % spt;
-    const int64_t kidx = local / steps_per_k;
-    if (local - kidx * steps_per_k == steps_per_k - 1) {
-      // all blocks of k-mer index kidx done: park this thread's counts
-      uint4 *dst = reinterpret_cast<uint4 *>(my_counts + kidx * k_stride);
+    // release the stage: warp 0 (which holds the producer) waits for every
+    // warp, the others only arrive and run ahead into the stages already armed
+    if (warp == 0) {
+      stage_sync<NT>(s);
+      if (tid == 0) produce(t + STAGES);
+    } else {
+      stage_arrive<NT>(s);
+    }
+
+    if (m.flags & kStepLastOfK) {
+      // counts of k-mer index m.kidx done: park them (own slot or split slot)
+      uint16_t *base = m.split >= 0
+                           ? lp.split_scratch + m.split * slot_size + static_cast<int64_t>(tid) * PT
+                           : my_counts;
+      uint4 *dst = reinterpret_cast<uint4 *>(base + m.kidx * slot_k_stride);
 #pragma unroll
       for (int w = 0; w < PT / 8; ++w) {
         uint32_t packed[4];
@@ -187,36 +295,44 @@ __global__ void __launch_bounds__((QT / TQ) * (RT / TR), MINB)
       for (int i = 0; i < TQ; ++i)
 #pragma unroll
         for (int j = 0; j < TR; ++j) cnt[i][j] = 0;
+    }
 
-      if (kidx == p.n_kmers - 1) {
-        // tile complete: this thread finishes its own TQ x TR pairs
-        int32_t ti, tj;
-        tile_coords(p, blockIdx.x + (t / spt) * gridDim.x, ti, tj);
-        const int64_t gi0 = static_cast<int64_t>(ti) * QT + row0;
-        const int64_t gj0 = static_cast<int64_t>(tj) * RT + col0;
+    if (m.flags & kStepLastOfItem) {
+      const JobParams &jp = lp.jobs[m.job];
+      bool finish = true;
+      if (m.split >= 0) {
+        // Split tile: every thread owns its pairs' counts, so each thread
+        // counts its own arrivals; the thread of the last part to arrive
+        // gathers all k from the split slot and finishes those pairs.  No
+        // CTA-wide barrier, so a stage that timed out cannot strand a warp.
+        __threadfence();
+        const unsigned int prev =
+            atomicAdd(&lp.split_done[static_cast<int64_t>(m.split) * NT + tid], 1u);
+        finish = prev + 1 == static_cast<unsigned int>(m.nparts);
+        if (finish) {
+          __threadfence();
+          const uint4 *src = reinterpret_cast<const uint4 *>(
+              lp.split_scratch + m.split * slot_size + static_cast<int64_t>(tid) * PT);
+          for (int k = 0; k < jp.n_kmers; ++k)
+#pragma unroll
+            for (int w = 0; w < PT / 8; ++w)
+              reinterpret_cast<uint4 *>(my_counts + k * slot_k_stride)[w] =
+                  __ldcg(src + k * (slot_k_stride / 8) + w);
+        }
+      }
+      if (finish) {
+        const int64_t gi0 = static_cast<int64_t>(m.ti) * QT + row0;
+        const int64_t gj0 = static_cast<int64_t>(m.tj) * RT + col0;
 #pragma unroll 1
         for (int q = 0; q < PT; ++q) {
           const int64_t gi = gi0 + q / TR;
           const int64_t gj = gj0 + q % TR;
-          const bool valid = p.self ? (gj > gi && gj < p.n_cols) : (gi < p.n_rows && gj < p.n_cols);
-          if (valid) finish_pair_any(p, gi, gj, my_counts + q, static_cast<int>(k_stride));
-        }
-        if (tid == 0) {
-          atomicAdd(&status->tiles_done, 1ull);
-          if (cancel != nullptr && *cancel != 0) {
-            s_abort = 1;   // seen by every thread after the next step's barrier
-            atomicOr(&status->error, 2u);
-          }
+          const bool valid =
+              jp.self ? (gj > gi && gj < jp.n_cols) : (gi < jp.n_rows && gj < jp.n_cols);
+          if (valid) finish_pair_any(jp, gi, gj, my_counts + q, static_cast<int>(slot_k_stride));
         }
       }
     }
-  }
-
-  if (tid == 0 && t < total) {
-    // unwinding early: let the copies already in flight land before exit
-    for (int64_t u = t; u < next_issue; ++u)
-      (void)mbar_wait_bounded(&full_bar[u % STAGES], static_cast<uint32_t>((u / STAGES) & 1),
-                              kWaitLimitNs);
   }
 }
 
@@ -224,32 +340,34 @@ __global__ void __launch_bounds__((QT / TQ) * (RT / TR), MINB)
 
 namespace {
 
+// Raises the instance's dynamic shared memory limit once (before any launch,
+// so never inside a stream capture).
 template <int QT, int RT, int TQ, int TR, int STAGES, int MINB>
-cudaError_t launch_cfg(const JobParams &p, uint16_t *scratch, DevStatus *status,
-                       const volatile int *cancel, int grid, cudaStream_t stream) {
+cudaError_t ensure_smem_attr() {
   using S = TileShape<QT, RT, TQ, TR, STAGES>;
-  auto kern = dist_tiles_kernel<QT, RT, TQ, TR, STAGES, MINB>;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         S::kSmemBytes);
-    if (e != cudaSuccess) return e;
-    attr_set = true;
-  }
-  kern<<<grid, S::kThreads, S::kSmemBytes, stream>>>(p, scratch, status, cancel);
+  static cudaError_t status = cudaFuncSetAttribute(
+      dist_items_kernel<QT, RT, TQ, TR, STAGES, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      S::kSmemBytes);
+  return status;
+}
+
+template <int QT, int RT, int TQ, int TR, int STAGES, int MINB>
+cudaError_t launch_cfg(const LaunchParams &lp, int grid, cudaStream_t stream) {
+  using S = TileShape<QT, RT, TQ, TR, STAGES>;
+  cudaError_t e = ensure_smem_attr<QT, RT, TQ, TR, STAGES, MINB>();
+  if (e != cudaSuccess) return e;
+  dist_items_kernel<QT, RT, TQ, TR, STAGES, MINB><<<grid, S::kThreads, S::kSmemBytes, stream>>>(lp);
   return cudaGetLastError();
 }
 
 template <int QT, int RT, int TQ, int TR, int STAGES, int MINB>
 int occupancy_cfg() {
   using S = TileShape<QT, RT, TQ, TR, STAGES>;
-  auto kern = dist_tiles_kernel<QT, RT, TQ, TR, STAGES, MINB>;
-  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, S::kSmemBytes) !=
-      cudaSuccess)
-    return 0;
+  if (ensure_smem_attr<QT, RT, TQ, TR, STAGES, MINB>() != cudaSuccess) return 0;
   int blocks = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kern, S::kThreads, S::kSmemBytes) !=
-      cudaSuccess)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &blocks, dist_items_kernel<QT, RT, TQ, TR, STAGES, MINB>, S::kThreads,
+          S::kSmemBytes) != cudaSuccess)
     return 0;
   return blocks;
 }
@@ -270,12 +388,12 @@ constexpr TileConfig make_cfg(int id) {
 }
 
 const TileConfig kConfigs[] = {
-    make_cfg<128, 64, 8, 4, 3, 2>(1),   // default: 2 CTAs x 8 warps per SM
-    make_cfg<64, 64, 4, 4, 3, 2>(2),    // small tiles, 16 pairs per thread
-    make_cfg<128, 128, 8, 8, 3, 1>(3),  // large tiles, 64 pairs per thread, 1 CTA per SM
-    make_cfg<64, 64, 8, 4, 4, 3>(4),    // 128 threads, 3 CTAs per SM
-    make_cfg<128, 64, 4, 8, 3, 2>(5),   // transposed thread block
-    make_cfg<128, 128, 8, 4, 3, 1>(6),  // 512 threads, 16 warps in one CTA
+    make_cfg<128, 128, 8, 4, 4, 1>(1),  // default: 512 threads, 16 warps, one CTA per SM
+    make_cfg<128, 64, 8, 4, 4, 2>(2),   // 256 threads, two CTAs per SM
+    make_cfg<64, 64, 4, 4, 4, 2>(3),    // small tiles, 16 pairs per thread
+    make_cfg<128, 128, 8, 8, 4, 1>(4),  // 256 threads, 64 pairs per thread
+    make_cfg<128, 64, 4, 8, 4, 2>(5),   // transposed thread block
+    make_cfg<64, 64, 8, 4, 4, 3>(6),    // 128 threads, three CTAs per SM
 };
 
 }  // namespace

@@ -379,6 +379,21 @@ py::dict load_sketch_db(const std::string &db_name, std::vector<std::string> nam
   return d;
 }
 
+py::dict load_random_model(const std::string &db_name) {
+  skhost::RandomModel r = skhost::get_random(db_name, true);
+  py::dict d;
+  d["mode"] = r.mode;
+  d["use_rc"] = r.use_rc;
+  d["k_min"] = r.min_k;
+  d["k_max"] = r.max_k;
+  d["n_clusters"] = r.n_clusters;
+  d["cluster_table"] = r.cluster_table;
+  d["matches"] = r.matches;
+  d["centroids"] = r.centroids;
+  d["min_supported_k"] = r.min_supported_k();
+  return d;
+}
+
 }  // namespace
 
 PYBIND11_MODULE(_pp_sketchlib, m) {
@@ -421,6 +436,8 @@ PYBIND11_MODULE(_pp_sketchlib, m) {
   // not in the reference module: reads a database's sketches (tests, tools)
   m.def("_load_sketch_db", &load_sketch_db, py::arg("db_name"),
         py::arg("names") = std::vector<std::string>{}, py::arg("klist"));
+
+  m.def("_load_random", &load_random_model, py::arg("db_name"));
 
   m.attr("version") = "2.1.5+b200";
   m.attr("sketchVersion") = "b200";

@@ -51,7 +51,7 @@ sk_status time_probe(sk_ctx *ctx, Kern kern, int iters, double *ops_per_s) {
   const int block = 256;
   const int grid = ctx->sm_count * 8;
   void *sink = nullptr;
-  sk_status st = scratch(ctx, 3, static_cast<size_t>(grid) * block * 4, &sink);
+  sk_status st = scratch(ctx, kSlotTemp, static_cast<size_t>(grid) * block * 4, &sink);
   if (st != SK_OK) return st;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);

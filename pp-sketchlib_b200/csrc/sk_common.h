@@ -70,6 +70,32 @@ struct JobParams {
   uint32_t one;                // 1 (a run-time operand for the count multiply-adds)
 };
 
+// One unit of work of the persistent distance kernel: k-mer indices
+// [k0, k1) of one tile of one job.  A tile whose k range is cut into several
+// items (the last wave's tiles, to even out the tail) shares a split slot; the
+// item that finishes last runs the tile's epilogue.
+struct WorkItem {
+  int64_t tile;     // tile index within the job
+  int32_t job;
+  int16_t k0, k1;
+  int32_t split;    // split slot, -1 for a whole tile
+  int32_t nparts;   // items sharing the split slot
+};
+
+// Everything one launch needs: the job table, the work list and the scratch.
+struct LaunchParams {
+  const JobParams *jobs;
+  const WorkItem *items;
+  int64_t n_items;
+  unsigned long long *item_counter;   // zeroed before each launch
+  unsigned int *split_done;           // [n_splits][threads], zeroed before each launch
+  uint16_t *cta_scratch;              // [grid][k_slots][threads][pairs per thread]
+  uint16_t *split_scratch;            // [n_splits][k_slots][threads][pairs per thread]
+  int32_t k_slots;                    // largest K over the jobs
+  DevStatus *status;
+  const volatile int *cancel;
+};
+
 // splitmix64 finaliser: the counter-based hash of the synthetic generator.
 // Identical on host and device (pure integer arithmetic).
 #if defined(__CUDACC__)

@@ -155,7 +155,8 @@ __device__ __forceinline__ float corrected_jaccard(uint32_t count, double union_
 // k-range from the first to the last J above tolerance (fit_slope,
 // src/dist/linear_regression.cpp:16-60).  Fewer than 2 points in the range
 // gives (0, 0), the reference GPU's result (src/gpu/dist.cu:95-97); the
-// reference CPU exits the process there.  Least squares in double:
+// reference CPU exits the process there; a zero J strictly inside the range
+// gives (0, 0) too.  Least squares in double:
 //   xm = sum x / n, ym = sum y / n,
 //   slope = sum (x - xm) y / sum (x - xm)^2, intercept = ym - slope xm,
 // without fused multiply-adds, in the same operation order as the oracle.
@@ -171,6 +172,13 @@ __device__ __forceinline__ float2 fit_core_acc(const float (&jf)[KMAX], const Jo
   }
   float2 res = make_float2(0.0f, 0.0f);
   if (first < 0 || last - first + 1 < 2) return res;
+  // A zero Jaccard inside the range has no logarithm: the reference's float
+  // solve turns it into NaN slopes, i.e. (0, 0).
+  bool zero_inside = false;
+#pragma unroll
+  for (int k = 0; k < KMAX; ++k)
+    if (k > first && k < last && jf[k] <= 0.0f) zero_inside = true;
+  if (zero_inside) return res;
   const double n = static_cast<double>(last - first + 1);
   double sx = 0.0;
 #pragma unroll

@@ -18,23 +18,17 @@ struct TileConfig {
   int stages;                    // pipeline depth
   int threads;
   int smem_bytes;
-  cudaError_t (*launch)(const JobParams &, uint16_t *scratch, DevStatus *,
-                        const volatile int *, int grid, cudaStream_t);
+  cudaError_t (*launch)(const LaunchParams &, int grid, cudaStream_t);
   int (*blocks_per_sm)();        // resident CTAs per SM at this shape's shared memory
 };
 
 int tile_config_count();
 const TileConfig *tile_config(int id);
-// Bytes of per-CTA count scratch a launch of `cfg` with `grid` CTAs needs.
-inline size_t count_scratch_bytes(const TileConfig &cfg, int grid, int n_kmers) {
-  return static_cast<size_t>(grid) * n_kmers * cfg.tile_rows * cfg.tile_cols * 2;
+// Bytes of count scratch per slot (one per CTA, one per split tile).
+inline size_t count_slot_bytes(const TileConfig &cfg, int k_slots) {
+  return static_cast<size_t>(k_slots) * cfg.tile_rows * cfg.tile_cols * 2;
 }
 
-// Batched persistent launch over many jobs (batch_kernel.cu).
-struct BatchJob;  // device-side job descriptor
-cudaError_t launch_batch(const TileConfig &cfg, const void *d_jobs, int n_jobs,
-                         const int64_t *d_tile_prefix, int64_t total_tiles, DevStatus *status,
-                         const volatile int *cancel, int grid, cudaStream_t stream);
 
 // aux_kernels.cu
 cudaError_t launch_pack(const uint64_t *words, int64_t n, int32_t n_kmers, int32_t s64,

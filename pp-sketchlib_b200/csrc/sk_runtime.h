@@ -19,6 +19,17 @@ struct Scratch {
   size_t bytes = 0;
 };
 
+// Context scratch slots (each a growable device buffer).
+enum ScratchSlot : int {
+  kSlotCounts = 0,        // per-CTA tile counts of the distance kernel
+  kSlotOut = 1,           // dense result staging
+  kSlotResult = 2,        // kNN / threshold results
+  kSlotTemp = 3,          // temporaries (scan storage, unpacking, probes)
+  kSlotSplitCounts = 4,   // counts of tiles split along k
+  kSlotLaunchMeta = 5,    // job table, work list, control block
+  kSlotCount = 6
+};
+
 struct sk_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -31,7 +42,7 @@ struct sk_ctx {
   unsigned long long last_tiles = 0;
   int tile_cfg = 0;                               // forced tile shape (0 = automatic)
   std::map<std::pair<int, int>, int> tuning;      // (K, s64) -> shape id
-  Scratch scratch[4];                             // reusable device buffers
+  Scratch scratch[kSlotCount];                    // reusable device buffers
   std::recursive_mutex mu;
   // Databases and random models keep their context alive: sk_ctx_destroy only
   // marks it, the last dependent handle to go frees it.
@@ -68,6 +79,22 @@ struct sk_sparse {
 
 namespace sk {
 
+// A launch of the persistent distance kernel: tile shape, grid and work list.
+struct Plan {
+  const TileConfig *cfg = nullptr;
+  int grid = 0;
+  std::vector<WorkItem> items;
+  int32_t n_splits = 0;
+  int32_t k_slots = 1;
+};
+
+struct LaunchBuffers {
+  void *meta = nullptr, *cta = nullptr, *split = nullptr;
+  void *ctrl = nullptr;
+  size_t ctrl_bytes = 0;
+  LaunchParams lp{};
+};
+
 class DeviceGuard {
  public:
   explicit DeviceGuard(int dev);
@@ -92,6 +119,13 @@ sk_status build_job(sk_ctx *ctx, const sk_db *ref, const sk_db *query, const sk_
                     int out_mode, int out_col, void *d_out, const TileConfig **cfg_out,
                     JobParams *jp);
 sk_status launch_job(sk_ctx *ctx, const JobParams &jp, const TileConfig &cfg);
+void plan_items(const std::vector<JobParams> &jobs, int grid, Plan &plan);
+sk_status make_plan(sk_ctx *ctx, const std::vector<JobParams> &jobs, const TileConfig &cfg,
+                    Plan &plan);
+sk_status upload_plan(sk_ctx *ctx, const std::vector<JobParams> &jobs, Plan &plan,
+                      LaunchBuffers &buf, bool owned);
+sk_status enqueue_plan(sk_ctx *ctx, const Plan &plan, const LaunchBuffers &buf);
+int resident_grid(sk_ctx *ctx, const TileConfig &cfg);
 sk_status dense_to_device(sk_ctx *ctx, const sk_db *ref, const sk_db *query,
                           const sk_random *random, int out_mode, int out_col, void *d_out);
 int64_t n_pairs(const sk_db *ref, const sk_db *query);

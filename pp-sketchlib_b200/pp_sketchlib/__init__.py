@@ -8,6 +8,7 @@ holds this package (pp-sketchlib_b200/) on sys.path and ``import pp_sketchlib``.
 """
 from ._pp_sketchlib import (  # noqa: F401
     HDF5Exception,
+    _load_random,
     _load_sketch_db,
     addRandom,
     constructDatabase,

@@ -64,7 +64,22 @@ _SIGNATURES = {
     "sk_synth_host": (_i32, [_p, _p, _i64, _i32, _i32, _u64, _i32, _p]),
     "sk_synth_device": (_i32, [_p, _p, _p, _i64, _i32, _i32, _u64, _p]),
     "sk_probe_alu_peak": (_i32, [_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "sk_batch_create": (_i32, [_p, _p, _i32, _i32, C.POINTER(_p)]),
+    "sk_batch_run": (_i32, [_p]),
+    "sk_batch_launch": (_i32, [_p]),
+    "sk_batch_info": (_i32, [_p, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i64),
+                             C.POINTER(_i64)]),
+    "sk_batch_destroy": (_i32, [_p]),
+    "sk_autotune": (_i32, [_p, _p, _p, _p, _i32, C.POINTER(_i32)]),
+    "sk_ctx_save_tuning": (_i32, [_p, C.c_char_p]),
 }
+
+BATCH_AUTOTUNE = 1
+
+
+class Job(C.Structure):
+    """sk_job: one distance job of a batch (outputs in device memory)."""
+    _fields_ = [("ref", _p), ("query", _p), ("random", _p), ("out_mode", _i32), ("out", _p)]
 
 # Entry points a newer header may add; bound when the library exports them.
 _OPTIONAL = {}
@@ -272,6 +287,59 @@ class Random:
 
 def _h(x):
     return None if x is None else x.handle
+
+
+class Batch:
+    """A captured persistent launch over many jobs (sk_batch).
+
+    jobs: list of (ref Database, query Database or None, Random or None,
+    out_mode, device address of the output)."""
+
+    def __init__(self, ctx: Context, jobs, autotune: bool = False):
+        self.ctx = ctx
+        self._keep = list(jobs)
+        arr = (Job * len(jobs))()
+        for i, (ref, query, rnd, mode, out) in enumerate(jobs):
+            arr[i] = Job(ref.handle, _h(query), _h(rnd), mode, out)
+        h = _p()
+        _check(lib.sk_batch_create(ctx.handle, C.cast(arr, _p), len(jobs),
+                                   BATCH_AUTOTUNE if autotune else 0, C.byref(h)), ctx)
+        self.handle = h.value
+
+    def run(self):
+        _check(lib.sk_batch_run(self.handle), self.ctx)
+
+    def launch(self):
+        _check(lib.sk_batch_launch(self.handle), self.ctx)
+
+    def info(self) -> dict:
+        c, g, n, p = _i32(), _i32(), _i64(), _i64()
+        _check(lib.sk_batch_info(self.handle, C.byref(c), C.byref(g), C.byref(n), C.byref(p)),
+               self.ctx)
+        return dict(tile_config=c.value, grid=g.value, n_items=n.value, n_pairs=p.value)
+
+    def close(self):
+        if self.handle:
+            lib.sk_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def autotune(ctx: Context, ref: Database, query: Database | None = None,
+             random: Random | None = None, repeats: int = 2) -> int:
+    best = _i32()
+    _check(lib.sk_autotune(ctx.handle, ref.handle, _h(query), _h(random), repeats,
+                           C.byref(best)), ctx)
+    return best.value
+
+
+def save_tuning(ctx: Context, path: str):
+    _check(lib.sk_ctx_save_tuning(ctx.handle, str(path).encode()), ctx)
 
 
 def dists_rows(ref: Database, query: Database | None = None) -> int:

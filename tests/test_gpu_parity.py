@@ -16,10 +16,11 @@ pytestmark = pytest.mark.gpu
 
 TOL_F64 = 1e-6   # GPU vs oracle, both double-precision fits
 # GPU vs the float LDLT restatement of fit_slope: that arithmetic is itself off
-# the exact fit by up to ~3e-5 on short k ranges (the golden vectors, which
-# match the double fit to 2e-7, show the reference's shipped results do not
-# carry that error); the bar here bounds the float restatement's own error.
-TOL_REF = 1e-4
+# the exact fit, by ~3e-5 on short k ranges and completely when only two
+# nearly collinear points remain (the golden vectors, which match the double
+# fit to 2e-7, show the reference's shipped results do not carry that error).
+# The bar therefore applies to 99% of pairs.
+TOL_REF = 1e-5
 
 SHAPES = [  # (n, K, s64)
     (1, 2, 16), (2, 2, 16), (31, 3, 1), (33, 8, 156), (65, 8, 156), (130, 4, 64),
@@ -105,8 +106,7 @@ def test_jaccard_and_coreacc(gpu_ctx, mode, self_):
     want64 = oracle.dists(rw, kmers, s64, query_words=qw, random=spec, regress=0)
     want32 = oracle.dists(rw, kmers, s64, query_words=qw, random=spec, regress=1)
     assert np.abs(ca - want64).max() <= TOL_F64
-    assert np.abs(ca - want32).max() <= TOL_REF
-    assert np.quantile(np.abs(ca - want32), 0.99) <= 1e-5
+    assert np.quantile(np.abs(ca - want32), 0.99) <= TOL_REF
     assert np.mean(ca == want64) > 0.99
 
 
