@@ -184,6 +184,34 @@ sk_status sk_query_knn(sk_ctx *ctx, const sk_db *ref, const sk_db *query,
                        const sk_random *random, int32_t kNN, int32_t dist_col,
                        int64_t *r_out, float *d_out);
 
+/* ---- dense distances without device allocation ---------------------------- */
+
+/* Bytes of the static device buffer behind sk_dists_dense_noalloc. */
+#define SK_NOALLOC_SCRATCH_BYTES (64u << 20)
+
+/* No counterpart in the reference.  Dense distances (as sk_dists_dense with
+ * out_on_device = 1) for callers that cannot allocate device memory at call
+ * time: services whose device memory is partitioned once at start-up, code
+ * inside a CUDA stream capture (where cudaMalloc breaks the capture), hosts
+ * that share the device with an allocator they do not control.  The call
+ * makes no cudaMalloc, cudaFree or other allocating call: the kernel's scratch
+ * (job descriptor, work list, queue counter, per-CTA count slots, equal-base
+ * random-match factors) lives in one static device array of
+ * SK_NOALLOC_SCRATCH_BYTES, which every GPU that loads this library holds
+ * until the process exits.  The databases (created earlier) are the inputs and
+ * `d_out` (caller-allocated device memory, sk_dists_rows(ref, query) rows) the
+ * output.  A job whose work list and one count slot do not fit the buffer is
+ * rejected with SK_ERANGE; when the count slots of all resident CTAs do not
+ * fit, fewer CTAs run.  The first call on a device looks up the buffer's
+ * device address (cudaGetSymbolAddress) and should come before any stream
+ * capture.  Every call shares the buffer and leaves its contents behind (the
+ * work counter is cleared by each call): calls that overlap on the GPU, from
+ * different contexts or streams of one device, race; calls queued on one
+ * stream do not.  Returns once the work is queued on the context's stream;
+ * sk_ctx_synchronize() waits and reports device-side errors. */
+sk_status sk_dists_dense_noalloc(sk_ctx *ctx, const sk_db *ref, const sk_db *query,
+                                 const sk_random *random, int32_t out_mode, void *d_out);
+
 /* ---- batched persistent launch ------------------------------------------- */
 
 /* One distance job of a batch: all-vs-all of `ref` (query NULL) or query vs

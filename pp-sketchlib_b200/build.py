@@ -23,8 +23,8 @@ LIB = PKG / "sketchlib_b200" / "libsketchlib_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-CUDA_SOURCES = ["dist_kernel.cu", "batch_kernel.cu", "aux_kernels.cu", "probe_kernels.cu",
-                "capi.cu", "batch.cu", "serve.cu"]
+CUDA_SOURCES = ["dist_kernel.cu", "aux_kernels.cu", "probe_kernels.cu", "capi.cu", "batch.cu",
+                "serve.cu", "noalloc.cu"]
 
 
 def _stale(target: Path, sources) -> bool:

@@ -72,6 +72,7 @@ _SIGNATURES = {
     "sk_batch_destroy": (_i32, [_p]),
     "sk_autotune": (_i32, [_p, _p, _p, _p, _i32, C.POINTER(_i32)]),
     "sk_ctx_save_tuning": (_i32, [_p, C.c_char_p]),
+    "sk_dists_dense_noalloc": (_i32, [_p, _p, _p, _p, _i32, _p]),
 }
 
 BATCH_AUTOTUNE = 1
