@@ -29,6 +29,8 @@ import sys
 import time
 from pathlib import Path
 
+import numpy as np
+
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT / "pp-sketchlib_b200"))
 
@@ -248,6 +250,166 @@ def profiled_traffic():
         return None
 
 
+# ------------------------------------------------------- batched (config 4)
+
+BATCH_SEED = 0x5EED0004
+
+
+def batched_jobs(rng):
+    """40 databases: N log-uniform in [50, 8000], 4-14 odd k from 13..39,
+    sketch_size from {1024, 4096, 10000, 20000} (sketchsize64 = round(size/64)),
+    half all-vs-all, half a 10% query slice against the rest."""
+    jobs = []
+    for _ in range(40):
+        n = int(round(np.exp(rng.uniform(np.log(50), np.log(8000)))))
+        K = int(rng.integers(4, 15))
+        kmers = sorted(int(k) for k in rng.choice(np.arange(13, 40, 2), K, replace=False))
+        s64 = int(round(int(rng.choice([1024, 4096, 10000, 20000])) / 64))
+        self_ = bool(rng.random() < 0.5)
+        jobs.append(dict(n=n, kmers=kmers, s64=s64, self=self_))
+    return jobs
+
+
+def run_batched(ctx, dev, lop3_peak, repeats=3):
+    import torch
+    from sketchlib_b200 import capi, synth
+    rng = np.random.default_rng(BATCH_SEED)
+    specs = batched_jobs(rng)
+    made, lop3_total, pairs_total = [], 0, 0
+    for j, sp in enumerate(specs):
+        parent, thresh = synth.random_tree(sp["n"], kmers=sp["kmers"], seed=BATCH_SEED + j)
+        words = torch.empty(sp["n"] * len(sp["kmers"]) * sp["s64"] * BBITS, dtype=torch.int64,
+                            device=dev)
+        capi.synth_device(ctx, parent, thresh, sp["s64"], seed=BATCH_SEED + j,
+                          d_words=words.data_ptr())
+        wps = len(sp["kmers"]) * sp["s64"] * BBITS
+        if sp["self"]:
+            ref = capi.Database(ctx, words.data_ptr(), sp["kmers"], sp["s64"], n_samples=sp["n"])
+            qry = None
+        else:
+            nq = max(1, sp["n"] // 10)
+            qry = capi.Database(ctx, words.data_ptr(), sp["kmers"], sp["s64"], n_samples=nq)
+            ref = capi.Database(ctx, words.data_ptr() + nq * wps * 8, sp["kmers"], sp["s64"],
+                                n_samples=sp["n"] - nq)
+        del words
+        rows = capi.dists_rows(ref, qry)
+        out = torch.empty((max(rows, 1), 2), dtype=torch.float32, device=dev)
+        made.append((ref, qry, None, capi.OUT_CORE_ACC, out))
+        pairs_total += rows
+        lop3_total += rows * len(sp["kmers"]) * 2 * sp["s64"] * BBITS
+    batch = capi.Batch(ctx, [(r, q, rnd, m, o.data_ptr()) for r, q, rnd, m, o in made])
+    info = batch.info()
+    batch.run()                      # warm-up
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(repeats):
+        batch.launch()
+    ctx.synchronize()
+    batched_s = (time.perf_counter() - t0) / repeats
+    ref_out = [o.clone() for *_, o in made]
+    # the same jobs one plain call after another (each its own launch)
+    capi_calls = 0
+    ctx.synchronize()
+    t0 = time.perf_counter()
+    for r, q, rnd, m, o in made:
+        capi.dists_dense(ctx, r, q, rnd, out_mode=m, out=o.data_ptr())
+        capi_calls += 1
+    ctx.synchronize()
+    plain_s = time.perf_counter() - t0
+    same = all(torch.equal(a, o) for a, (*_, o) in zip(ref_out, made))
+    batch.close()
+    for r, q, *_ in made:
+        r.close()
+        if q is not None:
+            q.close()
+    return {
+        "workload": "40 databases, N log-uniform [50, 8000], 4-14 odd k in 13..39, sketchsize64 "
+                    "in {16, 64, 156, 312}, half all-vs-all / half 10% queries vs the rest, "
+                    "one graph-captured persistent launch",
+        "value": pairs_total / batched_s, "unit": UNIT, "pairs": pairs_total,
+        "ms_per_batch": 1e3 * batched_s, "lop3_frac": lop3_total / batched_s / lop3_peak,
+        "tile_config": info["tile_config"], "work_items": info["n_items"],
+        "plain_sequential": {"value": pairs_total / plain_s, "ms": 1e3 * plain_s,
+                             "launches": capi_calls},
+        "pair_for_pair_equal_to_plain": bool(same), "timing": "host clock around graph replays"
+                                                              " (device work dominates)",
+    }
+
+
+# ------------------------------------------------------- serving (config 5)
+
+SERVE_SEED = 0x5EED0005
+
+
+def run_serving(ctx, dev, n_requests=120, rate_hz=10.0):
+    """50,000 resident references (10 k-mer lengths, 15..33, sketchsize64 156);
+    query batches of 1..2000 (log-uniform) arriving as a seeded Poisson stream,
+    drawn from a pool of 4,000 query sketches of the same tree with 5% novel
+    clades; every query against every reference, top-5 kNN returned."""
+    import threading
+    import torch
+    from sketchlib_b200 import capi, synth
+    kmers = list(range(15, 34, 2))
+    n_ref, pool = 50_000, 4_000
+    rp, rt = synth.clade_tree(n_ref, n_clades=200, kmers=kmers, seed=SERVE_SEED)
+    parent, thresh, qidx = synth.query_population(rp, rt, pool, novel_frac=0.05, kmers=kmers,
+                                                  seed=SERVE_SEED + 1)
+    n_all = len(parent)
+    wps = len(kmers) * S64 * BBITS
+    words = torch.empty(n_all * wps, dtype=torch.int64, device=dev)
+    capi.synth_device(ctx, parent, thresh, S64, seed=SERVE_SEED, d_words=words.data_ptr())
+    ref = capi.Database(ctx, words.data_ptr(), kmers, S64, n_samples=n_ref)
+    qwords = words.view(n_all, wps)[torch.as_tensor(qidx, device=dev)].cpu().numpy().view(np.uint64)
+    qwords = np.ascontiguousarray(qwords.reshape(pool, len(kmers), S64 * BBITS))
+    del words
+    rng = np.random.default_rng(SERVE_SEED + 2)
+    sizes = np.exp(rng.uniform(0, np.log(2000), n_requests)).astype(int).clip(1, 2000)
+    starts = rng.integers(0, pool - sizes + 1)
+    gaps = rng.exponential(1.0 / rate_hz, n_requests)
+    server = capi.Server(ctx, ref, slots=4, slice_queries=128, kNN=5)
+    # warm-up request
+    t = server.submit(qwords[:64])
+    server.wait(t)
+    server.result(t)
+    tickets = [None] * n_requests
+    t_begin = time.perf_counter()
+
+    def arrivals():
+        t_next = time.perf_counter()
+        for i in range(n_requests):
+            t_next += gaps[i]
+            d = t_next - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            tickets[i] = server.submit(qwords[starts[i]:starts[i] + sizes[i]])
+
+    th = threading.Thread(target=arrivals)
+    th.start()
+    th.join()
+    lat = np.zeros(n_requests)
+    for i in range(n_requests):
+        server.wait(tickets[i], timeout=600)
+        lat[i] = server.result(tickets[i])[3]
+    makespan = time.perf_counter() - t_begin
+    server.close()
+    ref.close()
+    pairs = int(sizes.sum()) * n_ref
+    mid = (sizes >= 50) & (sizes <= 200)
+    pct = lambda a, q: float(np.percentile(a, q) * 1e3) if len(a) else None
+    return {
+        "workload": "50,000 resident references, 10 k x 10k bins; seeded Poisson arrivals "
+                    f"({rate_hz} req/s), batches log-uniform 1..2000, top-5 kNN per query",
+        "requests": n_requests, "queries": int(sizes.sum()),
+        "value": pairs / makespan, "unit": UNIT,
+        "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99),
+        "p50_ms_batches_50_200": pct(lat[mid], 50), "p99_ms_batches_50_200": pct(lat[mid], 99),
+        "n_batches_50_200": int(mid.sum()),
+        "slots": 4, "slice_queries": 128,
+    }
+
+
 def run_ours(args, rank, world, local):
     import numpy as np
     import torch
@@ -318,6 +480,12 @@ def run_ours(args, rank, world, local):
     # the e2e result must be the resident run's result
     ok = bool(torch.equal(host_out, out.cpu()))
 
+    extra = {}
+    if not args.skip_batched:
+        extra["batched"] = run_batched(ctx, dev, lop3_peak)
+    if not args.skip_serving:
+        extra["serving"] = run_serving(ctx, dev)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         kind, threads, run, _ = cpu_reference_rate()
@@ -356,6 +524,7 @@ def run_ours(args, rank, world, local):
     }
     if cpu is not None:
         line["cpu_baseline"] = cpu
+    line.update(extra)
     if rank == 0:
         print(json.dumps(line), flush=True)
     db.close()
@@ -390,6 +559,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--skip-batched", action="store_true")
+    ap.add_argument("--skip-serving", action="store_true")
     ap.add_argument("--profile", type=int, default=0,
                     help="run only N-sample dense launches (a small case for ncu)")
     ap.add_argument("--profile-launches", type=int, default=2)

@@ -254,6 +254,43 @@ sk_status sk_autotune(sk_ctx *ctx, const sk_db *ref, const sk_db *query,
  * for sk_ctx_load_tuning. */
 sk_status sk_ctx_save_tuning(sk_ctx *ctx, const char *path);
 
+/* ---- query server: resident references, continuous batching --------------- */
+
+typedef struct sk_server sk_server;
+
+typedef struct sk_server_params {
+  int32_t slots;          /* slices on the device at once (one stream each), 1..16 */
+  int32_t slice_queries;  /* largest number of queries per slice */
+  int32_t kNN;            /* nearest references returned per query, 0..800 */
+  int32_t dist_col;       /* distance the kNN ranks by: 0 core, 1 accessory */
+  int32_t keep_rows;      /* 1: also return each query's core/accessory row */
+} sk_server_params;
+
+/* Starts a server over `ref` (kept resident; it must outlive the server).
+ * Every slot's buffers are allocated here, so the HBM footprint is fixed and
+ * requests are admitted as slots free up.  No reference counterpart: the
+ * reference answers one query_db_cuda call at a time (src/gpu/gpu_api.cpp:352). */
+sk_status sk_server_create(sk_ctx *ctx, const sk_db *ref, const sk_random *random,
+                           const sk_server_params *params, sk_server **out);
+/* Queues a request: n_queries sketches in the reference word layout (host
+ * memory that must stay valid until the request is done), optional per-query
+ * random-match cluster ids and sequence lengths.  Thread-safe. */
+sk_status sk_server_submit(sk_server *server, const uint64_t *query_words, int64_t n_queries,
+                           const uint16_t *cluster, const uint64_t *seq_len, int64_t *ticket);
+/* Waits for a request (bounded by timeout_s; SK_ETIMEDOUT when it runs out). */
+sk_status sk_server_wait(sk_server *server, int64_t ticket, double timeout_s);
+/* Copies a finished request's results: knn_idx / knn_dist [n_queries][kNN]
+ * (ascending, ties by smaller reference index), rows [n_queries][n_ref][2]
+ * when keep_rows; latency_s from submit to completion.  NULL skips a field. */
+sk_status sk_server_result(sk_server *server, int64_t ticket, int64_t *knn_idx, float *knn_dist,
+                           float *rows, double *latency_s);
+/* Forgets a finished request. */
+sk_status sk_server_release(sk_server *server, int64_t ticket);
+sk_status sk_server_stats(sk_server *server, int64_t *pairs_done, double *uptime_s,
+                          int64_t *queued_queries);
+/* Finishes the queued work, stops the scheduler thread and frees the slots. */
+sk_status sk_server_destroy(sk_server *server);
+
 /* ---- sparse / matrix transforms (device kernels over long-form data) ---- */
 
 /* Entries (i, j > i) of the square form of a long-form column with value

@@ -1,0 +1,453 @@
+// serve.cu -- a query server over a reference database resident in HBM.
+//
+// Requests (a batch of query sketches each) arrive at any time from any host
+// thread.  A scheduler thread cuts every request into slices of at most
+// `slice_queries` queries and runs slices on `slots`: each slot owns a
+// context (its own stream and kernel scratch), a packed query buffer, a
+// distance column for the slice against every reference and the kNN result
+// buffers, all allocated once at start-up, so admission is by free slot and
+// the server's HBM footprint is fixed (slots x slot bytes + the reference).
+// Slices of different requests run on different streams and overlap on the
+// device: a slot's persistent kernel takes SMs as another slot's kernel
+// releases them.  Scheduling is round-robin over requests with work
+// conservation: a request holds at most one slot while others wait, so a
+// 2,000-query request cannot delay a 10-query one by more than a slice.
+//
+// Per slice: pinned staging copy of the query words, H2D, pack, the distance
+// kernel (core or accessory column vs all references, optionally the full
+// core/accessory rows), per-query top-kNN, D2H of the kNN lists (and rows).
+// Results of each query depend only on that query and the references, so a
+// request gets bit-identical results alone or in any mix.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "sk_runtime.h"
+
+using namespace sk;
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+  int64_t id = 0;
+  const uint64_t *words = nullptr;   // caller's host buffer, kept alive until done
+  int64_t n = 0;
+  std::vector<uint16_t> cluster;
+  std::vector<uint64_t> seq_len;
+  int64_t dispatched = 0;            // queries handed to slots
+  int64_t completed = 0;             // queries finished
+  int inflight = 0;                  // slices on the device
+  bool failed = false;
+  std::string error;
+  std::vector<int64_t> knn_idx;      // [n][kNN]
+  std::vector<float> knn_dist;
+  std::vector<float> rows;           // [n][n_ref][2] when dense output is kept
+  Clock::time_point t_submit, t_done;
+  bool done = false;
+};
+
+struct Slot {
+  sk_ctx *ctx = nullptr;
+  sk_db qdb;                         // packed query buffer (pre-allocated)
+  uint64_t *d_words = nullptr;       // staging of the reference-layout words
+  uint64_t *h_words = nullptr;       // pinned host staging
+  float *d_col = nullptr;            // [slice][n_ref] distance column
+  float *d_rows = nullptr;           // [slice][n_ref][2] core/accessory (optional)
+  int64_t *d_knn = nullptr;
+  float *d_knn_d = nullptr;
+  int64_t *h_knn = nullptr;          // pinned results
+  float *h_knn_d = nullptr;
+  float *h_rows = nullptr;
+  cudaEvent_t done_ev = nullptr;
+  std::shared_ptr<Request> req;
+  int64_t q0 = 0, nq = 0;
+  bool busy = false;
+};
+
+}  // namespace
+
+struct sk_server {
+  sk_ctx *ctx = nullptr;             // the reference database's context
+  const sk_db *ref = nullptr;
+  const sk_random *random = nullptr;
+  sk_server_params params{};
+  size_t words_per_sample = 0;
+  std::vector<Slot> slots;
+  std::mutex mu;
+  std::condition_variable cv;        // wakes the scheduler
+  std::condition_variable done_cv;   // wakes waiters
+  std::deque<std::shared_ptr<Request>> pending;   // not fully dispatched
+  std::map<int64_t, std::shared_ptr<Request>> all;
+  int64_t next_id = 1;
+  bool stop = false;
+  std::thread worker;
+  // statistics
+  int64_t pairs_done = 0;
+  double busy_s = 0;
+  Clock::time_point t_start;
+  std::string fatal;
+};
+
+namespace {
+
+void free_slot(Slot &s) {
+  if (s.done_ev) cudaEventDestroy(s.done_ev);
+  if (s.d_words) cudaFree(s.d_words);
+  if (s.h_words) cudaFreeHost(s.h_words);
+  if (s.d_col) cudaFree(s.d_col);
+  if (s.d_rows) cudaFree(s.d_rows);
+  if (s.d_knn) cudaFree(s.d_knn);
+  if (s.h_knn) cudaFreeHost(s.h_knn);
+  if (s.h_rows) cudaFreeHost(s.h_rows);
+  if (s.qdb.packed) cudaFree(s.qdb.packed);
+  if (s.qdb.cluster) cudaFree(s.qdb.cluster);
+  if (s.qdb.jv) cudaFree(s.qdb.jv);
+  if (s.ctx) sk_ctx_destroy(s.ctx);
+  s = Slot{};
+}
+
+// Queues one slice on its slot's stream.  Called by the scheduler thread only.
+sk_status start_slice(sk_server *sv, Slot &s) {
+  sk_ctx *ctx = s.ctx;
+  const sk_db *ref = sv->ref;
+  const size_t wps = sv->words_per_sample;
+  Request &r = *s.req;
+  DeviceGuard g(ctx->device);
+  sk_status st = begin_call(ctx);
+  if (st != SK_OK) return st;
+  std::memcpy(s.h_words, r.words + s.q0 * wps, static_cast<size_t>(s.nq) * wps * 8);
+  // the query database of this slice: same packed buffer, new samples
+  s.qdb.n = s.nq;
+  s.qdb.jv_rc = -1;   // equal-base factors depend on the samples
+  if (!r.cluster.empty()) {
+    cudaError_t e = cudaMemcpyAsync(s.qdb.cluster, r.cluster.data() + s.q0, s.nq * 2,
+                                    cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "query clusters");
+  }
+  if (!r.seq_len.empty())
+    s.qdb.seq_len.assign(r.seq_len.begin() + s.q0, r.seq_len.begin() + s.q0 + s.nq);
+  else
+    s.qdb.seq_len.assign(s.nq, 0);
+  cudaError_t e = cudaMemcpyAsync(s.d_words, s.h_words, static_cast<size_t>(s.nq) * wps * 8,
+                                  cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess)
+    e = launch_pack(s.d_words, s.nq, ref->K, ref->s64, s.qdb.ng, s.qdb.packed, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "query upload");
+  const int col = sv->params.dist_col;
+  if (sv->params.keep_rows) {
+    st = dense_to_device(ctx, ref, &s.qdb, sv->random, kOutCoreAcc, 0, s.d_rows);
+    if (st != SK_OK) return st;
+    e = cudaMemcpyAsync(s.h_rows, s.d_rows, static_cast<size_t>(s.nq) * ref->n * 8,
+                        cudaMemcpyDeviceToHost, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "row copy");
+  }
+  st = dense_to_device(ctx, ref, &s.qdb, sv->random, kOutColumn, col, s.d_col);
+  if (st != SK_OK) return st;
+  const int knn = sv->params.kNN;
+  if (knn > 0) {
+    e = launch_knn_rows(s.d_col, s.nq, ref->n, knn, s.d_knn, s.d_knn_d, ctx->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(s.h_knn, s.d_knn, static_cast<size_t>(s.nq) * knn * 8,
+                          cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(s.h_knn_d, s.d_knn_d, static_cast<size_t>(s.nq) * knn * 4,
+                          cudaMemcpyDeviceToHost, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "kNN");
+  }
+  e = cudaEventRecord(s.done_ev, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "event");
+  return SK_OK;
+}
+
+void finish_slice(sk_server *sv, Slot &s) {
+  Request &r = *s.req;
+  const int knn = sv->params.kNN;
+  DevStatus dst{};
+  {
+    DeviceGuard g(s.ctx->device);
+    cudaMemcpy(&dst, s.ctx->status_dev, sizeof(dst), cudaMemcpyDeviceToHost);
+  }
+  if (dst.error) {
+    r.failed = true;
+    r.error = (dst.error & 2u) ? "cancelled" : "device-side error";
+  }
+  if (knn > 0) {
+    std::memcpy(r.knn_idx.data() + s.q0 * knn, s.h_knn, static_cast<size_t>(s.nq) * knn * 8);
+    std::memcpy(r.knn_dist.data() + s.q0 * knn, s.h_knn_d, static_cast<size_t>(s.nq) * knn * 4);
+  }
+  if (sv->params.keep_rows)
+    std::memcpy(r.rows.data() + s.q0 * sv->ref->n * 2, s.h_rows,
+                static_cast<size_t>(s.nq) * sv->ref->n * 8);
+  r.completed += s.nq;
+  r.inflight -= 1;
+  sv->pairs_done += s.nq * sv->ref->n;
+  if (r.completed == r.n) {
+    r.done = true;
+    r.t_done = Clock::now();
+  }
+  s.req.reset();
+  s.busy = false;
+}
+
+void scheduler(sk_server *sv) {
+  std::unique_lock<std::mutex> lock(sv->mu);
+  size_t rr = 0;   // round-robin cursor over pending requests
+  while (true) {
+    bool progressed = false;
+    // completions
+    for (Slot &s : sv->slots) {
+      if (!s.busy) continue;
+      cudaError_t q;
+      {
+        DeviceGuard g(s.ctx->device);
+        q = cudaEventQuery(s.done_ev);
+      }
+      if (q == cudaErrorNotReady) continue;
+      if (q != cudaSuccess) {
+        s.req->failed = true;
+        s.req->error = cudaGetErrorString(q);
+      }
+      finish_slice(sv, s);
+      progressed = true;
+    }
+    if (progressed) sv->done_cv.notify_all();
+    // admissions: give free slots to requests, one slice per request per round
+    for (Slot &s : sv->slots) {
+      if (s.busy || sv->pending.empty()) continue;
+      // prefer the next request with nothing in flight; else any with work left
+      std::shared_ptr<Request> pick;
+      const size_t np = sv->pending.size();
+      for (int pass = 0; pass < 2 && !pick; ++pass) {
+        for (size_t i = 0; i < np; ++i) {
+          auto &cand = sv->pending[(rr + i) % np];
+          if (cand->dispatched >= cand->n) continue;
+          if (pass == 0 && cand->inflight > 0) continue;
+          pick = cand;
+          rr = (rr + i + 1) % np;
+          break;
+        }
+      }
+      if (!pick) break;
+      s.req = pick;
+      s.q0 = pick->dispatched;
+      s.nq = std::min<int64_t>(sv->params.slice_queries, pick->n - pick->dispatched);
+      pick->dispatched += s.nq;
+      pick->inflight += 1;
+      s.busy = true;
+      sk_status st = start_slice(sv, s);
+      if (st != SK_OK) {
+        pick->failed = true;
+        pick->error = sk_last_error(s.ctx);
+        // the slice still completes through its event (recorded or not)
+        DeviceGuard g(s.ctx->device);
+        cudaEventRecord(s.done_ev, s.ctx->stream);
+      }
+      progressed = true;
+    }
+    // drop fully dispatched requests from the pending list
+    sv->pending.erase(std::remove_if(sv->pending.begin(), sv->pending.end(),
+                                     [](const std::shared_ptr<Request> &r) {
+                                       return r->dispatched >= r->n;
+                                     }),
+                      sv->pending.end());
+    bool any_busy = false;
+    for (Slot &s : sv->slots) any_busy |= s.busy;
+    if (sv->stop && !any_busy && sv->pending.empty()) break;
+    if (!progressed) {
+      if (any_busy)
+        sv->cv.wait_for(lock, std::chrono::microseconds(100));
+      else
+        sv->cv.wait_for(lock, std::chrono::milliseconds(50));
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+sk_status sk_server_create(sk_ctx *ctx, const sk_db *ref, const sk_random *random,
+                           const sk_server_params *params, sk_server **out) {
+  if (!ctx) return SK_EINVAL;
+  std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+  DeviceGuard g(ctx->device);
+  ctx->err.clear();
+  if (!out || !ref || !params) return fail(ctx, SK_EINVAL, "null argument");
+  *out = nullptr;
+  if (ref->n < 1) return fail(ctx, SK_EINVAL, "Query with empty ref or query list!");
+  const sk_server_params &p = *params;
+  if (p.slots < 1 || p.slots > 16 || p.slice_queries < 1 || p.slice_queries > 65536 ||
+      p.kNN < 0 || p.kNN > 800 || p.kNN > ref->n || (p.dist_col != 0 && p.dist_col != 1))
+    return fail(ctx, SK_EINVAL, "bad server parameters");
+  if (random && random->kmers != ref->kmers)
+    return fail(ctx, SK_EMISMATCH, "Random match table k-mer lengths differ from the sketches");
+  if (random && random->mode == kRandEqualBase) {
+    sk_status st = ensure_jv(ctx, const_cast<sk_db *>(ref), random->use_rc);   // before threads
+    if (st != SK_OK) return st;
+  }
+  sk_server *sv = new sk_server();
+  sv->ctx = ctx;
+  sv->ref = ref;
+  sv->random = random;
+  sv->params = p;
+  sv->words_per_sample = static_cast<size_t>(ref->K) * ref->s64 * kBbits;
+  sv->slots.resize(p.slots);
+  const int64_t sq = p.slice_queries;
+  const int64_t npad = ((sq + kSamplePad - 1) / kSamplePad) * kSamplePad;
+  sk_status st = SK_OK;
+  for (Slot &s : sv->slots) {
+    st = sk_ctx_create(ctx->device, &s.ctx);
+    if (st != SK_OK) break;
+    s.ctx->tile_cfg = ctx->tile_cfg;
+    s.ctx->tuning = ctx->tuning;
+    s.qdb.ctx = s.ctx;
+    s.qdb.K = ref->K;
+    s.qdb.s64 = ref->s64;
+    s.qdb.bbits = ref->bbits;
+    s.qdb.kmers = ref->kmers;
+    s.qdb.ng = static_cast<int32_t>(npad / kGranule);
+    cudaError_t e = cudaMalloc(&s.qdb.packed, static_cast<size_t>(ref->K) * 2 * ref->s64 *
+                                                  s.qdb.ng * kStripeWords * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&s.qdb.cluster, npad * 2);
+    if (e == cudaSuccess) e = cudaMemset(s.qdb.cluster, 0, npad * 2);
+    if (e == cudaSuccess) e = cudaMalloc(&s.d_words, sq * sv->words_per_sample * 8);
+    if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void **>(&s.h_words),
+                                            sq * sv->words_per_sample * 8, cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaMalloc(&s.d_col, sq * ref->n * 4);
+    if (e == cudaSuccess && p.keep_rows) e = cudaMalloc(&s.d_rows, sq * ref->n * 8);
+    if (e == cudaSuccess && p.keep_rows)
+      e = cudaHostAlloc(reinterpret_cast<void **>(&s.h_rows), sq * ref->n * 8, cudaHostAllocDefault);
+    if (e == cudaSuccess && p.kNN > 0) e = cudaMalloc(&s.d_knn, sq * p.kNN * 12);
+    if (e == cudaSuccess && p.kNN > 0)
+      e = cudaHostAlloc(reinterpret_cast<void **>(&s.h_knn), sq * p.kNN * 12, cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.done_ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+      st = cuda_fail(ctx, e, "server slot allocation");
+      break;
+    }
+    if (p.kNN > 0) {
+      s.d_knn_d = reinterpret_cast<float *>(s.d_knn + sq * p.kNN);
+      s.h_knn_d = reinterpret_cast<float *>(s.h_knn + sq * p.kNN);
+    }
+  }
+  if (st != SK_OK) {
+    for (Slot &s : sv->slots) free_slot(s);
+    delete sv;
+    return st;
+  }
+  ctx_retain(ctx);
+  sv->t_start = Clock::now();
+  sv->worker = std::thread(scheduler, sv);
+  *out = sv;
+  return SK_OK;
+}
+
+sk_status sk_server_submit(sk_server *sv, const uint64_t *query_words, int64_t n_queries,
+                           const uint16_t *cluster, const uint64_t *seq_len, int64_t *ticket) {
+  if (!sv || !ticket || n_queries < 1 || !query_words) return SK_EINVAL;
+  auto r = std::make_shared<Request>();
+  r->words = query_words;
+  r->n = n_queries;
+  if (cluster) r->cluster.assign(cluster, cluster + n_queries);
+  if (seq_len) r->seq_len.assign(seq_len, seq_len + n_queries);
+  if (sv->params.kNN > 0) {
+    r->knn_idx.assign(static_cast<size_t>(n_queries) * sv->params.kNN, -1);
+    r->knn_dist.assign(static_cast<size_t>(n_queries) * sv->params.kNN, 0.0f);
+  }
+  if (sv->params.keep_rows) r->rows.assign(static_cast<size_t>(n_queries) * sv->ref->n * 2, 0.0f);
+  r->t_submit = Clock::now();
+  {
+    std::lock_guard<std::mutex> lock(sv->mu);
+    if (sv->stop) return SK_EINVAL;
+    r->id = sv->next_id++;
+    sv->pending.push_back(r);
+    sv->all[r->id] = r;
+  }
+  sv->cv.notify_one();
+  *ticket = r->id;
+  return SK_OK;
+}
+
+sk_status sk_server_wait(sk_server *sv, int64_t ticket, double timeout_s) {
+  if (!sv) return SK_EINVAL;
+  std::unique_lock<std::mutex> lock(sv->mu);
+  auto it = sv->all.find(ticket);
+  if (it == sv->all.end()) return SK_EINVAL;
+  std::shared_ptr<Request> r = it->second;
+  const auto deadline = Clock::now() + std::chrono::duration<double>(timeout_s);
+  while (!r->done) {
+    if (sv->done_cv.wait_until(lock, deadline) == std::cv_status::timeout && !r->done)
+      return SK_ETIMEDOUT;
+  }
+  return r->failed ? SK_EKERNEL : SK_OK;
+}
+
+sk_status sk_server_result(sk_server *sv, int64_t ticket, int64_t *knn_idx, float *knn_dist,
+                           float *rows, double *latency_s) {
+  if (!sv) return SK_EINVAL;
+  std::lock_guard<std::mutex> lock(sv->mu);
+  auto it = sv->all.find(ticket);
+  if (it == sv->all.end()) return SK_EINVAL;
+  Request &r = *it->second;
+  if (!r.done) return SK_EINVAL;
+  if (knn_idx) std::copy(r.knn_idx.begin(), r.knn_idx.end(), knn_idx);
+  if (knn_dist) std::copy(r.knn_dist.begin(), r.knn_dist.end(), knn_dist);
+  if (rows) std::copy(r.rows.begin(), r.rows.end(), rows);
+  if (latency_s) *latency_s = std::chrono::duration<double>(r.t_done - r.t_submit).count();
+  return r.failed ? SK_EKERNEL : SK_OK;
+}
+
+sk_status sk_server_release(sk_server *sv, int64_t ticket) {
+  if (!sv) return SK_EINVAL;
+  std::lock_guard<std::mutex> lock(sv->mu);
+  auto it = sv->all.find(ticket);
+  if (it == sv->all.end() || !it->second->done) return SK_EINVAL;
+  sv->all.erase(it);
+  return SK_OK;
+}
+
+sk_status sk_server_stats(sk_server *sv, int64_t *pairs_done, double *uptime_s,
+                          int64_t *queued_queries) {
+  if (!sv) return SK_EINVAL;
+  std::lock_guard<std::mutex> lock(sv->mu);
+  if (pairs_done) *pairs_done = sv->pairs_done;
+  if (uptime_s) *uptime_s = std::chrono::duration<double>(Clock::now() - sv->t_start).count();
+  if (queued_queries) {
+    int64_t q = 0;
+    for (auto &r : sv->pending) q += r->n - r->dispatched;
+    *queued_queries = q;
+  }
+  return SK_OK;
+}
+
+sk_status sk_server_destroy(sk_server *sv) {
+  if (!sv) return SK_EINVAL;
+  {
+    std::lock_guard<std::mutex> lock(sv->mu);
+    sv->stop = true;
+  }
+  sv->cv.notify_all();
+  if (sv->worker.joinable()) sv->worker.join();
+  for (Slot &s : sv->slots) {
+    DeviceGuard g(s.ctx ? s.ctx->device : 0);
+    free_slot(s);
+  }
+  sk_ctx *ctx = sv->ctx;
+  delete sv;
+  ctx_release(ctx);
+  return SK_OK;
+}
+
+}  // extern "C"

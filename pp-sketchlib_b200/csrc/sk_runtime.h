@@ -129,6 +129,7 @@ int resident_grid(sk_ctx *ctx, const TileConfig &cfg);
 sk_status dense_to_device(sk_ctx *ctx, const sk_db *ref, const sk_db *query,
                           const sk_random *random, int out_mode, int out_col, void *d_out);
 int64_t n_pairs(const sk_db *ref, const sk_db *query);
+sk_status ensure_jv(sk_ctx *ctx, sk_db *db, int use_rc);
 size_t out_bytes(int out_mode, int64_t pairs, int K);
 
 }  // namespace sk

@@ -73,7 +73,19 @@ _SIGNATURES = {
     "sk_autotune": (_i32, [_p, _p, _p, _p, _i32, C.POINTER(_i32)]),
     "sk_ctx_save_tuning": (_i32, [_p, C.c_char_p]),
     "sk_dists_dense_noalloc": (_i32, [_p, _p, _p, _p, _i32, _p]),
+    "sk_server_create": (_i32, [_p, _p, _p, _p, C.POINTER(_p)]),
+    "sk_server_submit": (_i32, [_p, _p, _i64, _p, _p, C.POINTER(_i64)]),
+    "sk_server_wait": (_i32, [_p, _i64, C.c_double]),
+    "sk_server_result": (_i32, [_p, _i64, _p, _p, _p, C.POINTER(C.c_double)]),
+    "sk_server_release": (_i32, [_p, _i64]),
+    "sk_server_stats": (_i32, [_p, C.POINTER(_i64), C.POINTER(C.c_double), C.POINTER(_i64)]),
+    "sk_server_destroy": (_i32, [_p]),
 }
+
+
+class ServerParams(C.Structure):
+    _fields_ = [("slots", _i32), ("slice_queries", _i32), ("kNN", _i32), ("dist_col", _i32),
+                ("keep_rows", _i32)]
 
 BATCH_AUTOTUNE = 1
 
@@ -322,6 +334,72 @@ class Batch:
     def close(self):
         if self.handle:
             lib.sk_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """A query server over a resident reference database (sk_server)."""
+
+    def __init__(self, ctx: Context, ref: Database, random: Random | None = None, slots: int = 3,
+                 slice_queries: int = 128, kNN: int = 5, dist_col: int = 0,
+                 keep_rows: bool = False):
+        self.ctx = ctx
+        self.ref = ref
+        self.kNN = kNN
+        self.keep_rows = keep_rows
+        self._inputs = {}
+        prm = ServerParams(slots, slice_queries, kNN, dist_col, int(keep_rows))
+        h = _p()
+        _check(lib.sk_server_create(ctx.handle, ref.handle, _h(random), C.byref(prm), C.byref(h)),
+               ctx)
+        self.handle = h.value
+
+    def submit(self, words, cluster=None, seq_len=None) -> int:
+        w = np.ascontiguousarray(words, dtype=np.uint64)
+        cl = None if cluster is None else np.ascontiguousarray(cluster, np.uint16)
+        ln = None if seq_len is None else np.ascontiguousarray(seq_len, np.uint64)
+        t = _i64()
+        st = lib.sk_server_submit(self.handle, w.ctypes.data, w.shape[0], _ptr(cl), _ptr(ln),
+                                  C.byref(t))
+        if st != SK_OK:
+            raise SketchlibError(st, "submit failed")
+        self._inputs[t.value] = (w, cl, ln)       # the server reads them until done
+        return t.value
+
+    def wait(self, ticket: int, timeout: float = 60.0):
+        st = lib.sk_server_wait(self.handle, ticket, timeout)
+        if st != SK_OK:
+            raise SketchlibError(st, f"request {ticket} did not complete")
+
+    def result(self, ticket: int, release: bool = True):
+        n = self._inputs[ticket][0].shape[0]
+        idx = np.empty((n, self.kNN), np.int64)
+        dist = np.empty((n, self.kNN), np.float32)
+        rows = np.empty((n, self.ref.n, 2), np.float32) if self.keep_rows else None
+        lat = C.c_double()
+        st = lib.sk_server_result(self.handle, ticket, idx.ctypes.data, dist.ctypes.data,
+                                  _ptr(rows), C.byref(lat))
+        if st != SK_OK:
+            raise SketchlibError(st, f"request {ticket} failed")
+        if release:
+            lib.sk_server_release(self.handle, ticket)
+            self._inputs.pop(ticket, None)
+        return idx, dist, rows, lat.value
+
+    def stats(self):
+        p, u, q = _i64(), C.c_double(), _i64()
+        _check(lib.sk_server_stats(self.handle, C.byref(p), C.byref(u), C.byref(q)), self.ctx)
+        return dict(pairs_done=p.value, uptime_s=u.value, queued_queries=q.value)
+
+    def close(self):
+        if self.handle:
+            lib.sk_server_destroy(self.handle)
             self.handle = None
 
     def __del__(self):
