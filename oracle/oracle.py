@@ -242,3 +242,39 @@ class RefQueryDb:
 
 def ref_available() -> bool:
     return REF_PATH.exists()
+
+
+SKETCH_PATH = HERE / "_ref" / "libref_sketch.so"
+
+
+class RefSketcher:
+    """The reference's CPU sketcher (oracle/_ref/libref_sketch.so) and the
+    seeded genome generator of the CPU parity case."""
+
+    def __init__(self):
+        if not SKETCH_PATH.exists():
+            raise FileNotFoundError(f"{SKETCH_PATH} not built (needs the reference sources)")
+        lib_ = C.CDLL(str(SKETCH_PATH))
+        lib_.ref_make_genomes.restype = None
+        lib_.ref_make_genomes.argtypes = [C.c_int, C.c_int64, C.c_uint64, C.c_void_p]
+        lib_.ref_sketch_genomes.restype = C.c_int
+        lib_.ref_sketch_genomes.argtypes = [C.c_void_p, C.c_int, C.c_int64, C.c_void_p, C.c_int,
+                                            C.c_int, C.c_int, C.c_int, C.c_void_p]
+        self.lib = lib_
+
+    def genomes(self, n, length, seed):
+        out = np.empty((n, length), dtype=np.uint8)
+        self.lib.ref_make_genomes(n, length, seed, out.ctypes.data)
+        return out
+
+    def sketch(self, genomes, kmers, s64, use_rc=True, threads=NTHREADS):
+        g = np.ascontiguousarray(genomes, dtype=np.uint8)
+        km = np.ascontiguousarray(kmers, np.int32)
+        out = np.zeros((g.shape[0], len(km), s64 * 14), np.uint64)
+        self.lib.ref_sketch_genomes(g.ctypes.data, g.shape[0], g.shape[1], km.ctypes.data, len(km),
+                                    s64, int(use_rc), threads, out.ctypes.data)
+        return out
+
+
+def sketcher_available() -> bool:
+    return SKETCH_PATH.exists()

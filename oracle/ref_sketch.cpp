@@ -1,0 +1,98 @@
+// ref_sketch.cpp -- synthetic genomes sketched by the reference's own sketcher.
+//
+// TEST INFRASTRUCTURE ONLY.  Builds the inputs of the CPU-runnable parity
+// case: 64 genomes of 2.5 Mb derived from one seeded root, sketched with the
+// reference's sketch() (src/sketch/sketch.cpp:120-168, compiled from the
+// reference sources by oracle/Makefile with -DWEB_SKETCH, which leaves out
+// the GPU headers).  The sketches then go through the CUDA path and the
+// oracle like any other database.
+//
+// Genome model: i.i.d. bases at GC 0.38 (A = T = 0.31, C = G = 0.19) for the
+// root; genome i > 0 copies a uniformly chosen earlier genome, then mutates a
+// fraction c ~ U(0, 0.004) of positions to another base (core SNPs) and
+// replaces a fraction a ~ U(0, 0.03) of the sequence with fresh random 5 kb
+// segments (accessory).  Over the ~8 branches between two genomes of the
+// random recursive tree, pairs span about 0-3% core and 0-20% accessory
+// divergence.
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "sketch/sketch.hpp"   // from the reference sources
+
+namespace {
+
+struct Rng {  // splitmix64
+  uint64_t s;
+  uint64_t next() {
+    uint64_t z = (s += 0x9E3779B97F4A7C15ULL);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+  }
+  double uniform() { return (next() >> 11) * (1.0 / 9007199254740992.0); }
+  char base() {
+    const double u = uniform();
+    return u < 0.31 ? 'A' : u < 0.50 ? 'C' : u < 0.69 ? 'G' : 'T';
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+// Writes n genomes of `length` bases to out (n * length chars, no separators).
+void ref_make_genomes(int n, int64_t length, uint64_t seed, char *out) {
+  Rng rng{seed};
+  for (int64_t p = 0; p < length; ++p) out[p] = rng.base();
+  for (int g = 1; g < n; ++g) {
+    const int parent = static_cast<int>(rng.next() % static_cast<uint64_t>(g));
+    char *dst = out + static_cast<int64_t>(g) * length;
+    std::memcpy(dst, out + static_cast<int64_t>(parent) * length, length);
+    const double c = 0.004 * rng.uniform();
+    const double a = 0.03 * rng.uniform();
+    const int64_t snps = static_cast<int64_t>(c * length);
+    for (int64_t s = 0; s < snps; ++s) {
+      const int64_t p = static_cast<int64_t>(rng.next() % static_cast<uint64_t>(length));
+      char b;
+      do {
+        b = rng.base();
+      } while (b == dst[p]);
+      dst[p] = b;
+    }
+    const int64_t seg = 5000;
+    const int64_t segments = static_cast<int64_t>(a * length / seg);
+    for (int64_t s = 0; s < segments; ++s) {
+      const int64_t p = static_cast<int64_t>(rng.next() % static_cast<uint64_t>(length - seg));
+      for (int64_t q = 0; q < seg; ++q) dst[p + q] = rng.base();
+    }
+  }
+}
+
+// Sketches n genomes of `length` bases with the reference's sketch() at the
+// given k-mer lengths: out [n][K][sketchsize64 * 14] in the reference word
+// layout.  Returns the number of genomes that came out densified.
+int ref_sketch_genomes(const char *seqs, int n, int64_t length, const int32_t *kmers, int K,
+                       int sketchsize64, int use_rc, int threads, uint64_t *out) {
+  std::vector<size_t> kl(kmers, kmers + K);
+  const KmerSeeds seeds = generate_seeds(kl, false);
+  const int64_t W = static_cast<int64_t>(sketchsize64) * 14;
+  int densified = 0;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads) reduction(+ : densified)
+  for (int g = 0; g < n; ++g) {
+    SeqBuf buf(std::vector<std::string>{std::string(seqs + static_cast<int64_t>(g) * length, length)});
+    bool any = false;
+    for (int k = 0; k < K; ++k) {
+      auto res = sketch(buf, static_cast<uint64_t>(sketchsize64), seeds.at(kl[k]), 14, false,
+                        use_rc != 0, 0, false);
+      const std::vector<uint64_t> &usigs = std::get<0>(res);
+      std::memcpy(out + (static_cast<int64_t>(g) * K + k) * W, usigs.data(), W * 8);
+      any = any || std::get<2>(res);
+    }
+    densified += any ? 1 : 0;
+  }
+  return densified;
+}
+
+}  // extern "C"
