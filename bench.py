@@ -45,7 +45,7 @@ SEED = 0x5EED0002
 LOP3_PER_PAIR = len(KMERS) * 2 * S64 * BBITS        # one LOP3 per 32 bins per plane
 POPC_PER_PAIR = len(KMERS) * 2 * S64
 PUBLISHED_GPU = 6.0e6   # README.md:137,140 -- RTX 2080 Ti, 8 k x 10,000 bins
-PROFILE_SUMMARY = ROOT / "profiles" / "dist_tiles_kernel_4096.md"
+PROFILE_SUMMARY = ROOT / "profiles" / "dist_items_kernel_4096.md"
 
 
 def n_pairs(n: int) -> int:
