@@ -202,10 +202,30 @@ def sample_rate(run, target_s: float):
     return pairs, elapsed, row
 
 
+def reference_gpu_rate(words, launches: int):
+    """The reference's own GPU kernel (`calculate_dists`, src/gpu/dist.cu:164-317,
+    compiled for sm_100a from the reference sources into oracle/_ref) on the
+    full workload: inputs resident, one launch per step, CUDA events around
+    each launch, launch shape from the reference's getBlockSize."""
+    import torch
+    if not torch.cuda.is_available():
+        return None
+    import oracle
+    if not oracle.ref_gpu_available():
+        return {"unavailable": "oracle/_ref/libref_gpu.so not built (needs the reference sources)"}
+    _, ms = oracle.RefGpuKernel().self_dists(words, KMERS, S64, warmup=1, launches=launches,
+                                             want_out=False)
+    return {"value": n_pairs(N_SAMPLES) / (ms / 1e3), "unit": UNIT, "ms_per_launch": ms,
+            "launches": launches,
+            "kernel": "reference calculate_dists (src/gpu/dist.cu:164-317) built for sm_100a",
+            "timing": "CUDA events per launch, sketches resident in the reference's "
+                      "sample-minor layout, NoAdjust table"}
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
-    kind, threads, run, _ = cpu_reference_rate()
+    kind, threads, run, words = cpu_reference_rate()
     # calibrate the step size: ~2 s of CPU work per step
     pairs, elapsed, _ = sample_rate(run, 1.0)
     rate = pairs / elapsed
@@ -235,6 +255,10 @@ def run_reference_arm(args, rank, world):
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if not args.no_ref_gpu:
+        ref_gpu = reference_gpu_rate(words, max(1, min(args.steps, 5)))
+        if ref_gpu is not None:
+            line["reference_gpu_kernel"] = ref_gpu
     print(json.dumps(line), flush=True)
 
 
@@ -389,10 +413,21 @@ def run_serving(ctx, dev, n_requests=120, rate_hz=10.0):
     th.start()
     th.join()
     lat = np.zeros(n_requests)
+    check = [i for i in range(n_requests) if sizes[i] <= 500][:8]
+    mixed = {}
     for i in range(n_requests):
         server.wait(tickets[i], timeout=600)
-        lat[i] = server.result(tickets[i])[3]
+        idx, dist, _, lat[i] = server.result(tickets[i])
+        if i in check:
+            mixed[i] = (idx, dist)
     makespan = time.perf_counter() - t_begin
+    # the same requests again, one at a time on an idle server
+    alone_equal = True
+    for i in check:
+        t = server.submit(qwords[starts[i]:starts[i] + sizes[i]])
+        server.wait(t, timeout=600)
+        idx, dist, _, _ = server.result(t)
+        alone_equal &= bool(np.array_equal(idx, mixed[i][0]) and np.array_equal(dist, mixed[i][1]))
     server.close()
     ref.close()
     pairs = int(sizes.sum()) * n_ref
@@ -407,6 +442,60 @@ def run_serving(ctx, dev, n_requests=120, rate_hz=10.0):
         "p50_ms_batches_50_200": pct(lat[mid], 50), "p99_ms_batches_50_200": pct(lat[mid], 99),
         "n_batches_50_200": int(mid.sum()),
         "slots": 4, "slice_queries": 128,
+        "alone_vs_mixed_equal": alone_equal, "alone_vs_mixed_requests": len(check),
+    }
+
+
+# ------------------------------------------------------------ large (config 3)
+
+LARGE_SEED = 0x5EED0003
+LARGE_N = 31_610
+
+
+def run_large(ctx, dev, lop3_peak, launches=2, knn=10):
+    """31,610 samples (200 clades, log-normal sizes), K = 8, sketchsize64 156:
+    499,580,245 pairs written to a 4.0 GB device long form, then the
+    kNN = 10 sparse graph (316,100 entries) through sk_dists_knn."""
+    import torch
+    from sketchlib_b200 import capi, synth
+    n = LARGE_N
+    parent, thresh = synth.clade_tree(n, n_clades=200, kmers=KMERS, seed=LARGE_SEED)
+    words = torch.empty(n * len(KMERS) * S64 * BBITS, dtype=torch.int64, device=dev)
+    capi.synth_device(ctx, parent, thresh, S64, seed=LARGE_SEED, d_words=words.data_ptr())
+    db = capi.Database(ctx, words.data_ptr(), KMERS, S64, n_samples=n)
+    del words
+    pairs = n_pairs(n)
+    out = torch.empty((pairs, 2), dtype=torch.float32, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    ctx.set_stream(stream.cuda_stream)
+    capi.dists_dense(ctx, db, out=out.data_ptr())          # warm-up
+    ctx.synchronize()
+    times = []
+    with torch.cuda.stream(stream):
+        for _ in range(launches):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            capi.dists_dense(ctx, db, out=out.data_ptr())
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1) / 1e3)
+    finite = bool(torch.isfinite(out).all().item())
+    del out
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    i, j, d = capi.dists_knn(ctx, db, knn, dist_col=0)
+    knn_s = time.perf_counter() - t0
+    db.close()
+    sec = sum(times) / len(times)
+    return {
+        "workload": "31,610 samples, 200 clades (log-normal sizes), 8 k x 10k bins, "
+                    "float32 long form in HBM (4.0 GB) + kNN = 10 sparse graph",
+        "n_samples": n, "pairs": pairs, "value": pairs / sec, "unit": UNIT,
+        "ms_per_launch": 1e3 * sec, "launches": launches,
+        "lop3_frac": pairs * LOP3_PER_PAIR / sec / lop3_peak,
+        "knn": {"k": knn, "entries": int(len(i)), "ms": 1e3 * knn_s,
+                "timing": "host clock around sk_dists_knn (distance kernel + top-k + D2H)"},
+        "all_finite": finite,
     }
 
 
@@ -485,6 +574,8 @@ def run_ours(args, rank, world, local):
         extra["batched"] = run_batched(ctx, dev, lop3_peak)
     if not args.skip_serving:
         extra["serving"] = run_serving(ctx, dev)
+    if world == 1 and not args.skip_large:
+        extra["large"] = run_large(ctx, dev, lop3_peak)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -561,6 +652,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-batched", action="store_true")
     ap.add_argument("--skip-serving", action="store_true")
+    ap.add_argument("--skip-large", action="store_true",
+                    help="skip the 31,610-sample all-vs-all + kNN = 10 measurement")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="--impl reference: skip timing the reference's GPU kernel")
     ap.add_argument("--profile", type=int, default=0,
                     help="run only N-sample dense launches (a small case for ncu)")
     ap.add_argument("--profile-launches", type=int, default=2)

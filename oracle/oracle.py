@@ -1,5 +1,6 @@
 """ctypes wrapper of the CPU oracle (sk_oracle.c) and of the reference
-harness built from the reference sources (_ref/libref_querydb.so).
+harness built from the reference sources (_ref/libref_querydb.so, the
+reference sketcher _ref/libref_sketch.so and GPU kernel _ref/libref_gpu.so).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
 cpu_baseline / --impl reference legs of bench.py, as the checker and the CPU
@@ -278,3 +279,48 @@ class RefSketcher:
 
 def sketcher_available() -> bool:
     return SKETCH_PATH.exists()
+
+
+REF_GPU_PATH = HERE / "_ref" / "libref_gpu.so"
+
+
+class RefGpuKernel:
+    """The reference's own GPU distance kernel (`calculate_dists`,
+    src/gpu/dist.cu:164-317), compiled for sm_100a from the reference sources
+    and launched by oracle/ref_gpu_dists.cu the way dispatchDists does
+    (src/gpu/dist.cu:408-470).  Baseline on the same GPU; not the checker of
+    record (its float regression and first-low-k truncation differ from the
+    reference's CPU semantics)."""
+
+    def __init__(self):
+        if not REF_GPU_PATH.exists():
+            raise FileNotFoundError(f"{REF_GPU_PATH} not built (needs the reference sources)")
+        lib_ = C.CDLL(str(REF_GPU_PATH))
+        lib_.refgpu_self_dists.restype = C.c_int
+        lib_.refgpu_self_dists.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int, C.c_int,
+                                           C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                                           C.POINTER(C.c_double), C.c_char_p, C.c_int]
+        self.lib = lib_
+
+    def self_dists(self, words, kmers, s64, random_k=None, warmup=0, launches=1, want_out=True,
+                   bbits=14):
+        """All-vs-all (core, accessory) of `words` [n][K][s64*bbits]: returns
+        (float32 (n(n-1)/2, 2) or None, mean ms per timed launch)."""
+        w = np.ascontiguousarray(words, np.uint64)
+        n = w.shape[0]
+        km = np.ascontiguousarray(kmers, np.int32)
+        rk = None if random_k is None else np.ascontiguousarray(random_k, np.float32)
+        out = np.zeros((n * (n - 1) // 2, 2), np.float32) if want_out else None
+        ms = C.c_double(0.0)
+        err = C.create_string_buffer(512)
+        rc = self.lib.refgpu_self_dists(w.ctypes.data, n, km.ctypes.data, len(km), s64, bbits,
+                                        None if rk is None else rk.ctypes.data, warmup, launches,
+                                        None if out is None else out.ctypes.data, C.byref(ms),
+                                        err, len(err))
+        if rc != 0:
+            raise RuntimeError(err.value.decode())
+        return out, ms.value
+
+
+def ref_gpu_available() -> bool:
+    return REF_GPU_PATH.exists()

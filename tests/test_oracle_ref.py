@@ -38,3 +38,11 @@ def test_query_db_loop_matches_reference():
     assert np.abs(ref_out - f32).max() < 1e-5
     f64 = oracle.dists(words, kmers, 156, regress=0, threads=4)
     assert np.abs(ref_out - f64).max() < 1e-5
+
+
+@pytest.mark.skipif(not oracle.ref_gpu_available(), reason="oracle/_ref/libref_gpu.so not built")
+def test_reference_gpu_harness_loads():
+    """The reference GPU kernel harness loads on a host without a GPU (its
+    launches run only in the GPU tests and the reference arm of the bench)."""
+    k = oracle.RefGpuKernel()
+    assert hasattr(k.lib, "refgpu_self_dists")
