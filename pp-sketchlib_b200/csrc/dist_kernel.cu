@@ -11,8 +11,9 @@
 //     acc = AND over planes of ~(row_word ^ col_word)   (one LOP3 per plane)
 //     count += popc(acc)                                 (POPC + IMAD)
 // which is calc_intersize (src/dist/dist.cpp:50-78) for 32 bins at a time,
-// releases the stage with a per-stage named barrier (only warp 0, which
-// refills, waits on it), parks its per-k counts in L2-resident scratch, and
+// releases the stage with a per-stage named barrier (only the step's refill
+// warp, rotating over the SM's sub-partitions, waits on it and issues the
+// next copies), parks its per-k counts in L2-resident scratch, and
 // after an item's last k turns its own pairs into random-corrected Jaccards
 // and the log-linear core/accessory fit, written straight to the long form.
 //
@@ -59,28 +60,36 @@ struct TileShape {
   static_assert(TQ % 4 == 0 && TR % 4 == 0, "128-bit shared loads");
   static_assert(kPairsPerThread % 8 == 0, "counts are stored as 16-byte groups");
   static_assert(QT % RT == 0, "triangular map needs tile_rows multiple of tile_cols");
-  static_assert(STAGES >= 2 && STAGES <= 4, "one named barrier (ids 1..4) per stage");
+  static_assert(STAGES >= 2 && STAGES <= 8, "one named barrier (ids 1..8) per stage");
   static_assert(kThreads % 32 == 0, "whole warps");
 };
 
-// Per-stage named barriers 1..4 with literal ids (the hardware reserves only
-// the ids a kernel names).
-template <int NT>
+// Per-stage named barriers 1..STAGES with literal ids (the hardware reserves
+// only the ids a kernel names, so each instance names only its own).
+template <int NT, int STAGES>
 __device__ __forceinline__ void stage_sync(int s) {
   switch (s) {
     case 0: asm volatile("bar.sync 1, %0;" ::"n"(NT) : "memory"); break;
-    case 1: asm volatile("bar.sync 2, %0;" ::"n"(NT) : "memory"); break;
-    case 2: asm volatile("bar.sync 3, %0;" ::"n"(NT) : "memory"); break;
-    default: asm volatile("bar.sync 4, %0;" ::"n"(NT) : "memory"); break;
+    case 1: if constexpr (STAGES > 1) asm volatile("bar.sync 2, %0;" ::"n"(NT) : "memory"); break;
+    case 2: if constexpr (STAGES > 2) asm volatile("bar.sync 3, %0;" ::"n"(NT) : "memory"); break;
+    case 3: if constexpr (STAGES > 3) asm volatile("bar.sync 4, %0;" ::"n"(NT) : "memory"); break;
+    case 4: if constexpr (STAGES > 4) asm volatile("bar.sync 5, %0;" ::"n"(NT) : "memory"); break;
+    case 5: if constexpr (STAGES > 5) asm volatile("bar.sync 6, %0;" ::"n"(NT) : "memory"); break;
+    case 6: if constexpr (STAGES > 6) asm volatile("bar.sync 7, %0;" ::"n"(NT) : "memory"); break;
+    case 7: if constexpr (STAGES > 7) asm volatile("bar.sync 8, %0;" ::"n"(NT) : "memory"); break;
   }
 }
-template <int NT>
+template <int NT, int STAGES>
 __device__ __forceinline__ void stage_arrive(int s) {
   switch (s) {
     case 0: asm volatile("bar.arrive 1, %0;" ::"n"(NT) : "memory"); break;
-    case 1: asm volatile("bar.arrive 2, %0;" ::"n"(NT) : "memory"); break;
-    case 2: asm volatile("bar.arrive 3, %0;" ::"n"(NT) : "memory"); break;
-    default: asm volatile("bar.arrive 4, %0;" ::"n"(NT) : "memory"); break;
+    case 1: if constexpr (STAGES > 1) asm volatile("bar.arrive 2, %0;" ::"n"(NT) : "memory"); break;
+    case 2: if constexpr (STAGES > 2) asm volatile("bar.arrive 3, %0;" ::"n"(NT) : "memory"); break;
+    case 3: if constexpr (STAGES > 3) asm volatile("bar.arrive 4, %0;" ::"n"(NT) : "memory"); break;
+    case 4: if constexpr (STAGES > 4) asm volatile("bar.arrive 5, %0;" ::"n"(NT) : "memory"); break;
+    case 5: if constexpr (STAGES > 5) asm volatile("bar.arrive 6, %0;" ::"n"(NT) : "memory"); break;
+    case 6: if constexpr (STAGES > 6) asm volatile("bar.arrive 7, %0;" ::"n"(NT) : "memory"); break;
+    case 7: if constexpr (STAGES > 7) asm volatile("bar.arrive 8, %0;" ::"n"(NT) : "memory"); break;
   }
 }
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
@@ -89,12 +98,16 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 
 // Count scratch layout (per CTA slot, and per split slot): [k][threads][pairs
 // per thread] uint16; a thread writes and reads back only its own entries.
-template <int QT, int RT, int TQ, int TR, int STAGES, int MINB>
+// ROT: the refill duty (wait for every warp on the stage barrier, then issue
+// the next copies) moves round-robin over warps 0..ROT-1, one per SM
+// sub-partition for ROT = 4, so no scheduler carries all of it.
+template <int QT, int RT, int TQ, int TR, int STAGES, int MINB, int ROT>
 __global__ void __launch_bounds__((QT / TQ) * (RT / TR), MINB)
     dist_items_kernel(const LaunchParams lp) {
   using S = TileShape<QT, RT, TQ, TR, STAGES>;
   constexpr int NT = S::kThreads;
   constexpr int PT = S::kPairsPerThread;
+  static_assert(ROT >= 1 && ROT <= NT / 32, "refill warps must exist");
   constexpr int TCOLS = RT / TR;
 
   extern __shared__ __align__(128) unsigned char smem[];
@@ -106,6 +119,7 @@ __global__ void __launch_bounds__((QT / TQ) * (RT / TR), MINB)
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
+  const int lane = tid & 31;
   const int tq = tid / TCOLS;
   const int tr = tid % TCOLS;
   const int row0 = tq * TQ;   // first tile row of this thread
@@ -134,9 +148,9 @@ __global__ void __launch_bounds__((QT / TQ) * (RT / TR), MINB)
     ps.have = 0;
   }
 
-  auto produce = [&](int64_t u) {
+  // fills stage s with the next step of the stream (called in step order)
+  auto produce = [&](int s) {
     if (ps.done) return;
-    const int s = static_cast<int>(u % STAGES);
     if (s_abort != 0) {   // a consumer timed out: end the stream now
       meta[s].flags = kStepEnd;
       mbar_arrive(&full_bar[s]);
@@ -205,20 +219,25 @@ __global__ void __launch_bounds__((QT / TQ) * (RT / TR), MINB)
   };
 
   if (tid == 0) {
-    for (int64_t u = 0; u < STAGES; ++u) produce(u);
+    for (int u = 0; u < STAGES; ++u) produce(u);
   }
 
   // ---------------------------------------------------------------- consumers
-  const uint32_t one = lp.jobs[0].one;   // 1 at run time (count multiply-adds on the FMA pipe)
-  uint32_t cnt[TQ][TR];
+  // Counts of one k for columns 2c and 2c + 1 share a register (low / high
+  // 16 bits): at most 64 * sketchsize64 <= 65,472 per k, so the low half never
+  // carries.  `one` is 1 at run time, which keeps the count multiply-adds on
+  // the FMA pipe and the ALU free for the LOP3s.
+  const uint32_t one = lp.jobs[0].one;
+  const uint32_t hi_one = one << 16;
+  uint32_t cnt[TQ][TR / 2];
 #pragma unroll
   for (int i = 0; i < TQ; ++i)
 #pragma unroll
-    for (int j = 0; j < TR; ++j) cnt[i][j] = 0;
+    for (int j = 0; j < TR / 2; ++j) cnt[i][j] = 0;
 
-  for (int64_t t = 0;; ++t) {
-    const int s = static_cast<int>(t % STAGES);
-    const uint32_t parity = static_cast<uint32_t>((t / STAGES) & 1);
+  int s = 0;              // stage of step t
+  uint32_t parity = 0;    // phase parity of step t on that stage
+  for (uint32_t t = 0;; ++t) {
     StepMeta m;
     if (mbar_wait_bounded(&full_bar[s], parity, kWaitLimitNs)) {
       m = meta[s];
@@ -263,16 +282,27 @@ __global__ void __launch_bounds__((QT / TQ) * (RT / TR), MINB)
 #pragma unroll
       for (int i = 0; i < TQ; ++i)
 #pragma unroll
-        for (int j = 0; j < TR; ++j) cnt[i][j] = mad_u32(__popc(acc[i][j]), one, cnt[i][j]);
+        for (int j = 0; j < TR / 2; ++j)
+          cnt[i][j] = mad_u32(__popc(acc[i][2 * j + 1]), hi_one,
+                              mad_u32(__popc(acc[i][2 * j]), one, cnt[i][j]));
     }
 
-    // release the stage: warp 0 (which holds the producer) waits for every
-    // warp, the others only arrive and run ahead into the stages already armed
-    if (warp == 0) {
-      stage_sync<NT>(s);
-      if (tid == 0) produce(t + STAGES);
+    // release the stage: the refill warp of this step waits for every warp
+    // and refills it with step t + STAGES; the others only arrive and run
+    // ahead into the stages already armed.  A warp arrives at barrier s for
+    // step t + STAGES only after that refill armed it, so barrier
+    // generations never mix, and the producer state written by one refill
+    // is published to the next refill warp by the barrier itself.
+    const int refill_warp = ROT > 1 ? static_cast<int>(t % ROT) : 0;
+    if (warp == refill_warp) {
+      stage_sync<NT, STAGES>(s);
+      if (lane == 0) produce(s);
     } else {
-      stage_arrive<NT>(s);
+      stage_arrive<NT, STAGES>(s);
+    }
+    if (++s == STAGES) {
+      s = 0;
+      parity ^= 1u;
     }
 
     if (m.flags & kStepLastOfK) {
@@ -280,21 +310,18 @@ __global__ void __launch_bounds__((QT / TQ) * (RT / TR), MINB)
       uint16_t *base = m.split >= 0
                            ? lp.split_scratch + m.split * slot_size + static_cast<int64_t>(tid) * PT
                            : my_counts;
+      // pair q = i * TR + j is uint16 q of the slot: word q / 2 = cnt[i][j / 2]
       uint4 *dst = reinterpret_cast<uint4 *>(base + m.kidx * slot_k_stride);
+      constexpr int CW = TR / 2;
 #pragma unroll
-      for (int w = 0; w < PT / 8; ++w) {
-        uint32_t packed[4];
-#pragma unroll
-        for (int h = 0; h < 4; ++h) {
-          const int q0 = w * 8 + 2 * h, q1 = q0 + 1;
-          packed[h] = cnt[q0 / TR][q0 % TR] | (cnt[q1 / TR][q1 % TR] << 16);
-        }
-        dst[w] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
-      }
+      for (int w = 0; w < PT / 8; ++w)
+        dst[w] = make_uint4(cnt[(4 * w) / CW][(4 * w) % CW], cnt[(4 * w + 1) / CW][(4 * w + 1) % CW],
+                            cnt[(4 * w + 2) / CW][(4 * w + 2) % CW],
+                            cnt[(4 * w + 3) / CW][(4 * w + 3) % CW]);
 #pragma unroll
       for (int i = 0; i < TQ; ++i)
 #pragma unroll
-        for (int j = 0; j < TR; ++j) cnt[i][j] = 0;
+        for (int j = 0; j < TR / 2; ++j) cnt[i][j] = 0;
     }
 
     if (m.flags & kStepLastOfItem) {
@@ -342,37 +369,38 @@ namespace {
 
 // Raises the instance's dynamic shared memory limit once (before any launch,
 // so never inside a stream capture).
-template <int QT, int RT, int TQ, int TR, int STAGES, int MINB>
+template <int QT, int RT, int TQ, int TR, int STAGES, int MINB, int ROT>
 cudaError_t ensure_smem_attr() {
   using S = TileShape<QT, RT, TQ, TR, STAGES>;
   static cudaError_t status = cudaFuncSetAttribute(
-      dist_items_kernel<QT, RT, TQ, TR, STAGES, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-      S::kSmemBytes);
+      dist_items_kernel<QT, RT, TQ, TR, STAGES, MINB, ROT>,
+      cudaFuncAttributeMaxDynamicSharedMemorySize, S::kSmemBytes);
   return status;
 }
 
-template <int QT, int RT, int TQ, int TR, int STAGES, int MINB>
+template <int QT, int RT, int TQ, int TR, int STAGES, int MINB, int ROT>
 cudaError_t launch_cfg(const LaunchParams &lp, int grid, cudaStream_t stream) {
   using S = TileShape<QT, RT, TQ, TR, STAGES>;
-  cudaError_t e = ensure_smem_attr<QT, RT, TQ, TR, STAGES, MINB>();
+  cudaError_t e = ensure_smem_attr<QT, RT, TQ, TR, STAGES, MINB, ROT>();
   if (e != cudaSuccess) return e;
-  dist_items_kernel<QT, RT, TQ, TR, STAGES, MINB><<<grid, S::kThreads, S::kSmemBytes, stream>>>(lp);
+  dist_items_kernel<QT, RT, TQ, TR, STAGES, MINB, ROT>
+      <<<grid, S::kThreads, S::kSmemBytes, stream>>>(lp);
   return cudaGetLastError();
 }
 
-template <int QT, int RT, int TQ, int TR, int STAGES, int MINB>
+template <int QT, int RT, int TQ, int TR, int STAGES, int MINB, int ROT>
 int occupancy_cfg() {
   using S = TileShape<QT, RT, TQ, TR, STAGES>;
-  if (ensure_smem_attr<QT, RT, TQ, TR, STAGES, MINB>() != cudaSuccess) return 0;
+  if (ensure_smem_attr<QT, RT, TQ, TR, STAGES, MINB, ROT>() != cudaSuccess) return 0;
   int blocks = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-          &blocks, dist_items_kernel<QT, RT, TQ, TR, STAGES, MINB>, S::kThreads,
+          &blocks, dist_items_kernel<QT, RT, TQ, TR, STAGES, MINB, ROT>, S::kThreads,
           S::kSmemBytes) != cudaSuccess)
     return 0;
   return blocks;
 }
 
-template <int QT, int RT, int TQ, int TR, int STAGES, int MINB>
+template <int QT, int RT, int TQ, int TR, int STAGES, int MINB, int ROT = 1>
 constexpr TileConfig make_cfg(int id) {
   return TileConfig{id,
                     QT,
@@ -383,12 +411,12 @@ constexpr TileConfig make_cfg(int id) {
                     STAGES,
                     TileShape<QT, RT, TQ, TR, STAGES>::kThreads,
                     TileShape<QT, RT, TQ, TR, STAGES>::kSmemBytes,
-                    &launch_cfg<QT, RT, TQ, TR, STAGES, MINB>,
-                    &occupancy_cfg<QT, RT, TQ, TR, STAGES, MINB>};
+                    &launch_cfg<QT, RT, TQ, TR, STAGES, MINB, ROT>,
+                    &occupancy_cfg<QT, RT, TQ, TR, STAGES, MINB, ROT>};
 }
 
 const TileConfig kConfigs[] = {
-    make_cfg<128, 128, 8, 4, 4, 1>(1),  // default: 512 threads, 16 warps, one CTA per SM
+    make_cfg<128, 128, 8, 4, 4, 1, 4>(1),  // default: 512 threads, 16 warps, one CTA per SM
     make_cfg<128, 64, 8, 4, 4, 2>(2),   // 256 threads, two CTAs per SM
     make_cfg<64, 64, 4, 4, 4, 2>(3),    // small tiles, 16 pairs per thread
     make_cfg<128, 128, 8, 8, 4, 1>(4),  // 256 threads, 64 pairs per thread

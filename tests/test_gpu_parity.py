@@ -110,7 +110,7 @@ def test_jaccard_and_coreacc(gpu_ctx, mode, self_):
     assert np.mean(ca == want64) > 0.99
 
 
-@pytest.mark.parametrize("cfg", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("cfg", [c["id"] for c in capi.tile_configs()])
 def test_every_tile_shape_agrees(gpu_ctx, cfg):
     info = {c["id"]: c for c in capi.tile_configs()}[cfg]
     K = min(4, info["max_kmers"])
@@ -126,6 +126,26 @@ def test_every_tile_shape_agrees(gpu_ctx, cfg):
         gpu_ctx.set_tile_config(0)
     np.testing.assert_array_equal(got, oracle.dists(words, kmers, 16, out_mode=2))
     np.testing.assert_array_equal(gotq, oracle.dists(words, kmers, 16, query_words=qw, out_mode=2))
+
+
+@pytest.mark.parametrize("cfg", [1, 4])
+def test_counts_at_the_maximum_sketch_width(gpu_ctx, cfg):
+    """sketchsize64 1023: identical samples count 64 * 1023 = 65,472 bins per
+    k, the most a 16-bit count holds; two counts share a register in the
+    kernel, so a carry out of the low half would corrupt the neighbour."""
+    s64, K = 1023, 2
+    words, kmers = random_sketches(40, K, s64, seed=77, related=False)
+    words[1::3] = words[0]                      # many identical pairs
+    words[2, :, :] = ~words[0]                  # all planes differ from sample 0
+    db = _db(gpu_ctx, words, kmers, s64)
+    gpu_ctx.set_tile_config(cfg)
+    try:
+        got = capi.dists_dense(gpu_ctx, db, out_mode=capi.OUT_COUNTS)
+    finally:
+        gpu_ctx.set_tile_config(0)
+    want = oracle.dists(words, kmers, s64, out_mode=2)
+    assert want.max() == 64 * s64
+    np.testing.assert_array_equal(got, want)
 
 
 def test_pack_roundtrip_and_synth_device(gpu_ctx):
