@@ -553,21 +553,31 @@ def run_ours(args, rank, world, local):
     ho = host_out.numpy()
 
     def e2e_step():
+        # one sk_query_db call: chunked upload overlapped with the kernel
+        capi.query_db(ctx, hw, KMERS, S64, out=ho)
+
+    def e2e_step_unpipelined():
+        # upload, then compute, then copy back (sk_db_create + sk_dists_dense)
         d = capi.Database(ctx, hw, KMERS, S64)
         capi.dists_dense(ctx, d, out=ho)
         d.close()
 
-    for _ in range(min(args.warmup, 3)):
-        e2e_step()
+    def time_e2e(step, n):
+        for _ in range(min(args.warmup, 3)):
+            step()
+        barrier(world, local)
+        t0 = time.perf_counter()
+        for _ in range(n):
+            step()
+        return reduce_max(time.perf_counter() - t0, world, dev)
+
     e2e_steps = max(1, min(args.steps, args.e2e_steps))
-    barrier(world, local)
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        e2e_step()
-    e2e_s = reduce_max(time.perf_counter() - t0, world, dev)
+    e2e_s = time_e2e(e2e_step, e2e_steps)
     e2e_value = pairs * world * e2e_steps / e2e_s
     # the e2e result must be the resident run's result
     ok = bool(torch.equal(host_out, out.cpu()))
+    seq_s = time_e2e(e2e_step_unpipelined, e2e_steps)
+    ok = ok and bool(torch.equal(host_out, out.cpu()))
 
     extra = {}
     if not args.skip_batched:
@@ -607,7 +617,11 @@ def run_ours(args, rank, world, local):
         "e2e": {"value": e2e_value, "unit": UNIT,
                 "h2d_bytes_per_step": int(host_words.numel() * 8),
                 "d2h_bytes_per_step": int(host_out.numel() * 4),
-                "steps": e2e_steps, "matches_resident_result": ok},
+                "steps": e2e_steps, "matches_resident_result": ok,
+                "call": "sk_query_db (upload in sample chunks on a copy stream, each chunk's "
+                        "tiles computed while the next copies)",
+                "unpipelined": {"value": pairs * world * e2e_steps / seq_s,
+                                "call": "sk_db_create + sk_dists_dense"}},
         "gpu_launches": args.steps,
         "clocks": clocks.summary(),
         "kernel_ms": {"mean": statistics.mean(step_ms), "min": min(step_ms),

@@ -24,7 +24,9 @@
  *                              (src/gpu/gpu_api.cpp:352-494, src/gpu/dist.cu:164-317, 408-489)
  *                              and, for SK_OUT_JACCARD, the CPU-only jaccard branch of
  *                              query_db (src/api.cpp:206-211, 256-260)
- *   sk_dists_knn            <- query_db_sparse_cuda / sparseDists
+ *   sk_query_db             <- query_db_cuda as one host-in / host-out call
+ *                              (src/gpu/gpu_api.cpp:352-494)
+ *   sk_dists_knn         <- query_db_sparse_cuda / sparseDists
  *                              (src/gpu/gpu_api.cpp:496-531, src/gpu/dist.cu:495-791) and
  *                              query_db_sparse (src/api.cpp:332-432)
  *   sk_sparse_threshold     <- sparsify_dists_by_threshold (src/dist/matrix_ops.cpp:38-69)
@@ -168,6 +170,29 @@ int64_t sk_dists_rows(const sk_db *ref, const sk_db *query);
 sk_status sk_dists_dense(sk_ctx *ctx, const sk_db *ref, const sk_db *query,
                          const sk_random *random, int32_t out_mode, void *out,
                          int32_t out_on_device);
+
+/* Host sketches of one side of a query_db call. */
+typedef struct sk_host_sketches {
+  const uint64_t *words;     /* [n][n_kmers][sketchsize64 * bbits], reference layout */
+  int64_t n;                 /* samples */
+  const uint16_t *cluster;   /* [n] random-match cluster ids, or NULL */
+  const uint64_t *seq_len;   /* [n] sequence lengths, or NULL */
+} sk_host_sketches;
+
+/* Host sketches in, host distances out, in one call: the shape of
+ * query_db_cuda (src/gpu/gpu_api.cpp:352-494, what queryDatabase(use_gpu=True)
+ * runs).  query == NULL: all-vs-all of ref.  The sketch words go up in sample
+ * chunks on a second stream; each chunk is packed as it lands and the tiles
+ * whose samples have all arrived are computed while the next chunk is in
+ * flight, so the host-to-device copy overlaps the distance kernel.  `out` is a
+ * host buffer of sk_dists_rows-equivalent rows (n(n-1)/2 or n_query * n_ref)
+ * in the layout of out_mode; results are identical to sk_db_create +
+ * sk_dists_dense.  Pinned host buffers give the full copy rate; pageable ones
+ * work. */
+sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
+                      const sk_host_sketches *query, const int32_t *kmers,
+                      int32_t n_kmers, int32_t sketchsize64, int32_t bbits,
+                      const sk_random *random, int32_t out_mode, void *out);
 
 /* Self kNN (querySelfSparse with kNN > 0, src/sketchlib_bindings.cpp:136-187):
  * for every sample i, the kNN smallest distances d(i, j), j != i, of column

@@ -33,9 +33,11 @@ __device__ __forceinline__ int64_t condensed(int64_t i, int64_t j, int64_t n) {
 
 // One CTA per (k, 64-bin block, granule): reads the 64 samples' 14 words of
 // the block (112 contiguous bytes per sample) into shared memory and writes
-// the two 32-bin stripes (3584 contiguous bytes each).
+// the two 32-bin stripes (3584 contiguous bytes each).  `words` holds n
+// samples that become granules g0 .. g0 + ng - 1 of an array of ng_total
+// granules (samples past n are written as zeros).
 __global__ void pack_kernel(const uint64_t *__restrict__ words, int64_t n, int n_kmers, int s64,
-                            int ng, uint32_t *__restrict__ packed) {
+                            int ng, int g0, int ng_total, uint32_t *__restrict__ packed) {
   __shared__ uint64_t tile[kGranule * kBbits];
   const int64_t nblocks = static_cast<int64_t>(n_kmers) * s64 * ng;
   const int nb = 2 * s64;
@@ -55,7 +57,8 @@ __global__ void pack_kernel(const uint64_t *__restrict__ words, int64_t n, int n
       const int h = e / kStripeWords, w = e % kStripeWords;
       const uint64_t v = tile[w];
       const int64_t blk = static_cast<int64_t>(k) * nb + 2 * b64 + h;
-      packed[(blk * ng + g) * kStripeWords + w] = static_cast<uint32_t>(h ? (v >> 32) : v);
+      packed[(blk * ng_total + g0 + g) * kStripeWords + w] =
+          static_cast<uint32_t>(h ? (v >> 32) : v);
     }
     __syncthreads();
   }
@@ -299,9 +302,16 @@ __global__ void square_to_long_kernel(const float *__restrict__ square, int64_t 
 
 cudaError_t launch_pack(const uint64_t *words, int64_t n, int32_t n_kmers, int32_t s64, int32_t ng,
                         uint32_t *packed, cudaStream_t stream) {
+  return launch_pack_range(words, n, n_kmers, s64, ng, 0, ng, packed, stream);
+}
+
+cudaError_t launch_pack_range(const uint64_t *words, int64_t n, int32_t n_kmers, int32_t s64,
+                              int32_t ng, int32_t g0, int32_t ng_total, uint32_t *packed,
+                              cudaStream_t stream) {
   const int64_t items = static_cast<int64_t>(n_kmers) * s64 * ng;
+  if (items == 0) return cudaSuccess;
   pack_kernel<<<grid_for(items, 1, 148 * 64), kThreads, 0, stream>>>(words, n, n_kmers, s64, ng,
-                                                                     packed);
+                                                                     g0, ng_total, packed);
   return cudaGetLastError();
 }
 

@@ -58,6 +58,14 @@ static void ctx_free(sk_ctx *ctx) {
     if (ctx->status_dev) cudaFree(ctx->status_dev);
     if (ctx->cancel_host) cudaFreeHost(ctx->cancel_host);
     if (ctx->stream && ctx->own_stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->copy_stream) {
+      cudaStreamSynchronize(ctx->copy_stream);
+      cudaStreamDestroy(ctx->copy_stream);
+    }
+    for (int b = 0; b < 2; ++b) {
+      if (ctx->ev_landed[b]) cudaEventDestroy(ctx->ev_landed[b]);
+      if (ctx->ev_packed[b]) cudaEventDestroy(ctx->ev_packed[b]);
+    }
   }
   delete ctx;
 }
@@ -273,13 +281,20 @@ void plan_items(const std::vector<JobParams> &jobs, int grid, Plan &plan) {
     for (int64_t t = 0; t < jobs[j].n_tiles; ++t)
       plan.items.push_back(WorkItem{t, j, 0, static_cast<int16_t>(jobs[j].n_kmers), -1, 1});
   }
-  const int64_t T = static_cast<int64_t>(plan.items.size());
+  split_tail(plan.items, 0, grid, &plan.n_splits);
+}
+
+// Splits the last partial wave of items[begin..end) (whole tiles, k range
+// [0, K)) along k; split slots are numbered from 0 for this range.
+void split_tail(std::vector<WorkItem> &items, size_t begin, int grid, int32_t *n_splits) {
+  *n_splits = 0;
+  const int64_t T = static_cast<int64_t>(items.size() - begin);
   if (T == 0 || grid <= 0) return;
   const int64_t r = T % grid == 0 ? 0 : T % grid;
   if (r == 0) return;
   // tail tiles: the last r items; k is split by the smallest K among them
   int kmin = kMaxKmers;
-  for (int64_t i = T - r; i < T; ++i) kmin = std::min<int>(kmin, plan.items[i].k1);
+  for (size_t i = items.size() - r; i < items.size(); ++i) kmin = std::min<int>(kmin, items[i].k1);
   int best_p = 1;
   int64_t best = -1;
   for (int p = 1; p <= kmin; ++p) {
@@ -291,20 +306,20 @@ void plan_items(const std::vector<JobParams> &jobs, int grid, Plan &plan) {
     }
   }
   if (best_p == 1) return;
-  std::vector<WorkItem> tail(plan.items.end() - r, plan.items.end());
-  plan.items.resize(T - r);
+  std::vector<WorkItem> tail(items.end() - r, items.end());
+  items.resize(items.size() - r);
   int32_t slot = 0;
   for (const WorkItem &it : tail) {
     const int K = it.k1;
     const int parts = std::min(best_p, K);
     for (int q = 0; q < parts; ++q) {
       const int k0 = K * q / parts, k1 = K * (q + 1) / parts;
-      plan.items.push_back(WorkItem{it.tile, it.job, static_cast<int16_t>(k0),
-                                    static_cast<int16_t>(k1), slot, parts});
+      items.push_back(WorkItem{it.tile, it.job, static_cast<int16_t>(k0),
+                               static_cast<int16_t>(k1), slot, parts});
     }
     ++slot;
   }
-  plan.n_splits = slot;
+  *n_splits = slot;
 }
 
 // Device buffers for a plan: job table, work list, control block (queue
@@ -550,13 +565,17 @@ sk_status sk_ctx_load_tuning(sk_ctx *ctx, const char *path) {
 
 // ------------------------------------------------------------------ databases
 
-static sk_status db_create_impl(sk_ctx *ctx, const uint64_t *words, bool on_device, int64_t n,
-                                const int32_t *kmers, int32_t K, int32_t s64, int32_t bbits,
-                                sk_db **out) {
+}  // extern "C"
+
+namespace sk {
+
+// A database with its packed array allocated (contents not yet written); with
+// packed_slot >= 0 the array is that context scratch slot, kept across calls.
+sk_status db_alloc(sk_ctx *ctx, int64_t n, const int32_t *kmers, int32_t K, int32_t s64,
+                   int32_t bbits, sk_db **out, int packed_slot) {
   if (!out) return fail(ctx, SK_EINVAL, "null output handle");
   *out = nullptr;
   if (n < 0) return fail(ctx, SK_EINVAL, "negative sample count");
-  if (n > 0 && !words) return fail(ctx, SK_EINVAL, "null sketch words");
   if (bbits != kBbits)
     return fail(ctx, SK_ENOTSUP, "bbits %d not supported (sketches use %d bit planes)", bbits, kBbits);
   if (s64 < 1 || s64 > kMaxSketch64)
@@ -576,12 +595,55 @@ static sk_status db_create_impl(sk_ctx *ctx, const uint64_t *words, bool on_devi
   const int64_t npad = ((n + kSamplePad - 1) / kSamplePad) * kSamplePad;
   db->ng = static_cast<int32_t>(std::max<int64_t>(npad, kSamplePad) / kGranule);
   const size_t packed_words = static_cast<size_t>(K) * 2 * s64 * db->ng * kStripeWords;
-  cudaError_t e = cudaMalloc(&db->packed, packed_words * 4);
-  if (e != cudaSuccess) {
-    delete db;
-    ctx_release(ctx);
-    return cuda_fail(ctx, e, "sketch database allocation");
+  if (packed_slot >= 0) {
+    void *buf = nullptr;
+    sk_status st = scratch(ctx, packed_slot, packed_words * 4, &buf);
+    if (st != SK_OK) {
+      delete db;
+      ctx_release(ctx);
+      return st;
+    }
+    db->packed = static_cast<uint32_t *>(buf);
+    db->own_packed = false;
+  } else {
+    cudaError_t e = cudaMalloc(&db->packed, packed_words * 4);
+    if (e != cudaSuccess) {
+      delete db;
+      ctx_release(ctx);
+      return cuda_fail(ctx, e, "sketch database allocation");
+    }
   }
+  *out = db;
+  return SK_OK;
+}
+
+// Frees a database made by db_alloc (the context's stream must be idle).
+void db_free(sk_db *db) {
+  sk_ctx *ctx = db->ctx;
+  {
+    DeviceGuard g(ctx->device);
+    if (db->packed && db->own_packed) cudaFree(db->packed);
+    if (db->cluster) cudaFree(db->cluster);
+    if (db->jv) cudaFree(db->jv);
+  }
+  delete db;
+  ctx_release(ctx);
+}
+
+}  // namespace sk
+
+extern "C" {
+
+static sk_status db_create_impl(sk_ctx *ctx, const uint64_t *words, bool on_device, int64_t n,
+                                const int32_t *kmers, int32_t K, int32_t s64, int32_t bbits,
+                                sk_db **out) {
+  if (!out) return fail(ctx, SK_EINVAL, "null output handle");
+  *out = nullptr;
+  if (n > 0 && !words) return fail(ctx, SK_EINVAL, "null sketch words");
+  sk_db *db = nullptr;
+  sk_status st0 = db_alloc(ctx, n, kmers, K, s64, bbits, &db);
+  if (st0 != SK_OK) return st0;
+  cudaError_t e = cudaSuccess;
   const size_t in_words = static_cast<size_t>(n) * K * s64 * kBbits;
   const uint64_t *d_words = words;
   uint64_t *tmp = nullptr;
@@ -594,10 +656,8 @@ static sk_status db_create_impl(sk_ctx *ctx, const uint64_t *words, bool on_devi
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (tmp) cudaFree(tmp);
   if (e != cudaSuccess) {
-    cudaFree(db->packed);
-    delete db;
     sk_status st = cuda_fail(ctx, e, "sketch upload");
-    ctx_release(ctx);
+    db_free(db);
     return st;
   }
   *out = db;
@@ -621,16 +681,11 @@ sk_status sk_db_create_device(sk_ctx *ctx, const uint64_t *d_words, int64_t n_sa
 
 sk_status sk_db_destroy(sk_db *db) {
   if (!db) return SK_EINVAL;
-  sk_ctx *ctx = db->ctx;
   {
-    DeviceGuard g(ctx->device);
-    cudaStreamSynchronize(ctx->stream);
-    if (db->packed) cudaFree(db->packed);
-    if (db->cluster) cudaFree(db->cluster);
-    if (db->jv) cudaFree(db->jv);
+    DeviceGuard g(db->ctx->device);
+    cudaStreamSynchronize(db->ctx->stream);
   }
-  delete db;
-  ctx_release(ctx);
+  db_free(db);
   return SK_OK;
 }
 

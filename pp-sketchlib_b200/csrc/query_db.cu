@@ -1,0 +1,230 @@
+// query_db.cu -- host sketches in, host distances out, with the upload
+// overlapped with the distance kernel.
+//
+// The reference's query_db_cuda (src/gpu/gpu_api.cpp:352-494) flattens every
+// sketch on the host, copies them all, launches, waits, and copies the result
+// back, one step after another.  Here the reference-layout words go up in
+// sample chunks on the context's copy stream, double-buffered through a
+// device staging area; each chunk is packed on the compute stream as soon as
+// it lands, and the tiles whose samples have all arrived run as one
+// persistent launch while the next chunk is in flight.
+//
+//   self:  tile (ti, tj) reads samples up to max((ti+1) QT, (tj+1) RT) - 1, so
+//          it runs after the chunk holding that sample; chunk c adds the
+//          tiles of the (c+1)^2 - c^2 new block pairs.
+//   query: the query samples go up first, then the references in chunks;
+//          tile (ti, tj) runs after the reference chunk holding (tj+1) RT - 1.
+//
+// Each chunk's work list gets its own tail split (small early chunks are cut
+// along k to fill the GPU) and its own control block; the count scratch is
+// shared, as the launches run one after another on the compute stream.  The
+// packed arrays, staging area and output staging are context scratch, so a
+// repeated call allocates nothing.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <mutex>
+#include <vector>
+
+#include "sk_runtime.h"
+
+using namespace sk;
+
+namespace {
+
+constexpr int64_t kChunkAlign = 256;   // samples: a multiple of every tile side and of the padding
+constexpr int64_t kMinChunk = 512;     // samples per chunk at least (the copy must be worth a launch)
+constexpr int64_t kMaxChunks = 8;
+
+// Samples per chunk for n samples: about n / 8, at least 512, 256-aligned.
+int64_t chunk_samples(int64_t n) {
+  const int64_t c = std::clamp<int64_t>((n + kMinChunk - 1) / kMinChunk, 1, kMaxChunks);
+  const int64_t per = (n + c - 1) / c;
+  return std::max<int64_t>(kChunkAlign, (per + kChunkAlign - 1) / kChunkAlign * kChunkAlign);
+}
+
+sk_status ensure_pipeline(sk_ctx *ctx) {
+  cudaError_t e = cudaSuccess;
+  if (!ctx->copy_stream) e = cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking);
+  for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
+    if (!ctx->ev_landed[b]) e = cudaEventCreateWithFlags(&ctx->ev_landed[b], cudaEventDisableTiming);
+    if (e == cudaSuccess && !ctx->ev_packed[b])
+      e = cudaEventCreateWithFlags(&ctx->ev_packed[b], cudaEventDisableTiming);
+  }
+  return e == cudaSuccess ? SK_OK : cuda_fail(ctx, e, "copy stream setup");
+}
+
+// One host-to-device chunk.
+struct Unit {
+  sk_db *db;
+  const uint64_t *host;   // first word of the chunk
+  int64_t s0, n;          // first sample and sample count
+  int chunk;              // reference chunk whose tiles become runnable, or -1
+};
+
+// The databases of one call, released after both streams are idle.
+struct CallDbs {
+  sk_ctx *ctx;
+  sk_db *ref = nullptr, *query = nullptr;
+  ~CallDbs() {
+    if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+    cudaStreamSynchronize(ctx->stream);
+    if (ref) db_free(ref);
+    if (query) db_free(query);
+  }
+};
+
+sk_status make_side(sk_ctx *ctx, const sk_host_sketches *h, const int32_t *kmers, int32_t K,
+                    int32_t s64, int32_t bbits, int slot, sk_db **out) {
+  if (h->n < 0) return fail(ctx, SK_EINVAL, "negative sample count");
+  if (h->n > 0 && !h->words) return fail(ctx, SK_EINVAL, "null sketch words");
+  sk_status st = db_alloc(ctx, h->n, kmers, K, s64, bbits, out, slot);
+  if (st != SK_OK) return st;
+  if (h->cluster || h->seq_len) return sk_db_set_sample_info(*out, h->cluster, h->seq_len);
+  return SK_OK;
+}
+
+}  // namespace
+
+extern "C" sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
+                                 const sk_host_sketches *query, const int32_t *kmers,
+                                 int32_t n_kmers, int32_t sketchsize64, int32_t bbits,
+                                 const sk_random *random, int32_t out_mode, void *out) {
+  if (!ctx) return SK_EINVAL;
+  std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+  DeviceGuard dev(ctx->device);
+  sk_status st = begin_call(ctx);
+  if (st != SK_OK) return st;
+  if (!ref) return fail(ctx, SK_EINVAL, "null reference sketches");
+  if (out_mode != kOutCoreAcc && out_mode != kOutJaccard && out_mode != kOutCounts)
+    return fail(ctx, SK_EINVAL, "Unknown output mode %d", out_mode);
+  st = ensure_pipeline(ctx);
+  if (st != SK_OK) return st;
+
+  CallDbs dbs{ctx};
+  st = make_side(ctx, ref, kmers, n_kmers, sketchsize64, bbits, kSlotPackedRef, &dbs.ref);
+  if (st == SK_OK && query)
+    st = make_side(ctx, query, kmers, n_kmers, sketchsize64, bbits, kSlotPackedQuery, &dbs.query);
+  if (st != SK_OK) return st;
+  const int64_t pairs = n_pairs(dbs.ref, dbs.query);
+  if (pairs > 0 && !out) return fail(ctx, SK_EINVAL, "null output buffer");
+  if (pairs == 0) return finish_call(ctx);
+  const size_t out_sz = out_bytes(out_mode, pairs, n_kmers);
+  void *d_out = nullptr;
+  st = scratch(ctx, kSlotOut, out_sz, &d_out);
+  if (st != SK_OK) return st;
+
+  JobParams jp;
+  const TileConfig *cfg = nullptr;
+  st = build_job(ctx, dbs.ref, dbs.query, random, out_mode, 0, d_out, &cfg, &jp);
+  if (st != SK_OK) return st;
+  const int grid = resident_grid(ctx, *cfg);
+  if (grid < 1) return fail(ctx, SK_ECUDA, "Tile configuration %d does not fit the device", cfg->id);
+
+  // ---- work lists, one per reference chunk
+  const int64_t n_ref = dbs.ref->n;
+  const int64_t cs = chunk_samples(n_ref);
+  const int n_chunks = static_cast<int>((n_ref + cs - 1) / cs);
+  std::vector<std::vector<int64_t>> bucket(n_chunks);
+  {
+    int64_t tile = 0;
+    const int64_t m = jp.tile_rows / jp.tile_cols;
+    for (int64_t ti = 0; ti < jp.n_row_tiles; ++ti) {
+      const int64_t tj0 = jp.self ? ti * m : 0;
+      for (int64_t tj = tj0; tj < jp.n_col_tiles; ++tj, ++tile) {
+        const int64_t last_col = std::min<int64_t>((tj + 1) * jp.tile_cols, n_ref) - 1;
+        const int64_t last_row = jp.self ? std::min<int64_t>((ti + 1) * jp.tile_rows, n_ref) - 1 : 0;
+        bucket[std::max(last_col, last_row) / cs].push_back(tile);
+      }
+    }
+  }
+  std::vector<WorkItem> items;
+  std::vector<size_t> start(n_chunks), count(n_chunks);
+  std::vector<int32_t> splits(n_chunks);
+  int32_t max_splits = 0;
+  for (int c = 0; c < n_chunks; ++c) {
+    start[c] = items.size();
+    for (int64_t t : bucket[c])
+      items.push_back(WorkItem{t, 0, 0, static_cast<int16_t>(jp.n_kmers), -1, 1});
+    split_tail(items, start[c], grid, &splits[c]);
+    count[c] = items.size() - start[c];
+    max_splits = std::max(max_splits, splits[c]);
+  }
+
+  // ---- device buffers: job, all items, one control block per chunk
+  const size_t items_off = (sizeof(JobParams) + 255) & ~static_cast<size_t>(255);
+  const size_t ctrl_off = (items_off + items.size() * sizeof(WorkItem) + 255) & ~static_cast<size_t>(255);
+  std::vector<size_t> ctrl_at(n_chunks);
+  size_t meta_bytes = ctrl_off;
+  for (int c = 0; c < n_chunks; ++c) {
+    ctrl_at[c] = meta_bytes;
+    meta_bytes += (8 + static_cast<size_t>(splits[c]) * cfg->threads * 4 + 255) & ~static_cast<size_t>(255);
+  }
+  const size_t slot = count_slot_bytes(*cfg, jp.n_kmers);
+  const int64_t wps = static_cast<int64_t>(n_kmers) * sketchsize64 * bbits;   // words per sample
+  void *meta = nullptr, *cta = nullptr, *split = nullptr, *staging = nullptr;
+  st = scratch(ctx, kSlotLaunchMeta, meta_bytes, &meta);
+  if (st == SK_OK) st = scratch(ctx, kSlotCounts, static_cast<size_t>(grid) * slot, &cta);
+  if (st == SK_OK)
+    st = scratch(ctx, kSlotSplitCounts, std::max<size_t>(static_cast<size_t>(max_splits) * slot, 16), &split);
+  if (st == SK_OK) st = scratch(ctx, kSlotStaging, static_cast<size_t>(2 * cs * wps) * 8, &staging);
+  if (st != SK_OK) return st;
+  char *m = static_cast<char *>(meta);
+  cudaError_t e = cudaMemcpyAsync(m, &jp, sizeof(jp), cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(m + items_off, items.data(), items.size() * sizeof(WorkItem),
+                        cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(m + ctrl_off, 0, meta_bytes - ctrl_off, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "work list upload");
+  LaunchParams base{};
+  base.jobs = reinterpret_cast<const JobParams *>(m);
+  base.cta_scratch = static_cast<uint16_t *>(cta);
+  base.split_scratch = static_cast<uint16_t *>(split);
+  base.k_slots = jp.n_kmers;
+  base.status = ctx->status_dev;
+  base.cancel = ctx->cancel_dev;
+  const WorkItem *d_items = reinterpret_cast<const WorkItem *>(m + items_off);
+
+  // ---- upload units: the query side whole (in chunk-sized pieces), then the
+  // reference chunk by chunk
+  std::vector<Unit> units;
+  if (dbs.query)
+    for (int64_t s0 = 0; s0 < dbs.query->n; s0 += cs)
+      units.push_back(Unit{dbs.query, query->words + s0 * wps, s0, std::min(cs, dbs.query->n - s0), -1});
+  for (int c = 0; c < n_chunks; ++c) {
+    const int64_t s0 = c * cs;
+    units.push_back(Unit{dbs.ref, ref->words + s0 * wps, s0, std::min(cs, n_ref - s0), c});
+  }
+  uint64_t *stage[2] = {static_cast<uint64_t *>(staging), static_cast<uint64_t *>(staging) + cs * wps};
+  for (size_t i = 0; i < units.size(); ++i) {
+    const Unit &u = units[i];
+    const int b = static_cast<int>(i & 1);
+    if (i >= 2) e = cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_packed[b], 0);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(stage[b], u.host, static_cast<size_t>(u.n * wps) * 8, cudaMemcpyHostToDevice,
+                          ctx->copy_stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_landed[b], ctx->copy_stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, ctx->ev_landed[b], 0);
+    const int32_t g0 = static_cast<int32_t>(u.s0 / kGranule);
+    const bool last_of_db = u.s0 + u.n == u.db->n;
+    const int32_t ng = last_of_db ? u.db->ng - g0 : static_cast<int32_t>(u.n / kGranule);
+    if (e == cudaSuccess)
+      e = launch_pack_range(stage[b], u.n, n_kmers, sketchsize64, ng, g0, u.db->ng, u.db->packed,
+                            ctx->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_packed[b], ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "sketch upload");
+    if (u.chunk >= 0 && count[u.chunk] > 0) {
+      LaunchParams lp = base;
+      lp.items = d_items + start[u.chunk];
+      lp.n_items = static_cast<int64_t>(count[u.chunk]);
+      lp.item_counter = reinterpret_cast<unsigned long long *>(m + ctrl_at[u.chunk]);
+      lp.split_done = reinterpret_cast<unsigned int *>(m + ctrl_at[u.chunk] + 8);
+      const int g = static_cast<int>(std::min<int64_t>(grid, lp.n_items));
+      e = cfg->launch(lp, g, ctx->stream);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "distance kernel launch");
+    }
+  }
+  e = cudaMemcpyAsync(out, d_out, out_sz, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "result copy");
+  return finish_call(ctx);
+}

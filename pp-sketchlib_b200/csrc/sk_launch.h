@@ -33,6 +33,11 @@ inline size_t count_slot_bytes(const TileConfig &cfg, int k_slots) {
 // aux_kernels.cu
 cudaError_t launch_pack(const uint64_t *words, int64_t n, int32_t n_kmers, int32_t s64,
                         int32_t ng, uint32_t *packed, cudaStream_t stream);
+// Packs n samples (reference layout at `words`) into granules g0 .. g0+ng-1 of
+// a packed array of ng_total granules.
+cudaError_t launch_pack_range(const uint64_t *words, int64_t n, int32_t n_kmers, int32_t s64,
+                              int32_t ng, int32_t g0, int32_t ng_total, uint32_t *packed,
+                              cudaStream_t stream);
 cudaError_t launch_unpack(const uint32_t *packed, int64_t n, int32_t n_kmers, int32_t s64,
                           int32_t ng, uint64_t *words, cudaStream_t stream);
 cudaError_t launch_synth(const int32_t *parent, const uint32_t *thresh, int64_t n,

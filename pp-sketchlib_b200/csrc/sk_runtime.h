@@ -27,13 +27,19 @@ enum ScratchSlot : int {
   kSlotTemp = 3,          // temporaries (scan storage, unpacking, probes)
   kSlotSplitCounts = 4,   // counts of tiles split along k
   kSlotLaunchMeta = 5,    // job table, work list, control block
-  kSlotCount = 6
+  kSlotStaging = 6,       // sketch words in the reference layout on their way in
+  kSlotPackedRef = 7,     // packed arrays of the databases of one sk_query_db call
+  kSlotPackedQuery = 8,
+  kSlotCount = 9
 };
 
 struct sk_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = true;
+  cudaStream_t copy_stream = nullptr;   // uploads overlapped with kernels (created on first use)
+  cudaEvent_t ev_landed[2] = {};        // staging buffer b holds a chunk
+  cudaEvent_t ev_packed[2] = {};        // staging buffer b is free again
   int sm_count = 0;
   std::string err;
   int *cancel_host = nullptr;   // mapped pinned word polled by the kernels
@@ -57,6 +63,7 @@ struct sk_db {
   std::vector<int32_t> kmers;
   int32_t ng = 0;                 // granules in the packed array (padded samples / 64)
   uint32_t *packed = nullptr;     // [K][2*s64][ng][14][64]
+  bool own_packed = true;         // false: the array is context scratch
   uint16_t *cluster = nullptr;    // [ng*64] random-match cluster ids
   std::vector<uint64_t> seq_len;  // per-sample sequence lengths
   double *jv = nullptr;           // [K][ng*64] equal-base factors
@@ -120,6 +127,10 @@ sk_status build_job(sk_ctx *ctx, const sk_db *ref, const sk_db *query, const sk_
                     JobParams *jp);
 sk_status launch_job(sk_ctx *ctx, const JobParams &jp, const TileConfig &cfg);
 void plan_items(const std::vector<JobParams> &jobs, int grid, Plan &plan);
+void split_tail(std::vector<WorkItem> &items, size_t begin, int grid, int32_t *n_splits);
+sk_status db_alloc(sk_ctx *ctx, int64_t n, const int32_t *kmers, int32_t K, int32_t s64,
+                   int32_t bbits, sk_db **out, int packed_slot = -1);
+void db_free(sk_db *db);
 sk_status make_plan(sk_ctx *ctx, const std::vector<JobParams> &jobs, const TileConfig &cfg,
                     Plan &plan);
 sk_status upload_plan(sk_ctx *ctx, const std::vector<JobParams> &jobs, Plan &plan,

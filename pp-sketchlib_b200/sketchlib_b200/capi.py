@@ -52,6 +52,7 @@ _SIGNATURES = {
     "sk_random_destroy": (_i32, [_p]),
     "sk_dists_rows": (_i64, [_p, _p]),
     "sk_dists_dense": (_i32, [_p, _p, _p, _p, _i32, _p, _i32]),
+    "sk_query_db": (_i32, [_p, _p, _p, _p, _i32, _i32, _i32, _p, _i32, _p]),
     "sk_dists_knn": (_i32, [_p, _p, _p, _i32, _i32, _i32, _p, _p, _p]),
     "sk_query_knn": (_i32, [_p, _p, _p, _p, _i32, _i32, _p, _p]),
     "sk_sparse_threshold": (_i32, [_p, _p, _i64, _i32, _i32, _f32, C.POINTER(_p)]),
@@ -88,6 +89,11 @@ class ServerParams(C.Structure):
                 ("keep_rows", _i32)]
 
 BATCH_AUTOTUNE = 1
+
+
+class HostSketches(C.Structure):
+    """sk_host_sketches: one side of an sk_query_db call."""
+    _fields_ = [("words", _p), ("n", _i64), ("cluster", _p), ("seq_len", _p)]
 
 
 class Job(C.Structure):
@@ -444,6 +450,42 @@ def dists_dense(ctx: Context, ref: Database, query: Database | None = None,
             out = np.empty((rows, K), dtype=np.uint32)
     _check(lib.sk_dists_dense(ctx.handle, ref.handle, _h(query), _h(random), out_mode,
                               out.ctypes.data, 0), ctx)
+    return out
+
+
+def query_db(ctx: Context, ref_words, kmers, sketchsize64: int, query_words=None,
+             ref_cluster=None, ref_seq_len=None, query_cluster=None, query_seq_len=None,
+             random: Random | None = None, out_mode: int = OUT_CORE_ACC, out=None,
+             bbits: int = 14) -> np.ndarray:
+    """Host sketches in, host distances out (sk_query_db): the upload is
+    chunked and overlapped with the distance kernel.  `ref_words` /
+    `query_words`: uint64 [n][K][sketchsize64 * bbits]; query_words None =
+    all-vs-all.  Pinned arrays (e.g. from torch's pin_memory) copy fastest."""
+    keep = []
+
+    def side(words, cluster, seq_len):
+        w = words if isinstance(words, np.ndarray) and words.dtype == np.uint64 and \
+            words.flags.c_contiguous else np.ascontiguousarray(words, dtype=np.uint64)
+        cl = None if cluster is None else np.ascontiguousarray(cluster, np.uint16)
+        ln = None if seq_len is None else np.ascontiguousarray(seq_len, np.uint64)
+        keep.extend([w, cl, ln])
+        return HostSketches(w.ctypes.data, w.shape[0], _ptr(cl), _ptr(ln)), w.shape[0]
+
+    r, n_ref = side(ref_words, ref_cluster, ref_seq_len)
+    q, n_q = (None, 0) if query_words is None else side(query_words, query_cluster, query_seq_len)
+    K = len(kmers)
+    rows = n_ref * (n_ref - 1) // 2 if q is None else n_q * n_ref
+    if out is None:
+        if out_mode == OUT_CORE_ACC:
+            out = np.empty((rows, 2), dtype=np.float32)
+        elif out_mode == OUT_JACCARD:
+            out = np.empty((rows, K), dtype=np.float32)
+        else:
+            out = np.empty((rows, K), dtype=np.uint32)
+    km = np.ascontiguousarray(kmers, np.int32)
+    _check(lib.sk_query_db(ctx.handle, C.byref(r), None if q is None else C.byref(q),
+                           km.ctypes.data, K, sketchsize64, bbits, _h(random), out_mode,
+                           out.ctypes.data), ctx)
     return out
 
 
