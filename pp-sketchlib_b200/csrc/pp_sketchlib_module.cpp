@@ -172,24 +172,36 @@ py::array_t<float> queryDatabase(const std::string &ref_db_name, const std::stri
   skhost::SketchSet ref = skhost::load_sketches(ref_db_name, ref_names, kmers);
   const bool self = ref_db_name == query_db_name && ref_names == query_names;
   skhost::SketchSet query;
-  if (!self) query = skhost::load_sketches(query_db_name, query_names, kmers);
+  if (!self) {
+    query = skhost::load_sketches(query_db_name, query_names, kmers);
+    // checkSketchParamsMatch (src/gpu/gpu_api.cpp:170-185)
+    if (query.bbits != ref.bbits) throw std::runtime_error("Mismatching bbits in sketches");
+    if (query.sketchsize64 != ref.sketchsize64)
+      throw std::runtime_error("Mismatching sketchsize64 in sketches");
+  }
   skhost::RandomModel random = random_for(ref_db_name, random_correct);
   check_min_k(random, kmers);
 
   sk_ctx *ctx = context(device_id);
-  DbHandle rdb, qdb;
-  upload(ctx, ref, random.lookup(ref, false), rdb);
-  if (!self) upload(ctx, query, random.lookup(query, true), qdb);
   RandomHandle rnd;
   make_random(ctx, random, kmers, rnd);
-
-  const int64_t rows = sk_dists_rows(rdb.h, self ? nullptr : qdb.h);
+  // one sk_query_db call: the sketch upload overlaps the distance kernel
+  const std::vector<uint16_t> ref_cl = random.lookup(ref, false);
+  const std::vector<uint16_t> query_cl = self ? std::vector<uint16_t>() : random.lookup(query, true);
+  const sk_host_sketches r{ref.words.data(), static_cast<int64_t>(ref.size()), ref_cl.data(),
+                           ref.seq_len.data()};
+  const sk_host_sketches q{self ? nullptr : query.words.data(),
+                           self ? 0 : static_cast<int64_t>(query.size()),
+                           self ? nullptr : query_cl.data(), self ? nullptr : query.seq_len.data()};
+  const int64_t n_ref = static_cast<int64_t>(ref.size());
+  const int64_t rows = self ? n_ref * (n_ref - 1) / 2 : static_cast<int64_t>(query.size()) * n_ref;
   const int64_t cols = jaccard ? static_cast<int64_t>(kmers.size()) : 2;
   py::array_t<float> out({rows, cols});
   float *dst = out.mutable_data();
   run_gpu(ctx, [&] {
-    return sk_dists_dense(ctx, rdb.h, self ? nullptr : qdb.h, rnd.h,
-                          jaccard ? SK_OUT_JACCARD : SK_OUT_CORE_ACC, dst, 0);
+    return sk_query_db(ctx, &r, self ? nullptr : &q, kmers.data(),
+                       static_cast<int32_t>(kmers.size()), ref.sketchsize64, ref.bbits, rnd.h,
+                       jaccard ? SK_OUT_JACCARD : SK_OUT_CORE_ACC, dst);
   });
   return out;
 }

@@ -96,6 +96,8 @@ extern "C" sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
   sk_status st = begin_call(ctx);
   if (st != SK_OK) return st;
   if (!ref) return fail(ctx, SK_EINVAL, "null reference sketches");
+  if (ref->n < 1 || (query && query->n < 1))
+    return fail(ctx, SK_EINVAL, "Query with empty ref or query list!");
   if (out_mode != kOutCoreAcc && out_mode != kOutJaccard && out_mode != kOutCounts)
     return fail(ctx, SK_EINVAL, "Unknown output mode %d", out_mode);
   st = ensure_pipeline(ctx);

@@ -79,8 +79,12 @@ def test_against_oracle_and_pinned_buffers(gpu_ctx):
 
 
 def test_empty_and_single_sample(gpu_ctx):
+    """The reference refuses empty lists ("Query with empty ref or query
+    list!", src/api.cpp:146); one sample all-vs-all has no pairs."""
     words, kmers = random_sketches(5, 2, 4, seed=3)
     assert capi.query_db(gpu_ctx, words[:1], kmers, 4).shape == (0, 2)
-    assert capi.query_db(gpu_ctx, words, kmers, 4, query_words=words[:0]).shape == (0, 2)
+    for bad in (dict(ref_words=words[:0]), dict(ref_words=words, query_words=words[:0])):
+        with pytest.raises(capi.SketchlibError, match="empty ref or query"):
+            capi.query_db(gpu_ctx, kmers=kmers, sketchsize64=4, **bad)
     with pytest.raises(capi.SketchlibError):
         capi.query_db(gpu_ctx, words, kmers, 4, bbits=13)
