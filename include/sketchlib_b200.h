@@ -26,7 +26,7 @@
  *                              query_db (src/api.cpp:206-211, 256-260)
  *   sk_query_db             <- query_db_cuda as one host-in / host-out call
  *                              (src/gpu/gpu_api.cpp:352-494)
- *   sk_dists_knn         <- query_db_sparse_cuda / sparseDists
+ *   sk_dists_knn            <- query_db_sparse_cuda / sparseDists
  *                              (src/gpu/gpu_api.cpp:496-531, src/gpu/dist.cu:495-791) and
  *                              query_db_sparse (src/api.cpp:332-432)
  *   sk_sparse_threshold     <- sparsify_dists_by_threshold (src/dist/matrix_ops.cpp:38-69)
@@ -79,6 +79,14 @@ enum {
   SK_OUT_COUNTS = 2    /* uint32 (n_pairs, n_kmers) row-major: raw intersection counts */
 };
 
+/* Which of the reference's two distance paths the core/accessory output
+ * reproduces (the reference's CPU and GPU paths disagree, see
+ * sk_ctx_set_semantics). */
+enum {
+  SK_SEMANTICS_REFERENCE_CPU = 0, /* query_db + fit_slope (default) */
+  SK_SEMANTICS_REFERENCE_GPU = 1  /* calculate_dists, bit for bit */
+};
+
 /* ---- library / context ------------------------------------------------- */
 
 int32_t sk_abi_version(void);
@@ -105,6 +113,22 @@ sk_status sk_ctx_synchronize(sk_ctx *ctx);
 /* Chooses the dense kernel's tile shape (0 = automatic, from the tuning table
  * or the built-in default; >0 = a shape id from sk_tile_config_count()). */
 sk_status sk_ctx_set_tile_config(sk_ctx *ctx, int32_t config_id);
+/* Selects the arithmetic of the core/accessory fit for this context's later
+ * calls.  SK_SEMANTICS_REFERENCE_CPU (default): the reference CPU path
+ * (src/api.cpp:195-283, src/dist/linear_regression.cpp:16-60): Jaccard in
+ * double, fit over the k range from the first to the last Jaccard above
+ * 5 / (64 * sketchsize64), least squares in double, random table read as
+ * [k][cluster of row i][cluster of column j] for all-vs-all and 0 from k = max_k
+ * on (the table passed in decides that).  SK_SEMANTICS_REFERENCE_GPU: the
+ * reference GPU kernel's float arithmetic (calculate_dists, src/gpu/dist.cu:
+ * 164-317): Jaccard count / (64 * sketchsize64) rounded up, float
+ * observed_excess, the fit stops at the first k below tolerance, running
+ * float sums, correlation-form slope with round-up intrinsics, __logf /
+ * __expf; random table read as [k][cluster of the column (reference)
+ * sample][cluster of the row (query) sample]; SK_RANDOM_EQUAL_BASE uses the
+ * first reference sample's length for every pair (src/gpu/gpu_api.cpp:402-403).
+ * Jaccard and count outputs are the same under both. */
+sk_status sk_ctx_set_semantics(sk_ctx *ctx, int32_t semantics);
 int32_t sk_tile_config_count(void);
 /* Describes shape `config_id`: rows x cols of the CTA tile and per-thread block. */
 sk_status sk_tile_config_info(int32_t config_id, int32_t *tile_rows,

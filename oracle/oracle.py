@@ -296,6 +296,11 @@ class RefGpuKernel:
         if not REF_GPU_PATH.exists():
             raise FileNotFoundError(f"{REF_GPU_PATH} not built (needs the reference sources)")
         lib_ = C.CDLL(str(REF_GPU_PATH))
+        lib_.refgpu_dists.restype = C.c_int
+        lib_.refgpu_dists.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p,
+                                      C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                                      C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                                      C.POINTER(C.c_double), C.c_char_p, C.c_int]
         lib_.refgpu_self_dists.restype = C.c_int
         lib_.refgpu_self_dists.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int, C.c_int,
                                            C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
@@ -320,6 +325,33 @@ class RefGpuKernel:
         if rc != 0:
             raise RuntimeError(err.value.decode())
         return out, ms.value
+
+
+    def dists(self, ref_words, kmers, s64, query_words=None, table=None, ref_lookup=None,
+              query_lookup=None, bbits=14):
+        """(core, accessory) float32 (n_pairs, 2) of the reference kernel.
+        table: None (NoAdjust), float [K] (one chance per k) or [K][C][C]
+        with uint16 cluster lookups (RandomMC::flattened_random strides)."""
+        r = np.ascontiguousarray(ref_words, np.uint64)
+        q = None if query_words is None else np.ascontiguousarray(query_words, np.uint64)
+        km = np.ascontiguousarray(kmers, np.int32)
+        n_ref = r.shape[0]
+        n_q = 0 if q is None else q.shape[0]
+        pairs = n_ref * (n_ref - 1) // 2 if q is None else n_ref * n_q
+        t = None if table is None else np.ascontiguousarray(table, np.float32)
+        n_cl = 0 if t is None or t.ndim == 1 else t.shape[1]
+        rl = None if ref_lookup is None else np.ascontiguousarray(ref_lookup, np.uint16)
+        ql = None if query_lookup is None else np.ascontiguousarray(query_lookup, np.uint16)
+        out = np.zeros((pairs, 2), np.float32)
+        ms = C.c_double(0.0)
+        err = C.create_string_buffer(512)
+        ptr = lambda a: None if a is None else a.ctypes.data
+        rc = self.lib.refgpu_dists(r.ctypes.data, n_ref, ptr(q), n_q, km.ctypes.data, len(km), s64,
+                                   bbits, ptr(t), n_cl, ptr(rl), ptr(ql), 0, 1, out.ctypes.data,
+                                   C.byref(ms), err, len(err))
+        if rc != 0:
+            raise RuntimeError(err.value.decode())
+        return out
 
 
 def ref_gpu_available() -> bool:

@@ -165,6 +165,20 @@ void plan_tiles(JobParams &jp, const TileConfig &cfg) {
   }
 }
 
+// The reference GPU path's equal-base chances: csrs(k, use_rc, l0, l0) with l0
+// the first sample's length, narrowed to float (flattened_random,
+// src/random/random_match.cpp:278-310; csrs :318-336).
+std::vector<float> equal_base_gpu(const sk_db *db, int use_rc) {
+  std::vector<float> t(static_cast<size_t>(db->K), 0.0f);
+  const double len = static_cast<double>(db->seq_len.empty() ? 0 : db->seq_len[0]);
+  for (int k = 0; k < db->K; ++k) {
+    const double match_chance = std::ldexp(1.0, (db->kmers[k] - 1) * 2 + (use_rc ? 1 : 0));
+    const double j = 1 - std::pow(1 - (double)1 / match_chance, len);
+    t[k] = j > 0 ? static_cast<float>((j * j) / (j + j - j * j)) : 0.0f;
+  }
+  return t;
+}
+
 // Equal-base random-match factors j(k, len) = 1 - (1 - 4^-k')^len per sample
 // (csrs, src/random/random_match.cpp:318-336), computed with std::pow on the
 // host exactly as the reference does and cached on the database.
@@ -231,18 +245,41 @@ sk_status build_job(sk_ctx *ctx, const sk_db *ref, const sk_db *query, const sk_
   jp->tol = 5.0 / (ref->s64 * 64);
   jp->union_bits = static_cast<double>(64 * ref->s64);
   jp->one = 1;
+  jp->semantics = ctx->semantics;
+  const bool gpu_sem = ctx->semantics == kSemRefGpu;
   for (int k = 0; k < ref->K; ++k) jp->kmers[k] = ref->kmers[k];
   jp->rmode = random ? random->mode : kRandNone;
   if (jp->rmode == kRandTable) {
     const int C = random->n_clusters;
     jp->rtable = random->table;
     jp->rs_k = C * C;
-    // self: [k][cluster(i = row)][cluster(j = col)]  (random_match(r1=i, r2=j))
-    // query: [k][cluster(ref = col)][cluster(query = row)]  (src/api.cpp:264-266)
-    jp->rs_row = query ? 1 : C;
-    jp->rs_col = query ? C : 1;
+    // CPU path, self: [k][cluster(i = row)][cluster(j = col)]  (random_match(r1=i, r2=j))
+    // query (both paths) and GPU path self: [k][cluster(ref = col)][cluster(query = row)]
+    // (src/api.cpp:264-266; src/gpu/dist.cu:262-267 with ref_idx = j, query_idx = i)
+    const bool col_major = query || gpu_sem;
+    jp->rs_row = col_major ? 1 : C;
+    jp->rs_col = col_major ? C : 1;
     jp->cl_rows = rows->cluster;
     jp->cl_cols = ref->cluster;
+  } else if (jp->rmode == kRandEqualBase && gpu_sem) {
+    // GPU path: one chance per k from the first reference's length
+    // (flattened_random(kmer_lengths, ref_sketches[0].seq_length()),
+    // src/gpu/gpu_api.cpp:402-403, src/random/random_match.cpp:278-310)
+    sk_db *r = const_cast<sk_db *>(ref);
+    if (!r->jgpu || r->jgpu_rc != random->use_rc) {
+      const std::vector<float> t = equal_base_gpu(r, random->use_rc);
+      if (!r->jgpu) {
+        cudaError_t e = cudaMalloc(&r->jgpu, t.size() * sizeof(float));
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "random-match chances");
+      }
+      cudaError_t e = cudaMemcpy(r->jgpu, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "random-match chances");
+      r->jgpu_rc = random->use_rc;
+    }
+    jp->rmode = kRandTable;
+    jp->rtable = r->jgpu;
+    jp->rs_k = 1;
+    jp->rs_row = jp->rs_col = 0;
   } else if (jp->rmode == kRandEqualBase) {
     sk_status st = ensure_jv(ctx, const_cast<sk_db *>(ref), random->use_rc);
     if (st != SK_OK) return st;
@@ -503,6 +540,14 @@ sk_status sk_ctx_set_stream(sk_ctx *ctx, void *stream) {
   return SK_OK;
 }
 
+sk_status sk_ctx_set_semantics(sk_ctx *ctx, int32_t semantics) {
+  SK_GUARD(ctx);
+  if (semantics != kSemRefCpu && semantics != kSemRefGpu)
+    return fail(ctx, SK_EINVAL, "Unknown semantics %d", semantics);
+  ctx->semantics = semantics;
+  return SK_OK;
+}
+
 sk_status sk_cancel(sk_ctx *ctx) {
   if (!ctx) return SK_EINVAL;
   // deliberately no lock: called from another thread while a call runs
@@ -625,6 +670,7 @@ void db_free(sk_db *db) {
     if (db->packed && db->own_packed) cudaFree(db->packed);
     if (db->cluster) cudaFree(db->cluster);
     if (db->jv) cudaFree(db->jv);
+    if (db->jgpu) cudaFree(db->jgpu);
   }
   delete db;
   ctx_release(ctx);
@@ -717,6 +763,7 @@ sk_status sk_db_set_sample_info(sk_db *db, const uint16_t *cluster, const uint64
   if (seq_len) {
     db->seq_len.assign(seq_len, seq_len + db->n);
     db->jv_rc = -1;  // factors depend on lengths
+    db->jgpu_rc = -1;
   }
   return SK_OK;
 }

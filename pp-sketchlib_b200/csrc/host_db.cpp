@@ -131,13 +131,14 @@ std::vector<uint16_t> RandomModel::lookup(const SketchSet &s, bool queries_by_ce
   return ids;
 }
 
-std::vector<float> RandomModel::flat_table(const std::vector<int32_t> &kmers) const {
+std::vector<float> RandomModel::flat_table(const std::vector<int32_t> &kmers, bool gpu_rule) const {
   const size_t C = static_cast<size_t>(std::max(1, n_clusters));
   std::vector<float> t(kmers.size() * C * C, 0.0f);
   if (mode != 2) return t;
   for (size_t ki = 0; ki < kmers.size(); ++ki) {
     const int64_t k = kmers[ki];
-    if (k >= static_cast<int64_t>(max_k)) continue;  // strict <, as the CPU path
+    // CPU path: strict < (random_match.cpp:191); GPU path: <= (random_match.cpp:300)
+    if (gpu_rule ? k > static_cast<int64_t>(max_k) : k >= static_cast<int64_t>(max_k)) continue;
     auto it = matches.find(k);
     if (it == matches.end())
       throw std::runtime_error("Trying to choose a k-mer length below the minimum allowed\n");

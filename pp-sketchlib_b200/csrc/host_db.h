@@ -54,7 +54,10 @@ struct RandomModel {
   // cluster ids for samples: table entry, else nearest centroid
   std::vector<uint16_t> lookup(const SketchSet &s, bool queries_by_centroid) const;
   // [K][C][C] table with zeros for k >= max_k (random_match.cpp:191)
-  std::vector<float> flat_table(const std::vector<int32_t> &kmers) const;
+  // [K][C][C] table for the given k-mer lengths; k at or beyond max_k gives 0
+  // (CPU path, strict <) or copies the table up to max_k inclusive (GPU path,
+  // flattened_random's <=).
+  std::vector<float> flat_table(const std::vector<int32_t> &kmers, bool gpu_rule = false) const;
   // min_supported_k (random_match.cpp:165-182)
   size_t min_supported_k() const;
 };

@@ -81,7 +81,10 @@ extern "C" sk_status sk_dists_dense_noalloc(sk_ctx *ctx, const sk_db *ref, const
 
   // Layout of the static array for this call.
   std::vector<double> jv_rows, jv_cols;
-  if (random && random->mode == kRandEqualBase) {
+  std::vector<float> jgpu;   // equal-base chances of the reference GPU path
+  if (random && random->mode == kRandEqualBase && jp.semantics == kSemRefGpu) {
+    jgpu = equal_base_gpu(ref, random->use_rc);
+  } else if (random && random->mode == kRandEqualBase) {
     auto factors = [&](const sk_db *db, std::vector<double> &jv) {
       const int64_t ld = static_cast<int64_t>(db->ng) * kGranule;
       jv.assign(static_cast<size_t>(db->K) * ld, 0.0);
@@ -107,7 +110,8 @@ extern "C" sk_status sk_dists_dense_noalloc(sk_ctx *ctx, const sk_db *ref, const
   const size_t off_ctrl = align256(off_items + items.size() * sizeof(WorkItem));
   const size_t off_jv_cols = align256(off_ctrl + 8);
   const size_t off_jv_rows = align256(off_jv_cols + jv_cols.size() * sizeof(double));
-  const size_t off_counts = align256(off_jv_rows + jv_rows.size() * sizeof(double));
+  const size_t off_jgpu = align256(off_jv_rows + jv_rows.size() * sizeof(double));
+  const size_t off_counts = align256(off_jgpu + jgpu.size() * sizeof(float));
   const size_t slot = count_slot_bytes(*cfg, jp.n_kmers);
   const size_t fixed = off_counts;
   if (fixed + slot > kNoAllocBytes)
@@ -127,13 +131,19 @@ extern "C" sk_status sk_dists_dense_noalloc(sk_ctx *ctx, const sk_db *ref, const
     jp.jv_rows = query ? reinterpret_cast<const double *>(base + off_jv_rows) : jp.jv_cols;
     jp.jv_cols_ld = static_cast<int64_t>(ref->ng) * kGranule;
     jp.jv_rows_ld = static_cast<int64_t>(rows->ng) * kGranule;
+  } else if (!jgpu.empty()) {
+    jp.rmode = kRandTable;
+    jp.rtable = reinterpret_cast<const float *>(base + off_jgpu);
+    jp.rs_k = 1;
+    jp.rs_row = jp.rs_col = 0;
   } else if (random && random->mode == kRandTable) {
     const int C = random->n_clusters;
+    const bool col_major = query || jp.semantics == kSemRefGpu;
     jp.rmode = kRandTable;
     jp.rtable = random->table;
     jp.rs_k = C * C;
-    jp.rs_row = query ? 1 : C;
-    jp.rs_col = query ? C : 1;
+    jp.rs_row = col_major ? 1 : C;
+    jp.rs_col = col_major ? C : 1;
     jp.cl_rows = rows->cluster;
     jp.cl_cols = ref->cluster;
   }
@@ -146,6 +156,9 @@ extern "C" sk_status sk_dists_dense_noalloc(sk_ctx *ctx, const sk_db *ref, const
                         cudaMemcpyHostToDevice, ctx->stream);
   if (e == cudaSuccess && !jv_cols.empty())
     e = cudaMemcpyAsync(base + off_jv_cols, jv_cols.data(), jv_cols.size() * sizeof(double),
+                        cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess && !jgpu.empty())
+    e = cudaMemcpyAsync(base + off_jgpu, jgpu.data(), jgpu.size() * sizeof(float),
                         cudaMemcpyHostToDevice, ctx->stream);
   if (e == cudaSuccess && !jv_rows.empty())
     e = cudaMemcpyAsync(base + off_jv_rows, jv_rows.data(), jv_rows.size() * sizeof(double),

@@ -120,14 +120,30 @@ void upload(sk_ctx *ctx, const skhost::SketchSet &s, const std::vector<uint16_t>
   check(ctx, sk_db_set_sample_info(db.h, clusters.data(), s.seq_len.data()));
 }
 
+// The reference path a call reproduces: "cpu" (query_db + fit_slope, the
+// default) or "gpu" (the reference GPU kernel, bit for bit).  An extra keyword
+// beside the reference's own arguments; set on the shared context for the
+// call only.
+int parse_semantics(const std::string &s) {
+  if (s == "cpu") return SK_SEMANTICS_REFERENCE_CPU;
+  if (s == "gpu") return SK_SEMANTICS_REFERENCE_GPU;
+  throw py::value_error("semantics must be 'cpu' or 'gpu'");
+}
+
+struct SemanticsScope {
+  sk_ctx *ctx;
+  SemanticsScope(sk_ctx *c, int sem) : ctx(c) { check(ctx, sk_ctx_set_semantics(ctx, sem)); }
+  ~SemanticsScope() { sk_ctx_set_semantics(ctx, SK_SEMANTICS_REFERENCE_CPU); }
+};
+
 void make_random(sk_ctx *ctx, const skhost::RandomModel &r, const std::vector<int32_t> &kmers,
-                 RandomHandle &out) {
+                 RandomHandle &out, bool gpu_rule) {
   int mode = SK_RANDOM_NONE;
   std::vector<float> table;
   if (r.mode == 1) mode = SK_RANDOM_EQUAL_BASE;
   if (r.mode == 2) {
     mode = SK_RANDOM_TABLE;
-    table = r.flat_table(kmers);
+    table = r.flat_table(kmers, gpu_rule);
   }
   check(ctx, sk_random_create(ctx, mode, r.use_rc ? 1 : 0, kmers.data(),
                               static_cast<int32_t>(kmers.size()), r.n_clusters,
@@ -161,9 +177,10 @@ py::array_t<float> queryDatabase(const std::string &ref_db_name, const std::stri
                                  const std::vector<std::string> &query_names,
                                  std::vector<size_t> kmer_lengths, const bool random_correct,
                                  const bool jaccard, const size_t num_threads, const bool use_gpu,
-                                 const int device_id) {
+                                 const int device_id, const std::string &semantics) {
   (void)num_threads;
   (void)use_gpu;
+  const int sem = parse_semantics(semantics);
   if (ref_names.empty() || query_names.empty())
     throw std::runtime_error("Query with empty ref or query list!");
   if (!jaccard && kmer_lengths.size() < 2)
@@ -183,8 +200,9 @@ py::array_t<float> queryDatabase(const std::string &ref_db_name, const std::stri
   check_min_k(random, kmers);
 
   sk_ctx *ctx = context(device_id);
+  SemanticsScope scope(ctx, sem);
   RandomHandle rnd;
-  make_random(ctx, random, kmers, rnd);
+  make_random(ctx, random, kmers, rnd, sem == SK_SEMANTICS_REFERENCE_GPU);
   // one sk_query_db call: the sketch upload overlaps the distance kernel
   const std::vector<uint16_t> ref_cl = random.lookup(ref, false);
   const std::vector<uint16_t> query_cl = self ? std::vector<uint16_t>() : random.lookup(query, true);
@@ -215,19 +233,21 @@ sparse_coo querySelfSparse(const std::string &ref_db_name, const std::vector<std
                            std::vector<size_t> kmer_lengths, const bool random_correct,
                            const bool jaccard, const unsigned long int kNN, const float dist_cutoff,
                            const size_t dist_col, const size_t num_threads, const bool use_gpu,
-                           const int device_id) {
+                           const int device_id, const std::string &semantics) {
   (void)num_threads;
   (void)use_gpu;
+  const int sem = parse_semantics(semantics);
   if (ref_names.empty()) throw std::runtime_error("Query with empty ref or query list!");
   const std::vector<int32_t> kmers = to_kmers(kmer_lengths);
   skhost::SketchSet ref = skhost::load_sketches(ref_db_name, ref_names, kmers);
   skhost::RandomModel random = random_for(ref_db_name, random_correct);
   check_min_k(random, kmers);
   sk_ctx *ctx = context(device_id);
+  SemanticsScope scope(ctx, sem);
   DbHandle db;
   upload(ctx, ref, random.lookup(ref, false), db);
   RandomHandle rnd;
-  make_random(ctx, random, kmers, rnd);
+  make_random(ctx, random, kmers, rnd, sem == SK_SEMANTICS_REFERENCE_GPU);
 
   std::vector<int64_t> i, j;
   std::vector<float> d;
@@ -414,14 +434,15 @@ PYBIND11_MODULE(_pp_sketchlib, m) {
   m.def("queryDatabase", &queryDatabase, "Find distances between sketches; return all distances",
         py::arg("ref_db_name"), py::arg("query_db_name"), py::arg("rList"), py::arg("qList"),
         py::arg("klist"), py::arg("random_correct") = true, py::arg("jaccard") = false,
-        py::arg("num_threads") = 1, py::arg("use_gpu") = false, py::arg("device_id") = 0);
+        py::arg("num_threads") = 1, py::arg("use_gpu") = false, py::arg("device_id") = 0,
+        py::arg("semantics") = "cpu");
 
   m.def("querySelfSparse", &querySelfSparse,
         "Find self-self distances between sketches; return a sparse matrix",
         py::arg("ref_db_name"), py::arg("rList"), py::arg("klist"),
         py::arg("random_correct") = true, py::arg("jaccard") = false, py::arg("kNN") = 0,
         py::arg("dist_cutoff") = 0.0f, py::arg("dist_col") = 0, py::arg("num_threads") = 1,
-        py::arg("use_gpu") = false, py::arg("device_id") = 0);
+        py::arg("use_gpu") = false, py::arg("device_id") = 0, py::arg("semantics") = "cpu");
 
   m.def("jaccardDist", &jaccardDist, "Calculate a raw Jaccard distance", py::arg("db_name"),
         py::arg("ref_name"), py::arg("query_name"), py::arg("kmer_length"),

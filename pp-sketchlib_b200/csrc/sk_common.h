@@ -32,6 +32,7 @@ enum OutMode : int {
   kOutColumn = 3     // float per pair: core (col 0) / accessory (col 1)
 };
 enum RandMode : int { kRandNone = 0, kRandEqualBase = 1, kRandTable = 2 };
+enum Semantics : int { kSemRefCpu = 0, kSemRefGpu = 1 };
 
 // Device-side status word of a context.  error != 0 makes the host call fail.
 struct DevStatus {
@@ -68,6 +69,7 @@ struct JobParams {
   int64_t jv_rows_ld, jv_cols_ld;      // leading dimension (padded samples)
   int32_t kmers[kMaxKmers];
   uint32_t one;                // 1 (a run-time operand for the count multiply-adds)
+  int32_t semantics;           // Semantics: which reference path the fit follows
 };
 
 // One unit of work of the persistent distance kernel: k-mer indices

@@ -204,6 +204,63 @@ __device__ __forceinline__ float2 fit_core_acc(const float (&jf)[KMAX], const Jo
   return res;
 }
 
+// The reference GPU kernel's per-pair arithmetic, for
+// SK_SEMANTICS_REFERENCE_GPU (calculate_dists, src/gpu/dist.cu:199-289, with
+// jaccard_dist :57-84, observed_excess :46-54, simple_linear_regression
+// :89-129; no fast-math in the reference's CUDA flags, so `/` is the IEEE
+// division and nvcc fuses `sum += k * y` and `sum += y * y` into FMAs):
+//   J = count / (64 s64) rounded up, J' = max(J - r, 0) / (1 - r) in float;
+//   the fit takes k in order until the first J' below 5 / (64 s64) (fast
+//   division), summing x = k, y = __logf(J'), x y, x^2, y^2 in float;
+//   fewer than 2 points gives (0, 0); slope = r_xy * sd_y / sd_x from the
+//   correlation coefficient with round-up intrinsics, intercept =
+//   ybar - slope xbar (round-up FMA); core / accessory = 1 - __expf(.) when
+//   negative.  A pair whose Jaccards are all equal has sd_y = 0, r_xy = 0 / 0
+//   and so (0, 0), as in the reference kernel.
+__device__ __forceinline__ float2 refgpu_core_acc(const JobParams &p, int64_t gi, int64_t gj,
+                                                  const uint16_t *counts, int stride) {
+  const int bins = static_cast<int>(p.union_bits);
+  const float unionf = static_cast<float>(bins);
+  const float tol = __fdividef(5.0f, __int2float_rz(bins));
+  int used = 0;
+  float xsum = 0.0f, ysum = 0.0f, xysum = 0.0f, xsq = 0.0f, ysq = 0.0f;
+  bool stop = false;
+  for (int k = 0; k < p.n_kmers; ++k) {
+    const float obs = __fdiv_ru(static_cast<float>(counts[k * stride]), unionf);
+    const float r = static_cast<float>(random_match(p, k, gi, gj));
+    const float diff = obs > r ? __fsub_rn(obs, r) : 0.0f;
+    const float jac = __fdiv_rn(diff, __fsub_rn(1.0f, r));
+    if (jac < tol) {
+      stop = true;
+    } else if (!stop) {
+      const float y = __logf(jac);
+      const int km = p.kmers[k];
+      ++used;
+      xsum = __fadd_rn(xsum, static_cast<float>(km));
+      ysum = __fadd_rn(ysum, y);
+      xysum = __fmaf_rn(static_cast<float>(km), y, xysum);
+      xsq = __fadd_rn(xsq, static_cast<float>(km * km));
+      ysq = __fmaf_rn(y, y, ysq);
+    }
+  }
+  float2 res = make_float2(0.0f, 0.0f);
+  if (used < 2) return res;
+  const float n = static_cast<float>(used);
+  const float xbar = __fdiv_rn(xsum, n);
+  const float ybar = __fdiv_rn(ysum, n);
+  const float x_diff = __fsub_rn(xsq, __fdiv_rn(__fmul_ru(xsum, xsum), n));
+  const float y_diff = __fsub_rn(ysq, __fdiv_rn(__fmul_ru(ysum, ysum), n));
+  const float sd_x = __fsqrt_ru(__fdiv_rn(x_diff, n));
+  const float sd_y = __fsqrt_ru(__fdiv_rn(y_diff, n));
+  const float r_xy = __fdiv_ru(__fsub_rn(xysum, __fdiv_rn(__fmul_ru(xsum, ysum), n)),
+                               __fsqrt_ru(__fmul_rn(x_diff, y_diff)));
+  const float beta = __fmul_ru(r_xy, __fdiv_ru(sd_y, sd_x));
+  const float alpha = __fmaf_ru(-beta, xbar, ybar);
+  if (beta < 0.0f) res.x = __fsub_rn(1.0f, __expf(beta));
+  if (alpha < 0.0f) res.y = __fsub_rn(1.0f, __expf(alpha));
+  return res;
+}
+
 // Long-form row of pair (gi, gj): square_to_condensed (src/dist/matrix_idx.hpp:46-50)
 // for all-vs-all, gi * n_cols + gj for query-vs-reference (src/api.cpp:251).
 __device__ __forceinline__ int64_t pair_row(const JobParams &p, int64_t gi, int64_t gj) {
@@ -221,6 +278,13 @@ __device__ __forceinline__ void finish_pair(const JobParams &p, int64_t gi, int6
   if (p.out_mode == kOutCounts) {
     uint32_t *o = static_cast<uint32_t *>(p.out) + row * K;
     for (int k = 0; k < K; ++k) o[k] = counts[k * stride];
+    return;
+  }
+  if (p.semantics == kSemRefGpu &&
+      (p.out_mode == kOutCoreAcc || (p.out_mode == kOutColumn && p.out_col < 2))) {
+    const float2 ca = refgpu_core_acc(p, gi, gj, counts, stride);
+    if (p.out_mode == kOutCoreAcc) static_cast<float2 *>(p.out)[row] = ca;
+    else static_cast<float *>(p.out)[row] = p.out_col == 0 ? ca.x : ca.y;
     return;
   }
   float jf[KMAX];

@@ -47,6 +47,7 @@ struct sk_ctx {
   sk::DevStatus *status_dev = nullptr;
   unsigned long long last_tiles = 0;
   int tile_cfg = 0;                               // forced tile shape (0 = automatic)
+  int semantics = 0;                              // sk::Semantics of later calls
   std::map<std::pair<int, int>, int> tuning;      // (K, s64) -> shape id
   Scratch scratch[kSlotCount];                    // reusable device buffers
   std::recursive_mutex mu;
@@ -68,6 +69,8 @@ struct sk_db {
   std::vector<uint64_t> seq_len;  // per-sample sequence lengths
   double *jv = nullptr;           // [K][ng*64] equal-base factors
   int jv_rc = -1;
+  float *jgpu = nullptr;          // [K] equal-base chances of the reference GPU path
+  int jgpu_rc = -1;
 };
 
 struct sk_random {
@@ -141,6 +144,7 @@ sk_status dense_to_device(sk_ctx *ctx, const sk_db *ref, const sk_db *query,
                           const sk_random *random, int out_mode, int out_col, void *d_out);
 int64_t n_pairs(const sk_db *ref, const sk_db *query);
 sk_status ensure_jv(sk_ctx *ctx, sk_db *db, int use_rc);
+std::vector<float> equal_base_gpu(const sk_db *db, int use_rc);
 size_t out_bytes(int out_mode, int64_t pairs, int K);
 
 }  // namespace sk

@@ -23,6 +23,7 @@ STATUS_NAMES = {
     5: "SK_ECANCELLED", 6: "SK_ETIMEDOUT", 7: "SK_ENOTSUP", 8: "SK_EKERNEL", 9: "SK_ERANGE",
 }
 RANDOM_NONE, RANDOM_EQUAL_BASE, RANDOM_TABLE = 0, 1, 2
+SEMANTICS_REFERENCE_CPU, SEMANTICS_REFERENCE_GPU = 0, 1
 OUT_CORE_ACC, OUT_JACCARD, OUT_COUNTS = 0, 1, 2
 
 _p = C.c_void_p
@@ -39,6 +40,7 @@ _SIGNATURES = {
     "sk_device_info": (_i32, [_p, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i32)]),
     "sk_ctx_synchronize": (_i32, [_p]),
     "sk_ctx_set_tile_config": (_i32, [_p, _i32]),
+    "sk_ctx_set_semantics": (_i32, [_p, _i32]),
     "sk_tile_config_count": (_i32, []),
     "sk_tile_config_info": (_i32, [_i32] + [C.POINTER(_i32)] * 5),
     "sk_ctx_load_tuning": (_i32, [_p, C.c_char_p]),
@@ -193,6 +195,11 @@ class Context:
 
     def set_tile_config(self, config_id: int):
         _check(lib.sk_ctx_set_tile_config(self.handle, config_id), self)
+
+    def set_semantics(self, semantics: int):
+        """SEMANTICS_REFERENCE_CPU (default) or SEMANTICS_REFERENCE_GPU: which
+        reference path the core/accessory fit reproduces (sk_ctx_set_semantics)."""
+        _check(lib.sk_ctx_set_semantics(self.handle, semantics), self)
 
     def load_tuning(self, path: str):
         _check(lib.sk_ctx_load_tuning(self.handle, str(path).encode()), self)

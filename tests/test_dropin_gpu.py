@@ -195,3 +195,42 @@ def test_api_errors(small_mass):
         pp_sketchlib.constructDatabase("x", ["a"], [["a.fa"]], [15], 10000)
     with pytest.raises(RuntimeError, match="dist_col out of range"):
         pp_sketchlib.querySelfSparse(s["ref"], r, s["kmers"], kNN=2, dist_col=3)
+
+
+@pytest.mark.skipif(not oracle.ref_gpu_available(), reason="oracle/_ref/libref_gpu.so not built")
+def test_semantics_gpu_matches_reference_kernel(tmp_path):
+    """queryDatabase(..., semantics="gpu") reproduces the reference GPU path:
+    the Monte Carlo table is copied up to k_max inclusive (flattened_random,
+    src/random/random_match.cpp:300) and indexed [k][ref cluster][query
+    cluster], and the fit is the reference kernel's, bit for bit."""
+    n, nq, K = 80, 20, 6
+    words, _ = random_sketches(n + nq, K, 64, seed=93)
+    kmers = np.arange(11, 11 + 2 * K, 2, dtype=np.int32)
+    names = [f"s{i:03d}" for i in range(n + nq)]
+    rng = np.random.default_rng(9)
+    C = 3
+    centroids = rng.dirichlet(np.ones(4) * 20, C).astype(np.float32)
+    bases = rng.dirichlet(np.ones(4) * 20, n + nq)
+    rand = dict(k_min=3, k_max=int(kmers[-1]), use_rc=1,        # last k == k_max: GPU keeps it
+                table={nm: int(rng.integers(C)) for nm in names[:n]},
+                matches={k: rng.uniform(0, 0.02, (C, C)).astype(np.float32) for k in range(3, 40)},
+                centroids=centroids)
+    h5write.write_sketch_db(str(tmp_path / "r.h5"), names[:n], words[:n], kmers, 64,
+                            base_freq=bases[:n], random=rand)
+    h5write.write_sketch_db(str(tmp_path / "q.h5"), names[n:], words[n:], kmers, 64,
+                            base_freq=bases[n:])
+    info = pp_sketchlib._load_random(str(tmp_path / "r"))
+    table = np.stack([rand["matches"][int(k)] for k in kmers]).astype(np.float32)
+    cl_ref = np.array([rand["table"][nm] for nm in names[:n]], np.uint16)
+    r = names[:n]
+    got = pp_sketchlib.queryDatabase(str(tmp_path / "r"), str(tmp_path / "r"), r, r, list(kmers),
+                                     use_gpu=True, semantics="gpu")
+    want = oracle.RefGpuKernel().dists(words[:n], kmers, 64, table=table, ref_lookup=cl_ref)
+    np.testing.assert_array_equal(got, want)
+    # the default follows the CPU path, which differs
+    cpu = pp_sketchlib.queryDatabase(str(tmp_path / "r"), str(tmp_path / "r"), r, r, list(kmers))
+    assert np.any(cpu != want)
+    assert info["k_max"] == int(kmers[-1])
+    with pytest.raises(ValueError):
+        pp_sketchlib.queryDatabase(str(tmp_path / "r"), str(tmp_path / "r"), r, r, list(kmers),
+                                   semantics="fast")

@@ -102,3 +102,104 @@ def test_reference_gpu_kernel_on_synthetic_tree(gpu_ctx, random_k, c_max, min_ke
     ours, ref, keep, bad = compare(gpu_ctx, words, kmers, s64, random_k=rk)
     assert keep.mean() > min_keep
     assert not bad.any(), np.argwhere(bad)[:10]
+
+
+# ---------------------------------------------------------------------------
+# SK_SEMANTICS_REFERENCE_GPU: the same kernel with the reference GPU path's
+# arithmetic must give the reference kernel's output bit for bit, including
+# the pairs the CPU semantics treat differently (first-low-k truncation,
+# equal Jaccards, float rounding).
+
+@pytest.fixture
+def gpu_semantics(gpu_ctx):
+    from sketchlib_b200 import capi
+    gpu_ctx.set_semantics(capi.SEMANTICS_REFERENCE_GPU)
+    yield gpu_ctx
+    gpu_ctx.set_semantics(capi.SEMANTICS_REFERENCE_CPU)
+
+
+def _synthetic(n, kmers, s64, seed, c_max=0.03):
+    from sketchlib_b200 import capi, synth
+    parent, thresh = synth.random_tree(n, kmers=kmers, seed=seed, c_max=c_max)
+    return capi.synth_host(parent, thresh, s64, seed=seed)
+
+
+def test_gpu_semantics_bit_identical_on_reference_sketches(gpu_semantics):
+    from sketchlib_b200 import capi
+    if not oracle.sketcher_available():
+        pytest.skip("oracle/_ref/libref_sketch.so not built")
+    kmers = list(range(15, 31, 2))
+    rs = oracle.RefSketcher()
+    words = rs.sketch(rs.genomes(64, 2_500_000, 0x5EED0001), kmers, 156)
+    db = capi.Database(gpu_semantics, words, kmers, 156)
+    np.testing.assert_array_equal(capi.dists_dense(gpu_semantics, db),
+                                  oracle.RefGpuKernel().dists(words, kmers, 156))
+
+
+@pytest.mark.parametrize("kind", ["none", "equal_base", "table"])
+def test_gpu_semantics_bit_identical_self(gpu_semantics, kind):
+    from sketchlib_b200 import capi
+    kmers = [13, 17, 21, 25, 29, 33]
+    words = _synthetic(300, kmers, 64, 0x5EED00A1)     # includes truncated and flat pairs
+    n = words.shape[0]
+    rng = np.random.default_rng(5)
+    lens = rng.integers(1_000_000, 6_000_000, n).astype(np.uint64)
+    cl = rng.integers(0, 3, n).astype(np.uint16)
+    table = rng.uniform(0, 0.02, (len(kmers), 3, 3)).astype(np.float32)
+    if kind == "none":
+        rnd, witness = None, {}
+    elif kind == "equal_base":
+        rnd = capi.Random(gpu_semantics, capi.RANDOM_EQUAL_BASE, kmers)
+        per_k = np.array([oracle.csrs(k, True, int(lens[0]), int(lens[0])) for k in kmers], np.float32)
+        witness = dict(table=per_k)
+    else:
+        rnd = capi.Random(gpu_semantics, capi.RANDOM_TABLE, kmers, table=table)
+        witness = dict(table=table, ref_lookup=cl)
+    db = capi.Database(gpu_semantics, words, kmers, 64, cluster=cl, seq_len=lens)
+    got = capi.dists_dense(gpu_semantics, db, random=rnd)
+    want = oracle.RefGpuKernel().dists(words, kmers, 64, **witness)
+    np.testing.assert_array_equal(got, want)
+    # the CPU semantics differ on some of these pairs: the comparison has teeth
+    gpu_semantics.set_semantics(capi.SEMANTICS_REFERENCE_CPU)
+    assert np.any(capi.dists_dense(gpu_semantics, db, random=rnd) != want)
+
+
+@pytest.mark.parametrize("kind", ["none", "table"])
+def test_gpu_semantics_bit_identical_query(gpu_semantics, kind):
+    from sketchlib_b200 import capi
+    kmers = [15, 19, 23, 27, 31]
+    words = _synthetic(900, kmers, 32, 0x5EED00A2)
+    qw, rw = words[:150], words[150:]
+    rng = np.random.default_rng(6)
+    rcl = rng.integers(0, 4, rw.shape[0]).astype(np.uint16)
+    qcl = rng.integers(0, 4, qw.shape[0]).astype(np.uint16)
+    table = rng.uniform(0, 0.02, (len(kmers), 4, 4)).astype(np.float32)
+    rnd = None if kind == "none" else capi.Random(gpu_semantics, capi.RANDOM_TABLE, kmers, table=table)
+    witness = {} if kind == "none" else dict(table=table, ref_lookup=rcl, query_lookup=qcl)
+    ref = capi.Database(gpu_semantics, rw, kmers, 32, cluster=rcl)
+    qry = capi.Database(gpu_semantics, qw, kmers, 32, cluster=qcl)
+    got = capi.dists_dense(gpu_semantics, ref, qry, random=rnd)
+    want = oracle.RefGpuKernel().dists(rw, kmers, 32, query_words=qw, **witness)
+    np.testing.assert_array_equal(got, want)
+    # the pipelined host-to-host call follows the same semantics
+    got2 = capi.query_db(gpu_semantics, rw, kmers, 32, query_words=qw, ref_cluster=rcl,
+                         query_cluster=qcl, random=rnd)
+    np.testing.assert_array_equal(got2, want)
+
+
+def test_gpu_semantics_knn(gpu_semantics):
+    """kNN under GPU semantics ranks the reference kernel's distances."""
+    from sketchlib_b200 import capi
+    kmers = [13, 17, 21, 25, 29, 33]
+    words = _synthetic(300, kmers, 64, 0x5EED00A3)
+    n = words.shape[0]
+    db = capi.Database(gpu_semantics, words, kmers, 64)
+    want = oracle.RefGpuKernel().dists(words, kmers, 64)
+    i, j, d = capi.dists_knn(gpu_semantics, db, 5, dist_col=1)
+    sq = np.full((n, n), np.inf)
+    iu = np.triu_indices(n, 1)
+    sq[iu] = want[:, 1]
+    sq[(iu[1], iu[0])] = want[:, 1]
+    order = np.lexsort((np.tile(np.arange(n), (n, 1)), sq), axis=1)[:, :5]
+    np.testing.assert_array_equal(j.reshape(n, 5), order)
+    np.testing.assert_array_equal(d.reshape(n, 5), np.take_along_axis(sq, order, 1).astype(np.float32))
