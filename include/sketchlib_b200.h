@@ -317,8 +317,10 @@ typedef struct sk_server_params {
 
 /* Starts a server over `ref` (kept resident; it must outlive the server).
  * Every slot's buffers are allocated here, so the HBM footprint is fixed and
- * requests are admitted as slots free up.  No reference counterpart: the
- * reference answers one query_db_cuda call at a time (src/gpu/gpu_api.cpp:352). */
+ * requests are admitted as slots free up.  The context's tile shape, tuning
+ * and semantics at this moment apply to every request.  No reference
+ * counterpart: the reference answers one query_db_cuda call at a time
+ * (src/gpu/gpu_api.cpp:352). */
 sk_status sk_server_create(sk_ctx *ctx, const sk_db *ref, const sk_random *random,
                            const sk_server_params *params, sk_server **out);
 /* Queues a request: n_queries sketches in the reference word layout (host

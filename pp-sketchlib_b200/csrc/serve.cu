@@ -312,6 +312,7 @@ sk_status sk_server_create(sk_ctx *ctx, const sk_db *ref, const sk_random *rando
     if (st != SK_OK) break;
     s.ctx->tile_cfg = ctx->tile_cfg;
     s.ctx->tuning = ctx->tuning;
+    s.ctx->semantics = ctx->semantics;   // fixed for the server's lifetime
     s.qdb.ctx = s.ctx;
     s.qdb.K = ref->K;
     s.qdb.s64 = ref->s64;

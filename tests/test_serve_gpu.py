@@ -91,3 +91,26 @@ def test_server_wait_timeout_and_bad_ticket(setup):
         assert np.all(np.diff(dist, axis=1) >= 0)
     finally:
         server.close()
+
+
+def test_server_keeps_the_context_semantics(setup):
+    """A server created under the reference-GPU semantics answers with them."""
+    ctx, ref, queries, kmers = setup
+    q = queries[:40]
+    ctx.set_semantics(capi.SEMANTICS_REFERENCE_GPU)
+    try:
+        e_rows, e_idx, e_dist = _expected(ctx, ref, q, kmers, 5)
+        server = capi.Server(ctx, ref, slots=2, slice_queries=16, kNN=5, keep_rows=True)
+    finally:
+        ctx.set_semantics(capi.SEMANTICS_REFERENCE_CPU)
+    try:
+        t = server.submit(q)
+        server.wait(t)
+        idx, dist, rows, _ = server.result(t)
+        np.testing.assert_array_equal(rows, e_rows)
+        np.testing.assert_array_equal(idx, e_idx)
+        np.testing.assert_array_equal(dist, e_dist)
+        cpu_rows, _, _ = _expected(ctx, ref, q, kmers, 5)
+        assert np.any(cpu_rows != rows)
+    finally:
+        server.close()
