@@ -129,6 +129,13 @@ sk_status sk_ctx_set_tile_config(sk_ctx *ctx, int32_t config_id);
  * first reference sample's length for every pair (src/gpu/gpu_api.cpp:402-403).
  * Jaccard and count outputs are the same under both. */
 sk_status sk_ctx_set_semantics(sk_ctx *ctx, int32_t semantics);
+/* Device memory, in bytes, a dense call returning to the host may use for its
+ * output (0 = the free memory less 2 GiB, the default).  A larger output is
+ * computed in blocks of rows that are copied back while the next block
+ * computes, as the reference splits an all-vs-all that exceeds device memory
+ * into chunks (query_db_cuda, src/gpu/gpu_api.cpp:357-389); query-vs-reference
+ * outputs are blocked the same way (the reference refuses them). */
+sk_status sk_ctx_set_memory_limit(sk_ctx *ctx, int64_t bytes);
 int32_t sk_tile_config_count(void);
 /* Describes shape `config_id`: rows x cols of the CTA tile and per-thread block. */
 sk_status sk_tile_config_info(int32_t config_id, int32_t *tile_rows,

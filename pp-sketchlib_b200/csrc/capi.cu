@@ -63,8 +63,8 @@ static void ctx_free(sk_ctx *ctx) {
       cudaStreamDestroy(ctx->copy_stream);
     }
     for (int b = 0; b < 2; ++b) {
-      if (ctx->ev_landed[b]) cudaEventDestroy(ctx->ev_landed[b]);
-      if (ctx->ev_packed[b]) cudaEventDestroy(ctx->ev_packed[b]);
+      if (ctx->ev_ready[b]) cudaEventDestroy(ctx->ev_ready[b]);
+      if (ctx->ev_free[b]) cudaEventDestroy(ctx->ev_free[b]);
     }
   }
   delete ctx;
@@ -481,6 +481,152 @@ sk_status dense_to_device(sk_ctx *ctx, const sk_db *ref, const sk_db *query,
   return launch_job(ctx, jp, *cfg);
 }
 
+// The context's second stream and its double-buffer events.
+sk_status ensure_copy_stream(sk_ctx *ctx) {
+  cudaError_t e = cudaSuccess;
+  if (!ctx->copy_stream) e = cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking);
+  for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
+    if (!ctx->ev_ready[b]) e = cudaEventCreateWithFlags(&ctx->ev_ready[b], cudaEventDisableTiming);
+    if (e == cudaSuccess && !ctx->ev_free[b])
+      e = cudaEventCreateWithFlags(&ctx->ev_free[b], cudaEventDisableTiming);
+  }
+  return e == cudaSuccess ? SK_OK : cuda_fail(ctx, e, "copy stream setup");
+}
+
+// Device bytes a dense call may use to stage its output: the context's limit,
+// else the free memory less a 2 GiB margin.
+size_t dense_budget(sk_ctx *ctx) {
+  if (ctx->mem_limit > 0) return static_cast<size_t>(ctx->mem_limit);
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return 0;
+  const size_t margin = size_t(2) << 30;
+  return free_b > 2 * margin ? free_b - margin : free_b / 2;
+}
+
+// Dense distances to a host buffer in blocks of row tiles, for outputs larger
+// than the device memory allowed for them (the reference's query_db_cuda
+// estimates memory and splits the all-vs-all into chunks,
+// src/gpu/gpu_api.cpp:357-389, and refuses query mode).  A block of row tiles
+// is a contiguous range of tiles and of long-form rows, so each block is one
+// persistent launch into one of two device buffers, copied back on the copy
+// stream while the next block computes.
+sk_status dense_blocked_to_host(sk_ctx *ctx, const sk_db *ref, const sk_db *query,
+                                const sk_random *random, int out_mode, void *out, size_t budget) {
+  JobParams base;
+  const TileConfig *cfg = nullptr;
+  sk_status st = build_job(ctx, ref, query, random, out_mode, 0, nullptr, &cfg, &base);
+  if (st != SK_OK) return st;
+  st = ensure_copy_stream(ctx);
+  if (st != SK_OK) return st;
+  const int grid = resident_grid(ctx, *cfg);
+  if (grid < 1) return fail(ctx, SK_ECUDA, "Tile configuration %d does not fit the device", cfg->id);
+  const size_t elem = out_bytes(out_mode, 1, base.n_kmers);
+  const int64_t nrt = base.n_row_tiles;
+  const int64_t m = base.tile_rows / base.tile_cols;
+  auto first_row = [&](int64_t ti) -> int64_t {   // first long-form row of row tile ti
+    if (base.self) {
+      const int64_t i = std::min<int64_t>(ti * base.tile_rows, base.n_rows - 1);
+      return base.n_rows * i - i * (i + 1) / 2;
+    }
+    return std::min<int64_t>(ti * base.tile_rows, base.n_rows) * base.n_cols;
+  };
+  auto first_tile = [&](int64_t ti) -> int64_t {
+    return base.self ? ti * base.n_col_tiles - m * ti * (ti - 1) / 2 : ti * base.n_col_tiles;
+  };
+  // blocks of whole row tiles, each within half the budget (two buffers)
+  const int64_t cap = std::max<int64_t>(1, static_cast<int64_t>(budget / 2 / elem));
+  std::vector<int64_t> cut{0};
+  int64_t max_rows = 0;
+  while (cut.back() < nrt) {
+    const int64_t t0 = cut.back();
+    int64_t t1 = t0 + 1;
+    while (t1 < nrt && first_row(t1 + 1) - first_row(t0) <= cap) ++t1;
+    max_rows = std::max(max_rows, first_row(t1) - first_row(t0));
+    cut.push_back(t1);
+  }
+  const int nblk = static_cast<int>(cut.size() - 1);
+  std::vector<JobParams> jobs(nblk, base);
+  std::vector<WorkItem> items;
+  std::vector<size_t> start(nblk), count(nblk);
+  std::vector<int32_t> splits(nblk);
+  for (int c = 0; c < nblk; ++c) {
+    jobs[c].out_row0 = first_row(cut[c]);
+    start[c] = items.size();
+    for (int64_t t = first_tile(cut[c]); t < first_tile(cut[c + 1]); ++t)
+      items.push_back(WorkItem{t, c, 0, static_cast<int16_t>(base.n_kmers), -1, 1});
+    split_tail(items, start[c], grid, &splits[c]);
+    count[c] = items.size() - start[c];
+  }
+  int32_t max_splits = *std::max_element(splits.begin(), splits.end());
+  const size_t items_off = (jobs.size() * sizeof(JobParams) + 255) & ~static_cast<size_t>(255);
+  const size_t ctrl_off = (items_off + items.size() * sizeof(WorkItem) + 255) & ~static_cast<size_t>(255);
+  std::vector<size_t> ctrl_at(nblk);
+  size_t meta_bytes = ctrl_off;
+  for (int c = 0; c < nblk; ++c) {
+    ctrl_at[c] = meta_bytes;
+    meta_bytes += (8 + static_cast<size_t>(splits[c]) * cfg->threads * 4 + 255) & ~static_cast<size_t>(255);
+  }
+  const size_t slot = count_slot_bytes(*cfg, base.n_kmers);
+  void *meta = nullptr, *cta = nullptr, *split = nullptr, *obuf = nullptr;
+  st = scratch(ctx, kSlotLaunchMeta, meta_bytes, &meta);
+  if (st == SK_OK) st = scratch(ctx, kSlotCounts, static_cast<size_t>(grid) * slot, &cta);
+  if (st == SK_OK)
+    st = scratch(ctx, kSlotSplitCounts, std::max<size_t>(static_cast<size_t>(max_splits) * slot, 16), &split);
+  if (st == SK_OK) st = scratch(ctx, kSlotOut, 2 * static_cast<size_t>(max_rows) * elem, &obuf);
+  if (st != SK_OK) return st;
+  char *buf[2] = {static_cast<char *>(obuf), static_cast<char *>(obuf) + max_rows * elem};
+  for (int c = 0; c < nblk; ++c) jobs[c].out = buf[c & 1];
+  char *mt = static_cast<char *>(meta);
+  cudaError_t e = cudaMemcpyAsync(mt, jobs.data(), jobs.size() * sizeof(JobParams),
+                                  cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(mt + items_off, items.data(), items.size() * sizeof(WorkItem),
+                        cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(mt + ctrl_off, 0, meta_bytes - ctrl_off, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "work list upload");
+  LaunchParams lp{};
+  lp.jobs = reinterpret_cast<const JobParams *>(mt);
+  lp.cta_scratch = static_cast<uint16_t *>(cta);
+  lp.split_scratch = static_cast<uint16_t *>(split);
+  lp.k_slots = base.n_kmers;
+  lp.status = ctx->status_dev;
+  lp.cancel = ctx->cancel_dev;
+  // block c computes into buf[c & 1] once the copy of block c - 2 has left it;
+  // its copy is queued after block c + 1's launch, so a pageable destination
+  // (whose copy returns only when done) still overlaps the next block
+  auto copy_back = [&](int c) -> cudaError_t {
+    const int b = c & 1;
+    const size_t rows = static_cast<size_t>(first_row(cut[c + 1]) - first_row(cut[c]));
+    cudaError_t e2 = cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_ready[b], 0);
+    if (e2 == cudaSuccess)
+      e2 = cudaMemcpyAsync(static_cast<char *>(out) + first_row(cut[c]) * elem, buf[b], rows * elem,
+                           cudaMemcpyDeviceToHost, ctx->copy_stream);
+    if (e2 == cudaSuccess) e2 = cudaEventRecord(ctx->ev_free[b], ctx->copy_stream);
+    return e2;
+  };
+  for (int c = 0; c <= nblk && e == cudaSuccess; ++c) {
+    if (c < nblk) {
+      const int b = c & 1;
+      if (c >= 2) e = cudaStreamWaitEvent(ctx->stream, ctx->ev_free[b], 0);
+      if (e == cudaSuccess && count[c] > 0) {
+        LaunchParams l = lp;
+        l.items = reinterpret_cast<const WorkItem *>(mt + items_off) + start[c];
+        l.n_items = static_cast<int64_t>(count[c]);
+        l.item_counter = reinterpret_cast<unsigned long long *>(mt + ctrl_at[c]);
+        l.split_done = reinterpret_cast<unsigned int *>(mt + ctrl_at[c] + 8);
+        e = cfg->launch(l, static_cast<int>(std::min<int64_t>(grid, l.n_items)), ctx->stream);
+      }
+      if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_ready[b], ctx->stream);
+    }
+    if (e == cudaSuccess && c >= 1) e = copy_back(c - 1);
+  }
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "blocked distance computation");
+  // the compute stream (whose completion finish_call reports) waits for the last copies
+  for (int b = 0; b < 2 && e == cudaSuccess; ++b) e = cudaStreamWaitEvent(ctx->stream, ctx->ev_free[b], 0);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "blocked distance computation");
+  return SK_OK;
+}
+
 }  // namespace sk
 
 // ------------------------------------------------------------------ context
@@ -537,6 +683,13 @@ sk_status sk_ctx_set_stream(sk_ctx *ctx, void *stream) {
   if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
   ctx->stream = static_cast<cudaStream_t>(stream);
   ctx->own_stream = false;
+  return SK_OK;
+}
+
+sk_status sk_ctx_set_memory_limit(sk_ctx *ctx, int64_t bytes) {
+  SK_GUARD(ctx);
+  if (bytes < 0) return fail(ctx, SK_EINVAL, "negative memory limit");
+  ctx->mem_limit = bytes;
   return SK_OK;
 }
 
@@ -850,6 +1003,14 @@ sk_status sk_dists_dense(sk_ctx *ctx, const sk_db *ref, const sk_db *query, cons
   const int64_t pairs = n_pairs(ref, query);
   if (pairs > 0 && !out) return fail(ctx, SK_EINVAL, "null output buffer");
   const size_t bytes = ref ? out_bytes(out_mode, pairs, ref->K) : 0;
+  if (!out_on_device && bytes > 0) {
+    const size_t budget = dense_budget(ctx);
+    if (bytes > budget) {
+      st = dense_blocked_to_host(ctx, ref, query, random, out_mode, out, budget);
+      if (st != SK_OK) return st;
+      return finish_call(ctx);
+    }
+  }
   void *d_out = out;
   if (!out_on_device && bytes > 0) {
     st = scratch(ctx, kSlotOut, bytes, &d_out);

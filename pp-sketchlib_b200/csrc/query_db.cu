@@ -43,17 +43,6 @@ int64_t chunk_samples(int64_t n) {
   return std::max<int64_t>(kChunkAlign, (per + kChunkAlign - 1) / kChunkAlign * kChunkAlign);
 }
 
-sk_status ensure_pipeline(sk_ctx *ctx) {
-  cudaError_t e = cudaSuccess;
-  if (!ctx->copy_stream) e = cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking);
-  for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
-    if (!ctx->ev_landed[b]) e = cudaEventCreateWithFlags(&ctx->ev_landed[b], cudaEventDisableTiming);
-    if (e == cudaSuccess && !ctx->ev_packed[b])
-      e = cudaEventCreateWithFlags(&ctx->ev_packed[b], cudaEventDisableTiming);
-  }
-  return e == cudaSuccess ? SK_OK : cuda_fail(ctx, e, "copy stream setup");
-}
-
 // One host-to-device chunk.
 struct Unit {
   sk_db *db;
@@ -100,7 +89,7 @@ extern "C" sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
     return fail(ctx, SK_EINVAL, "Query with empty ref or query list!");
   if (out_mode != kOutCoreAcc && out_mode != kOutJaccard && out_mode != kOutCounts)
     return fail(ctx, SK_EINVAL, "Unknown output mode %d", out_mode);
-  st = ensure_pipeline(ctx);
+  st = ensure_copy_stream(ctx);
   if (st != SK_OK) return st;
 
   CallDbs dbs{ctx};
@@ -112,9 +101,15 @@ extern "C" sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
   if (pairs > 0 && !out) return fail(ctx, SK_EINVAL, "null output buffer");
   if (pairs == 0) return finish_call(ctx);
   const size_t out_sz = out_bytes(out_mode, pairs, n_kmers);
+  // an output above the device memory allowed for it is computed in row
+  // blocks after the upload (dense_blocked_to_host); the upload still streams
+  const size_t budget = dense_budget(ctx);
+  const bool blocked = out_sz > budget;
   void *d_out = nullptr;
-  st = scratch(ctx, kSlotOut, out_sz, &d_out);
-  if (st != SK_OK) return st;
+  if (!blocked) {
+    st = scratch(ctx, kSlotOut, out_sz, &d_out);
+    if (st != SK_OK) return st;
+  }
 
   JobParams jp;
   const TileConfig *cfg = nullptr;
@@ -201,21 +196,21 @@ extern "C" sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
   for (size_t i = 0; i < units.size(); ++i) {
     const Unit &u = units[i];
     const int b = static_cast<int>(i & 1);
-    if (i >= 2) e = cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_packed[b], 0);
+    if (i >= 2) e = cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_free[b], 0);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(stage[b], u.host, static_cast<size_t>(u.n * wps) * 8, cudaMemcpyHostToDevice,
                           ctx->copy_stream);
-    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_landed[b], ctx->copy_stream);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, ctx->ev_landed[b], 0);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_ready[b], ctx->copy_stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, ctx->ev_ready[b], 0);
     const int32_t g0 = static_cast<int32_t>(u.s0 / kGranule);
     const bool last_of_db = u.s0 + u.n == u.db->n;
     const int32_t ng = last_of_db ? u.db->ng - g0 : static_cast<int32_t>(u.n / kGranule);
     if (e == cudaSuccess)
       e = launch_pack_range(stage[b], u.n, n_kmers, sketchsize64, ng, g0, u.db->ng, u.db->packed,
                             ctx->stream);
-    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_packed[b], ctx->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_free[b], ctx->stream);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "sketch upload");
-    if (u.chunk >= 0 && count[u.chunk] > 0) {
+    if (!blocked && u.chunk >= 0 && count[u.chunk] > 0) {
       LaunchParams lp = base;
       lp.items = d_items + start[u.chunk];
       lp.n_items = static_cast<int64_t>(count[u.chunk]);
@@ -225,6 +220,10 @@ extern "C" sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
       e = cfg->launch(lp, g, ctx->stream);
       if (e != cudaSuccess) return cuda_fail(ctx, e, "distance kernel launch");
     }
+  }
+  if (blocked) {
+    st = dense_blocked_to_host(ctx, dbs.ref, dbs.query, random, out_mode, out, budget);
+    return st == SK_OK ? finish_call(ctx) : st;
   }
   e = cudaMemcpyAsync(out, d_out, out_sz, cudaMemcpyDeviceToHost, ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "result copy");

@@ -58,6 +58,7 @@ struct JobParams {
   int64_t n_tiles;
   int32_t n_row_tiles, n_col_tiles;
   void *out;                   // device output
+  int64_t out_row0;            // long-form row held by out[0] (0 unless the output is blocked)
   double tol;                  // 5 / (64 * s64) (src/dist/linear_regression.cpp:22)
   double union_bits;           // 64 * s64 (src/reference.cpp:91)
   // random-match correction

@@ -262,10 +262,11 @@ __device__ __forceinline__ float2 refgpu_core_acc(const JobParams &p, int64_t gi
 }
 
 // Long-form row of pair (gi, gj): square_to_condensed (src/dist/matrix_idx.hpp:46-50)
-// for all-vs-all, gi * n_cols + gj for query-vs-reference (src/api.cpp:251).
+// for all-vs-all, gi * n_cols + gj for query-vs-reference (src/api.cpp:251),
+// relative to the first row held by the output buffer.
 __device__ __forceinline__ int64_t pair_row(const JobParams &p, int64_t gi, int64_t gj) {
-  if (p.self) return p.n_rows * gi - ((gi * (gi + 1)) >> 1) + gj - 1 - gi;
-  return gi * p.n_cols + gj;
+  if (p.self) return p.n_rows * gi - ((gi * (gi + 1)) >> 1) + gj - 1 - gi - p.out_row0;
+  return gi * p.n_cols + gj - p.out_row0;
 }
 
 // Finishes one pair from its K intersection counts (counts[k * stride]) and

@@ -37,9 +37,10 @@ struct sk_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = true;
-  cudaStream_t copy_stream = nullptr;   // uploads overlapped with kernels (created on first use)
-  cudaEvent_t ev_landed[2] = {};        // staging buffer b holds a chunk
-  cudaEvent_t ev_packed[2] = {};        // staging buffer b is free again
+  cudaStream_t copy_stream = nullptr;   // copies overlapped with kernels (created on first use)
+  cudaEvent_t ev_ready[2] = {};         // double buffer b holds data
+  cudaEvent_t ev_free[2] = {};          // double buffer b may be overwritten
+  int64_t mem_limit = 0;                // bytes a dense call may stage output in (0 = free memory)
   int sm_count = 0;
   std::string err;
   int *cancel_host = nullptr;   // mapped pinned word polled by the kernels
@@ -145,6 +146,10 @@ sk_status dense_to_device(sk_ctx *ctx, const sk_db *ref, const sk_db *query,
 int64_t n_pairs(const sk_db *ref, const sk_db *query);
 sk_status ensure_jv(sk_ctx *ctx, sk_db *db, int use_rc);
 std::vector<float> equal_base_gpu(const sk_db *db, int use_rc);
+sk_status ensure_copy_stream(sk_ctx *ctx);
+size_t dense_budget(sk_ctx *ctx);
+sk_status dense_blocked_to_host(sk_ctx *ctx, const sk_db *ref, const sk_db *query,
+                                const sk_random *random, int out_mode, void *out, size_t budget);
 size_t out_bytes(int out_mode, int64_t pairs, int K);
 
 }  // namespace sk

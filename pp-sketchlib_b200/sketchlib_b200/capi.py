@@ -41,6 +41,7 @@ _SIGNATURES = {
     "sk_ctx_synchronize": (_i32, [_p]),
     "sk_ctx_set_tile_config": (_i32, [_p, _i32]),
     "sk_ctx_set_semantics": (_i32, [_p, _i32]),
+    "sk_ctx_set_memory_limit": (_i32, [_p, _i64]),
     "sk_tile_config_count": (_i32, []),
     "sk_tile_config_info": (_i32, [_i32] + [C.POINTER(_i32)] * 5),
     "sk_ctx_load_tuning": (_i32, [_p, C.c_char_p]),
@@ -200,6 +201,11 @@ class Context:
         """SEMANTICS_REFERENCE_CPU (default) or SEMANTICS_REFERENCE_GPU: which
         reference path the core/accessory fit reproduces (sk_ctx_set_semantics)."""
         _check(lib.sk_ctx_set_semantics(self.handle, semantics), self)
+
+    def set_memory_limit(self, nbytes: int):
+        """Device bytes a dense call to host memory may stage its output in
+        (0 = free memory less 2 GiB); larger outputs are computed in row blocks."""
+        _check(lib.sk_ctx_set_memory_limit(self.handle, nbytes), self)
 
     def load_tuning(self, path: str):
         _check(lib.sk_ctx_load_tuning(self.handle, str(path).encode()), self)
