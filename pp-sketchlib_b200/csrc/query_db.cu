@@ -43,6 +43,20 @@ int64_t chunk_samples(int64_t n) {
   return std::max<int64_t>(kChunkAlign, (per + kChunkAlign - 1) / kChunkAlign * kChunkAlign);
 }
 
+// The second compute stream, the high-priority pack stream and the join event.
+sk_status ensure_compute_streams(sk_ctx *ctx) {
+  cudaError_t e = cudaSuccess;
+  if (!ctx->stream_b) e = cudaStreamCreateWithFlags(&ctx->stream_b, cudaStreamNonBlocking);
+  if (e == cudaSuccess && !ctx->pack_stream) {
+    int least = 0, greatest = 0;
+    e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if (e == cudaSuccess)
+      e = cudaStreamCreateWithPriority(&ctx->pack_stream, cudaStreamNonBlocking, greatest);
+  }
+  if (e == cudaSuccess && !ctx->ev_join) e = cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming);
+  return e == cudaSuccess ? SK_OK : cuda_fail(ctx, e, "compute stream setup");
+}
+
 // One host-to-device chunk.
 struct Unit {
   sk_db *db;
@@ -56,7 +70,8 @@ struct CallDbs {
   sk_ctx *ctx;
   sk_db *ref = nullptr, *query = nullptr;
   ~CallDbs() {
-    if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+    for (cudaStream_t st : {ctx->copy_stream, ctx->pack_stream, ctx->stream_b})
+      if (st) cudaStreamSynchronize(st);
     cudaStreamSynchronize(ctx->stream);
     if (ref) db_free(ref);
     if (query) db_free(query);
@@ -90,6 +105,7 @@ extern "C" sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
   if (out_mode != kOutCoreAcc && out_mode != kOutJaccard && out_mode != kOutCounts)
     return fail(ctx, SK_EINVAL, "Unknown output mode %d", out_mode);
   st = ensure_copy_stream(ctx);
+  if (st == SK_OK) st = ensure_compute_streams(ctx);
   if (st != SK_OK) return st;
 
   CallDbs dbs{ctx};
@@ -159,11 +175,13 @@ extern "C" sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
   }
   const size_t slot = count_slot_bytes(*cfg, jp.n_kmers);
   const int64_t wps = static_cast<int64_t>(n_kmers) * sketchsize64 * bbits;   // words per sample
-  void *meta = nullptr, *cta = nullptr, *split = nullptr, *staging = nullptr;
+  void *meta = nullptr, *staging = nullptr, *cta[2] = {}, *split[2] = {};
+  const size_t split_bytes = std::max<size_t>(static_cast<size_t>(max_splits) * slot, 16);
   st = scratch(ctx, kSlotLaunchMeta, meta_bytes, &meta);
-  if (st == SK_OK) st = scratch(ctx, kSlotCounts, static_cast<size_t>(grid) * slot, &cta);
-  if (st == SK_OK)
-    st = scratch(ctx, kSlotSplitCounts, std::max<size_t>(static_cast<size_t>(max_splits) * slot, 16), &split);
+  if (st == SK_OK) st = scratch(ctx, kSlotCounts, static_cast<size_t>(grid) * slot, &cta[0]);
+  if (st == SK_OK) st = scratch(ctx, kSlotCountsB, static_cast<size_t>(grid) * slot, &cta[1]);
+  if (st == SK_OK) st = scratch(ctx, kSlotSplitCounts, split_bytes, &split[0]);
+  if (st == SK_OK) st = scratch(ctx, kSlotSplitCountsB, split_bytes, &split[1]);
   if (st == SK_OK) st = scratch(ctx, kSlotStaging, static_cast<size_t>(2 * cs * wps) * 8, &staging);
   if (st != SK_OK) return st;
   char *m = static_cast<char *>(meta);
@@ -172,11 +190,12 @@ extern "C" sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
     e = cudaMemcpyAsync(m + items_off, items.data(), items.size() * sizeof(WorkItem),
                         cudaMemcpyHostToDevice, ctx->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(m + ctrl_off, 0, meta_bytes - ctrl_off, ctx->stream);
+  // the second compute stream starts after the status reset and the work list
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_join, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream_b, ctx->ev_join, 0);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "work list upload");
   LaunchParams base{};
   base.jobs = reinterpret_cast<const JobParams *>(m);
-  base.cta_scratch = static_cast<uint16_t *>(cta);
-  base.split_scratch = static_cast<uint16_t *>(split);
   base.k_slots = jp.n_kmers;
   base.status = ctx->status_dev;
   base.cancel = ctx->cancel_dev;
@@ -192,8 +211,22 @@ extern "C" sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
     const int64_t s0 = c * cs;
     units.push_back(Unit{dbs.ref, ref->words + s0 * wps, s0, std::min(cs, n_ref - s0), c});
   }
+  while (ctx->ev_chunk.size() < units.size()) {
+    cudaEvent_t ev = nullptr;
+    e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "chunk events");
+    ctx->ev_chunk.push_back(ev);
+  }
+  // copy stream: H2D of unit i into staging buffer i & 1 (once unit i - 2 is
+  // packed); pack stream (high priority, so its CTAs take SMs first): pack unit
+  // i; compute streams, alternating: the tiles chunk c completes, after its
+  // pack.  Chunk launches on the two streams overlap, so one launch's tail
+  // wave is filled by the next launch's CTAs; each stream has its own count
+  // scratch and every launch its own control block.
   uint64_t *stage[2] = {static_cast<uint64_t *>(staging), static_cast<uint64_t *>(staging) + cs * wps};
-  for (size_t i = 0; i < units.size(); ++i) {
+  cudaStream_t compute[2] = {ctx->stream, ctx->stream_b};
+  int launches = 0;
+  for (size_t i = 0; i < units.size() && e == cudaSuccess; ++i) {
     const Unit &u = units[i];
     const int b = static_cast<int>(i & 1);
     if (i >= 2) e = cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_free[b], 0);
@@ -201,26 +234,36 @@ extern "C" sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
       e = cudaMemcpyAsync(stage[b], u.host, static_cast<size_t>(u.n * wps) * 8, cudaMemcpyHostToDevice,
                           ctx->copy_stream);
     if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_ready[b], ctx->copy_stream);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, ctx->ev_ready[b], 0);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->pack_stream, ctx->ev_ready[b], 0);
     const int32_t g0 = static_cast<int32_t>(u.s0 / kGranule);
     const bool last_of_db = u.s0 + u.n == u.db->n;
     const int32_t ng = last_of_db ? u.db->ng - g0 : static_cast<int32_t>(u.n / kGranule);
     if (e == cudaSuccess)
       e = launch_pack_range(stage[b], u.n, n_kmers, sketchsize64, ng, g0, u.db->ng, u.db->packed,
-                            ctx->stream);
-    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_free[b], ctx->stream);
+                            ctx->pack_stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_free[b], ctx->pack_stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_chunk[i], ctx->pack_stream);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "sketch upload");
     if (!blocked && u.chunk >= 0 && count[u.chunk] > 0) {
+      const int w = launches++ & 1;
       LaunchParams lp = base;
+      lp.cta_scratch = static_cast<uint16_t *>(cta[w]);
+      lp.split_scratch = static_cast<uint16_t *>(split[w]);
       lp.items = d_items + start[u.chunk];
       lp.n_items = static_cast<int64_t>(count[u.chunk]);
       lp.item_counter = reinterpret_cast<unsigned long long *>(m + ctrl_at[u.chunk]);
       lp.split_done = reinterpret_cast<unsigned int *>(m + ctrl_at[u.chunk] + 8);
       const int g = static_cast<int>(std::min<int64_t>(grid, lp.n_items));
-      e = cfg->launch(lp, g, ctx->stream);
+      e = cudaStreamWaitEvent(compute[w], ctx->ev_chunk[i], 0);   // packs complete in unit order
+      if (e == cudaSuccess) e = cfg->launch(lp, g, compute[w]);
       if (e != cudaSuccess) return cuda_fail(ctx, e, "distance kernel launch");
     }
   }
+  // join: the context stream waits for the last pack and the second stream
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, ctx->ev_chunk[units.size() - 1], 0);
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_join, ctx->stream_b);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "stream join");
   if (blocked) {
     st = dense_blocked_to_host(ctx, dbs.ref, dbs.query, random, out_mode, out, budget);
     return st == SK_OK ? finish_call(ctx) : st;

@@ -30,7 +30,9 @@ enum ScratchSlot : int {
   kSlotStaging = 6,       // sketch words in the reference layout on their way in
   kSlotPackedRef = 7,     // packed arrays of the databases of one sk_query_db call
   kSlotPackedQuery = 8,
-  kSlotCount = 9
+  kSlotCountsB = 9,       // count scratch of launches on the second compute stream
+  kSlotSplitCountsB = 10,
+  kSlotCount = 11
 };
 
 struct sk_ctx {
@@ -40,6 +42,10 @@ struct sk_ctx {
   cudaStream_t copy_stream = nullptr;   // copies overlapped with kernels (created on first use)
   cudaEvent_t ev_ready[2] = {};         // double buffer b holds data
   cudaEvent_t ev_free[2] = {};          // double buffer b may be overwritten
+  cudaStream_t stream_b = nullptr;      // second compute stream (chunk launches alternate)
+  cudaStream_t pack_stream = nullptr;   // high-priority stream for packing uploaded chunks
+  std::vector<cudaEvent_t> ev_chunk;    // chunk c packed
+  cudaEvent_t ev_join = nullptr;        // second compute stream done
   int64_t mem_limit = 0;                // bytes a dense call may stage output in (0 = free memory)
   int sm_count = 0;
   std::string err;
