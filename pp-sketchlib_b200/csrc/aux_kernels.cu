@@ -164,8 +164,11 @@ __global__ void knn_self_kernel(const float *__restrict__ vals, int64_t n, int k
 
 // Row kNN over a dense (n_rows, n_cols) column: one warp per row, lanes take
 // every 32nd column, then lane 0 merges the 32 sorted lists by (key, col).
+// diag0 >= 0: row r is sample diag0 + r of the column set, whose own column
+// counts as +inf (as in knn_self_kernel); jaccard: keys are 1 - J.
 __global__ void knn_rows_kernel(const float *__restrict__ vals, int64_t n_rows, int64_t n_cols,
-                                int knn, int64_t *__restrict__ j_out, float *__restrict__ d_out) {
+                                int knn, int64_t diag0, int jaccard, int64_t *__restrict__ j_out,
+                                float *__restrict__ d_out) {
   extern __shared__ unsigned char smem[];
   float *key = reinterpret_cast<float *>(smem);
   int32_t *idx = reinterpret_cast<int32_t *>(key + 32 * knn);
@@ -176,7 +179,13 @@ __global__ void knn_rows_kernel(const float *__restrict__ vals, int64_t n_rows, 
     int count = 0;
     float worst = FLT_MAX;
     for (int64_t c = lane; c < n_cols; c += 32) {
-      const float d = v[c];
+      float d;
+      if (diag0 >= 0 && c == diag0 + row) {
+        d = INFINITY;
+      } else {
+        d = v[c];
+        if (jaccard) d = 1.0f - d;
+      }
       if (count < knn || d < worst) {
         int pos = count < knn ? count++ : knn - 1;
         while (pos > 0 && key[(pos - 1) * 32 + lane] > d) {
@@ -207,7 +216,7 @@ __global__ void knn_rows_kernel(const float *__restrict__ vals, int64_t n_rows, 
         if (best < 0) { j_out[row * knn + e] = -1; d_out[row * knn + e] = INFINITY; continue; }
         ++head[best];
         j_out[row * knn + e] = bj;
-        d_out[row * knn + e] = bk;
+        d_out[row * knn + e] = jaccard ? 1.0f - bk : bk;
       }
     }
     __syncwarp();
@@ -346,7 +355,8 @@ cudaError_t launch_knn_self(const float *col_vals, int64_t n, int32_t knn, int32
 }
 
 cudaError_t launch_knn_rows(const float *vals, int64_t n_rows, int64_t n_cols, int32_t knn,
-                            int64_t *j_out, float *d_out, cudaStream_t stream) {
+                            int64_t diag0, int32_t jaccard, int64_t *j_out, float *d_out,
+                            cudaStream_t stream) {
   const int smem = 32 * knn * 8;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(knn_rows_kernel,
@@ -354,8 +364,8 @@ cudaError_t launch_knn_rows(const float *vals, int64_t n_rows, int64_t n_cols, i
     if (e != cudaSuccess) return e;
   }
   const int blocks = static_cast<int>(n_rows < 148 * 64 ? n_rows : 148 * 64);
-  knn_rows_kernel<<<blocks > 0 ? blocks : 1, 32, smem, stream>>>(vals, n_rows, n_cols, knn, j_out,
-                                                                 d_out);
+  knn_rows_kernel<<<blocks > 0 ? blocks : 1, 32, smem, stream>>>(vals, n_rows, n_cols, knn, diag0,
+                                                                 jaccard, j_out, d_out);
   return cudaGetLastError();
 }
 

@@ -635,6 +635,63 @@ sk_status dense_blocked_to_host(sk_ctx *ctx, const sk_db *ref, const sk_db *quer
   return SK_OK;
 }
 
+
+// kNN over rows of `rows` against every column of `cols`, in blocks of rows
+// whose distance columns fit `budget` bytes, for when the whole column does not
+// fit (the reference's sparseDists likewise works in chunks,
+// src/gpu/dist.cu:495-791).  A block is a view of the row database: the packed
+// array offset by whole granules (the kernel strides by the full array's
+// granule count), cluster ids and equal-base factors offset by the first row.
+// self: rows and cols are the same database; each row's own column is +inf and
+// random-table lookups keep the all-vs-all orientation (self_view), so the
+// result is bit-identical to the one-column path, at twice its compute.
+// Results go to d_j / d_d at [row][kNN]; everything is queued on the stream.
+sk_status knn_blocked(sk_ctx *ctx, const sk_db *cols, const sk_db *rows, bool self,
+                      const sk_random *random, int kNN, int out_col, int jaccard, int64_t *d_j,
+                      float *d_d, size_t budget) {
+  if (random && random->mode == kRandEqualBase) {
+    sk_status st = ensure_jv(ctx, const_cast<sk_db *>(rows), random->use_rc);
+    if (st == SK_OK) st = ensure_jv(ctx, const_cast<sk_db *>(cols), random->use_rc);
+    if (st != SK_OK) return st;
+  }
+  const int64_t n_cols = cols->n;
+  int64_t per = static_cast<int64_t>(budget / (static_cast<size_t>(n_cols) * 4));
+  per = std::max<int64_t>(kSamplePad, per / kSamplePad * kSamplePad);
+  void *d_vals = nullptr;
+  sk_status st = scratch(ctx, kSlotOut, static_cast<size_t>(std::min(per, rows->n)) * n_cols * 4, &d_vals);
+  if (st != SK_OK) return st;
+  for (int64_t r0 = 0; r0 < rows->n; r0 += per) {
+    sk_db view = *rows;
+    view.n = std::min(per, rows->n - r0);
+    view.packed = rows->packed + (r0 / kGranule) * kStripeWords;
+    view.cluster = rows->cluster ? rows->cluster + r0 : nullptr;
+    view.jv = rows->jv ? rows->jv + r0 : nullptr;
+    view.jgpu = nullptr;
+    JobParams jp;
+    const TileConfig *cfg = nullptr;
+    st = build_job(ctx, cols, &view, random, kOutColumn, out_col, d_vals, &cfg, &jp);
+    if (st != SK_OK) return st;
+    if (self) {
+      jp.self_view = 1;
+      jp.row_base = r0;
+      if (jp.rmode == kRandTable && random && random->mode == kRandTable) {
+        // the all-vs-all orientation: CPU path [k][cluster(i)][cluster(j)],
+        // GPU path [k][cluster(j)][cluster(i)], i < j
+        const int C = random->n_clusters;
+        jp.rs_row = jp.semantics == kSemRefGpu ? 1 : C;
+        jp.rs_col = jp.semantics == kSemRefGpu ? C : 1;
+      }
+    }
+    st = launch_job(ctx, jp, *cfg);
+    if (st != SK_OK) return st;
+    cudaError_t e = launch_knn_rows(static_cast<float *>(d_vals), view.n, n_cols, kNN,
+                                    self ? r0 : -1, jaccard, d_j + r0 * kNN, d_d + r0 * kNN,
+                                    ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "kNN");
+  }
+  return SK_OK;
+}
+
 }  // namespace sk
 
 // ------------------------------------------------------------------ context
@@ -1051,18 +1108,26 @@ sk_status sk_dists_knn(sk_ctx *ctx, const sk_db *db, const sk_random *random, in
   if (kNN == 0) return SK_OK;
   const int64_t n = db->n, pairs = n_pairs(db, nullptr);
   void *d_vals = nullptr, *d_res = nullptr;
-  st = scratch(ctx, kSlotOut, std::max<size_t>(pairs, 1) * 4, &d_vals);
-  if (st != SK_OK) return st;
   const size_t res_elems = static_cast<size_t>(n) * kNN;
   st = scratch(ctx, kSlotResult, res_elems * 12, &d_res);
   if (st != SK_OK) return st;
   int64_t *d_j = static_cast<int64_t *>(d_res);
   float *d_d = reinterpret_cast<float *>(d_j + res_elems);
-  if (pairs > 0) {
-    st = dense_to_device(ctx, db, nullptr, random, kOutColumn, jaccard ? 2 + dist_col : dist_col, d_vals);
+  const int out_col = jaccard ? 2 + dist_col : dist_col;
+  const size_t budget = dense_budget(ctx);
+  cudaError_t e = cudaSuccess;
+  if (static_cast<size_t>(pairs) * 4 > budget) {
+    st = knn_blocked(ctx, db, db, true, random, kNN, out_col, jaccard, d_j, d_d, budget);
     if (st != SK_OK) return st;
+  } else {
+    st = scratch(ctx, kSlotOut, std::max<size_t>(pairs, 1) * 4, &d_vals);
+    if (st != SK_OK) return st;
+    if (pairs > 0) {
+      st = dense_to_device(ctx, db, nullptr, random, kOutColumn, out_col, d_vals);
+      if (st != SK_OK) return st;
+    }
+    e = launch_knn_self(static_cast<float *>(d_vals), n, kNN, jaccard, d_j, d_d, ctx->stream);
   }
-  cudaError_t e = launch_knn_self(static_cast<float *>(d_vals), n, kNN, jaccard, d_j, d_d, ctx->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(j_out, d_j, res_elems * 8, cudaMemcpyDeviceToHost, ctx->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(d_out, d_d, res_elems * 4, cudaMemcpyDeviceToHost, ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "kNN");
@@ -1085,16 +1150,24 @@ sk_status sk_query_knn(sk_ctx *ctx, const sk_db *ref, const sk_db *query, const 
   if (kNN == 0) return SK_OK;
   const int64_t pairs = n_pairs(ref, query);
   void *d_vals = nullptr, *d_res = nullptr;
-  st = scratch(ctx, kSlotOut, pairs * 4, &d_vals);
-  if (st != SK_OK) return st;
   const size_t res_elems = static_cast<size_t>(query->n) * kNN;
   st = scratch(ctx, kSlotResult, res_elems * 12, &d_res);
   if (st != SK_OK) return st;
   int64_t *d_j = static_cast<int64_t *>(d_res);
   float *d_d = reinterpret_cast<float *>(d_j + res_elems);
-  st = dense_to_device(ctx, ref, query, random, kOutColumn, dist_col, d_vals);
-  if (st != SK_OK) return st;
-  cudaError_t e = launch_knn_rows(static_cast<float *>(d_vals), query->n, ref->n, kNN, d_j, d_d, ctx->stream);
+  const size_t budget = dense_budget(ctx);
+  cudaError_t e = cudaSuccess;
+  if (static_cast<size_t>(pairs) * 4 > budget) {
+    st = knn_blocked(ctx, ref, query, false, random, kNN, dist_col, 0, d_j, d_d, budget);
+    if (st != SK_OK) return st;
+  } else {
+    st = scratch(ctx, kSlotOut, pairs * 4, &d_vals);
+    if (st != SK_OK) return st;
+    st = dense_to_device(ctx, ref, query, random, kOutColumn, dist_col, d_vals);
+    if (st != SK_OK) return st;
+    e = launch_knn_rows(static_cast<float *>(d_vals), query->n, ref->n, kNN, -1, 0, d_j, d_d,
+                        ctx->stream);
+  }
   if (e == cudaSuccess) e = cudaMemcpyAsync(r_out, d_j, res_elems * 8, cudaMemcpyDeviceToHost, ctx->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(d_out, d_d, res_elems * 4, cudaMemcpyDeviceToHost, ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "query kNN");

@@ -157,7 +157,7 @@ sk_status start_slice(sk_server *sv, Slot &s) {
   if (st != SK_OK) return st;
   const int knn = sv->params.kNN;
   if (knn > 0) {
-    e = launch_knn_rows(s.d_col, s.nq, ref->n, knn, s.d_knn, s.d_knn_d, ctx->stream);
+    e = launch_knn_rows(s.d_col, s.nq, ref->n, knn, -1, 0, s.d_knn, s.d_knn_d, ctx->stream);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(s.h_knn, s.d_knn, static_cast<size_t>(s.nq) * knn * 8,
                           cudaMemcpyDeviceToHost, ctx->stream);

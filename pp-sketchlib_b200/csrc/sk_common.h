@@ -71,6 +71,11 @@ struct JobParams {
   int32_t kmers[kMaxKmers];
   uint32_t one;                // 1 (a run-time operand for the count multiply-adds)
   int32_t semantics;           // Semantics: which reference path the fit follows
+  // Rows that are a block of the column database itself (blocked self kNN):
+  // row r is sample row_base + r, and a random-table lookup orders the pair's
+  // clusters by sample index as the all-vs-all path does.
+  int32_t self_view;
+  int64_t row_base;
 };
 
 // One unit of work of the persistent distance kernel: k-mer indices

@@ -125,8 +125,13 @@ __device__ __forceinline__ void tile_coords(const JobParams &p, int64_t tile, in
 // (RandomMC::random_match, src/random/random_match.cpp:185-206; csrs :318-336).
 __device__ __forceinline__ double random_match(const JobParams &p, int k, int64_t gi, int64_t gj) {
   if (p.rmode == kRandTable) {
-    const int cr = p.cl_rows ? p.cl_rows[gi] : 0;
-    const int cc = p.cl_cols ? p.cl_cols[gj] : 0;
+    int cr = p.cl_rows ? p.cl_rows[gi] : 0;
+    int cc = p.cl_cols ? p.cl_cols[gj] : 0;
+    if (p.self_view && p.row_base + gi > gj) {   // the all-vs-all path sees (gj, row)
+      const int t = cr;
+      cr = cc;
+      cc = t;
+    }
     return static_cast<double>(p.rtable[k * p.rs_k + cr * p.rs_row + cc * p.rs_col]);
   }
   if (p.rmode == kRandEqualBase) {
