@@ -432,6 +432,7 @@ def run_serving(ctx, dev, n_requests=120, rate_hz=10.0):
     ref.close()
     pairs = int(sizes.sum()) * n_ref
     mid = (sizes >= 50) & (sizes <= 200)
+    small = sizes <= 64
     pct = lambda a, q: float(np.percentile(a, q) * 1e3) if len(a) else None
     return {
         "workload": "50,000 resident references, 10 k x 10k bins; seeded Poisson arrivals "
@@ -441,6 +442,7 @@ def run_serving(ctx, dev, n_requests=120, rate_hz=10.0):
         "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99),
         "p50_ms_batches_50_200": pct(lat[mid], 50), "p99_ms_batches_50_200": pct(lat[mid], 99),
         "n_batches_50_200": int(mid.sum()),
+        "p50_ms_batches_le_64": pct(lat[small], 50), "n_batches_le_64": int(small.sum()),
         "slots": 4, "slice_queries": 128,
         "alone_vs_mixed_equal": alone_equal, "alone_vs_mixed_requests": len(check),
     }

@@ -233,6 +233,15 @@ sk_status build_job(sk_ctx *ctx, const sk_db *ref, const sk_db *query, const sk_
   if (random && random->kmers != ref->kmers)
     return fail(ctx, SK_EMISMATCH, "Random match table k-mer lengths differ from the sketches");
   const TileConfig *cfg = choose_config(ctx, ref->K, ref->s64);
+  // A query batch of at most 64 samples fills one 64-row tile: with the
+  // default 128-row tile more than half of every tile's work would be padding
+  // (serving slices of a few queries), so use the 64 x 64 shape unless a shape
+  // was forced or tuned for this (K, sketchsize64).
+  if (query && query->n <= 64 && cfg && cfg->tile_rows > 64 && ctx->tile_cfg == 0 &&
+      ctx->tuning.find({ref->K, ref->s64}) == ctx->tuning.end()) {
+    const TileConfig *small = tile_config(kSmallQueryConfig);
+    if (small && small->tile_rows == 64 && small->max_kmers >= ref->K) cfg = small;
+  }
   if (!cfg || cfg->max_kmers < ref->K)
     return fail(ctx, SK_ENOTSUP, "No tile configuration holds %d k-mer lengths (at most 16)",
                 ref->K);

@@ -24,6 +24,9 @@ struct TileConfig {
 
 int tile_config_count();
 const TileConfig *tile_config(int id);
+// The 64 x 64 shape (8 x 4 pairs per thread, three CTAs per SM) used for
+// query batches of at most 64 samples.
+constexpr int kSmallQueryConfig = 6;
 // Bytes of count scratch per slot (one per CTA, one per split tile).
 inline size_t count_slot_bytes(const TileConfig &cfg, int k_slots) {
   return static_cast<size_t>(k_slots) * cfg.tile_rows * cfg.tile_cols * 2;
