@@ -20,6 +20,8 @@
  *                              (src/gpu/gpu_api.cpp:232-305, src/gpu/device_memory.cu:7-65)
  *   sk_random_create        <- RandomMC::flattened_random / lookup_array / csrs
  *                              (src/random/random_match.cpp:254-310, 318-336)
+ *   sk_closest_cluster      <- RandomMC::closest_cluster / nearest_neighbour / apply_rc
+ *                              (src/random/random_match.cpp:222-227, 338-360)
  *   sk_dists_dense          <- query_db_cuda / dispatchDists / calculate_dists
  *                              (src/gpu/gpu_api.cpp:352-494, src/gpu/dist.cu:164-317, 408-489)
  *                              and, for SK_OUT_JACCARD, the CPU-only jaccard branch of
@@ -184,6 +186,19 @@ sk_status sk_random_create(sk_ctx *ctx, int32_t mode, int32_t use_rc,
                            int32_t n_clusters, const float *table,
                            sk_random **out);
 sk_status sk_random_destroy(sk_random *random);
+
+/* Random-match cluster of each of n samples from its base composition, for
+ * queries that are not in the model's cluster table (RandomMC::closest_cluster
+ * / nearest_neighbour / apply_rc, src/random/random_match.cpp:222-227,
+ * 338-360): with use_rc the A/T and C/G frequencies are averaged, then the
+ * nearest of the n_clusters centroids [C][4] (A, C, G, T) by squared distance in
+ * float is chosen, the first on a tie (the reference sums the four squares in
+ * Eigen's order, so centroids equidistant within float rounding may resolve
+ * differently).  base_freq is [n][4] in A, C, G, T order.  Host-only: no
+ * context or device.  Feeds `cluster` of sk_db_set_sample_info and
+ * sk_server_submit. */
+sk_status sk_closest_cluster(const float *centroids, int32_t n_clusters, int32_t use_rc,
+                             const double *base_freq, int64_t n, uint16_t *cluster_out);
 
 /* ---- dense distances ---------------------------------------------------- */
 

@@ -13,6 +13,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <fstream>
 #include <map>
 #include <mutex>
@@ -1048,6 +1049,38 @@ sk_status sk_random_create(sk_ctx *ctx, int32_t mode, int32_t use_rc, const int3
     }
   }
   *out = r;
+  return SK_OK;
+}
+
+sk_status sk_closest_cluster(const float *centroids, int32_t n_clusters, int32_t use_rc,
+                             const double *base_freq, int64_t n, uint16_t *cluster_out) {
+  if (n < 0 || n_clusters < 0 || (n > 0 && (!base_freq || !cluster_out)) ||
+      (n_clusters > 0 && !centroids))
+    return SK_EINVAL;
+  for (int64_t i = 0; i < n; ++i) {
+    double b[4] = {base_freq[4 * i], base_freq[4 * i + 1], base_freq[4 * i + 2],
+                   base_freq[4 * i + 3]};
+    if (use_rc) {  // strand unknown: A/T and C/G cannot be told apart
+      b[0] = 0.5 * (b[0] + b[3]);
+      b[1] = 0.5 * (b[1] + b[2]);
+      b[2] = b[1];
+      b[3] = b[0];
+    }
+    int best = 0;
+    float best_d = std::numeric_limits<float>::infinity();
+    for (int c = 0; c < n_clusters; ++c) {
+      float d = 0.0f;
+      for (int j = 0; j < 4; ++j) {
+        const float diff = centroids[c * 4 + j] - static_cast<float>(b[j]);
+        d += diff * diff;
+      }
+      if (d < best_d) {
+        best_d = d;
+        best = c;
+      }
+    }
+    cluster_out[i] = static_cast<uint16_t>(best);
+  }
   return SK_OK;
 }
 

@@ -1,5 +1,6 @@
 // host_db.cpp -- see host_db.h.
 #include "host_db.h"
+#include "sketchlib_b200.h"
 
 #include <algorithm>
 #include <cmath>
@@ -93,28 +94,9 @@ SketchSet load_sketches(const std::string &db_name, const std::vector<std::strin
 
 uint16_t RandomModel::closest_cluster(const std::vector<double> &bases_in, bool rc) const {
   if (mode != 2 || n_clusters == 0) return 0;
-  std::vector<double> b(bases_in);
-  if (rc) {  // apply_rc (random_match.cpp:338-348)
-    b[0] = 0.5 * (b[0] + b[3]);
-    b[1] = 0.5 * (b[1] + b[2]);
-    b[2] = b[1];
-    b[3] = b[0];
-  }
-  // nearest centroid by squared distance in float, first minimum wins
-  int best = 0;
-  float best_d = std::numeric_limits<float>::infinity();
-  for (int c = 0; c < n_clusters; ++c) {
-    float d = 0.0f;
-    for (int j = 0; j < 4; ++j) {
-      const float diff = centroids[c * 4 + j] - static_cast<float>(b[j]);
-      d += diff * diff;
-    }
-    if (d < best_d) {
-      best_d = d;
-      best = c;
-    }
-  }
-  return static_cast<uint16_t>(best);
+  uint16_t id = 0;
+  sk_closest_cluster(centroids.data(), n_clusters, rc ? 1 : 0, bases_in.data(), 1, &id);
+  return id;
 }
 
 std::vector<uint16_t> RandomModel::lookup(const SketchSet &s, bool queries_by_centroid) const {

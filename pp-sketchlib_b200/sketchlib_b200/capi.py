@@ -53,6 +53,7 @@ _SIGNATURES = {
     "sk_db_download": (_i32, [_p, _p, _p]),
     "sk_random_create": (_i32, [_p, _i32, _i32, _p, _i32, _i32, _p, C.POINTER(_p)]),
     "sk_random_destroy": (_i32, [_p]),
+    "sk_closest_cluster": (_i32, [_p, _i32, _i32, _p, _i64, _p]),
     "sk_dists_rows": (_i64, [_p, _p]),
     "sk_dists_dense": (_i32, [_p, _p, _p, _p, _i32, _p, _i32]),
     "sk_query_db": (_i32, [_p, _p, _p, _p, _i32, _i32, _i32, _p, _i32, _p]),
@@ -212,6 +213,20 @@ class Context:
 
     def cancel(self):
         lib.sk_cancel(self.handle)
+
+
+def closest_cluster(centroids, base_freq, use_rc: bool = True) -> np.ndarray:
+    """Random-match cluster of each sample from its A, C, G, T frequencies
+    (sk_closest_cluster): the nearest centroid [C][4] after averaging A/T and
+    C/G when the strand is unknown (use_rc)."""
+    c = np.ascontiguousarray(centroids, np.float32).reshape(-1, 4)
+    b = np.ascontiguousarray(base_freq, np.float64).reshape(-1, 4)
+    out = np.zeros(b.shape[0], np.uint16)
+    st = lib.sk_closest_cluster(c.ctypes.data, c.shape[0], int(use_rc), b.ctypes.data,
+                                b.shape[0], out.ctypes.data)
+    if st != SK_OK:
+        raise SketchlibError(st, "closest_cluster: bad arguments")
+    return out
 
 
 def probe_alu_peak(ctx: Context) -> tuple[float, float]:
