@@ -264,6 +264,14 @@ def run_reference_arm(args, rank, world):
 
 # ---------------------------------------------------------------- our arm
 
+def measured_hbm_gbs():
+    """The pool's measured copy bandwidth (GB/s) from MEASURED_PEAKS.json, or None."""
+    try:
+        return float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        return None
+
+
 def profiled_traffic():
     """DRAM bytes per launch of the distance kernel from the committed ncu
     summary (line `dram_bytes_per_launch: N`), or None."""
@@ -604,6 +612,7 @@ def run_ours(args, rank, world, local):
 
     achieved = pairs * LOP3_PER_PAIR / launch_s
     traffic = profiled_traffic()
+    hbm_peak = measured_hbm_gbs()
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps,
@@ -616,6 +625,9 @@ def run_ours(args, rank, world, local):
         "roofline": {"bound": "alu", "achieved": achieved / 1e12, "peak": lop3_peak / 1e12,
                      "unit": "T LOP3/s", "frac": achieved / lop3_peak,
                      "traffic": traffic,
+                     "dram_gbs": None if traffic is None else traffic / launch_s / 1e9,
+                     "dram_frac_of_copy_peak": None if traffic is None or not hbm_peak
+                                               else traffic / launch_s / 1e9 / hbm_peak,
                      "peak_source": "sk_probe_alu_peak, measured in this run (LOP3 chains on "
                                     "every SM); popc peak %.3g/s" % popc_peak,
                      "algorithmic": f"{LOP3_PER_PAIR} LOP3 + {POPC_PER_PAIR} POPC per pair x "
