@@ -296,3 +296,24 @@ def test_context_outlives_its_handles():
     ctx.handle = None
     rnd.close()
     db.close()
+
+
+@pytest.mark.parametrize("query", [False, True])
+def test_maximum_kmer_count(gpu_ctx, query):
+    """K = 32 (the most this build takes), k = 5..36: counts bit-exact,
+    Jaccard exact, core/accessory within the double-fit bar."""
+    from sketchlib_b200 import synth
+    kmers = np.arange(5, 37, dtype=np.int32)
+    parent, thresh = synth.random_tree(90, kmers=kmers, seed=0x5EED0032, c_max=0.01)
+    words = capi.synth_host(parent, thresh, 8, seed=0x5EED0032)
+    rw, qw = (words[30:], words[:30]) if query else (words, None)
+    ref = _db(gpu_ctx, rw, kmers, 8)
+    qry = _db(gpu_ctx, qw, kmers, 8) if query else None
+    np.testing.assert_array_equal(capi.dists_dense(gpu_ctx, ref, qry, out_mode=capi.OUT_COUNTS),
+                                  oracle.dists(rw, kmers, 8, query_words=qw, out_mode=2))
+    np.testing.assert_array_equal(capi.dists_dense(gpu_ctx, ref, qry, out_mode=capi.OUT_JACCARD),
+                                  oracle.dists(rw, kmers, 8, query_words=qw, out_mode=1))
+    got = capi.dists_dense(gpu_ctx, ref, qry)
+    want = oracle.dists(rw, kmers, 8, query_words=qw)
+    assert np.abs(got - want).max() <= TOL_F64
+    assert (want[:, 0] > 0).mean() > 0.5                  # the fits are not all degenerate
