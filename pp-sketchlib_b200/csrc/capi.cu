@@ -67,13 +67,14 @@ static void ctx_free(sk_ctx *ctx) {
       if (ctx->ev_ready[b]) cudaEventDestroy(ctx->ev_ready[b]);
       if (ctx->ev_free[b]) cudaEventDestroy(ctx->ev_free[b]);
     }
-    for (cudaStream_t st : {ctx->stream_b, ctx->pack_stream}) {
+    for (cudaStream_t st : {ctx->stream_b, ctx->pack_stream, ctx->d2h_stream}) {
       if (st) {
         cudaStreamSynchronize(st);
         cudaStreamDestroy(st);
       }
     }
     for (cudaEvent_t ev : ctx->ev_chunk) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : ctx->ev_out) cudaEventDestroy(ev);
     if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
   }
   delete ctx;

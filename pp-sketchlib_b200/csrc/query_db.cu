@@ -9,9 +9,12 @@
 // it lands, and the tiles whose samples have all arrived run as one
 // persistent launch while the next chunk is in flight.
 //
-//   self:  tile (ti, tj) reads samples up to max((ti+1) QT, (tj+1) RT) - 1, so
-//          it runs after the chunk holding that sample; chunk c adds the
-//          tiles of the (c+1)^2 - c^2 new block pairs.
+//   self:  the chunks go up from the last samples down: tile (ti, tj) reads
+//          samples from ti QT on, so it runs after the chunk holding ti QT,
+//          and that chunk's launch writes every pair of the chunk's rows.  With
+//          a pinned destination those rows (one contiguous range of the long
+//          form) are copied back on their own stream while lower chunks
+//          compute.
 //   query: the query samples go up first, then the references in chunks;
 //          tile (ti, tj) runs after the reference chunk holding (tj+1) RT - 1.
 //
@@ -54,6 +57,8 @@ sk_status ensure_compute_streams(sk_ctx *ctx) {
       e = cudaStreamCreateWithPriority(&ctx->pack_stream, cudaStreamNonBlocking, greatest);
   }
   if (e == cudaSuccess && !ctx->ev_join) e = cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming);
+  if (e == cudaSuccess && !ctx->d2h_stream)
+    e = cudaStreamCreateWithFlags(&ctx->d2h_stream, cudaStreamNonBlocking);
   return e == cudaSuccess ? SK_OK : cuda_fail(ctx, e, "compute stream setup");
 }
 
@@ -70,7 +75,7 @@ struct CallDbs {
   sk_ctx *ctx;
   sk_db *ref = nullptr, *query = nullptr;
   ~CallDbs() {
-    for (cudaStream_t st : {ctx->copy_stream, ctx->pack_stream, ctx->stream_b})
+    for (cudaStream_t st : {ctx->copy_stream, ctx->pack_stream, ctx->stream_b, ctx->d2h_stream})
       if (st) cudaStreamSynchronize(st);
     cudaStreamSynchronize(ctx->stream);
     if (ref) db_free(ref);
@@ -139,6 +144,14 @@ extern "C" sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
   const int64_t cs = chunk_samples(n_ref);
   const int n_chunks = static_cast<int>((n_ref + cs - 1) / cs);
   std::vector<std::vector<int64_t>> bucket(n_chunks);
+  const bool reverse = jp.self && !blocked;
+  bool pinned_out = false;
+  {
+    cudaPointerAttributes pa{};
+    if (cudaPointerGetAttributes(&pa, out) == cudaSuccess) pinned_out = pa.type == cudaMemoryTypeHost;
+    else cudaGetLastError();   // not a pointer CUDA knows: pageable
+  }
+  const bool stream_out = reverse && pinned_out;
   {
     int64_t tile = 0;
     const int64_t m = jp.tile_rows / jp.tile_cols;
@@ -147,7 +160,7 @@ extern "C" sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
       for (int64_t tj = tj0; tj < jp.n_col_tiles; ++tj, ++tile) {
         const int64_t last_col = std::min<int64_t>((tj + 1) * jp.tile_cols, n_ref) - 1;
         const int64_t last_row = jp.self ? std::min<int64_t>((ti + 1) * jp.tile_rows, n_ref) - 1 : 0;
-        bucket[std::max(last_col, last_row) / cs].push_back(tile);
+        bucket[reverse ? (ti * jp.tile_rows) / cs : std::max(last_col, last_row) / cs].push_back(tile);
       }
     }
   }
@@ -207,10 +220,19 @@ extern "C" sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
   if (dbs.query)
     for (int64_t s0 = 0; s0 < dbs.query->n; s0 += cs)
       units.push_back(Unit{dbs.query, query->words + s0 * wps, s0, std::min(cs, dbs.query->n - s0), -1});
-  for (int c = 0; c < n_chunks; ++c) {
+  for (int k = 0; k < n_chunks; ++k) {
+    const int c = reverse ? n_chunks - 1 - k : k;
     const int64_t s0 = c * cs;
     units.push_back(Unit{dbs.ref, ref->words + s0 * wps, s0, std::min(cs, n_ref - s0), c});
   }
+  while (ctx->ev_out.size() < static_cast<size_t>(n_chunks)) {
+    cudaEvent_t ev = nullptr;
+    e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "chunk events");
+    ctx->ev_out.push_back(ev);
+  }
+  const size_t elem = out_bytes(out_mode, 1, n_kmers);
+  auto first_row = [&](int64_t i) { return n_ref * i - i * (i + 1) / 2; };   // rows of sample i start
   while (ctx->ev_chunk.size() < units.size()) {
     cudaEvent_t ev = nullptr;
     e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
@@ -257,6 +279,19 @@ extern "C" sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
       e = cudaStreamWaitEvent(compute[w], ctx->ev_chunk[i], 0);   // packs complete in unit order
       if (e == cudaSuccess) e = cfg->launch(lp, g, compute[w]);
       if (e != cudaSuccess) return cuda_fail(ctx, e, "distance kernel launch");
+      if (stream_out) {   // this chunk's rows are final: copy them back now
+        const int64_t i0 = u.chunk * cs, i1 = std::min<int64_t>((u.chunk + 1) * cs, n_ref - 1);
+        if (i1 > i0) {
+          const int64_t r0 = first_row(i0), r1 = first_row(i1);
+          e = cudaEventRecord(ctx->ev_out[u.chunk], compute[w]);
+          if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->d2h_stream, ctx->ev_out[u.chunk], 0);
+          if (e == cudaSuccess)
+            e = cudaMemcpyAsync(static_cast<char *>(out) + r0 * elem,
+                                static_cast<char *>(d_out) + r0 * elem, (r1 - r0) * elem,
+                                cudaMemcpyDeviceToHost, ctx->d2h_stream);
+          if (e != cudaSuccess) return cuda_fail(ctx, e, "result copy");
+        }
+      }
     }
   }
   // join: the context stream waits for the last pack and the second stream
@@ -267,6 +302,12 @@ extern "C" sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
   if (blocked) {
     st = dense_blocked_to_host(ctx, dbs.ref, dbs.query, random, out_mode, out, budget);
     return st == SK_OK ? finish_call(ctx) : st;
+  }
+  if (stream_out) {   // the rows went back chunk by chunk: wait for the last copies
+    e = cudaEventRecord(ctx->ev_join, ctx->d2h_stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "result copy");
+    return finish_call(ctx);
   }
   e = cudaMemcpyAsync(out, d_out, out_sz, cudaMemcpyDeviceToHost, ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "result copy");

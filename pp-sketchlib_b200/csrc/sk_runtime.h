@@ -45,6 +45,8 @@ struct sk_ctx {
   cudaStream_t stream_b = nullptr;      // second compute stream (chunk launches alternate)
   cudaStream_t pack_stream = nullptr;   // high-priority stream for packing uploaded chunks
   std::vector<cudaEvent_t> ev_chunk;    // chunk c packed
+  cudaStream_t d2h_stream = nullptr;    // result rows copied back while later chunks compute
+  std::vector<cudaEvent_t> ev_out;      // chunk c's output rows written
   cudaEvent_t ev_join = nullptr;        // second compute stream done
   int64_t mem_limit = 0;                // bytes a dense call may stage output in (0 = free memory)
   int sm_count = 0;

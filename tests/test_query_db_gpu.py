@@ -46,11 +46,18 @@ def _plain(ctx, words, kmers, s64, qwords, rnd, info, mode):
 def test_self_matches_plain_path(gpu_ctx, n, kind):
     words, kmers = random_sketches(n, 3, 16, seed=900 + n)
     rnd, info = _random(gpu_ctx, kind, kmers, n, 0, seed=n)
+    import torch
     for mode in MODES:
         got = capi.query_db(gpu_ctx, words, kmers, 16, ref_cluster=info["ref_cluster"],
                             ref_seq_len=info["ref_seq_len"], random=rnd, out_mode=mode)
         want = _plain(gpu_ctx, words, kmers, 16, None, rnd, info, mode)
         np.testing.assert_array_equal(got, want)
+        # a pinned destination takes each chunk's rows back as soon as they are final
+        pinned = torch.zeros(want.shape, dtype=torch.float32 if want.dtype == np.float32
+                             else torch.int32).pin_memory().numpy().view(want.dtype)
+        got2 = capi.query_db(gpu_ctx, words, kmers, 16, ref_cluster=info["ref_cluster"],
+                             ref_seq_len=info["ref_seq_len"], random=rnd, out_mode=mode, out=pinned)
+        np.testing.assert_array_equal(got2, want)
 
 
 @pytest.mark.parametrize("n_ref,n_q", [(1100, 300), (600, 1), (70, 700)])
