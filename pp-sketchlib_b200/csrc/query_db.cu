@@ -5,8 +5,8 @@
 // sketch on the host, copies them all, launches, waits, and copies the result
 // back, one step after another.  Here the reference-layout words go up in
 // sample chunks on the context's copy stream, double-buffered through a
-// device staging area; each chunk is packed on the compute stream as soon as
-// it lands, and the tiles whose samples have all arrived run as one
+// device staging area; each chunk is packed on a high-priority stream as soon
+// as it lands, and the tiles whose samples have all arrived run as one
 // persistent launch while the next chunk is in flight.
 //
 //   self:  the chunks go up from the last samples down: tile (ti, tj) reads
@@ -19,10 +19,11 @@
 //          tile (ti, tj) runs after the reference chunk holding (tj+1) RT - 1.
 //
 // Each chunk's work list gets its own tail split (small early chunks are cut
-// along k to fill the GPU) and its own control block; the count scratch is
-// shared, as the launches run one after another on the compute stream.  The
-// packed arrays, staging area and output staging are context scratch, so a
-// repeated call allocates nothing.
+// along k to fill the GPU) and its own control block.  Launches alternate
+// between two compute streams with a count scratch each, so one launch's tail
+// wave is filled by the next launch's CTAs.  The packed arrays, staging area
+// and output staging are context scratch, so a repeated call allocates
+// nothing.
 #include <cuda_runtime.h>
 
 #include <algorithm>
