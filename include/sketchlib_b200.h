@@ -415,6 +415,12 @@ sk_status sk_synth_device(sk_ctx *ctx, const int32_t *parent,
  * second: 32-bit LOP3 (the distance kernel's bound) and POPC.  Each is one
  * ~20 ms saturating kernel on the context's stream. */
 sk_status sk_probe_alu_peak(sk_ctx *ctx, double *lop3_per_s, double *popc_per_s);
+/* Checks the device-side bounded wait on this context: one CTA waits on a
+ * barrier that nothing completes, gives up after limit_ms (1..10000) and
+ * reports it, so the call returns SK_ETIMEDOUT ("A device-side bounded wait
+ * timed out") and the context stays usable.  Every wait in this library's
+ * kernels uses the same bounded wait (a 2 s limit in the distance kernel). */
+sk_status sk_probe_wait_limit(sk_ctx *ctx, int32_t limit_ms);
 
 #ifdef __cplusplus
 }

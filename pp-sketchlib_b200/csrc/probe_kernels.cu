@@ -7,6 +7,7 @@
 
 #include <cstdint>
 
+#include "sk_device.cuh"
 #include "sk_runtime.h"
 
 namespace sk {
@@ -84,4 +85,41 @@ extern "C" sk_status sk_probe_alu_peak(sk_ctx *ctx, double *lop3_per_s, double *
   if (lop3_per_s) *lop3_per_s = l;
   if (popc_per_s) *popc_per_s = p;
   return SK_OK;
+}
+
+namespace sk {
+namespace {
+
+// Waits on an mbarrier that nothing arrives on, with the same bounded wait the
+// distance kernel uses for its stages: the wait gives up after limit_ns and
+// the kernel records a timeout in the status word instead of spinning on.
+__global__ void wait_limit_kernel(uint64_t limit_ns, DevStatus *status) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  const bool landed = mbar_wait_bounded(&bar, 0, limit_ns);   // phase 0 never completes
+  if (!landed && threadIdx.x == 0) {
+    atomicOr(&status->error, 1u);
+    status->where = 2;
+  }
+}
+
+}  // namespace
+}  // namespace sk
+
+extern "C" sk_status sk_probe_wait_limit(sk_ctx *ctx, int32_t limit_ms) {
+  if (!ctx) return SK_EINVAL;
+  std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+  sk::DeviceGuard g(ctx->device);
+  if (limit_ms < 1 || limit_ms > 10000) return sk::fail(ctx, SK_EINVAL, "limit_ms outside [1, 10000]");
+  sk_status st = sk::begin_call(ctx);
+  if (st != SK_OK) return st;
+  sk::wait_limit_kernel<<<1, 32, 0, ctx->stream>>>(static_cast<uint64_t>(limit_ms) * 1000000ull,
+                                                   ctx->status_dev);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return sk::cuda_fail(ctx, e, "wait probe launch");
+  return sk::finish_call(ctx);
 }

@@ -17,7 +17,8 @@ import numpy as np
 
 LIB_PATH = Path(__file__).resolve().with_name("libsketchlib_b200.so")
 
-SK_OK = 0
+SK_OK, SK_EINVAL, SK_ENOMEM, SK_ECUDA, SK_EMISMATCH = 0, 1, 2, 3, 4
+SK_ECANCELLED, SK_ETIMEDOUT, SK_ENOTSUP, SK_EKERNEL, SK_ERANGE = 5, 6, 7, 8, 9
 STATUS_NAMES = {
     0: "SK_OK", 1: "SK_EINVAL", 2: "SK_ENOMEM", 3: "SK_ECUDA", 4: "SK_EMISMATCH",
     5: "SK_ECANCELLED", 6: "SK_ETIMEDOUT", 7: "SK_ENOTSUP", 8: "SK_EKERNEL", 9: "SK_ERANGE",
@@ -69,6 +70,7 @@ _SIGNATURES = {
     "sk_synth_host": (_i32, [_p, _p, _i64, _i32, _i32, _u64, _i32, _p]),
     "sk_synth_device": (_i32, [_p, _p, _p, _i64, _i32, _i32, _u64, _p]),
     "sk_probe_alu_peak": (_i32, [_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "sk_probe_wait_limit": (_i32, [_p, _i32]),
     "sk_batch_create": (_i32, [_p, _p, _i32, _i32, C.POINTER(_p)]),
     "sk_batch_run": (_i32, [_p]),
     "sk_batch_launch": (_i32, [_p]),
