@@ -302,7 +302,7 @@ def batched_jobs(rng):
     return jobs
 
 
-def run_batched(ctx, dev, lop3_peak, repeats=3):
+def run_batched(ctx, dev, lop3_peak, repeats=3, autotune=False):
     import torch
     from sketchlib_b200 import capi, synth
     rng = np.random.default_rng(BATCH_SEED)
@@ -329,7 +329,8 @@ def run_batched(ctx, dev, lop3_peak, repeats=3):
         made.append((ref, qry, None, capi.OUT_CORE_ACC, out))
         pairs_total += rows
         lop3_total += rows * len(sp["kmers"]) * 2 * sp["s64"] * BBITS
-    batch = capi.Batch(ctx, [(r, q, rnd, m, o.data_ptr()) for r, q, rnd, m, o in made])
+    batch = capi.Batch(ctx, [(r, q, rnd, m, o.data_ptr()) for r, q, rnd, m, o in made],
+                       autotune=autotune)
     info = batch.info()
     batch.run()                      # warm-up
     stream = torch.cuda.current_stream(dev)
@@ -596,7 +597,7 @@ def run_ours(args, rank, world, local):
 
     extra = {}
     if not args.skip_batched:
-        extra["batched"] = run_batched(ctx, dev, lop3_peak)
+        extra["batched"] = run_batched(ctx, dev, lop3_peak, autotune=args.batch_autotune)
     if not args.skip_serving:
         extra["serving"] = run_serving(ctx, dev)
     if world == 1 and not args.skip_large:
@@ -685,6 +686,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-batched", action="store_true")
     ap.add_argument("--skip-serving", action="store_true")
+    ap.add_argument("--batch-autotune", action="store_true",
+                    help="let the batch time every tile shape at creation (outside the timed region)")
     ap.add_argument("--skip-large", action="store_true",
                     help="skip the 31,610-sample all-vs-all + kNN = 10 measurement")
     ap.add_argument("--no-ref-gpu", action="store_true",
