@@ -513,11 +513,13 @@ sk_status ensure_copy_stream(sk_ctx *ctx) {
 }
 
 // Device bytes a dense call may use to stage its output: the context's limit,
-// else the free memory less a 2 GiB margin.
+// else the free memory less a 2 GiB margin.  The output staging buffer the
+// context already holds counts as available: growing it frees it first.
 size_t dense_budget(sk_ctx *ctx) {
   if (ctx->mem_limit > 0) return static_cast<size_t>(ctx->mem_limit);
   size_t free_b = 0, total_b = 0;
   if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return 0;
+  free_b += ctx->scratch[kSlotOut].bytes;
   const size_t margin = size_t(2) << 30;
   return free_b > 2 * margin ? free_b - margin : free_b / 2;
 }
