@@ -31,34 +31,76 @@ __device__ __forceinline__ int64_t condensed(int64_t i, int64_t j, int64_t n) {
 
 // ------------------------------------------------------------------- packing
 
-// One CTA per (k, 64-bin block, granule): reads the 64 samples' 14 words of
-// the block (112 contiguous bytes per sample) into shared memory and writes
-// the two 32-bin stripes (3584 contiguous bytes each).  `words` holds n
+// One CTA per (k, granule of 64 samples, group of up to kPackBlocks 64-bin
+// blocks): each sample's words for the group are kPackBlocks * 14 contiguous
+// uint64 in the reference layout, read with consecutive threads on
+// consecutive words into a shared tile, then written out as the group's
+// 2 * kPackBlocks stripes (3584 contiguous bytes each).  `words` holds n
 // samples that become granules g0 .. g0 + ng - 1 of an array of ng_total
 // granules (samples past n are written as zeros).
+constexpr int kPackBlocks = 4;
+constexpr int kPackRow = kPackBlocks * kBbits + 1;   // tile row stride in uint64 (odd: fewer bank conflicts)
+
 __global__ void pack_kernel(const uint64_t *__restrict__ words, int64_t n, int n_kmers, int s64,
                             int ng, int g0, int ng_total, uint32_t *__restrict__ packed) {
-  __shared__ uint64_t tile[kGranule * kBbits];
-  const int64_t nblocks = static_cast<int64_t>(n_kmers) * s64 * ng;
+  __shared__ uint64_t tile[kGranule * kPackRow];
+  const bool vec = (reinterpret_cast<uintptr_t>(words) & 15) == 0;   // rows are 112-byte multiples
+  const int groups = (s64 + kPackBlocks - 1) / kPackBlocks;
+  const int64_t n_items = static_cast<int64_t>(n_kmers) * ng * groups;
   const int nb = 2 * s64;
-  for (int64_t item = blockIdx.x; item < nblocks; item += gridDim.x) {
-    const int g = static_cast<int>(item % ng);
-    const int64_t rest = item / ng;
-    const int b64 = static_cast<int>(rest % s64);
-    const int k = static_cast<int>(rest / s64);
-    for (int e = threadIdx.x; e < kGranule * kBbits; e += blockDim.x) {
-      const int lane = e / kBbits, plane = e % kBbits;
-      const int64_t s = static_cast<int64_t>(g) * kGranule + lane;
-      tile[plane * kGranule + lane] =
-          s < n ? words[((s * n_kmers + k) * s64 + b64) * kBbits + plane] : 0ull;
+  for (int64_t item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int grp = static_cast<int>(item % groups);
+    const int64_t rest = item / groups;
+    const int g = static_cast<int>(rest % ng);
+    const int k = static_cast<int>(rest / ng);
+    const int b0 = grp * kPackBlocks;
+    const int nblk = min(kPackBlocks, s64 - b0);
+    const int row_words = nblk * kBbits;
+    if (nblk == kPackBlocks && vec) {
+      // full group, 16-byte aligned rows: every 128-bit load in flight at once
+      constexpr int kRowVec = kPackBlocks * kBbits / 2;            // uint4 per sample row
+      constexpr int kPerThread = kGranule * kRowVec / kThreads;     // 7
+      static_assert(kGranule * kRowVec % kThreads == 0, "whole loads per thread");
+      uint4 v[kPerThread];
+#pragma unroll
+      for (int r = 0; r < kPerThread; ++r) {
+        const int e = threadIdx.x + r * kThreads;
+        const int lane = e / kRowVec, q = e % kRowVec;
+        const int64_t smp = static_cast<int64_t>(g) * kGranule + lane;
+        v[r] = smp < n ? reinterpret_cast<const uint4 *>(
+                             words + ((smp * n_kmers + k) * s64 + b0) * kBbits)[q]
+                       : make_uint4(0u, 0u, 0u, 0u);
+      }
+#pragma unroll
+      for (int r = 0; r < kPerThread; ++r) {
+        const int e = threadIdx.x + r * kThreads;
+        const int lane = e / kRowVec, q = e % kRowVec;
+        tile[lane * kPackRow + 2 * q] = (static_cast<uint64_t>(v[r].y) << 32) | v[r].x;
+        tile[lane * kPackRow + 2 * q + 1] = (static_cast<uint64_t>(v[r].w) << 32) | v[r].z;
+      }
+    } else {
+      for (int e = threadIdx.x; e < kGranule * row_words; e += blockDim.x) {
+        const int lane = e / row_words, w = e % row_words;
+        const int64_t smp = static_cast<int64_t>(g) * kGranule + lane;
+        tile[lane * kPackRow + w] =
+            smp < n ? words[((smp * n_kmers + k) * s64 + b0) * kBbits + w] : 0ull;
+      }
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < 2 * kStripeWords; e += blockDim.x) {
-      const int h = e / kStripeWords, w = e % kStripeWords;
-      const uint64_t v = tile[w];
-      const int64_t blk = static_cast<int64_t>(k) * nb + 2 * b64 + h;
-      packed[(blk * ng_total + g0 + g) * kStripeWords + w] =
-          static_cast<uint32_t>(h ? (v >> 32) : v);
+    // four consecutive samples of one plane per 128-bit store
+    constexpr int kStripeVec = kStripeWords / 4;
+    for (int e = threadIdx.x; e < 2 * nblk * kStripeVec; e += blockDim.x) {
+      const int stripe = e / kStripeVec, w = (e % kStripeVec) * 4;
+      const int b = stripe >> 1, h = stripe & 1;
+      const int plane = w / kGranule, lane = w % kGranule;
+      const uint64_t *t = tile + lane * kPackRow + b * kBbits + plane;
+      const int sh = h ? 32 : 0;
+      const uint4 o = make_uint4(static_cast<uint32_t>(t[0] >> sh),
+                                 static_cast<uint32_t>(t[kPackRow] >> sh),
+                                 static_cast<uint32_t>(t[2 * kPackRow] >> sh),
+                                 static_cast<uint32_t>(t[3 * kPackRow] >> sh));
+      const int64_t blk = static_cast<int64_t>(k) * nb + 2 * (b0 + b) + h;
+      reinterpret_cast<uint4 *>(packed + (blk * ng_total + g0 + g) * kStripeWords)[w / 4] = o;
     }
     __syncthreads();
   }
@@ -317,7 +359,7 @@ cudaError_t launch_pack(const uint64_t *words, int64_t n, int32_t n_kmers, int32
 cudaError_t launch_pack_range(const uint64_t *words, int64_t n, int32_t n_kmers, int32_t s64,
                               int32_t ng, int32_t g0, int32_t ng_total, uint32_t *packed,
                               cudaStream_t stream) {
-  const int64_t items = static_cast<int64_t>(n_kmers) * s64 * ng;
+  const int64_t items = static_cast<int64_t>(n_kmers) * ng * ((s64 + kPackBlocks - 1) / kPackBlocks);
   if (items == 0) return cudaSuccess;
   pack_kernel<<<grid_for(items, 1, 148 * 64), kThreads, 0, stream>>>(words, n, n_kmers, s64, ng,
                                                                      g0, ng_total, packed);
