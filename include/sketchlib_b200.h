@@ -36,6 +36,9 @@
  *   sk_square_to_long       <- square_to_long (src/dist/matrix_ops.cpp:130-150)
  *   sk_cancel               <- progress_atomics::set_kill (src/gpu/cuda.cuh:41-87),
  *                              without the reference's __trap()
+ *   sk_sketch               <- sketch() per sample and k (src/sketch/sketch.cpp:120-168)
+ *                              and its GPU counterpart sketch_gpu / get_signs
+ *                              (src/sketch/sketch.cpp:170-205, src/gpu/sketch.cu:404-470)
  */
 #ifndef SKETCHLIB_B200_H
 #define SKETCHLIB_B200_H
@@ -408,6 +411,41 @@ sk_status sk_synth_device(sk_ctx *ctx, const int32_t *parent,
                           const uint32_t *thresh, int64_t n_samples,
                           int32_t n_kmers, int32_t sketchsize64, uint64_t seed,
                           uint64_t *d_words);
+
+/* ---- sketching -------------------------------------------------------------- */
+
+/* MinHash sketches of sequences, the words every distance entry point takes.
+ * The sequences of all samples lie back to back in `bases` (host memory):
+ * sequence i is bases[seq_offsets[i], seq_offsets[i+1]), and sample s owns
+ * sequences sample_seqs[s] .. sample_seqs[s+1]-1 (at least one; the reference
+ * throws "... contains no sequence").  Each sample is sketched as the
+ * reference's sketch() does for every k of `kmers` (each k >= 3, "Minimum k
+ * must be 3 or higher"): every window of k bases A, C, G, T/U (either case)
+ * inside one sequence is hashed with ntHash (canonical when use_rc = 1), the
+ * hash mod 2^61-1 is kept as the minimum of its bin among 64 * sketchsize64,
+ * empty bins are filled by the reference's probe sequence, and the low 14 bits
+ * of each bin are written as bit planes.  Sequences go in as given; the
+ * reference's file reader upper-cases them and drops those shorter than the
+ * largest k (SeqBuf, src/sketch/seqio.cpp:55-100), which callers reproduce by
+ * what they pass.  Bytes other than the ten base letters count as non-bases
+ * (the reference's seed table also takes the control bytes 1, 3, 4, 5 and 7
+ * as bases; sequence text never holds them).
+ *
+ * min_count > 0 (read sets, 1..255) keeps only k-mers seen at least min_count
+ * times in the sample: the reference's exact counter (`exact = true`,
+ * HashCounter, src/sketch/countmin.cpp:55-72).  The reference's default
+ * count-min filter is an approximation whose answer depends on read order
+ * (and, in its GPU sketcher, on a data race); it is not reproduced.
+ *
+ * Outputs (host): words [n_samples][n_kmers][sketchsize64 * 14] in the
+ * reference layout; inv_minhash [n_samples][n_kmers] (bin 0's value over
+ * 2^61-1 before densifying, whose per-sample sum gives the reference's read-set
+ * size estimate K / sum) or NULL; densified [n_samples] (any k had empty bins)
+ * or NULL. */
+sk_status sk_sketch(sk_ctx *ctx, const char *bases, const int64_t *seq_offsets,
+                    const int64_t *sample_seqs, int64_t n_samples, const int32_t *kmers,
+                    int32_t n_kmers, int32_t sketchsize64, int32_t use_rc, int32_t min_count,
+                    uint64_t *words, double *inv_minhash, uint8_t *densified);
 
 /* ---- measurement ---------------------------------------------------------- */
 

@@ -59,6 +59,9 @@ def _load():
     lib.sko_long_to_square.argtypes = [vp, i64, vp, vp, i64, vp]
     lib.sko_square_to_long.restype = None
     lib.sko_square_to_long.argtypes = [vp, i64, vp]
+    lib.sko_sketch_samples.restype = None
+    lib.sko_sketch_samples.argtypes = [vp, vp, vp, i64, vp, i32, i32, i32, i32, i32, vp, vp, vp,
+                                       i32]
     return lib
 
 
@@ -241,6 +244,39 @@ class RefQueryDb:
         return out, done
 
 
+def pack_samples(samples):
+    """Samples given as lists of sequences (str or bytes) -> (bases uint8,
+    seq_off int64 [n_seqs + 1], sample_seqs int64 [n + 1])."""
+    seqs = [q.encode() if isinstance(q, str) else bytes(q) for smp in samples for q in smp]
+    lens = np.array([len(q) for q in seqs], np.int64)
+    seq_off = np.zeros(len(seqs) + 1, np.int64)
+    np.cumsum(lens, out=seq_off[1:])
+    counts = np.array([len(smp) for smp in samples], np.int64)
+    sample_seqs = np.zeros(len(samples) + 1, np.int64)
+    np.cumsum(counts, out=sample_seqs[1:])
+    bases = np.frombuffer(b"".join(seqs), np.uint8).copy() if seqs else np.zeros(0, np.uint8)
+    return bases, seq_off, sample_seqs
+
+
+def sketch(bases, seq_off, sample_seqs, kmers, s64, use_rc=True, min_count=0, threads=NTHREADS,
+           bbits=14):
+    """The oracle's sketcher (sko_sketch_samples): words [n][K][s64*bbits],
+    inv_minhash [n][K], densified [n]; min_count > 0 keeps hashes seen that
+    many times (exact counting)."""
+    b = np.ascontiguousarray(bases, np.uint8)
+    so = np.ascontiguousarray(seq_off, np.int64)
+    ss = np.ascontiguousarray(sample_seqs, np.int64)
+    km = np.ascontiguousarray(kmers, np.int32)
+    n = len(ss) - 1
+    words = np.zeros((n, len(km), s64 * bbits), np.uint64)
+    inv = np.zeros((n, len(km)), np.float64)
+    dens = np.zeros(n, np.uint8)
+    lib.sko_sketch_samples(b.ctypes.data, so.ctypes.data, ss.ctypes.data, n, km.ctypes.data,
+                           len(km), s64, bbits, int(use_rc), int(min_count), words.ctypes.data,
+                           inv.ctypes.data, dens.ctypes.data, threads)
+    return words, inv, dens.astype(bool)
+
+
 def ref_available() -> bool:
     return REF_PATH.exists()
 
@@ -261,6 +297,13 @@ class RefSketcher:
         lib_.ref_sketch_genomes.restype = C.c_int
         lib_.ref_sketch_genomes.argtypes = [C.c_void_p, C.c_int, C.c_int64, C.c_void_p, C.c_int,
                                             C.c_int, C.c_int, C.c_int, C.c_void_p]
+        lib_.ref_sketch_file.restype = C.c_int
+        lib_.ref_sketch_file.argtypes = [C.c_char_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                         C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        lib_.ref_sketch_seqs.restype = None
+        lib_.ref_sketch_seqs.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                         C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                         C.c_void_p, C.c_void_p]
         self.lib = lib_
 
     def genomes(self, n, length, seed):
@@ -275,6 +318,36 @@ class RefSketcher:
         self.lib.ref_sketch_genomes(g.ctypes.data, g.shape[0], g.shape[1], km.ctypes.data, len(km),
                                     s64, int(use_rc), threads, out.ctypes.data)
         return out
+
+
+    def sketch_seqs(self, bases, seq_off, sample_seqs, kmers, s64, use_rc=True, threads=NTHREADS):
+        """The reference's sketch() over samples of several sequences:
+        words [n][K][s64*14], inv_minhash [n][K], densified [n]."""
+        b = np.ascontiguousarray(bases, np.uint8)
+        so = np.ascontiguousarray(seq_off, np.int64)
+        ss = np.ascontiguousarray(sample_seqs, np.int64)
+        km = np.ascontiguousarray(kmers, np.int32)
+        n = len(ss) - 1
+        words = np.zeros((n, len(km), s64 * 14), np.uint64)
+        inv = np.zeros((n, len(km)), np.float64)
+        dens = np.zeros(n, np.uint8)
+        self.lib.ref_sketch_seqs(b.ctypes.data, so.ctypes.data, ss.ctypes.data, n, km.ctypes.data,
+                                 len(km), s64, int(use_rc), threads, words.ctypes.data,
+                                 inv.ctypes.data, dens.ctypes.data)
+        return words, inv, dens.astype(bool)
+
+
+    def sketch_file(self, path, kmers, s64, use_rc=True, min_count=0, exact=True):
+        """The reference's SeqBuf + sketch() on one sequence file (one sample):
+        (words [K][s64*14], inv_minhash [K], densified, is_reads)."""
+        km = np.ascontiguousarray(kmers, np.int32)
+        words = np.zeros((len(km), s64 * 14), np.uint64)
+        inv = np.zeros(len(km), np.float64)
+        dens = np.zeros(1, np.uint8)
+        reads = self.lib.ref_sketch_file(str(path).encode(), km.ctypes.data, len(km), s64,
+                                         int(use_rc), int(min_count), int(exact),
+                                         words.ctypes.data, inv.ctypes.data, dens.ctypes.data)
+        return words, inv, bool(dens[0]), bool(reads)
 
 
 def sketcher_available() -> bool:

@@ -14,6 +14,7 @@
 // segments (accessory).  Over the ~8 branches between two genomes of the
 // random recursive tree, pairs span about 0-3% core and 0-20% accessory
 // divergence.
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 #include <string>
@@ -93,6 +94,60 @@ int ref_sketch_genomes(const char *seqs, int n, int64_t length, const int32_t *k
     densified += any ? 1 : 0;
   }
   return densified;
+}
+
+// Sketches n samples given as sequences with the reference's sketch():
+// sample s owns sequences sample_seqs[s] .. sample_seqs[s+1], sequence i is
+// bases[seq_off[i], seq_off[i+1]).  Outputs words [n][K][sketchsize64 * 14],
+// inv_minhash [n][K] (bin 0 over 2^61-1 before densifying) and densified [n]
+// (any k densified).  The sequences go in as given (no case change, no length
+// filter): the reference's SeqBuf(std::vector<std::string>) constructor.
+void ref_sketch_seqs(const char *bases, const int64_t *seq_off, const int64_t *sample_seqs, int n,
+                     const int32_t *kmers, int K, int sketchsize64, int use_rc, int threads,
+                     uint64_t *out, double *inv_minhash, uint8_t *densified) {
+  std::vector<size_t> kl(kmers, kmers + K);
+  const KmerSeeds seeds = generate_seeds(kl, false);
+  const int64_t W = static_cast<int64_t>(sketchsize64) * 14;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
+  for (int s = 0; s < n; ++s) {
+    std::vector<std::string> seqs;
+    for (int64_t q = sample_seqs[s]; q < sample_seqs[s + 1]; ++q)
+      seqs.emplace_back(bases + seq_off[q], static_cast<size_t>(seq_off[q + 1] - seq_off[q]));
+    SeqBuf buf(seqs);
+    bool any = false;
+    for (int k = 0; k < K; ++k) {
+      auto res = sketch(buf, static_cast<uint64_t>(sketchsize64), seeds.at(kl[k]), 14, false,
+                        use_rc != 0, 0, false);
+      std::memcpy(out + (static_cast<int64_t>(s) * K + k) * W, std::get<0>(res).data(), W * 8);
+      inv_minhash[static_cast<int64_t>(s) * K + k] = std::get<1>(res);
+      any = any || std::get<2>(res);
+    }
+    densified[s] = any ? 1 : 0;
+  }
+}
+
+// Sketches one sample read from sequence files the way constructDatabase does
+// (src/api.cpp:87-89): SeqBuf(files, largest k) -- upper-cased, sequences
+// shorter than the largest k dropped, FASTQ input marks a read set -- then
+// sketch() at each k with the given min_count and exact flag.  Outputs as
+// ref_sketch_seqs for one sample; returns 1 if the input was a read set.
+int ref_sketch_file(const char *path, const int32_t *kmers, int K, int sketchsize64, int use_rc,
+                    int min_count, int exact, uint64_t *out, double *inv_minhash,
+                    uint8_t *densified) {
+  std::vector<size_t> kl(kmers, kmers + K);
+  const KmerSeeds seeds = generate_seeds(kl, false);
+  const int64_t W = static_cast<int64_t>(sketchsize64) * 14;
+  SeqBuf buf(std::vector<std::string>{std::string(path)}, *std::max_element(kl.begin(), kl.end()));
+  bool any = false;
+  for (int k = 0; k < K; ++k) {
+    auto res = sketch(buf, static_cast<uint64_t>(sketchsize64), seeds.at(kl[k]), 14, false,
+                      use_rc != 0, static_cast<uint8_t>(min_count), exact != 0);
+    std::memcpy(out + k * W, std::get<0>(res).data(), W * 8);
+    inv_minhash[k] = std::get<1>(res);
+    any = any || std::get<2>(res);
+  }
+  *densified = any ? 1 : 0;
+  return buf.is_reads() ? 1 : 0;
 }
 
 }  // extern "C"

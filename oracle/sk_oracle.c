@@ -18,6 +18,11 @@
  *   sko_sparsify       sparsify_dists_by_threshold src/dist/matrix_ops.cpp:38-69
  *   sko_long_to_square long_to_square            src/dist/matrix_ops.cpp:71-126
  *   sko_square_to_long square_to_long            src/dist/matrix_ops.cpp:130-150
+ *   sko_sketch         sketch (one sample, one k) src/sketch/sketch.cpp:120-168
+ *                      stHashIterator / NTMC64   src/sketch/stHashIterator.hpp:63-120,
+ *                                                src/sketch/nthash.hpp:57-126, 341-372
+ *                      binsign, fillusigs, densifybin, univhash, inverse_minhash
+ *                                                src/sketch/sketch.cpp:63-118
  *
  * Pinning: the golden vectors of the reference's own regression test
  * (test/ppsketch_ref*.npy, checked by test/test-dists.py) pin the Jaccard,
@@ -332,4 +337,172 @@ void sko_long_to_square(const float *rr, int64_t n_rr, const float *qr, const fl
 void sko_square_to_long(const float *square, int64_t n, float *long_out) {
   for (int64_t i = 0; i < n; i++)
     for (int64_t j = i + 1; j < n; j++) long_out[condensed(i, j, n)] = square[i * n + j];
+}
+
+/* -------------------------------------------------------------- sketching */
+
+/* ntHash (Mohamadi et al., Bioinformatics 2016) as the reference uses it:
+ * 64-bit per-base seeds (src/sketch/nthash_tables.hpp:25-29), combined with a
+ * "split rotation" that rotates the low 33 bits and the high 31 bits of the
+ * hash independently (nthash.hpp:17-55).  Forward hash of b_0..b_{k-1}:
+ * XOR_i srol^(k-1-i)(seed[b_i]); reverse: XOR_i srol^i(seed[comp(b_i)]);
+ * canonical: the smaller of the two (nthash.hpp:103-118). */
+static const uint64_t kNtSeed[4] = {0x3c8bfbb395c60474ULL, 0x3193c18562a02b4cULL,
+                                    0x20323ed082572324ULL, 0x295549f54be24456ULL};
+#define SKO_LO33 0x1FFFFFFFFULL
+#define SKO_SIGN_MOD ((1ULL << 61) - 1ULL)
+
+static uint64_t sko_srol(uint64_t v, unsigned n) {
+  const uint64_t lo = v & SKO_LO33, hi = v >> 33;
+  const unsigned a = n % 33, b = n % 31;
+  const uint64_t lo2 = a ? (((lo << a) | (lo >> (33 - a))) & SKO_LO33) : lo;
+  const uint64_t hi2 = b ? (((hi << b) | (hi >> (31 - b))) & 0x7FFFFFFFULL) : hi;
+  return (hi2 << 33) | lo2;
+}
+
+static uint64_t sko_sror1(uint64_t v) {
+  const uint64_t lo = v & SKO_LO33, hi = v >> 33;
+  const uint64_t lo2 = ((lo >> 1) | (lo << 32)) & SKO_LO33;
+  const uint64_t hi2 = ((hi >> 1) | (hi << 30)) & 0x7FFFFFFFULL;
+  return (hi2 << 33) | lo2;
+}
+
+/* 0..3 for A, C, G, T (U counts as T), either case; -1 for anything else,
+ * which the reference's seed table maps to the zero seed and skips. */
+static int sko_base(unsigned char c) {
+  switch (c) {
+    case 'A': case 'a': return 0;
+    case 'C': case 'c': return 1;
+    case 'G': case 'g': return 2;
+    case 'T': case 't': case 'U': case 'u': return 3;
+    default: return -1;
+  }
+}
+
+static uint64_t sko_univhash(uint64_t s, uint64_t t) {
+  const uint64_t x = 1009ULL * s + (1000ULL * 1000ULL + 3ULL) * t;
+  return (48271ULL * x + 11ULL) % ((1ULL << 31) - 1ULL);
+}
+
+/* Sketch of one sample at one k: the sequences seq_off[first..last) (each
+ * sequence i is bases[seq_off[i], seq_off[i+1])), every window of k valid
+ * bases inside one sequence hashed, the hash reduced mod 2^61-1 and kept as
+ * its bin's minimum; then the empty bins are filled in order by the
+ * reference's probe sequence and the low bbits bits of each bin value are
+ * written as bit planes, 64 bins per word.  Returns the densify result
+ * (0 no empty bin, 1 filled, -1 all empty); *inv_minhash is bin 0's value
+ * over 2^61-1 before filling. */
+static int sko_cmp_u64(const void *a, const void *b) {
+  const uint64_t x = *(const uint64_t *)a, y = *(const uint64_t *)b;
+  return x < y ? -1 : x > y;
+}
+
+static void sko_binsign(uint64_t *signs, uint64_t h, uint64_t binsize) {
+  const uint64_t sign = h % SKO_SIGN_MOD;
+  const uint64_t bin = sign / binsize;
+  if (sign < signs[bin]) signs[bin] = sign;
+}
+
+/* min_count > 0: only hashes that occur at least min_count times in the
+ * sample enter the bins -- the reference's exact counter (HashCounter,
+ * src/sketch/countmin.cpp:55-72, counting full 64-bit hash values; its uint8
+ * saturation at 255 never changes the answer for min_count <= 255). */
+int sko_sketch(const char *bases, const int64_t *seq_off, int64_t first, int64_t last, int k,
+               int s64, int bbits, int use_rc, int min_count, uint64_t *signs, uint64_t *words,
+               double *inv_minhash) {
+  const uint64_t nbins = (uint64_t)s64 * 64;
+  const uint64_t binsize = (SKO_SIGN_MOD + nbins - 1) / nbins;
+  uint64_t rk[4];
+  uint64_t *hashes = NULL;
+  int64_t n_hashes = 0;
+  if (min_count > 0) hashes = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)(seq_off[last] - seq_off[first] + 1));
+  for (int c = 0; c < 4; c++) rk[c] = sko_srol(kNtSeed[c], (unsigned)k);
+  for (uint64_t b = 0; b < nbins; b++) signs[b] = UINT64_MAX;
+  for (int64_t sq = first; sq < last; sq++) {
+    const unsigned char *s = (const unsigned char *)bases + seq_off[sq];
+    const int64_t len = seq_off[sq + 1] - seq_off[sq];
+    uint64_t fh = 0, rh = 0;
+    int64_t run = 0;
+    for (int64_t p = 0; p < len; p++) {
+      const int c = sko_base(s[p]);
+      if (c < 0) {  /* restart after a non-base, as stHashIterator::init does */
+        run = 0;
+        fh = rh = 0;
+        continue;
+      }
+      /* roll in base p; roll out base p-k once the window is full */
+      uint64_t f = sko_srol(fh, 1) ^ kNtSeed[c];
+      uint64_t r = rh ^ rk[3 - c];
+      if (run >= k) {
+        const int o = sko_base(s[p - k]);
+        f ^= rk[o];
+        r ^= kNtSeed[3 - o];
+      }
+      fh = f;
+      rh = sko_sror1(r);
+      if (run < k) run++;
+      if (run >= k) {
+        const uint64_t h = (use_rc && rh < fh) ? rh : fh;
+        if (hashes) hashes[n_hashes++] = h;
+        else sko_binsign(signs, h, binsize);
+      }
+    }
+  }
+  if (hashes) {
+    qsort(hashes, (size_t)n_hashes, sizeof(uint64_t), sko_cmp_u64);
+    for (int64_t i = 0; i < n_hashes;) {
+      int64_t j = i;
+      while (j < n_hashes && hashes[j] == hashes[i]) j++;
+      if (j - i >= min_count) sko_binsign(signs, hashes[i], binsize);
+      i = j;
+    }
+    free(hashes);
+  }
+  if (inv_minhash) *inv_minhash = (double)signs[0] / (double)SKO_SIGN_MOD;
+  uint64_t mn = UINT64_MAX, mx = 0;
+  for (uint64_t b = 0; b < nbins; b++) {
+    if (signs[b] < mn) mn = signs[b];
+    if (signs[b] > mx) mx = signs[b];
+  }
+  int densified = 0;
+  if (mx == UINT64_MAX) {
+    if (mn == UINT64_MAX) {
+      densified = -1;
+    } else {
+      for (uint64_t i = 0; i < nbins; i++) {
+        uint64_t j = i, attempt = 0;
+        while (signs[j] == UINT64_MAX) j = sko_univhash(i, attempt++) % nbins;
+        signs[i] = signs[j];
+      }
+      densified = 1;
+    }
+  }
+  memset(words, 0, sizeof(uint64_t) * (size_t)s64 * (size_t)bbits);
+  for (uint64_t b = 0; b < nbins; b++)
+    for (int i = 0; i < bbits; i++)
+      words[(b / 64) * (uint64_t)bbits + (uint64_t)i] |= ((signs[b] >> i) & 1ULL) << (b % 64);
+  return densified;
+}
+
+/* sko_sketch over n samples (sample s owns sequences sample_seqs[s] ..
+ * sample_seqs[s+1]) and K k-mer lengths: words [n][K][s64*bbits],
+ * inv_minhash [n][K], densified [n] (any k with a nonzero densify result). */
+void sko_sketch_samples(const char *bases, const int64_t *seq_off, const int64_t *sample_seqs,
+                        int64_t n, const int *kmers, int K, int s64, int bbits, int use_rc,
+                        int min_count, uint64_t *words, double *inv_minhash, uint8_t *densified,
+                        int threads) {
+  const int64_t W = (int64_t)s64 * bbits;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
+  for (int64_t s = 0; s < n; s++) {
+    uint64_t *signs = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)s64 * 64);
+    uint8_t any = 0;
+    for (int k = 0; k < K; k++) {
+      const int d = sko_sketch(bases, seq_off, sample_seqs[s], sample_seqs[s + 1], kmers[k], s64,
+                               bbits, use_rc, min_count, signs, words + (s * K + k) * W,
+                               inv_minhash ? inv_minhash + s * K + k : NULL);
+      if (d != 0) any = 1;
+    }
+    if (densified) densified[s] = any;
+    free(signs);
+  }
 }

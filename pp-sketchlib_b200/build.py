@@ -24,7 +24,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 CUDA_SOURCES = ["dist_kernel.cu", "aux_kernels.cu", "probe_kernels.cu", "capi.cu", "batch.cu",
-                "serve.cu", "noalloc.cu", "query_db.cu"]
+                "serve.cu", "noalloc.cu", "query_db.cu", "sketch.cu"]
 
 
 def _stale(target: Path, sources) -> bool:

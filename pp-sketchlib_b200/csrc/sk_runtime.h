@@ -32,7 +32,15 @@ enum ScratchSlot : int {
   kSlotPackedQuery = 8,
   kSlotCountsB = 9,       // count scratch of launches on the second compute stream
   kSlotSplitCountsB = 10,
-  kSlotCount = 11
+  kSlotSketchCodes = 11,  // bases of one sketching batch, rewritten as base codes
+  kSlotSketchSeqs = 12,   // sequence offsets of the batch
+  kSlotSketchItems = 13,  // sketching work items
+  kSlotSketchTables = 14, // rolling-hash tables per k
+  kSlotSketchBins = 15,   // bin minima per (sample, k)
+  kSlotSketchWords = 16,  // finished sketches, inverse minhashes, densify flags
+  kSlotSketchKeys = 17,   // hash-count table of read sets (keys, counts)
+  kSlotSketchCounts = 18,
+  kSlotCount = 19
 };
 
 struct sk_ctx {

@@ -1,0 +1,714 @@
+// sketch.cu -- MinHash sketches of sequences on the device: the producer of
+// the distance path's input.
+//
+// The reference sketches on the CPU, one sample and one k at a time
+// (sketch(), src/sketch/sketch.cpp:120-168): ntHash rolls along each sequence
+// (stHashIterator, src/sketch/stHashIterator.hpp:63-120), each canonical hash
+// mod 2^61-1 keeps its bin's minimum (binsign, :69-73), empty bins are filled
+// from a probe sequence (densifybin, :93-118) and the low 14 bits of every
+// bin become bit planes, 64 bins per word (fillusigs, :82-91).  Here:
+//
+//   codes      the bases go up as they are and are rewritten in place as one
+//              byte per base: 0..3 for A, C, G, T/U in either case, 4 for any
+//              other byte, plus kCodeStart on the first base of each sequence.
+//   hashing    a work item is (sample, k, range of window starts).  Its CTA
+//              keeps the item's bin minima in shared memory; each thread rolls
+//              the forward and reverse hashes over its share of the range.  A
+//              non-base contributes zero to both hashes, so the roll never
+//              restarts: a window is emitted once the bases since the last
+//              non-base or sequence start number k, and the hash then equals
+//              the reference's freshly initialised one.  The CTA folds its
+//              minima into the sample's bins with atomicMin.
+//   finishing  one CTA per (sample, k) records bin 0 (inverse_minhash), fills
+//              empty bins in the reference's order and writes the bit planes
+//              with warp ballots.
+//   counting   with min_count > 0 (read sets), hashes are first counted in a
+//              device hash table and only those seen min_count times enter
+//              the bins: the reference's exact counter (HashCounter,
+//              src/sketch/countmin.cpp:55-72, `exact = true`), whose answer
+//              does not depend on read order.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "sk_runtime.h"
+
+namespace sk {
+namespace {
+
+constexpr uint64_t kSignMod = (1ULL << 61) - 1;   // SIGN_MOD (src/sketch/sketch.cpp:23)
+constexpr uint64_t kLo33 = 0x1FFFFFFFFULL;
+constexpr uint8_t kCodeInvalid = 4;
+constexpr uint8_t kCodeStart = 8;
+constexpr int kSketchThreads = 512;
+constexpr int kPerThread = 512;                    // window starts per thread
+constexpr int64_t kItemWindows = static_cast<int64_t>(kSketchThreads) * kPerThread;
+constexpr int kFinishThreads = 512;
+constexpr int kMinK = 3;                           // generate_seeds (src/sketch/sketch.cpp:33-40)
+constexpr int kMaxK = 255;
+constexpr unsigned long long kEmptyKey = ~0ULL;
+constexpr unsigned kErrDensify = 4u;               // DevStatus.error bits of the sketcher
+constexpr unsigned kErrTable = 8u;
+
+// ntHash per-base seeds for A, C, G, T (ntHash, Mohamadi et al. 2016; the
+// values of the reference's src/sketch/nthash_tables.hpp:25-29).
+constexpr uint64_t kNtSeed[4] = {0x3c8bfbb395c60474ULL, 0x3193c18562a02b4cULL,
+                                 0x20323ed082572324ULL, 0x295549f54be24456ULL};
+
+// ntHash's split rotation: the low 33 bits and the high 31 bits of the hash
+// rotate independently (src/sketch/nthash.hpp:17-55).
+__host__ __device__ __forceinline__ uint64_t srol1(uint64_t v) {
+  const uint64_t lo = v & kLo33, hi = v & ~kLo33;
+  return (((lo << 1) | (lo >> 32)) & kLo33) | ((hi << 1) & ~kLo33) | ((hi >> 30) & (1ULL << 33));
+}
+
+__host__ __device__ __forceinline__ uint64_t sror1(uint64_t v) {
+  const uint64_t lo = v & kLo33, hi = v & ~kLo33;
+  return (((lo >> 1) | (lo << 32)) & kLo33) | ((hi >> 1) & ~kLo33) | ((hi << 30) & (1ULL << 63));
+}
+
+uint64_t srol_n(uint64_t v, unsigned n) {
+  for (unsigned i = 0; i < n % (33ULL * 31ULL); ++i) v = srol1(v);
+  return v;
+}
+
+struct SketchItem {
+  int64_t begin, end;     // window starts, offsets into the code buffer
+  int32_t row;            // sample * K + k index (bins row)
+  int32_t k;
+  int32_t tab;            // k index (table row)
+  int32_t pad;
+};
+
+// Rolling tables of one k: in[c] = {seed[c], srol^k(seed[3-c])} for the base
+// entering the window, out[c] = {srol^k(seed[c]), seed[3-c]} for the base
+// leaving it; c = 4 (not a base) contributes zero.
+struct RollTable {
+  ulonglong2 in[8];
+  ulonglong2 out[8];
+};
+
+RollTable make_table(int k) {
+  RollTable t{};
+  for (int c = 0; c < 4; ++c) {
+    t.in[c] = make_ulonglong2(kNtSeed[c], srol_n(kNtSeed[3 - c], k));
+    t.out[c] = make_ulonglong2(srol_n(kNtSeed[c], k), kNtSeed[3 - c]);
+  }
+  return t;
+}
+
+__device__ __forceinline__ uint64_t mod_sign(uint64_t h) {
+  const uint64_t r = (h & kSignMod) + (h >> 61);
+  return r >= kSignMod ? r - kSignMod : r;
+}
+
+// sign / binsize exactly: magic = floor((2^64-1) / binsize) under-estimates
+// the quotient by at most one for sign < 2^61.
+__device__ __forceinline__ uint32_t bin_of(uint64_t sign, uint64_t binsize, uint64_t magic) {
+  uint64_t q = __umul64hi(sign, magic);
+  if (sign - q * binsize >= binsize) ++q;
+  return static_cast<uint32_t>(q);
+}
+
+__device__ __forceinline__ uint8_t base_code(uint8_t c) {
+  const uint8_t l = c | 0x20;   // letters to lower case
+  return l == 'a' ? 0 : l == 'c' ? 1 : l == 'g' ? 2 : (l == 't' || l == 'u') ? 3 : kCodeInvalid;
+}
+
+__global__ void codes_kernel(uint8_t *__restrict__ buf, int64_t n) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  const int64_t nv = n / 16;
+  uint4 *v = reinterpret_cast<uint4 *>(buf);
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < nv; i += stride) {
+    uint4 x = v[i];
+    uint32_t w[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      uint32_t o = 0;
+#pragma unroll
+      for (int b = 0; b < 4; ++b) o |= static_cast<uint32_t>(base_code((w[j] >> (8 * b)) & 0xFF)) << (8 * b);
+      w[j] = o;
+    }
+    v[i] = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+  for (int64_t i = nv * 16 + blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n; i += stride)
+    buf[i] = base_code(buf[i]);
+}
+
+__global__ void mark_starts_kernel(uint8_t *__restrict__ codes, const int64_t *__restrict__ seq_off,
+                                   int64_t n_seqs) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n_seqs; i += stride) {
+    const int64_t a = seq_off[i] - seq_off[0], b = seq_off[i + 1] - seq_off[0];
+    if (b > a) codes[a] |= kCodeStart;
+  }
+}
+
+// Rolls over the window starts [s, e) and calls emit(hash) for every window of
+// k bases inside one sequence.  Reads codes[s .. e+k-2].
+template <typename Emit>
+__device__ __forceinline__ void roll_windows(const uint8_t *__restrict__ codes, int64_t s, int64_t e,
+                                             int k, const RollTable &t, bool use_rc, Emit emit) {
+  uint64_t fh = 0, rh = 0;
+  int run = 0;
+  const int64_t last = e + k - 1;
+  // first k bases: nothing leaves the window
+  const int64_t warm = min(s + k, last);
+  for (int64_t p = s; p < warm; ++p) {
+    const uint8_t ci = codes[p];
+    const ulonglong2 a = t.in[ci & 7];
+    fh = srol1(fh) ^ a.x;
+    rh = sror1(rh ^ a.y);
+    run = (ci & 7) == kCodeInvalid ? 0 : ((ci & kCodeStart) ? 1 : min(run + 1, k));
+  }
+  if (run >= k) emit(use_rc && rh < fh ? rh : fh);
+#pragma unroll 4
+  for (int64_t p = s + k; p < last; ++p) {
+    const uint8_t ci = codes[p], co = codes[p - k];
+    const ulonglong2 a = t.in[ci & 7], b = t.out[co & 7];
+    fh = srol1(fh) ^ a.x ^ b.x;
+    rh = sror1(rh ^ a.y ^ b.y);
+    run = (ci & 7) == kCodeInvalid ? 0 : ((ci & kCodeStart) ? 1 : min(run + 1, k));
+    if (run >= k) emit(use_rc && rh < fh ? rh : fh);
+  }
+}
+
+struct SketchArgs {
+  const uint8_t *codes;
+  const SketchItem *items;
+  const RollTable *tables;
+  unsigned long long *signs;     // [rows][nbins]
+  int nbins;
+  int use_rc;
+  uint64_t binsize, magic;
+  // counting mode
+  unsigned long long *keys;      // hash table keys (kEmptyKey = free)
+  unsigned int *counts;
+  uint64_t table_mask;
+  unsigned int *max_key_count;   // occurrences of the one hash equal to kEmptyKey
+  uint32_t bin_lo, bin_hi;       // bins this pass counts
+  DevStatus *status;
+};
+
+// Bin minima of one item; kShared keeps them in shared memory (nbins * 8
+// bytes of dynamic shared memory), else the CTA updates the global row.
+template <bool kShared>
+__global__ void __launch_bounds__(kSketchThreads, 1)
+sketch_kernel(SketchArgs a) {
+  extern __shared__ unsigned long long sh_bins[];
+  __shared__ RollTable tab;
+  const SketchItem it = a.items[blockIdx.x];
+  unsigned long long *row = a.signs + static_cast<int64_t>(it.row) * a.nbins;
+  unsigned long long *bins = kShared ? sh_bins : row;
+  if (kShared)
+    for (int i = threadIdx.x; i < a.nbins; i += kSketchThreads) sh_bins[i] = kEmptyKey;
+  if (threadIdx.x < 16) {
+    const ulonglong2 *src = reinterpret_cast<const ulonglong2 *>(a.tables + it.tab);
+    reinterpret_cast<ulonglong2 *>(&tab)[threadIdx.x] = src[threadIdx.x];
+  }
+  __syncthreads();
+  const int64_t s = it.begin + static_cast<int64_t>(threadIdx.x) * kPerThread;
+  const int64_t e = min(s + kPerThread, it.end);
+  if (s < e) {
+    const uint64_t binsize = a.binsize, magic = a.magic;
+    roll_windows(a.codes, s, e, it.k, tab, a.use_rc != 0, [&](uint64_t h) {
+      const uint64_t sign = mod_sign(h);
+      const uint32_t q = bin_of(sign, binsize, magic);
+      if (sign < bins[q]) atomicMin(bins + q, static_cast<unsigned long long>(sign));
+    });
+  }
+  if (kShared) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < a.nbins; i += kSketchThreads) {
+      const unsigned long long v = sh_bins[i];
+      if (v < row[i]) atomicMin(row + i, v);
+    }
+  }
+}
+
+__device__ __forceinline__ uint64_t table_slot(uint64_t h, uint64_t mask) {
+  h ^= h >> 33;
+  h *= 0xff51afd7ed558ccdULL;
+  h ^= h >> 33;
+  return h & mask;
+}
+
+// Counting pass: every hash whose bin lies in [bin_lo, bin_hi) is counted.
+__global__ void __launch_bounds__(kSketchThreads)
+count_kernel(SketchArgs a) {
+  __shared__ RollTable tab;
+  const SketchItem it = a.items[blockIdx.x];
+  if (threadIdx.x < 16) {
+    const ulonglong2 *src = reinterpret_cast<const ulonglong2 *>(a.tables + it.tab);
+    reinterpret_cast<ulonglong2 *>(&tab)[threadIdx.x] = src[threadIdx.x];
+  }
+  __syncthreads();
+  const int64_t s = it.begin + static_cast<int64_t>(threadIdx.x) * kPerThread;
+  const int64_t e = min(s + kPerThread, it.end);
+  if (s >= e) return;
+  roll_windows(a.codes, s, e, it.k, tab, a.use_rc != 0, [&](uint64_t h) {
+    const uint32_t q = bin_of(mod_sign(h), a.binsize, a.magic);
+    if (q < a.bin_lo || q >= a.bin_hi) return;
+    if (h == kEmptyKey) {
+      atomicAdd(a.max_key_count, 1u);
+      return;
+    }
+    uint64_t slot = table_slot(h, a.table_mask);
+    for (uint64_t probe = 0; probe <= a.table_mask; ++probe) {
+      unsigned long long cur = a.keys[slot];
+      if (cur == kEmptyKey) {
+        cur = atomicCAS(a.keys + slot, kEmptyKey, static_cast<unsigned long long>(h));
+        if (cur == kEmptyKey) cur = h;
+      }
+      if (cur == h) {
+        atomicAdd(a.counts + slot, 1u);
+        return;
+      }
+      slot = (slot + 1) & a.table_mask;
+    }
+    atomicOr(&a.status->error, kErrTable);   // table full (sized at twice the windows: not reached)
+  });
+}
+
+// Hashes counted at least min_count times enter the bins of `row`.
+__global__ void table_bins_kernel(SketchArgs a, int row_index, unsigned min_count) {
+  unsigned long long *row = a.signs + static_cast<int64_t>(row_index) * a.nbins;
+  const uint64_t n = a.table_mask + 1;
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n; i += stride) {
+    const unsigned long long h = a.keys[i];
+    if (h == kEmptyKey || a.counts[i] < min_count) continue;
+    const uint64_t sign = mod_sign(h);
+    const uint32_t q = bin_of(sign, a.binsize, a.magic);
+    if (sign < row[q]) atomicMin(row + q, static_cast<unsigned long long>(sign));
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && *a.max_key_count >= min_count && *a.max_key_count > 0) {
+    const uint64_t sign = mod_sign(kEmptyKey);
+    const uint32_t q = bin_of(sign, a.binsize, a.magic);
+    atomicMin(row + q, static_cast<unsigned long long>(sign));
+  }
+}
+
+__device__ __forceinline__ uint64_t univhash(uint64_t s, uint64_t t) {
+  const uint64_t x = 1009ULL * s + (1000ULL * 1000ULL + 3ULL) * t;
+  return (48271ULL * x + 11ULL) % ((1ULL << 31) - 1ULL);
+}
+
+// One CTA per bins row: inverse minhash, densify, bit planes.
+__global__ void __launch_bounds__(kFinishThreads)
+finish_kernel(unsigned long long *__restrict__ signs, int nbins, int s64, uint64_t *__restrict__ words,
+              double *__restrict__ inv_minhash, int8_t *__restrict__ densified, DevStatus *status) {
+  unsigned long long *row = signs + static_cast<int64_t>(blockIdx.x) * nbins;
+  __shared__ unsigned long long smin, smax;
+  if (threadIdx.x == 0) {
+    smin = kEmptyKey;
+    smax = 0;
+    inv_minhash[blockIdx.x] = static_cast<double>(row[0]) / static_cast<double>(kSignMod);
+  }
+  __syncthreads();
+  unsigned long long mn = kEmptyKey, mx = 0;
+  for (int i = threadIdx.x; i < nbins; i += kFinishThreads) {
+    const unsigned long long v = row[i];
+    mn = min(mn, v);
+    mx = max(mx, v);
+  }
+  atomicMin(&smin, mn);
+  atomicMax(&smax, mx);
+  __syncthreads();
+  const bool some_empty = smax == kEmptyKey, all_empty = smin == kEmptyKey;
+  if (threadIdx.x == 0) densified[blockIdx.x] = some_empty ? (all_empty ? -1 : 1) : 0;
+  if (some_empty && !all_empty && threadIdx.x < 32) {
+    // empty bins in increasing order, each from the first filled bin of its
+    // probe sequence (bins filled earlier in the loop count as filled)
+    const unsigned lane = threadIdx.x;
+    for (int base = 0; base < nbins; base += 32) {
+      const int i0 = base + static_cast<int>(lane);
+      unsigned m = __ballot_sync(0xffffffffu, i0 < nbins && row[i0] == kEmptyKey);
+      while (m) {
+        const int i = base + __ffs(m) - 1;
+        m &= m - 1;
+        uint64_t j = static_cast<uint64_t>(i), attempt = 0;
+        unsigned long long v = kEmptyKey;
+        while ((v = row[j]) == kEmptyKey) {
+          if (attempt > (1ULL << 24)) {
+            if (lane == 0) atomicOr(&status->error, kErrDensify);
+            break;
+          }
+          j = univhash(static_cast<uint64_t>(i), attempt++) % static_cast<uint64_t>(nbins);
+        }
+        __syncwarp();
+        if (lane == 0) row[i] = v;
+        __syncwarp();
+      }
+    }
+  }
+  __syncthreads();
+  // bit planes: word (block b, plane p) holds bit p of bins 64b .. 64b+63
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  uint64_t *out = words + static_cast<int64_t>(blockIdx.x) * s64 * kBbits;
+  for (int b = warp; b < s64; b += kFinishThreads / 32) {
+    const unsigned long long v0 = row[64 * b + lane], v1 = row[64 * b + 32 + lane];
+    uint64_t mine = 0;
+#pragma unroll
+    for (int p = 0; p < kBbits; ++p) {
+      const unsigned lo = __ballot_sync(0xffffffffu, (v0 >> p) & 1ULL);
+      const unsigned hi = __ballot_sync(0xffffffffu, (v1 >> p) & 1ULL);
+      if (lane == p) mine = (static_cast<uint64_t>(hi) << 32) | lo;
+    }
+    if (lane < kBbits) out[static_cast<int64_t>(b) * kBbits + lane] = mine;
+  }
+}
+
+int max_dyn_smem(int device) {
+  int v = 0;
+  cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  return v;
+}
+
+// Largest bins row kept in shared memory.
+bool bins_fit_shared(int device, int nbins) {
+  return static_cast<int64_t>(nbins) * 8 + static_cast<int64_t>(sizeof(RollTable)) + 1024 <=
+         max_dyn_smem(device);
+}
+
+struct Batch {
+  int64_t s0, s1;          // samples
+  int64_t q0, q1;          // sequences
+  int64_t b0, b1;          // bytes (offsets in the caller's buffer)
+};
+
+constexpr int64_t kBatchBytes = 1LL << 30;         // bases per batch
+constexpr int64_t kBatchBins = 1LL << 30;          // bytes of bins rows per batch
+
+}  // namespace
+}  // namespace sk
+
+using namespace sk;
+
+namespace {
+
+struct SketchCall {
+  sk_ctx *ctx;
+  const char *bases;
+  const int64_t *seq_off;
+  const int64_t *sample_seqs;
+  int64_t n;
+  std::vector<int32_t> kmers;
+  int s64, use_rc, min_count;
+  int nbins;
+  uint64_t binsize, magic;
+  // device buffers (context scratch)
+  uint8_t *d_codes = nullptr;
+  int64_t *d_seq_off = nullptr;
+  SketchItem *d_items = nullptr;
+  RollTable *d_tables = nullptr;
+  unsigned long long *d_signs = nullptr;
+  uint64_t *d_words = nullptr;
+  double *d_inv = nullptr;
+  int8_t *d_dens = nullptr;
+};
+
+sk_status check_inputs(sk_ctx *ctx, const char *bases, const int64_t *seq_off,
+                       const int64_t *sample_seqs, int64_t n, const int32_t *kmers, int32_t K,
+                       int32_t s64, int32_t use_rc, int32_t min_count) {
+  if (n < 0) return fail(ctx, SK_EINVAL, "negative sample count");
+  if (n == 0) return SK_OK;
+  if (!seq_off || !sample_seqs || !kmers) return fail(ctx, SK_EINVAL, "null argument");
+  if (K < 1 || K > kMaxKmers) return fail(ctx, SK_ERANGE, "n_kmers %d outside [1, %d]", K, kMaxKmers);
+  for (int k = 0; k < K; ++k) {
+    if (kmers[k] < kMinK) return fail(ctx, SK_EINVAL, "Minimum k must be 3 or higher");
+    if (kmers[k] > kMaxK) return fail(ctx, SK_EINVAL, "k-mer length %d above %d", kmers[k], kMaxK);
+  }
+  if (s64 < 1 || s64 > kMaxSketch64)
+    return fail(ctx, SK_ERANGE, "sketchsize64 %d outside [1, %d]", s64, kMaxSketch64);
+  if (use_rc != 0 && use_rc != 1) return fail(ctx, SK_EINVAL, "use_rc must be 0 or 1");
+  if (min_count < 0 || min_count > 255) return fail(ctx, SK_EINVAL, "min_count %d outside [0, 255]", min_count);
+  if (sample_seqs[0] < 0) return fail(ctx, SK_EINVAL, "negative sequence index");
+  for (int64_t s = 0; s < n; ++s)
+    if (sample_seqs[s + 1] <= sample_seqs[s])
+      return fail(ctx, SK_EINVAL, "sample %lld contains no sequence", static_cast<long long>(s));
+  for (int64_t q = sample_seqs[0]; q < sample_seqs[n]; ++q)
+    if (seq_off[q + 1] < seq_off[q])
+      return fail(ctx, SK_EINVAL, "sequence offsets decrease at %lld", static_cast<long long>(q));
+  if (seq_off[sample_seqs[n]] > seq_off[sample_seqs[0]] && !bases)
+    return fail(ctx, SK_EINVAL, "null bases");
+  return SK_OK;
+}
+
+std::vector<Batch> make_batches(const SketchCall &c) {
+  std::vector<Batch> out;
+  const int64_t row_bytes = static_cast<int64_t>(c.kmers.size()) * c.nbins * 8;
+  int64_t s = 0;
+  while (s < c.n) {
+    Batch b{};
+    b.s0 = s;
+    b.q0 = c.sample_seqs[s];
+    b.b0 = c.seq_off[b.q0];
+    int64_t e = s + 1;
+    while (e < c.n && c.seq_off[c.sample_seqs[e + 1]] - b.b0 <= kBatchBytes &&
+           (e + 1 - s) * row_bytes <= kBatchBins)
+      ++e;
+    b.s1 = e;
+    b.q1 = c.sample_seqs[e];
+    b.b1 = c.seq_off[b.q1];
+    out.push_back(b);
+    s = e;
+  }
+  return out;
+}
+
+// Work items of samples [s0, s1) of a batch whose bytes start at b0: window
+// starts of each sample in pieces of kItemWindows, every k of a piece
+// adjacent (they read the same bases).
+void make_items(const SketchCall &c, const Batch &b, int64_t s0, int64_t s1, int k_only,
+                std::vector<SketchItem> &items) {
+  items.clear();
+  const int K = static_cast<int>(c.kmers.size());
+  for (int64_t s = s0; s < s1; ++s) {
+    const int64_t a = c.seq_off[c.sample_seqs[s]] - b.b0, e = c.seq_off[c.sample_seqs[s + 1]] - b.b0;
+    for (int64_t p = a; p < e; p += kItemWindows)
+      for (int k = 0; k < K; ++k) {
+        if (k_only >= 0 && k != k_only) continue;
+        SketchItem it{};
+        it.begin = p;
+        it.end = std::min(p + kItemWindows, e);
+        it.row = static_cast<int32_t>((s - b.s0) * K + k);
+        it.k = c.kmers[k];
+        it.tab = k;
+        items.push_back(it);
+      }
+  }
+}
+
+sk_status upload(sk_ctx *ctx, void *dst, const void *src, size_t bytes) {
+  if (!bytes) return SK_OK;
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream);
+  return e == cudaSuccess ? SK_OK : cuda_fail(ctx, e, "sketch upload");
+}
+
+// Bins rows of one batch without a count filter.
+sk_status hash_batch(SketchCall &c, const Batch &b, SketchArgs &args, std::vector<SketchItem> &items) {
+  sk_ctx *ctx = c.ctx;
+  make_items(c, b, b.s0, b.s1, -1, items);
+  if (items.empty()) return SK_OK;
+  void *p = nullptr;
+  sk_status st = scratch(ctx, kSlotSketchItems, items.size() * sizeof(SketchItem), &p);
+  if (st != SK_OK) return st;
+  args.items = static_cast<SketchItem *>(p);
+  st = upload(ctx, p, items.data(), items.size() * sizeof(SketchItem));
+  if (st != SK_OK) return st;
+  const bool shared = bins_fit_shared(ctx->device, c.nbins);
+  const size_t smem = shared ? static_cast<size_t>(c.nbins) * 8 : 0;
+  cudaError_t e = cudaSuccess;
+  if (shared) {
+    e = cudaFuncSetAttribute(sketch_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem));
+    if (e == cudaSuccess)
+      sketch_kernel<true><<<static_cast<unsigned>(items.size()), kSketchThreads, smem, ctx->stream>>>(args);
+  } else {
+    sketch_kernel<false><<<static_cast<unsigned>(items.size()), kSketchThreads, 0, ctx->stream>>>(args);
+  }
+  if (e == cudaSuccess) e = cudaGetLastError();
+  return e == cudaSuccess ? SK_OK : cuda_fail(ctx, e, "sketch kernel");
+}
+
+uint64_t next_pow2(uint64_t v) {
+  uint64_t p = 1;
+  while (p < v) p <<= 1;
+  return p;
+}
+
+// Bins rows of one batch with the exact count filter: per sample and k, the
+// hashes are counted in a table of twice the sample's windows (in bin-range
+// passes when that exceeds the table budget), then the ones counted
+// min_count times enter the bins.
+sk_status count_batch(SketchCall &c, const Batch &b, SketchArgs &args, std::vector<SketchItem> &items) {
+  sk_ctx *ctx = c.ctx;
+  const int K = static_cast<int>(c.kmers.size());
+  constexpr uint64_t kTableBudget = 1ULL << 31;   // bytes of keys + counts per pass
+  for (int64_t s = b.s0; s < b.s1; ++s) {
+    const int64_t windows = c.seq_off[c.sample_seqs[s + 1]] - c.seq_off[c.sample_seqs[s]];
+    if (windows <= 0) continue;
+    const uint64_t want = next_pow2(static_cast<uint64_t>(windows) * 2);
+    const uint64_t passes = std::max<uint64_t>(1, (want * 12 + kTableBudget - 1) / kTableBudget);
+    const uint64_t slots = std::max<uint64_t>(1024, next_pow2((want + passes - 1) / passes));
+    void *tk = nullptr, *tc = nullptr;
+    sk_status st = scratch(ctx, kSlotSketchKeys, slots * 8, &tk);
+    if (st == SK_OK) st = scratch(ctx, kSlotSketchCounts, slots * 4 + 16, &tc);
+    if (st != SK_OK) return st;
+    args.keys = static_cast<unsigned long long *>(tk);
+    args.counts = static_cast<unsigned int *>(tc);
+    args.max_key_count = reinterpret_cast<unsigned int *>(static_cast<char *>(tc) + slots * 4);
+    args.table_mask = slots - 1;
+    for (int k = 0; k < K; ++k) {
+      make_items(c, b, s, s + 1, k, items);
+      void *p = nullptr;
+      st = scratch(ctx, kSlotSketchItems, items.size() * sizeof(SketchItem), &p);
+      if (st == SK_OK) st = upload(ctx, p, items.data(), items.size() * sizeof(SketchItem));
+      if (st != SK_OK) return st;
+      args.items = static_cast<SketchItem *>(p);
+      for (uint64_t pass = 0; pass < passes; ++pass) {
+        args.bin_lo = static_cast<uint32_t>(c.nbins * pass / passes);
+        args.bin_hi = static_cast<uint32_t>(c.nbins * (pass + 1) / passes);
+        cudaError_t e = cudaMemsetAsync(tk, 0xFF, slots * 8, ctx->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(tc, 0, slots * 4 + 16, ctx->stream);
+        if (e == cudaSuccess) {
+          count_kernel<<<static_cast<unsigned>(items.size()), kSketchThreads, 0, ctx->stream>>>(args);
+          e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) {
+          const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(4096, (slots + 255) / 256));
+          table_bins_kernel<<<grid, 256, 0, ctx->stream>>>(args, static_cast<int>((s - b.s0) * K + k),
+                                                           static_cast<unsigned>(c.min_count));
+          e = cudaGetLastError();
+        }
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "sketch counting");
+      }
+    }
+  }
+  return SK_OK;
+}
+
+// Sketches the samples of one batch into d_words / d_inv / d_dens (rows of the
+// batch's samples) on the context's stream.
+sk_status sketch_batch(SketchCall &c, const Batch &b, std::vector<SketchItem> &items) {
+  sk_ctx *ctx = c.ctx;
+  const int K = static_cast<int>(c.kmers.size());
+  const int64_t nb = b.s1 - b.s0;
+  const int64_t rows = nb * K;
+  const int64_t bytes = b.b1 - b.b0;
+  const int64_t n_seqs = b.q1 - b.q0;
+  const int64_t pad = kMaxK + 64;
+  void *p = nullptr;
+  sk_status st = scratch(ctx, kSlotSketchCodes, static_cast<size_t>(bytes + pad), &p);
+  if (st != SK_OK) return st;
+  c.d_codes = static_cast<uint8_t *>(p);
+  st = scratch(ctx, kSlotSketchSeqs, static_cast<size_t>(n_seqs + 1) * 8, &p);
+  if (st != SK_OK) return st;
+  c.d_seq_off = static_cast<int64_t *>(p);
+  st = scratch(ctx, kSlotSketchBins, static_cast<size_t>(rows) * c.nbins * 8, &p);
+  if (st != SK_OK) return st;
+  c.d_signs = static_cast<unsigned long long *>(p);
+  cudaError_t e = cudaMemsetAsync(c.d_codes + bytes, kCodeInvalid, pad, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c.d_signs, 0xFF, static_cast<size_t>(rows) * c.nbins * 8, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "sketch buffers");
+  st = upload(ctx, c.d_codes, c.bases + b.b0, static_cast<size_t>(bytes));
+  if (st == SK_OK) st = upload(ctx, c.d_seq_off, c.seq_off + b.q0, static_cast<size_t>(n_seqs + 1) * 8);
+  if (st != SK_OK) return st;
+  const unsigned g = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(ctx->sm_count * 8, (bytes / 16 + 255) / 256)));
+  codes_kernel<<<g, 256, 0, ctx->stream>>>(c.d_codes, bytes);
+  mark_starts_kernel<<<static_cast<unsigned>(std::min<int64_t>(ctx->sm_count * 8, (n_seqs + 255) / 256)), 256, 0,
+                       ctx->stream>>>(c.d_codes, c.d_seq_off, n_seqs);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "sketch codes");
+  SketchArgs args{};
+  args.codes = c.d_codes;
+  args.tables = c.d_tables;
+  args.signs = c.d_signs;
+  args.nbins = c.nbins;
+  args.use_rc = c.use_rc;
+  args.binsize = c.binsize;
+  args.magic = c.magic;
+  args.status = ctx->status_dev;
+  st = c.min_count > 0 ? count_batch(c, b, args, items) : hash_batch(c, b, args, items);
+  if (st != SK_OK) return st;
+  finish_kernel<<<static_cast<unsigned>(rows), kFinishThreads, 0, ctx->stream>>>(
+      c.d_signs, c.nbins, c.s64, c.d_words + b.s0 * K * static_cast<int64_t>(c.s64) * kBbits,
+      c.d_inv + b.s0 * K, c.d_dens + b.s0 * K, ctx->status_dev);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? SK_OK : cuda_fail(ctx, e, "sketch finish");
+}
+
+// Everything up to device-resident words / inverse minhashes / densify flags
+// of all samples (d_words, d_inv, d_dens sized by the caller).
+sk_status sketch_to_device(SketchCall &c) {
+  sk_ctx *ctx = c.ctx;
+  const int K = static_cast<int>(c.kmers.size());
+  std::vector<RollTable> tables(K);
+  for (int k = 0; k < K; ++k) tables[k] = make_table(c.kmers[k]);
+  void *p = nullptr;
+  sk_status st = scratch(ctx, kSlotSketchTables, tables.size() * sizeof(RollTable), &p);
+  if (st == SK_OK) st = upload(ctx, p, tables.data(), tables.size() * sizeof(RollTable));
+  if (st != SK_OK) return st;
+  c.d_tables = static_cast<RollTable *>(p);
+  std::vector<SketchItem> items;
+  for (const Batch &b : make_batches(c)) {
+    st = sketch_batch(c, b, items);
+    if (st != SK_OK) return st;
+    // the next batch reuses the scratch buffers
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "sketch batch");
+  }
+  return SK_OK;
+}
+
+sk_status setup_call(SketchCall &c, sk_ctx *ctx, const char *bases, const int64_t *seq_offsets,
+                     const int64_t *sample_seqs, int64_t n, const int32_t *kmers, int32_t K,
+                     int32_t s64, int32_t use_rc, int32_t min_count) {
+  c.ctx = ctx;
+  c.bases = bases;
+  c.seq_off = seq_offsets;
+  c.sample_seqs = sample_seqs;
+  c.n = n;
+  c.kmers.assign(kmers, kmers + K);
+  c.s64 = s64;
+  c.use_rc = use_rc;
+  c.min_count = min_count;
+  c.nbins = s64 * 64;
+  c.binsize = (kSignMod + static_cast<uint64_t>(c.nbins) - 1) / static_cast<uint64_t>(c.nbins);
+  c.magic = ~0ULL / c.binsize;
+  const size_t words = static_cast<size_t>(n) * K * s64 * kBbits;
+  void *p = nullptr;
+  sk_status st = scratch(ctx, kSlotSketchWords, words * 8 + static_cast<size_t>(n) * K * 9 + 16, &p);
+  if (st != SK_OK) return st;
+  c.d_words = static_cast<uint64_t *>(p);
+  c.d_inv = reinterpret_cast<double *>(c.d_words + words);
+  c.d_dens = reinterpret_cast<int8_t *>(c.d_inv + static_cast<size_t>(n) * K);
+  return SK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+sk_status sk_sketch(sk_ctx *ctx, const char *bases, const int64_t *seq_offsets,
+                    const int64_t *sample_seqs, int64_t n_samples, const int32_t *kmers,
+                    int32_t n_kmers, int32_t sketchsize64, int32_t use_rc, int32_t min_count,
+                    uint64_t *words, double *inv_minhash, uint8_t *densified) {
+  if (!ctx) return SK_EINVAL;
+  std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+  DeviceGuard dev(ctx->device);
+  sk_status st = begin_call(ctx);
+  if (st != SK_OK) return st;
+  st = check_inputs(ctx, bases, seq_offsets, sample_seqs, n_samples, kmers, n_kmers, sketchsize64,
+                    use_rc, min_count);
+  if (st != SK_OK || n_samples == 0) return st;
+  if (!words) return fail(ctx, SK_EINVAL, "null output words");
+  SketchCall c{};
+  st = setup_call(c, ctx, bases, seq_offsets, sample_seqs, n_samples, kmers, n_kmers, sketchsize64,
+                  use_rc, min_count);
+  if (st == SK_OK) st = sketch_to_device(c);
+  if (st != SK_OK) return st;
+  const size_t n_words = static_cast<size_t>(n_samples) * n_kmers * sketchsize64 * kBbits;
+  const size_t rows = static_cast<size_t>(n_samples) * n_kmers;
+  std::vector<int8_t> dens(rows);
+  cudaError_t e = cudaMemcpyAsync(words, c.d_words, n_words * 8, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess && inv_minhash)
+    e = cudaMemcpyAsync(inv_minhash, c.d_inv, rows * 8, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dens.data(), c.d_dens, rows, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "sketch download");
+  st = finish_call(ctx);
+  if (st != SK_OK) return st;
+  if (densified)
+    for (int64_t s = 0; s < n_samples; ++s) {
+      uint8_t any = 0;
+      for (int k = 0; k < n_kmers; ++k) any |= dens[s * n_kmers + k] != 0;
+      densified[s] = any;
+    }
+  return SK_OK;
+}
+
+}  // extern "C"

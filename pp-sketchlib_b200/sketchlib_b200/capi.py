@@ -87,6 +87,7 @@ _SIGNATURES = {
     "sk_server_release": (_i32, [_p, _i64]),
     "sk_server_stats": (_i32, [_p, C.POINTER(_i64), C.POINTER(C.c_double), C.POINTER(_i64)]),
     "sk_server_destroy": (_i32, [_p]),
+    "sk_sketch": (_i32, [_p, _p, _p, _p, _i64, _p, _i32, _i32, _i32, _i32, _p, _p, _p]),
 }
 
 
@@ -517,6 +518,42 @@ def query_db(ctx: Context, ref_words, kmers, sketchsize64: int, query_words=None
                            km.ctypes.data, K, sketchsize64, bbits, _h(random), out_mode,
                            out.ctypes.data), ctx)
     return out
+
+
+def pack_sequences(samples):
+    """Samples as lists of sequences (str or bytes) -> (bases uint8,
+    seq_offsets int64 [n_seqs + 1], sample_seqs int64 [n_samples + 1]), the
+    flat form sk_sketch takes."""
+    seqs = [q.encode() if isinstance(q, str) else bytes(q) for smp in samples for q in smp]
+    seq_off = np.zeros(len(seqs) + 1, np.int64)
+    np.cumsum([len(q) for q in seqs], out=seq_off[1:])
+    sample_seqs = np.zeros(len(samples) + 1, np.int64)
+    np.cumsum([len(smp) for smp in samples], out=sample_seqs[1:])
+    bases = np.frombuffer(b"".join(seqs), np.uint8) if seqs else np.zeros(0, np.uint8)
+    return bases, seq_off, sample_seqs
+
+
+def sketch(ctx: Context, bases, seq_offsets, sample_seqs, kmers, sketchsize64: int,
+           use_rc: bool = True, min_count: int = 0, words=None):
+    """MinHash sketches of sequences on the device (sk_sketch).  `bases`
+    uint8 (or bytes) holding every sequence back to back; sequence i is
+    bases[seq_offsets[i]:seq_offsets[i+1]]; sample s owns sequences
+    sample_seqs[s] .. sample_seqs[s+1]-1.  Returns (words uint64
+    [n][K][sketchsize64 * 14], inv_minhash float64 [n][K], densified bool [n])."""
+    b = np.frombuffer(bases, np.uint8) if isinstance(bases, (bytes, bytearray)) else \
+        np.ascontiguousarray(bases, np.uint8)
+    so = np.ascontiguousarray(seq_offsets, np.int64)
+    ss = np.ascontiguousarray(sample_seqs, np.int64)
+    km = np.ascontiguousarray(kmers, np.int32)
+    n = len(ss) - 1
+    if words is None:
+        words = np.empty((n, len(km), sketchsize64 * 14), np.uint64)
+    inv = np.empty((n, len(km)), np.float64)
+    dens = np.empty(n, np.uint8)
+    _check(lib.sk_sketch(ctx.handle, b.ctypes.data if b.size else None, so.ctypes.data,
+                         ss.ctypes.data, n, km.ctypes.data, len(km), sketchsize64, int(use_rc),
+                         int(min_count), words.ctypes.data, inv.ctypes.data, dens.ctypes.data), ctx)
+    return words, inv, dens.astype(bool)
 
 
 def dists_knn(ctx: Context, db: Database, kNN: int, dist_col: int = 0, jaccard: bool = False,
