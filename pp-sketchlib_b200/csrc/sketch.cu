@@ -50,6 +50,9 @@ constexpr int kFinishThreads = 512;
 constexpr int kMinK = 3;                           // generate_seeds (src/sketch/sketch.cpp:33-40)
 constexpr int kMaxK = 255;
 constexpr unsigned long long kEmptyKey = ~0ULL;
+// Invalid codes before and after a batch's bases: the roll reads up to
+// 16 * ceil(k / 16) bytes before a range and k + 31 bytes after it.
+constexpr int64_t kCodePad = 512;
 constexpr unsigned kErrDensify = 4u;               // DevStatus.error bits of the sketcher
 constexpr unsigned kErrTable = 8u;
 
@@ -83,20 +86,26 @@ struct SketchItem {
   int32_t pad;
 };
 
-// Rolling tables of one k: in[c] = {seed[c], srol^k(seed[3-c])} for the base
-// entering the window, out[c] = {srol^k(seed[c]), seed[3-c]} for the base
-// leaving it; c = 4 (not a base) contributes zero.
+// Rolling table of one k, indexed by (entering base | leaving base << 3):
+// the XOR of seed[in] and srol^k(seed[out]) for the forward hash and of
+// srol^k(seed[3-in]) and seed[3-out] for the reverse one; a code of 4 (not a
+// base) contributes zero.
 struct RollTable {
-  ulonglong2 in[8];
-  ulonglong2 out[8];
+  ulonglong2 v[64];
 };
 
 RollTable make_table(int k) {
-  RollTable t{};
+  uint64_t fin[8] = {}, rin[8] = {}, fout[8] = {}, rout[8] = {};
   for (int c = 0; c < 4; ++c) {
-    t.in[c] = make_ulonglong2(kNtSeed[c], srol_n(kNtSeed[3 - c], k));
-    t.out[c] = make_ulonglong2(srol_n(kNtSeed[c], k), kNtSeed[3 - c]);
+    fin[c] = kNtSeed[c];
+    rin[c] = srol_n(kNtSeed[3 - c], k);
+    fout[c] = srol_n(kNtSeed[c], k);
+    rout[c] = kNtSeed[3 - c];
   }
+  RollTable t{};
+  for (int ci = 0; ci < 8; ++ci)
+    for (int co = 0; co < 8; ++co)
+      t.v[ci | (co << 3)] = make_ulonglong2(fin[ci] ^ fout[co], rin[ci] ^ rout[co]);
   return t;
 }
 
@@ -147,32 +156,72 @@ __global__ void mark_starts_kernel(uint8_t *__restrict__ codes, const int64_t *_
   }
 }
 
-// Rolls over the window starts [s, e) and calls emit(hash) for every window of
-// k bases inside one sequence.  Reads codes[s .. e+k-2].
+// Sixteen roll steps over one aligned chunk of codes.  `in` holds the bases
+// entering at relative positions p0 .. p0+15; the bases leaving (k earlier)
+// are bytes d .. d+15 of the 32-byte pair (oa, ob), d = (-k) mod 16, picked
+// with a uniform word select and funnel shift.  kMask: the chunk lies within
+// the first k positions, where a leaving position before the range start
+// contributes nothing.
+template <bool kMask, typename Emit>
+__device__ __forceinline__ void roll_chunk(const uint4 &in, const uint4 &oa, const uint4 &ob, int D,
+                                           int sh, int p0, int k, int lo, int hi,
+                                           const RollTable &t, bool use_rc, uint64_t &fh,
+                                           uint64_t &rh, int &run, Emit &emit) {
+  const uint32_t X[8] = {oa.x, oa.y, oa.z, oa.w, ob.x, ob.y, ob.z, ob.w};
+  uint32_t Y[5];
+#pragma unroll
+  for (int m = 0; m < 5; ++m) Y[m] = D == 0 ? X[m] : D == 1 ? X[m + 1] : D == 2 ? X[m + 2] : X[m + 3];
+  uint32_t O[4];
+#pragma unroll
+  for (int w = 0; w < 4; ++w) O[w] = __funnelshift_r(Y[w], Y[w + 1], sh);
+  const uint32_t I[4] = {in.x, in.y, in.z, in.w};
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    const uint32_t ci = (I[i >> 2] >> (8 * (i & 3))) & 0xFF;
+    uint32_t co = (O[i >> 2] >> (8 * (i & 3))) & 0xFF;
+    const int p = p0 + i;
+    if (kMask && p < k) co = kCodeInvalid;
+    const ulonglong2 v = t.v[(ci & 7) | ((co & 7) << 3)];
+    fh = srol1(fh) ^ v.x;
+    rh = sror1(rh ^ v.y);
+    run = (ci & 7) == kCodeInvalid ? 0 : ((ci & kCodeStart) ? 1 : min(run + 1, k));
+    const int w = p - k + 1;   // start of the window ending at p
+    if (run >= k && w >= lo && w < hi) emit(use_rc && rh < fh ? rh : fh);
+  }
+}
+
+// Calls emit(hash) for every window of k bases inside one sequence whose
+// start lies in [s, e).  Rolls from s rounded down to 16 with a zero state (a
+// non-base contributes zero, so the state after k positions is the window's
+// hash whatever came before); reads the 16-byte chunks of codes from 16 * c
+// bytes before that through e + k + 31 (the code buffer's pads cover both).
 template <typename Emit>
 __device__ __forceinline__ void roll_windows(const uint8_t *__restrict__ codes, int64_t s, int64_t e,
                                              int k, const RollTable &t, bool use_rc, Emit emit) {
+  const int64_t s0 = s & ~static_cast<int64_t>(15);
+  const int lo = static_cast<int>(s - s0), hi = static_cast<int>(e - s0);
+  const int n_chunks = (hi + k - 1 + 15) >> 4;
+  const int d = (-k) & 15, D = d >> 2, sh = 8 * (d & 3);
+  const int c = (k + d) >> 4;            // the leaving bytes start in chunk j - c
+  const uint4 *base = reinterpret_cast<const uint4 *>(codes + s0);
   uint64_t fh = 0, rh = 0;
   int run = 0;
-  const int64_t last = e + k - 1;
-  // first k bases: nothing leaves the window
-  const int64_t warm = min(s + k, last);
-  for (int64_t p = s; p < warm; ++p) {
-    const uint8_t ci = codes[p];
-    const ulonglong2 a = t.in[ci & 7];
-    fh = srol1(fh) ^ a.x;
-    rh = sror1(rh ^ a.y);
-    run = (ci & 7) == kCodeInvalid ? 0 : ((ci & kCodeStart) ? 1 : min(run + 1, k));
+  uint4 oa = base[-c], ob = base[1 - c], in = base[0];
+  const int masked = min(n_chunks, c);
+  int j = 0;
+  for (; j < masked; ++j) {
+    const uint4 in_n = base[j + 1], ob_n = base[j + 2 - c];
+    roll_chunk<true>(in, oa, ob, D, sh, 16 * j, k, lo, hi, t, use_rc, fh, rh, run, emit);
+    oa = ob;
+    ob = ob_n;
+    in = in_n;
   }
-  if (run >= k) emit(use_rc && rh < fh ? rh : fh);
-#pragma unroll 4
-  for (int64_t p = s + k; p < last; ++p) {
-    const uint8_t ci = codes[p], co = codes[p - k];
-    const ulonglong2 a = t.in[ci & 7], b = t.out[co & 7];
-    fh = srol1(fh) ^ a.x ^ b.x;
-    rh = sror1(rh ^ a.y ^ b.y);
-    run = (ci & 7) == kCodeInvalid ? 0 : ((ci & kCodeStart) ? 1 : min(run + 1, k));
-    if (run >= k) emit(use_rc && rh < fh ? rh : fh);
+  for (; j < n_chunks; ++j) {
+    const uint4 in_n = base[j + 1], ob_n = base[j + 2 - c];
+    roll_chunk<false>(in, oa, ob, D, sh, 16 * j, k, lo, hi, t, use_rc, fh, rh, run, emit);
+    oa = ob;
+    ob = ob_n;
+    in = in_n;
   }
 }
 
@@ -205,7 +254,7 @@ sketch_kernel(SketchArgs a) {
   unsigned long long *bins = kShared ? sh_bins : row;
   if (kShared)
     for (int i = threadIdx.x; i < a.nbins; i += kSketchThreads) sh_bins[i] = kEmptyKey;
-  if (threadIdx.x < 16) {
+  if (threadIdx.x < 64) {
     const ulonglong2 *src = reinterpret_cast<const ulonglong2 *>(a.tables + it.tab);
     reinterpret_cast<ulonglong2 *>(&tab)[threadIdx.x] = src[threadIdx.x];
   }
@@ -241,7 +290,7 @@ __global__ void __launch_bounds__(kSketchThreads)
 count_kernel(SketchArgs a) {
   __shared__ RollTable tab;
   const SketchItem it = a.items[blockIdx.x];
-  if (threadIdx.x < 16) {
+  if (threadIdx.x < 64) {
     const ulonglong2 *src = reinterpret_cast<const ulonglong2 *>(a.tables + it.tab);
     reinterpret_cast<ulonglong2 *>(&tab)[threadIdx.x] = src[threadIdx.x];
   }
@@ -581,18 +630,18 @@ sk_status sketch_batch(SketchCall &c, const Batch &b, std::vector<SketchItem> &i
   const int64_t rows = nb * K;
   const int64_t bytes = b.b1 - b.b0;
   const int64_t n_seqs = b.q1 - b.q0;
-  const int64_t pad = kMaxK + 64;
   void *p = nullptr;
-  sk_status st = scratch(ctx, kSlotSketchCodes, static_cast<size_t>(bytes + pad), &p);
+  sk_status st = scratch(ctx, kSlotSketchCodes, static_cast<size_t>(bytes + 2 * kCodePad), &p);
   if (st != SK_OK) return st;
-  c.d_codes = static_cast<uint8_t *>(p);
+  c.d_codes = static_cast<uint8_t *>(p) + kCodePad;
   st = scratch(ctx, kSlotSketchSeqs, static_cast<size_t>(n_seqs + 1) * 8, &p);
   if (st != SK_OK) return st;
   c.d_seq_off = static_cast<int64_t *>(p);
   st = scratch(ctx, kSlotSketchBins, static_cast<size_t>(rows) * c.nbins * 8, &p);
   if (st != SK_OK) return st;
   c.d_signs = static_cast<unsigned long long *>(p);
-  cudaError_t e = cudaMemsetAsync(c.d_codes + bytes, kCodeInvalid, pad, ctx->stream);
+  cudaError_t e = cudaMemsetAsync(c.d_codes - kCodePad, kCodeInvalid, kCodePad, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c.d_codes + bytes, kCodeInvalid, kCodePad, ctx->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(c.d_signs, 0xFF, static_cast<size_t>(rows) * c.nbins * 8, ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "sketch buffers");
   st = upload(ctx, c.d_codes, c.bases + b.b0, static_cast<size_t>(bytes));
