@@ -447,6 +447,18 @@ sk_status sk_sketch(sk_ctx *ctx, const char *bases, const int64_t *seq_offsets,
                     int32_t n_kmers, int32_t sketchsize64, int32_t use_rc, int32_t min_count,
                     uint64_t *words, double *inv_minhash, uint8_t *densified);
 
+/* sk_sketch with the bases already in device memory (d_bases, not modified)
+ * and device outputs: d_words [n_samples][n_kmers][sketchsize64 * 14],
+ * d_inv_minhash [n_samples][n_kmers] or NULL, d_densified [n_samples] or NULL.
+ * seq_offsets and sample_seqs stay host arrays (the work is planned on the
+ * host).  For sequences produced on the GPU, and to sketch straight into
+ * memory that sk_db_create_device packs. */
+sk_status sk_sketch_device(sk_ctx *ctx, const char *d_bases, const int64_t *seq_offsets,
+                           const int64_t *sample_seqs, int64_t n_samples, const int32_t *kmers,
+                           int32_t n_kmers, int32_t sketchsize64, int32_t use_rc,
+                           int32_t min_count, uint64_t *d_words, double *d_inv_minhash,
+                           uint8_t *d_densified);
+
 /* ---- measurement ---------------------------------------------------------- */
 
 /* Measured integer-ALU peaks of the context's device, in operations per

@@ -127,33 +127,51 @@ __device__ __forceinline__ uint8_t base_code(uint8_t c) {
   return l == 'a' ? 0 : l == 'c' ? 1 : l == 'g' ? 2 : (l == 't' || l == 'u') ? 3 : kCodeInvalid;
 }
 
-__global__ void codes_kernel(uint8_t *__restrict__ buf, int64_t n) {
+// Base codes of n bytes, src -> dst (the same buffer when converting in place).
+__global__ void codes_kernel(const uint8_t *src, uint8_t *dst, int64_t n) {
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-  const int64_t nv = n / 16;
-  uint4 *v = reinterpret_cast<uint4 *>(buf);
-  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < nv; i += stride) {
-    uint4 x = v[i];
-    uint32_t w[4] = {x.x, x.y, x.z, x.w};
+  const int64_t first = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  int64_t done = 0;
+  if (((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0) {
+    const int64_t nv = n / 16;
+    const uint4 *vs = reinterpret_cast<const uint4 *>(src);
+    uint4 *vd = reinterpret_cast<uint4 *>(dst);
+    for (int64_t i = first; i < nv; i += stride) {
+      const uint4 x = vs[i];
+      uint32_t w[4] = {x.x, x.y, x.z, x.w};
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      uint32_t o = 0;
+      for (int j = 0; j < 4; ++j) {
+        uint32_t o = 0;
 #pragma unroll
-      for (int b = 0; b < 4; ++b) o |= static_cast<uint32_t>(base_code((w[j] >> (8 * b)) & 0xFF)) << (8 * b);
-      w[j] = o;
+        for (int b = 0; b < 4; ++b) o |= static_cast<uint32_t>(base_code((w[j] >> (8 * b)) & 0xFF)) << (8 * b);
+        w[j] = o;
+      }
+      vd[i] = make_uint4(w[0], w[1], w[2], w[3]);
     }
-    v[i] = make_uint4(w[0], w[1], w[2], w[3]);
+    done = nv * 16;
   }
-  for (int64_t i = nv * 16 + blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n; i += stride)
-    buf[i] = base_code(buf[i]);
+  for (int64_t i = done + first; i < n; i += stride) dst[i] = base_code(src[i]);
 }
 
+// Flags the first base of sequences 0 .. n_seqs-1; seq_off[i] - base is the
+// sequence's offset in the code buffer.
 __global__ void mark_starts_kernel(uint8_t *__restrict__ codes, const int64_t *__restrict__ seq_off,
-                                   int64_t n_seqs) {
+                                   int64_t n_seqs, int64_t base) {
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n_seqs; i += stride) {
-    const int64_t a = seq_off[i] - seq_off[0], b = seq_off[i + 1] - seq_off[0];
+    const int64_t a = seq_off[i] - base, b = seq_off[i + 1] - base;
     if (b > a) codes[a] |= kCodeStart;
   }
+}
+
+// Per-sample densify flags from the per-(sample, k) densify results.
+__global__ void densified_kernel(const int8_t *__restrict__ rows, int64_t n, int K,
+                                 uint8_t *__restrict__ out) {
+  const int64_t s = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  if (s >= n) return;
+  uint8_t any = 0;
+  for (int k = 0; k < K; ++k) any |= rows[s * K + k] != 0;
+  out[s] = any;
 }
 
 // Sixteen roll steps over one aligned chunk of codes.  `in` holds the bases
@@ -441,7 +459,8 @@ namespace {
 
 struct SketchCall {
   sk_ctx *ctx;
-  const char *bases;
+  const char *bases;               // host or (device_in) device
+  bool device_in = false;
   const int64_t *seq_off;
   const int64_t *sample_seqs;
   int64_t n;
@@ -449,10 +468,9 @@ struct SketchCall {
   int s64, use_rc, min_count;
   int nbins;
   uint64_t binsize, magic;
-  // device buffers (context scratch)
+  // device buffers (context scratch unless the caller gave them)
   uint8_t *d_codes = nullptr;
   int64_t *d_seq_off = nullptr;
-  SketchItem *d_items = nullptr;
   RollTable *d_tables = nullptr;
   unsigned long long *d_signs = nullptr;
   uint64_t *d_words = nullptr;
@@ -487,34 +505,58 @@ sk_status check_inputs(sk_ctx *ctx, const char *bases, const int64_t *seq_off,
   return SK_OK;
 }
 
+// Samples [s0, s1): their sequences [q0, q1) and bytes [b0, b1) of the caller's buffer.
+Batch span(const SketchCall &c, int64_t s0, int64_t s1) {
+  Batch b{};
+  b.s0 = s0;
+  b.s1 = s1;
+  b.q0 = c.sample_seqs[s0];
+  b.q1 = c.sample_seqs[s1];
+  b.b0 = c.seq_off[b.q0];
+  b.b1 = c.seq_off[b.q1];
+  return b;
+}
+
 std::vector<Batch> make_batches(const SketchCall &c) {
   std::vector<Batch> out;
   const int64_t row_bytes = static_cast<int64_t>(c.kmers.size()) * c.nbins * 8;
   int64_t s = 0;
   while (s < c.n) {
-    Batch b{};
-    b.s0 = s;
-    b.q0 = c.sample_seqs[s];
-    b.b0 = c.seq_off[b.q0];
+    const int64_t b0 = c.seq_off[c.sample_seqs[s]];
     int64_t e = s + 1;
-    while (e < c.n && c.seq_off[c.sample_seqs[e + 1]] - b.b0 <= kBatchBytes &&
+    while (e < c.n && c.seq_off[c.sample_seqs[e + 1]] - b0 <= kBatchBytes &&
            (e + 1 - s) * row_bytes <= kBatchBins)
       ++e;
-    b.s1 = e;
-    b.q1 = c.sample_seqs[e];
-    b.b1 = c.seq_off[b.q1];
-    out.push_back(b);
+    out.push_back(span(c, s, e));
     s = e;
   }
   return out;
 }
 
-// Work items of samples [s0, s1) of a batch whose bytes start at b0: window
-// starts of each sample in pieces of kItemWindows, every k of a piece
-// adjacent (they read the same bases).
+// Upload pieces of a batch: whole samples, about bytes / kUploadChunks each
+// and at least kMinUploadBytes.
+constexpr int kUploadChunks = 8;
+constexpr int64_t kMinUploadBytes = 8LL << 20;
+
+std::vector<Batch> upload_chunks(const SketchCall &c, const Batch &b) {
+  std::vector<Batch> out;
+  const int64_t target = std::max<int64_t>(kMinUploadBytes, (b.b1 - b.b0 + kUploadChunks - 1) / kUploadChunks);
+  int64_t s = b.s0;
+  while (s < b.s1) {
+    int64_t e = s + 1;
+    while (e < b.s1 && c.seq_off[c.sample_seqs[e]] - c.seq_off[c.sample_seqs[s]] < target) ++e;
+    out.push_back(span(c, s, e));
+    s = e;
+  }
+  return out;
+}
+
+// Work items of samples [s0, s1) of batch b (code offsets relative to b.b0):
+// window starts of each sample in pieces of kItemWindows, every k of a piece
+// adjacent (they read the same bases).  Windows end inside their sample, so a
+// sample's items read no other sample's codes that they depend on.
 void make_items(const SketchCall &c, const Batch &b, int64_t s0, int64_t s1, int k_only,
                 std::vector<SketchItem> &items) {
-  items.clear();
   const int K = static_cast<int>(c.kmers.size());
   for (int64_t s = s0; s < s1; ++s) {
     const int64_t a = c.seq_off[c.sample_seqs[s]] - b.b0, e = c.seq_off[c.sample_seqs[s + 1]] - b.b0;
@@ -523,7 +565,8 @@ void make_items(const SketchCall &c, const Batch &b, int64_t s0, int64_t s1, int
         if (k_only >= 0 && k != k_only) continue;
         SketchItem it{};
         it.begin = p;
-        it.end = std::min(p + kItemWindows, e);
+        it.end = std::min(p + kItemWindows, e - c.kmers[k] + 1);
+        if (it.end <= it.begin) continue;
         it.row = static_cast<int32_t>((s - b.s0) * K + k);
         it.k = c.kmers[k];
         it.tab = k;
@@ -538,17 +581,10 @@ sk_status upload(sk_ctx *ctx, void *dst, const void *src, size_t bytes) {
   return e == cudaSuccess ? SK_OK : cuda_fail(ctx, e, "sketch upload");
 }
 
-// Bins rows of one batch without a count filter.
-sk_status hash_batch(SketchCall &c, const Batch &b, SketchArgs &args, std::vector<SketchItem> &items) {
-  sk_ctx *ctx = c.ctx;
-  make_items(c, b, b.s0, b.s1, -1, items);
-  if (items.empty()) return SK_OK;
-  void *p = nullptr;
-  sk_status st = scratch(ctx, kSlotSketchItems, items.size() * sizeof(SketchItem), &p);
-  if (st != SK_OK) return st;
-  args.items = static_cast<SketchItem *>(p);
-  st = upload(ctx, p, items.data(), items.size() * sizeof(SketchItem));
-  if (st != SK_OK) return st;
+sk_status launch_hash(sk_ctx *ctx, const SketchCall &c, SketchArgs args, const SketchItem *d_items,
+                      size_t n_items) {
+  if (n_items == 0) return SK_OK;
+  args.items = d_items;
   const bool shared = bins_fit_shared(ctx->device, c.nbins);
   const size_t smem = shared ? static_cast<size_t>(c.nbins) * 8 : 0;
   cudaError_t e = cudaSuccess;
@@ -556,12 +592,31 @@ sk_status hash_batch(SketchCall &c, const Batch &b, SketchArgs &args, std::vecto
     e = cudaFuncSetAttribute(sketch_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(smem));
     if (e == cudaSuccess)
-      sketch_kernel<true><<<static_cast<unsigned>(items.size()), kSketchThreads, smem, ctx->stream>>>(args);
+      sketch_kernel<true><<<static_cast<unsigned>(n_items), kSketchThreads, smem, ctx->stream>>>(args);
   } else {
-    sketch_kernel<false><<<static_cast<unsigned>(items.size()), kSketchThreads, 0, ctx->stream>>>(args);
+    sketch_kernel<false><<<static_cast<unsigned>(n_items), kSketchThreads, 0, ctx->stream>>>(args);
   }
   if (e == cudaSuccess) e = cudaGetLastError();
   return e == cudaSuccess ? SK_OK : cuda_fail(ctx, e, "sketch kernel");
+}
+
+// Codes of bytes [a, b) of the caller's buffer (offsets relative to the
+// batch) and start flags of sequences [q0, q1), on the context's stream.
+sk_status make_codes(SketchCall &c, const Batch &batch, const Batch &part) {
+  sk_ctx *ctx = c.ctx;
+  const int64_t bytes = part.b1 - part.b0;
+  uint8_t *dst = c.d_codes + (part.b0 - batch.b0);
+  const uint8_t *src = c.device_in ? reinterpret_cast<const uint8_t *>(c.bases) + part.b0 : dst;
+  const unsigned g = static_cast<unsigned>(
+      std::max<int64_t>(1, std::min<int64_t>(ctx->sm_count * 8, (bytes / 16 + 255) / 256)));
+  if (bytes > 0) codes_kernel<<<g, 256, 0, ctx->stream>>>(src, dst, bytes);
+  const int64_t n_seqs = part.q1 - part.q0;
+  if (n_seqs > 0)
+    mark_starts_kernel<<<static_cast<unsigned>(std::min<int64_t>(ctx->sm_count * 8, (n_seqs + 255) / 256)),
+                         256, 0, ctx->stream>>>(c.d_codes, c.d_seq_off + (part.q0 - batch.q0), n_seqs,
+                                                batch.b0);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? SK_OK : cuda_fail(ctx, e, "sketch codes");
 }
 
 uint64_t next_pow2(uint64_t v) {
@@ -593,7 +648,9 @@ sk_status count_batch(SketchCall &c, const Batch &b, SketchArgs &args, std::vect
     args.max_key_count = reinterpret_cast<unsigned int *>(static_cast<char *>(tc) + slots * 4);
     args.table_mask = slots - 1;
     for (int k = 0; k < K; ++k) {
+      items.clear();
       make_items(c, b, s, s + 1, k, items);
+      if (items.empty()) continue;
       void *p = nullptr;
       st = scratch(ctx, kSlotSketchItems, items.size() * sizeof(SketchItem), &p);
       if (st == SK_OK) st = upload(ctx, p, items.data(), items.size() * sizeof(SketchItem));
@@ -621,13 +678,65 @@ sk_status count_batch(SketchCall &c, const Batch &b, SketchArgs &args, std::vect
   return SK_OK;
 }
 
+// Bins rows of one batch without a count filter.  Host bases go up in sample
+// chunks on the copy stream; each chunk's codes and items run on the
+// context's stream as soon as it has landed, while later chunks copy.
+sk_status hash_batch(SketchCall &c, const Batch &b, SketchArgs &args, std::vector<SketchItem> &items) {
+  sk_ctx *ctx = c.ctx;
+  const std::vector<Batch> parts = c.device_in ? std::vector<Batch>{b} : upload_chunks(c, b);
+  std::vector<size_t> first(parts.size() + 1, 0);
+  items.clear();
+  for (size_t i = 0; i < parts.size(); ++i) {
+    make_items(c, b, parts[i].s0, parts[i].s1, -1, items);
+    first[i + 1] = items.size();
+  }
+  void *p = nullptr;
+  sk_status st = SK_OK;
+  if (!items.empty()) {
+    st = scratch(ctx, kSlotSketchItems, items.size() * sizeof(SketchItem), &p);
+    if (st == SK_OK) st = upload(ctx, p, items.data(), items.size() * sizeof(SketchItem));
+    if (st != SK_OK) return st;
+  }
+  const SketchItem *d_items = static_cast<const SketchItem *>(p);
+  if (c.device_in) {
+    st = make_codes(c, b, b);
+    return st == SK_OK ? launch_hash(ctx, c, args, d_items, items.size()) : st;
+  }
+  st = ensure_copy_stream(ctx);
+  if (st != SK_OK) return st;
+  cudaError_t e = cudaSuccess;
+  while (e == cudaSuccess && ctx->ev_chunk.size() < parts.size()) {
+    cudaEvent_t ev = nullptr;
+    e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) ctx->ev_chunk.push_back(ev);
+  }
+  // the copies start after the buffers' set-up on the context's stream
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_chunk[0], ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_chunk[0], 0);
+  for (size_t i = 0; i < parts.size() && e == cudaSuccess; ++i) {
+    const int64_t bytes = parts[i].b1 - parts[i].b0;
+    if (bytes > 0)
+      e = cudaMemcpyAsync(c.d_codes + (parts[i].b0 - b.b0), c.bases + parts[i].b0, static_cast<size_t>(bytes),
+                          cudaMemcpyHostToDevice, ctx->copy_stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_chunk[i], ctx->copy_stream);
+  }
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "sketch upload");
+  for (size_t i = 0; i < parts.size(); ++i) {
+    e = cudaStreamWaitEvent(ctx->stream, ctx->ev_chunk[i], 0);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "sketch upload");
+    st = make_codes(c, b, parts[i]);
+    if (st == SK_OK) st = launch_hash(ctx, c, args, d_items + first[i], first[i + 1] - first[i]);
+    if (st != SK_OK) return st;
+  }
+  return SK_OK;
+}
+
 // Sketches the samples of one batch into d_words / d_inv / d_dens (rows of the
 // batch's samples) on the context's stream.
 sk_status sketch_batch(SketchCall &c, const Batch &b, std::vector<SketchItem> &items) {
   sk_ctx *ctx = c.ctx;
   const int K = static_cast<int>(c.kmers.size());
-  const int64_t nb = b.s1 - b.s0;
-  const int64_t rows = nb * K;
+  const int64_t rows = (b.s1 - b.s0) * K;
   const int64_t bytes = b.b1 - b.b0;
   const int64_t n_seqs = b.q1 - b.q0;
   void *p = nullptr;
@@ -644,15 +753,8 @@ sk_status sketch_batch(SketchCall &c, const Batch &b, std::vector<SketchItem> &i
   if (e == cudaSuccess) e = cudaMemsetAsync(c.d_codes + bytes, kCodeInvalid, kCodePad, ctx->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(c.d_signs, 0xFF, static_cast<size_t>(rows) * c.nbins * 8, ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "sketch buffers");
-  st = upload(ctx, c.d_codes, c.bases + b.b0, static_cast<size_t>(bytes));
-  if (st == SK_OK) st = upload(ctx, c.d_seq_off, c.seq_off + b.q0, static_cast<size_t>(n_seqs + 1) * 8);
+  st = upload(ctx, c.d_seq_off, c.seq_off + b.q0, static_cast<size_t>(n_seqs + 1) * 8);
   if (st != SK_OK) return st;
-  const unsigned g = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(ctx->sm_count * 8, (bytes / 16 + 255) / 256)));
-  codes_kernel<<<g, 256, 0, ctx->stream>>>(c.d_codes, bytes);
-  mark_starts_kernel<<<static_cast<unsigned>(std::min<int64_t>(ctx->sm_count * 8, (n_seqs + 255) / 256)), 256, 0,
-                       ctx->stream>>>(c.d_codes, c.d_seq_off, n_seqs);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "sketch codes");
   SketchArgs args{};
   args.codes = c.d_codes;
   args.tables = c.d_tables;
@@ -662,7 +764,13 @@ sk_status sketch_batch(SketchCall &c, const Batch &b, std::vector<SketchItem> &i
   args.binsize = c.binsize;
   args.magic = c.magic;
   args.status = ctx->status_dev;
-  st = c.min_count > 0 ? count_batch(c, b, args, items) : hash_batch(c, b, args, items);
+  if (c.min_count > 0) {
+    if (!c.device_in) st = upload(ctx, c.d_codes, c.bases + b.b0, static_cast<size_t>(bytes));
+    if (st == SK_OK) st = make_codes(c, b, b);
+    if (st == SK_OK) st = count_batch(c, b, args, items);
+  } else {
+    st = hash_batch(c, b, args, items);
+  }
   if (st != SK_OK) return st;
   finish_kernel<<<static_cast<unsigned>(rows), kFinishThreads, 0, ctx->stream>>>(
       c.d_signs, c.nbins, c.s64, c.d_words + b.s0 * K * static_cast<int64_t>(c.s64) * kBbits,
@@ -672,7 +780,7 @@ sk_status sketch_batch(SketchCall &c, const Batch &b, std::vector<SketchItem> &i
 }
 
 // Everything up to device-resident words / inverse minhashes / densify flags
-// of all samples (d_words, d_inv, d_dens sized by the caller).
+// of all samples.
 sk_status sketch_to_device(SketchCall &c) {
   sk_ctx *ctx = c.ctx;
   const int K = static_cast<int>(c.kmers.size());
@@ -684,21 +792,27 @@ sk_status sketch_to_device(SketchCall &c) {
   if (st != SK_OK) return st;
   c.d_tables = static_cast<RollTable *>(p);
   std::vector<SketchItem> items;
-  for (const Batch &b : make_batches(c)) {
-    st = sketch_batch(c, b, items);
+  const std::vector<Batch> batches = make_batches(c);
+  for (size_t i = 0; i < batches.size(); ++i) {
+    st = sketch_batch(c, batches[i], items);
     if (st != SK_OK) return st;
-    // the next batch reuses the scratch buffers
-    cudaError_t e = cudaStreamSynchronize(ctx->stream);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "sketch batch");
+    if (i + 1 < batches.size()) {   // the next batch reuses the scratch buffers
+      cudaError_t e = cudaStreamSynchronize(ctx->stream);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "sketch batch");
+    }
   }
   return SK_OK;
 }
 
-sk_status setup_call(SketchCall &c, sk_ctx *ctx, const char *bases, const int64_t *seq_offsets,
-                     const int64_t *sample_seqs, int64_t n, const int32_t *kmers, int32_t K,
-                     int32_t s64, int32_t use_rc, int32_t min_count) {
+// Call set-up; d_words / d_inv given by the caller are written directly,
+// else they are context scratch.
+sk_status setup_call(SketchCall &c, sk_ctx *ctx, const char *bases, bool device_in,
+                     const int64_t *seq_offsets, const int64_t *sample_seqs, int64_t n,
+                     const int32_t *kmers, int32_t K, int32_t s64, int32_t use_rc, int32_t min_count,
+                     uint64_t *d_words, double *d_inv) {
   c.ctx = ctx;
   c.bases = bases;
+  c.device_in = device_in;
   c.seq_off = seq_offsets;
   c.sample_seqs = sample_seqs;
   c.n = n;
@@ -710,12 +824,17 @@ sk_status setup_call(SketchCall &c, sk_ctx *ctx, const char *bases, const int64_
   c.binsize = (kSignMod + static_cast<uint64_t>(c.nbins) - 1) / static_cast<uint64_t>(c.nbins);
   c.magic = ~0ULL / c.binsize;
   const size_t words = static_cast<size_t>(n) * K * s64 * kBbits;
+  const size_t rows = static_cast<size_t>(n) * K;
+  const size_t bytes = (d_words ? 0 : words * 8) + (d_inv ? 0 : rows * 8) + rows + 16;
   void *p = nullptr;
-  sk_status st = scratch(ctx, kSlotSketchWords, words * 8 + static_cast<size_t>(n) * K * 9 + 16, &p);
+  sk_status st = scratch(ctx, kSlotSketchWords, bytes, &p);
   if (st != SK_OK) return st;
-  c.d_words = static_cast<uint64_t *>(p);
-  c.d_inv = reinterpret_cast<double *>(c.d_words + words);
-  c.d_dens = reinterpret_cast<int8_t *>(c.d_inv + static_cast<size_t>(n) * K);
+  char *q = static_cast<char *>(p);
+  c.d_words = d_words ? d_words : reinterpret_cast<uint64_t *>(q);
+  if (!d_words) q += words * 8;
+  c.d_inv = d_inv ? d_inv : reinterpret_cast<double *>(q);
+  if (!d_inv) q += rows * 8;
+  c.d_dens = reinterpret_cast<int8_t *>(q);
   return SK_OK;
 }
 
@@ -737,8 +856,8 @@ sk_status sk_sketch(sk_ctx *ctx, const char *bases, const int64_t *seq_offsets,
   if (st != SK_OK || n_samples == 0) return st;
   if (!words) return fail(ctx, SK_EINVAL, "null output words");
   SketchCall c{};
-  st = setup_call(c, ctx, bases, seq_offsets, sample_seqs, n_samples, kmers, n_kmers, sketchsize64,
-                  use_rc, min_count);
+  st = setup_call(c, ctx, bases, false, seq_offsets, sample_seqs, n_samples, kmers, n_kmers,
+                  sketchsize64, use_rc, min_count, nullptr, nullptr);
   if (st == SK_OK) st = sketch_to_device(c);
   if (st != SK_OK) return st;
   const size_t n_words = static_cast<size_t>(n_samples) * n_kmers * sketchsize64 * kBbits;
@@ -758,6 +877,33 @@ sk_status sk_sketch(sk_ctx *ctx, const char *bases, const int64_t *seq_offsets,
       densified[s] = any;
     }
   return SK_OK;
+}
+
+sk_status sk_sketch_device(sk_ctx *ctx, const char *d_bases, const int64_t *seq_offsets,
+                           const int64_t *sample_seqs, int64_t n_samples, const int32_t *kmers,
+                           int32_t n_kmers, int32_t sketchsize64, int32_t use_rc, int32_t min_count,
+                           uint64_t *d_words, double *d_inv_minhash, uint8_t *d_densified) {
+  if (!ctx) return SK_EINVAL;
+  std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+  DeviceGuard dev(ctx->device);
+  sk_status st = begin_call(ctx);
+  if (st != SK_OK) return st;
+  st = check_inputs(ctx, d_bases, seq_offsets, sample_seqs, n_samples, kmers, n_kmers, sketchsize64,
+                    use_rc, min_count);
+  if (st != SK_OK || n_samples == 0) return st;
+  if (!d_words) return fail(ctx, SK_EINVAL, "null output words");
+  SketchCall c{};
+  st = setup_call(c, ctx, d_bases, true, seq_offsets, sample_seqs, n_samples, kmers, n_kmers,
+                  sketchsize64, use_rc, min_count, d_words, d_inv_minhash);
+  if (st == SK_OK) st = sketch_to_device(c);
+  if (st != SK_OK) return st;
+  if (d_densified) {
+    densified_kernel<<<static_cast<unsigned>((n_samples + 255) / 256), 256, 0, ctx->stream>>>(
+        c.d_dens, n_samples, n_kmers, d_densified);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "densify flags");
+  }
+  return finish_call(ctx);
 }
 
 }  // extern "C"

@@ -88,6 +88,7 @@ _SIGNATURES = {
     "sk_server_stats": (_i32, [_p, C.POINTER(_i64), C.POINTER(C.c_double), C.POINTER(_i64)]),
     "sk_server_destroy": (_i32, [_p]),
     "sk_sketch": (_i32, [_p, _p, _p, _p, _i64, _p, _i32, _i32, _i32, _i32, _p, _p, _p]),
+    "sk_sketch_device": (_i32, [_p, _p, _p, _p, _i64, _p, _i32, _i32, _i32, _i32, _p, _p, _p]),
 }
 
 
@@ -554,6 +555,22 @@ def sketch(ctx: Context, bases, seq_offsets, sample_seqs, kmers, sketchsize64: i
                          ss.ctypes.data, n, km.ctypes.data, len(km), sketchsize64, int(use_rc),
                          int(min_count), words.ctypes.data, inv.ctypes.data, dens.ctypes.data), ctx)
     return words, inv, dens.astype(bool)
+
+
+def sketch_device(ctx: Context, d_bases: int, seq_offsets, sample_seqs, kmers, sketchsize64: int,
+                  d_words: int, use_rc: bool = True, min_count: int = 0, d_inv_minhash: int = 0,
+                  d_densified: int = 0) -> None:
+    """sk_sketch_device: device bases in (address d_bases), device outputs
+    (addresses d_words [n][K][sketchsize64 * 14] uint64, d_inv_minhash [n][K]
+    float64 and d_densified [n] uint8, 0 to skip); e.g. torch tensors'
+    data_ptr().  Offsets are host arrays as for sketch()."""
+    so = np.ascontiguousarray(seq_offsets, np.int64)
+    ss = np.ascontiguousarray(sample_seqs, np.int64)
+    km = np.ascontiguousarray(kmers, np.int32)
+    _check(lib.sk_sketch_device(ctx.handle, d_bases or None, so.ctypes.data, ss.ctypes.data,
+                                len(ss) - 1, km.ctypes.data, len(km), sketchsize64, int(use_rc),
+                                int(min_count), d_words, d_inv_minhash or None,
+                                d_densified or None), ctx)
 
 
 def dists_knn(ctx: Context, db: Database, kNN: int, dist_col: int = 0, jaccard: bool = False,

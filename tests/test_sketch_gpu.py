@@ -163,3 +163,29 @@ def test_64_genomes_match_reference_sketcher(gpu_ctx):
     ss = np.arange(65, dtype=np.int64)
     words, inv, dens = capi.sketch(gpu_ctx, genomes.reshape(-1), off, ss, kmers, 156)
     np.testing.assert_array_equal(words, want)
+
+
+@pytest.mark.parametrize("min_count,shift", [(0, 0), (0, 3), (2, 5)])
+def test_device_entry_point_matches_host_one(gpu_ctx, min_count, shift):
+    """sk_sketch_device (device bases, possibly unaligned; device outputs)
+    gives sk_sketch's results and leaves the bases unchanged."""
+    import torch
+    from sketchlib_b200 import capi
+    rng = np.random.default_rng(40 + shift)
+    samples = random_samples(rng, 9, 200_000)
+    bases, off, ss = capi.pack_sequences(samples)
+    kmers, s64 = [15, 21, 31], 64
+    want = capi.sketch(gpu_ctx, bases, off, ss, kmers, s64, min_count=min_count)
+    buf = torch.zeros(bases.size + 16, dtype=torch.uint8, device="cuda")
+    buf[shift:shift + bases.size] = torch.from_numpy(bases.copy()).cuda()
+    n = len(ss) - 1
+    words = torch.empty((n, len(kmers), s64 * 14), dtype=torch.int64, device="cuda")
+    inv = torch.empty((n, len(kmers)), dtype=torch.float64, device="cuda")
+    dens = torch.empty(n, dtype=torch.uint8, device="cuda")
+    capi.sketch_device(gpu_ctx, buf.data_ptr() + shift, off, ss, kmers, s64, words.data_ptr(),
+                       min_count=min_count, d_inv_minhash=inv.data_ptr(),
+                       d_densified=dens.data_ptr())
+    np.testing.assert_array_equal(words.cpu().numpy().view(np.uint64), want[0])
+    np.testing.assert_array_equal(inv.cpu().numpy(), want[1])
+    np.testing.assert_array_equal(dens.cpu().numpy().astype(bool), want[2])
+    np.testing.assert_array_equal(buf[shift:shift + bases.size].cpu().numpy(), bases)
