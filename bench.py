@@ -282,6 +282,98 @@ def profiled_traffic():
         return None
 
 
+# ------------------------------------------------------------- sketching
+
+SKETCH_GENOMES, SKETCH_LEN, SKETCH_SEED = 64, 2_500_000, 0x5EED0001
+SKETCH_PROFILE = ROOT / "profiles" / "sketch_kernel_64_genomes.md"
+
+
+def profiled_alu_pct():
+    """ALU-pipe utilisation of the sketch kernel from the committed ncu
+    summary (line `alu_pipe_pct: N`), or None."""
+    try:
+        m = re.search(r"alu_pipe_pct:\s*([0-9.]+)", SKETCH_PROFILE.read_text())
+        return float(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
+def run_sketch(ctx, dev, steps, warmup, cpu=True):
+    """Sketching of 64 genomes of 2.5 Mb at k = 15..29 odd, sketchsize64 156
+    (the CPU parity case's shape): device-resident bases through
+    sk_sketch_device (`value`), pinned host bases through sk_sketch (`e2e`),
+    and the reference's own CPU sketcher on this host's cores."""
+    import torch
+    from sketchlib_b200 import capi, synth
+    g = synth.genomes(SKETCH_GENOMES, SKETCH_LEN, seed=SKETCH_SEED)
+    n, L = g.shape
+    off = np.arange(n + 1, dtype=np.int64) * L
+    ss = np.arange(n + 1, dtype=np.int64)
+    kmers_step = sum(n * (L - k + 1) for k in KMERS)
+    W = S64 * BBITS
+    d_bases = torch.from_numpy(g.reshape(-1)).to(dev)
+    d_words = torch.empty((n, len(KMERS), W), dtype=torch.int64, device=dev)
+
+    def dev_step():
+        capi.sketch_device(ctx, d_bases.data_ptr(), off, ss, KMERS, S64, d_words.data_ptr())
+
+    for _ in range(warmup):
+        dev_step()
+    torch.cuda.synchronize(dev)
+    call_ms = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        dev_step()      # returns after its stream has finished
+        call_ms.append(1e3 * (time.perf_counter() - t0))
+    sec = statistics.median(call_ms) / 1e3
+    words_dev = d_words.cpu().numpy().view(np.uint64)
+
+    pinned = torch.empty(n * L, dtype=torch.uint8).pin_memory()
+    pinned.numpy()[:] = g.reshape(-1)
+    host_words = torch.empty((n, len(KMERS), W), dtype=torch.int64).pin_memory().numpy().view(np.uint64)
+    for _ in range(warmup):
+        capi.sketch(ctx, pinned.numpy(), off, ss, KMERS, S64, words=host_words)
+    e2e_ms = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        capi.sketch(ctx, pinned.numpy(), off, ss, KMERS, S64, words=host_words)
+        e2e_ms.append(1e3 * (time.perf_counter() - t0))
+    e2e_sec = statistics.median(e2e_ms) / 1e3
+    out = {
+        "workload": f"{n} genomes x {L:,} bases (i.i.d. bases at GC 0.38 on a random tree of "
+                    "SNPs and 5 kb replacements), k = 15..29 odd, sketchsize64 156",
+        "unit": "k-mers/s", "kmers_per_step": kmers_step,
+        "value": kmers_step / sec, "ms_per_step": 1e3 * sec, "steps": steps,
+        "timing": "host clock around each sk_sketch_device call (its planning, kernels and "
+                  "the final synchronisation), median of the steps; bases resident in HBM",
+        "e2e": {"value": kmers_step / e2e_sec, "unit": "k-mers/s", "ms_per_step": 1e3 * e2e_sec,
+                "h2d_bytes_per_step": int(n * L),
+                "d2h_bytes_per_step": int(host_words.nbytes + n * len(KMERS) * 9),
+                "call": "sk_sketch from pinned host bases to pinned host sketches (upload in "
+                        "sample chunks overlapped with hashing)",
+                "matches_device_result": bool(np.array_equal(host_words, words_dev))},
+        "roofline": {"bound": "alu", "alu_pipe_pct_ncu": profiled_alu_pct(),
+                     "source": str(SKETCH_PROFILE.relative_to(ROOT))},
+    }
+    if cpu:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        if oracle.sketcher_available():
+            kind = "reference"
+            want = oracle.RefSketcher().sketch(g, KMERS, S64, threads=threads)
+        else:
+            kind = "port"
+            want = oracle.sketch(g.reshape(-1), off, ss, KMERS, S64, True, threads=threads)[0]
+        ct = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": kmers_step / ct, "unit": "k-mers/s", "cores": threads,
+                               "kind": kind, "sample": f"the whole workload ({n} genomes, "
+                                                       f"{ct:.2f} s)"}
+        out["matches_cpu_sketcher"] = bool(np.array_equal(want, words_dev))
+    return out
+
+
 # ------------------------------------------------------- batched (config 4)
 
 BATCH_SEED = 0x5EED0004
@@ -602,6 +694,9 @@ def run_ours(args, rank, world, local):
         extra["serving"] = run_serving(ctx, dev)
     if world == 1 and not args.skip_large:
         extra["large"] = run_large(ctx, dev, lop3_peak)
+    if not args.skip_sketch:
+        extra["sketch"] = run_sketch(ctx, dev, max(3, min(args.steps, 10)), max(1, args.warmup),
+                                     cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -674,6 +769,23 @@ def run_profile_case(n: int, launches: int):
     ctx.close()
 
 
+def run_profile_sketch(n: int, launches: int):
+    """A small sketching case for ncu: n genomes of 2.5 Mb from device memory,
+    `launches` sk_sketch_device calls, nothing else."""
+    import torch
+    from sketchlib_b200 import capi, synth
+    ctx = capi.Context(0)
+    g = synth.genomes(n, SKETCH_LEN, seed=SKETCH_SEED)
+    off = np.arange(n + 1, dtype=np.int64) * SKETCH_LEN
+    ss = np.arange(n + 1, dtype=np.int64)
+    d_bases = torch.from_numpy(g.reshape(-1)).cuda()
+    d_words = torch.empty((n, len(KMERS), S64 * BBITS), dtype=torch.int64, device="cuda")
+    for _ in range(launches):
+        capi.sketch_device(ctx, d_bases.data_ptr(), off, ss, KMERS, S64, d_words.data_ptr())
+    print(json.dumps({"profile_sketch": n, "launches": launches}))
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -686,6 +798,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-batched", action="store_true")
     ap.add_argument("--skip-serving", action="store_true")
+    ap.add_argument("--skip-sketch", action="store_true",
+                    help="skip the sketching section (64 genomes x 2.5 Mb)")
     ap.add_argument("--batch-autotune", action="store_true",
                     help="let the batch time every tile shape at creation (outside the timed region)")
     ap.add_argument("--skip-large", action="store_true",
@@ -695,7 +809,12 @@ def main():
     ap.add_argument("--profile", type=int, default=0,
                     help="run only N-sample dense launches (a small case for ncu)")
     ap.add_argument("--profile-launches", type=int, default=2)
+    ap.add_argument("--profile-sketch", type=int, default=0,
+                    help="run only N genomes through sk_sketch_device (for ncu)")
     args = ap.parse_args()
+    if args.profile_sketch:
+        run_profile_sketch(args.profile_sketch, args.profile_launches)
+        return
     if args.profile:
         run_profile_case(args.profile, args.profile_launches)
         return

@@ -9,6 +9,9 @@ inherited from the parent, or resampled uniformly with probability
 sk_synth_device), which turns (seed, sample, k, bin) into bits identically on
 the CPU and the GPU.
 
+Sequences for the sketcher (`genomes`): a seeded population of whole genomes
+on a random recursive tree, base by base.
+
 Shapes used by the benchmarks and tests:
   random_tree          a random recursive tree (parents uniform over earlier samples)
   clade_tree           n_clades clades with log-normal sizes under one root
@@ -91,3 +94,28 @@ def query_population(ref_parent: np.ndarray, ref_thresh: np.ndarray, n_queries: 
     parent = np.asarray(parent, dtype=np.int32)
     th = np.concatenate([ref_thresh, thresholds(np.asarray(extra_c), np.asarray(extra_a), kmers)])
     return parent, th, np.asarray(q_idx, dtype=np.int64)
+
+
+def genomes(n: int, length: int, seed: int = 0x5EED0001, gc: float = 0.38,
+            snp_max: float = 0.004, acc_max: float = 0.03, segment: int = 5000) -> np.ndarray:
+    """n genomes of `length` bases (uint8 ASCII, shape (n, length)): the root
+    draws i.i.d. bases at the given GC content; genome g > 0 copies a uniformly
+    chosen earlier genome, changes a fraction U(0, snp_max) of positions to
+    another base (core SNPs) and replaces a fraction U(0, acc_max) of the
+    sequence with fresh random segments of `segment` bases (accessory)."""
+    rng = np.random.default_rng(seed)
+    p = [(1 - gc) / 2, gc / 2, gc / 2, (1 - gc) / 2]
+    letters = np.frombuffer(b"ACGT", np.uint8)
+    code = np.zeros(256, np.uint8)
+    code[letters] = np.arange(4, dtype=np.uint8)
+    out = np.empty((n, length), np.uint8)
+    out[0] = letters[rng.choice(4, length, p=p)]
+    for g in range(1, n):
+        out[g] = out[int(rng.integers(0, g))]
+        snps = int(rng.uniform(0, snp_max) * length)
+        pos = rng.integers(0, length, snps)
+        out[g, pos] = letters[(code[out[g, pos]] + rng.integers(1, 4, snps)) % 4]
+        for _ in range(int(rng.uniform(0, acc_max) * length / segment)):
+            start = int(rng.integers(0, length - segment))
+            out[g, start:start + segment] = letters[rng.choice(4, segment, p=p)]
+    return out
