@@ -679,6 +679,25 @@ def run_ours(args, rank, world, local):
             step()
         return reduce_max(time.perf_counter() - t0, world, dev)
 
+    def link_gbs():
+        """Plain pinned copies of this step's input (H2D) and output (D2H), GB/s."""
+        dev_in = torch.empty_like(host_words, device=dev)
+        dev_out = torch.empty_like(host_out, device=dev)
+        rates = []
+        for src, dst in ((host_words, dev_in), (dev_out, host_out)):
+            dst.copy_(src, non_blocking=True)
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(3):
+                dst.copy_(src, non_blocking=True)
+            e1.record()
+            e1.synchronize()
+            rates.append(3 * src.numel() * src.element_size() / (e0.elapsed_time(e1) / 1e3) / 1e9)
+        del dev_in, dev_out
+        return rates
+
+    h2d_gbs, d2h_gbs = link_gbs()
     e2e_steps = max(1, min(args.steps, args.e2e_steps))
     e2e_s = time_e2e(e2e_step, e2e_steps)
     e2e_value = pairs * world * e2e_steps / e2e_s
@@ -733,6 +752,10 @@ def run_ours(args, rank, world, local):
                 "h2d_bytes_per_step": int(host_words.numel() * 8),
                 "d2h_bytes_per_step": int(host_out.numel() * 4),
                 "steps": e2e_steps, "matches_resident_result": ok,
+                "link_gbs": {"h2d": h2d_gbs, "d2h": d2h_gbs,
+                             "note": "plain pinned copies of the step's input and output on "
+                                     "this box; the upload alone takes "
+                                     f"{host_words.numel() * 8 / h2d_gbs / 1e6:.1f} ms"},
                 "call": "sk_query_db (upload in sample chunks on a copy stream, each chunk's "
                         "tiles computed while the next copies)",
                 "unpipelined": {"value": pairs * world * e2e_steps / seq_s,

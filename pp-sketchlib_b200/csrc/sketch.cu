@@ -179,12 +179,13 @@ __global__ void densified_kernel(const int8_t *__restrict__ rows, int64_t n, int
 // are bytes d .. d+15 of the 32-byte pair (oa, ob), d = (-k) mod 16, picked
 // with a uniform word select and funnel shift.  kMask: the chunk lies within
 // the first k positions, where a leaving position before the range start
-// contributes nothing.
-template <bool kMask, typename Emit>
+// contributes nothing.  kRange: some windows ending in the chunk start outside
+// [lo, hi).  kRc: canonical hashes (the reverse strand is rolled too).
+template <bool kMask, bool kRange, bool kRc, typename Emit>
 __device__ __forceinline__ void roll_chunk(const uint4 &in, const uint4 &oa, const uint4 &ob, int D,
                                            int sh, int p0, int k, int lo, int hi,
-                                           const RollTable &t, bool use_rc, uint64_t &fh,
-                                           uint64_t &rh, int &run, Emit &emit) {
+                                           const RollTable &t, uint64_t &fh, uint64_t &rh, int &run,
+                                           Emit &emit) {
   const uint32_t X[8] = {oa.x, oa.y, oa.z, oa.w, ob.x, ob.y, ob.z, ob.w};
   uint32_t Y[5];
 #pragma unroll
@@ -201,10 +202,31 @@ __device__ __forceinline__ void roll_chunk(const uint4 &in, const uint4 &oa, con
     if (kMask && p < k) co = kCodeInvalid;
     const ulonglong2 v = t.v[(ci & 7) | ((co & 7) << 3)];
     fh = srol1(fh) ^ v.x;
-    rh = sror1(rh ^ v.y);
+    if (kRc) rh = sror1(rh ^ v.y);
     run = (ci & 7) == kCodeInvalid ? 0 : ((ci & kCodeStart) ? 1 : min(run + 1, k));
     const int w = p - k + 1;   // start of the window ending at p
-    if (run >= k && w >= lo && w < hi) emit(use_rc && rh < fh ? rh : fh);
+    if (run >= k && (!kRange || (w >= lo && w < hi))) emit(kRc && rh < fh ? rh : fh);
+  }
+}
+
+struct RollState {
+  uint64_t fh, rh;
+  int run;
+  uint4 oa, ob, in;
+};
+
+// Chunks j0 .. j1-1 of a range, each chunk's loads issued one chunk ahead.
+template <bool kMask, bool kRange, bool kRc, typename Emit>
+__device__ __forceinline__ void roll_span(const uint4 *base, int j0, int j1, int c, int D, int sh,
+                                          int k, int lo, int hi, const RollTable &t, RollState &st,
+                                          Emit &emit) {
+  for (int j = j0; j < j1; ++j) {
+    const uint4 in_n = base[j + 1], ob_n = base[j + 2 - c];
+    roll_chunk<kMask, kRange, kRc>(st.in, st.oa, st.ob, D, sh, 16 * j, k, lo, hi, t, st.fh, st.rh,
+                                   st.run, emit);
+    st.oa = st.ob;
+    st.ob = ob_n;
+    st.in = in_n;
   }
 }
 
@@ -213,34 +235,25 @@ __device__ __forceinline__ void roll_chunk(const uint4 &in, const uint4 &oa, con
 // non-base contributes zero, so the state after k positions is the window's
 // hash whatever came before); reads the 16-byte chunks of codes from 16 * c
 // bytes before that through e + k + 31 (the code buffer's pads cover both).
-template <typename Emit>
+// Chunks whose windows all start inside [s, e) skip the range test.
+template <bool kRc, typename Emit>
 __device__ __forceinline__ void roll_windows(const uint8_t *__restrict__ codes, int64_t s, int64_t e,
-                                             int k, const RollTable &t, bool use_rc, Emit emit) {
+                                             int k, const RollTable &t, Emit emit) {
   const int64_t s0 = s & ~static_cast<int64_t>(15);
   const int lo = static_cast<int>(s - s0), hi = static_cast<int>(e - s0);
   const int n_chunks = (hi + k - 1 + 15) >> 4;
   const int d = (-k) & 15, D = d >> 2, sh = 8 * (d & 3);
   const int c = (k + d) >> 4;            // the leaving bytes start in chunk j - c
   const uint4 *base = reinterpret_cast<const uint4 *>(codes + s0);
-  uint64_t fh = 0, rh = 0;
-  int run = 0;
-  uint4 oa = base[-c], ob = base[1 - c], in = base[0];
+  RollState st{0, 0, 0, base[-c], base[1 - c], base[0]};
   const int masked = min(n_chunks, c);
-  int j = 0;
-  for (; j < masked; ++j) {
-    const uint4 in_n = base[j + 1], ob_n = base[j + 2 - c];
-    roll_chunk<true>(in, oa, ob, D, sh, 16 * j, k, lo, hi, t, use_rc, fh, rh, run, emit);
-    oa = ob;
-    ob = ob_n;
-    in = in_n;
-  }
-  for (; j < n_chunks; ++j) {
-    const uint4 in_n = base[j + 1], ob_n = base[j + 2 - c];
-    roll_chunk<false>(in, oa, ob, D, sh, 16 * j, k, lo, hi, t, use_rc, fh, rh, run, emit);
-    oa = ob;
-    ob = ob_n;
-    in = in_n;
-  }
+  // chunk j ends windows starting at 16j - k + 1 .. 16j + 16 - k
+  const int inner0 = max(masked, (lo + k - 1 + 15) >> 4);
+  const int inner1 = max(inner0, min(n_chunks, (hi + k - 1) >> 4));
+  roll_span<true, true, kRc>(base, 0, masked, c, D, sh, k, lo, hi, t, st, emit);
+  roll_span<false, true, kRc>(base, masked, inner0, c, D, sh, k, lo, hi, t, st, emit);
+  roll_span<false, false, kRc>(base, inner0, inner1, c, D, sh, k, lo, hi, t, st, emit);
+  roll_span<false, true, kRc>(base, inner1, n_chunks, c, D, sh, k, lo, hi, t, st, emit);
 }
 
 struct SketchArgs {
@@ -262,7 +275,7 @@ struct SketchArgs {
 
 // Bin minima of one item; kShared keeps them in shared memory (nbins * 8
 // bytes of dynamic shared memory), else the CTA updates the global row.
-template <bool kShared>
+template <bool kShared, bool kRc>
 __global__ void __launch_bounds__(kSketchThreads, 1)
 sketch_kernel(SketchArgs a) {
   extern __shared__ unsigned long long sh_bins[];
@@ -281,7 +294,7 @@ sketch_kernel(SketchArgs a) {
   const int64_t e = min(s + kPerThread, it.end);
   if (s < e) {
     const uint64_t binsize = a.binsize, magic = a.magic;
-    roll_windows(a.codes, s, e, it.k, tab, a.use_rc != 0, [&](uint64_t h) {
+    roll_windows<kRc>(a.codes, s, e, it.k, tab, [&](uint64_t h) {
       const uint64_t sign = mod_sign(h);
       const uint32_t q = bin_of(sign, binsize, magic);
       if (sign < bins[q]) atomicMin(bins + q, static_cast<unsigned long long>(sign));
@@ -304,6 +317,7 @@ __device__ __forceinline__ uint64_t table_slot(uint64_t h, uint64_t mask) {
 }
 
 // Counting pass: every hash whose bin lies in [bin_lo, bin_hi) is counted.
+template <bool kRc>
 __global__ void __launch_bounds__(kSketchThreads)
 count_kernel(SketchArgs a) {
   __shared__ RollTable tab;
@@ -316,7 +330,7 @@ count_kernel(SketchArgs a) {
   const int64_t s = it.begin + static_cast<int64_t>(threadIdx.x) * kPerThread;
   const int64_t e = min(s + kPerThread, it.end);
   if (s >= e) return;
-  roll_windows(a.codes, s, e, it.k, tab, a.use_rc != 0, [&](uint64_t h) {
+  roll_windows<kRc>(a.codes, s, e, it.k, tab, [&](uint64_t h) {
     const uint32_t q = bin_of(mod_sign(h), a.binsize, a.magic);
     if (q < a.bin_lo || q >= a.bin_hi) return;
     if (h == kEmptyKey) {
@@ -588,13 +602,14 @@ sk_status launch_hash(sk_ctx *ctx, const SketchCall &c, SketchArgs args, const S
   const bool shared = bins_fit_shared(ctx->device, c.nbins);
   const size_t smem = shared ? static_cast<size_t>(c.nbins) * 8 : 0;
   cudaError_t e = cudaSuccess;
+  const unsigned grid = static_cast<unsigned>(n_items);
   if (shared) {
-    e = cudaFuncSetAttribute(sketch_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(smem));
-    if (e == cudaSuccess)
-      sketch_kernel<true><<<static_cast<unsigned>(n_items), kSketchThreads, smem, ctx->stream>>>(args);
+    auto kern = c.use_rc ? sketch_kernel<true, true> : sketch_kernel<true, false>;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e == cudaSuccess) kern<<<grid, kSketchThreads, smem, ctx->stream>>>(args);
   } else {
-    sketch_kernel<false><<<static_cast<unsigned>(n_items), kSketchThreads, 0, ctx->stream>>>(args);
+    auto kern = c.use_rc ? sketch_kernel<false, true> : sketch_kernel<false, false>;
+    kern<<<grid, kSketchThreads, 0, ctx->stream>>>(args);
   }
   if (e == cudaSuccess) e = cudaGetLastError();
   return e == cudaSuccess ? SK_OK : cuda_fail(ctx, e, "sketch kernel");
@@ -662,7 +677,8 @@ sk_status count_batch(SketchCall &c, const Batch &b, SketchArgs &args, std::vect
         cudaError_t e = cudaMemsetAsync(tk, 0xFF, slots * 8, ctx->stream);
         if (e == cudaSuccess) e = cudaMemsetAsync(tc, 0, slots * 4 + 16, ctx->stream);
         if (e == cudaSuccess) {
-          count_kernel<<<static_cast<unsigned>(items.size()), kSketchThreads, 0, ctx->stream>>>(args);
+          auto kern = c.use_rc ? count_kernel<true> : count_kernel<false>;
+          kern<<<static_cast<unsigned>(items.size()), kSketchThreads, 0, ctx->stream>>>(args);
           e = cudaGetLastError();
         }
         if (e == cudaSuccess) {
