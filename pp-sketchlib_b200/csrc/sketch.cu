@@ -115,11 +115,19 @@ __device__ __forceinline__ uint64_t mod_sign(uint64_t h) {
 }
 
 // sign / binsize exactly: magic = floor((2^64-1) / binsize) under-estimates
-// the quotient by at most one for sign < 2^61.
+// the quotient by at most one for sign < 2^61.  magic < 2^20 (binsize >
+// 2^45 for at most 65,472 bins), so the high half of sign * magic is
+// (hi(sign) * magic + umulhi(lo(sign), magic)) >> 32, two multiplies; the
+// quotient is below 2^16, so q * binsize needs two more.
 __device__ __forceinline__ uint32_t bin_of(uint64_t sign, uint64_t binsize, uint64_t magic) {
-  uint64_t q = __umul64hi(sign, magic);
-  if (sign - q * binsize >= binsize) ++q;
-  return static_cast<uint32_t>(q);
+  const uint32_t m = static_cast<uint32_t>(magic);
+  const uint32_t s_lo = static_cast<uint32_t>(sign), s_hi = static_cast<uint32_t>(sign >> 32);
+  const uint64_t t = static_cast<uint64_t>(s_hi) * m + __umulhi(s_lo, m);
+  uint32_t q = static_cast<uint32_t>(t >> 32);
+  const uint64_t qb = static_cast<uint64_t>(q) * static_cast<uint32_t>(binsize) +
+                      (static_cast<uint64_t>(q * static_cast<uint32_t>(binsize >> 32)) << 32);
+  if (sign - qb >= binsize) ++q;
+  return q;
 }
 
 __device__ __forceinline__ uint8_t base_code(uint8_t c) {
@@ -194,13 +202,16 @@ __device__ __forceinline__ void roll_chunk(const uint4 &in, const uint4 &oa, con
 #pragma unroll
   for (int w = 0; w < 4; ++w) O[w] = __funnelshift_r(Y[w], Y[w + 1], sh);
   const uint32_t I[4] = {in.x, in.y, in.z, in.w};
+  uint32_t IX[4];   // table indices of the 16 steps, four per word
+#pragma unroll
+  for (int w = 0; w < 4; ++w) IX[w] = (I[w] & 0x07070707u) | ((O[w] & 0x07070707u) << 3);
 #pragma unroll
   for (int i = 0; i < 16; ++i) {
     const uint32_t ci = (I[i >> 2] >> (8 * (i & 3))) & 0xFF;
-    uint32_t co = (O[i >> 2] >> (8 * (i & 3))) & 0xFF;
+    uint32_t idx = (IX[i >> 2] >> (8 * (i & 3))) & 0x3F;
     const int p = p0 + i;
-    if (kMask && p < k) co = kCodeInvalid;
-    const ulonglong2 v = t.v[(ci & 7) | ((co & 7) << 3)];
+    if (kMask && p < k) idx = (idx & 7) | (kCodeInvalid << 3);
+    const ulonglong2 v = t.v[idx];
     fh = srol1(fh) ^ v.x;
     if (kRc) rh = sror1(rh ^ v.y);
     run = (ci & 7) == kCodeInvalid ? 0 : ((ci & kCodeStart) ? 1 : min(run + 1, k));
@@ -839,6 +850,7 @@ sk_status setup_call(SketchCall &c, sk_ctx *ctx, const char *bases, bool device_
   c.nbins = s64 * 64;
   c.binsize = (kSignMod + static_cast<uint64_t>(c.nbins) - 1) / static_cast<uint64_t>(c.nbins);
   c.magic = ~0ULL / c.binsize;
+  if (c.magic >> 32) return fail(ctx, SK_ERANGE, "bin divisor out of range");   // nbins <= 65,472 keeps it < 2^20
   const size_t words = static_cast<size_t>(n) * K * s64 * kBbits;
   const size_t rows = static_cast<size_t>(n) * K;
   const size_t bytes = (d_words ? 0 : words * 8) + (d_inv ? 0 : rows * 8) + rows + 16;
