@@ -73,6 +73,25 @@ __host__ __device__ __forceinline__ uint64_t sror1(uint64_t v) {
   return (((lo >> 1) | (lo << 32)) & kLo33) | ((hi >> 1) & ~kLo33) | ((hi << 30) & (1ULL << 63));
 }
 
+// The same rotations on the two 32-bit halves of the hash: low word L holds
+// bits 0..31, high word H bit 0 is bit 32 (the top of the 33-bit part) and
+// bits 1..31 the 31-bit part.
+__device__ __forceinline__ uint64_t srol1_w(uint64_t v) {
+  const uint32_t L = static_cast<uint32_t>(v), H = static_cast<uint32_t>(v >> 32);
+  const uint32_t lo = __funnelshift_l(H << 31, L, 1);     // L << 1 | bit 32
+  const uint32_t f = __funnelshift_l(L, H, 1);            // H << 1 | bit 31
+  const uint32_t hi = (f & ~2u) | ((H >> 30) & 2u);        // bit 33 <- bit 63
+  return (static_cast<uint64_t>(hi) << 32) | lo;
+}
+
+__device__ __forceinline__ uint64_t sror1_w(uint64_t v) {
+  const uint32_t L = static_cast<uint32_t>(v), H = static_cast<uint32_t>(v >> 32);
+  const uint32_t lo = __funnelshift_r(L, H, 1);           // L >> 1 | bit 32 << 31
+  const uint32_t t = __funnelshift_r(H, H, 1);
+  const uint32_t hi = (t & 0x7FFFFFFEu) | (L & 1u) | ((H & 2u) << 30);   // bit 32 <- bit 0, bit 63 <- bit 33
+  return (static_cast<uint64_t>(hi) << 32) | lo;
+}
+
 uint64_t srol_n(uint64_t v, unsigned n) {
   for (unsigned i = 0; i < n % (33ULL * 31ULL); ++i) v = srol1(v);
   return v;
@@ -212,8 +231,8 @@ __device__ __forceinline__ void roll_chunk(const uint4 &in, const uint4 &oa, con
     const int p = p0 + i;
     if (kMask && p < k) idx = (idx & 7) | (kCodeInvalid << 3);
     const ulonglong2 v = t.v[idx];
-    fh = srol1(fh) ^ v.x;
-    if (kRc) rh = sror1(rh ^ v.y);
+    fh = srol1_w(fh) ^ v.x;
+    if (kRc) rh = sror1_w(rh ^ v.y);
     run = (ci & 7) == kCodeInvalid ? 0 : ((ci & kCodeStart) ? 1 : min(run + 1, k));
     const int w = p - k + 1;   // start of the window ending at p
     if (run >= k && (!kRange || (w >= lo && w < hi))) emit(kRc && rh < fh ? rh : fh);
