@@ -102,7 +102,7 @@ struct SketchItem {
   int32_t row;            // sample * K + k index (bins row)
   int32_t k;
   int32_t tab;            // k index (table row)
-  int32_t pad;
+  int32_t per;            // window starts per thread (a multiple of 16, at most kPerThread)
 };
 
 // Rolling table of one k, indexed by (entering base | leaving base << 3):
@@ -320,8 +320,8 @@ sketch_kernel(SketchArgs a) {
     reinterpret_cast<ulonglong2 *>(&tab)[threadIdx.x] = src[threadIdx.x];
   }
   __syncthreads();
-  const int64_t s = it.begin + static_cast<int64_t>(threadIdx.x) * kPerThread;
-  const int64_t e = min(s + kPerThread, it.end);
+  const int64_t s = it.begin + static_cast<int64_t>(threadIdx.x) * it.per;
+  const int64_t e = min(s + it.per, it.end);
   if (s < e) {
     const uint64_t binsize = a.binsize, magic = a.magic;
     roll_windows<kRc>(a.codes, s, e, it.k, tab, [&](uint64_t h) {
@@ -357,8 +357,8 @@ count_kernel(SketchArgs a) {
     reinterpret_cast<ulonglong2 *>(&tab)[threadIdx.x] = src[threadIdx.x];
   }
   __syncthreads();
-  const int64_t s = it.begin + static_cast<int64_t>(threadIdx.x) * kPerThread;
-  const int64_t e = min(s + kPerThread, it.end);
+  const int64_t s = it.begin + static_cast<int64_t>(threadIdx.x) * it.per;
+  const int64_t e = min(s + it.per, it.end);
   if (s >= e) return;
   roll_windows<kRc>(a.codes, s, e, it.k, tab, [&](uint64_t h) {
     const uint32_t q = bin_of(mod_sign(h), a.binsize, a.magic);
@@ -596,20 +596,27 @@ std::vector<Batch> upload_chunks(const SketchCall &c, const Batch &b) {
 }
 
 // Work items of samples [s0, s1) of batch b (code offsets relative to b.b0):
-// window starts of each sample in pieces of kItemWindows, every k of a piece
-// adjacent (they read the same bases).  Windows end inside their sample, so a
-// sample's items read no other sample's codes that they depend on.
+// window starts of each sample in equal pieces of at most kItemWindows (so
+// the threads of every item get the same share), every k of a piece adjacent
+// (they read the same bases).  Windows end inside their sample, so a sample's
+// items read no other sample's codes that they depend on.
 void make_items(const SketchCall &c, const Batch &b, int64_t s0, int64_t s1, int k_only,
                 std::vector<SketchItem> &items) {
   const int K = static_cast<int>(c.kmers.size());
   for (int64_t s = s0; s < s1; ++s) {
     const int64_t a = c.seq_off[c.sample_seqs[s]] - b.b0, e = c.seq_off[c.sample_seqs[s + 1]] - b.b0;
-    for (int64_t p = a; p < e; p += kItemWindows)
+    const int64_t pieces = std::max<int64_t>(1, (e - a + kItemWindows - 1) / kItemWindows);
+    const int64_t piece = (e - a + pieces - 1) / pieces;
+    const int32_t per = static_cast<int32_t>(
+        std::max<int64_t>(16, ((piece + kSketchThreads - 1) / kSketchThreads + 15) / 16 * 16));
+    const int64_t step = static_cast<int64_t>(per) * kSketchThreads;
+    for (int64_t p = a; p < e; p += step)
       for (int k = 0; k < K; ++k) {
         if (k_only >= 0 && k != k_only) continue;
         SketchItem it{};
         it.begin = p;
-        it.end = std::min(p + kItemWindows, e - c.kmers[k] + 1);
+        it.per = per;
+        it.end = std::min(p + step, e - c.kmers[k] + 1);
         if (it.end <= it.begin) continue;
         it.row = static_cast<int32_t>((s - b.s0) * K + k);
         it.k = c.kmers[k];
