@@ -300,6 +300,9 @@ class RefSketcher:
         lib_.ref_sketch_file.restype = C.c_int
         lib_.ref_sketch_file.argtypes = [C.c_char_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
                                          C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        lib_.ref_seqbuf.restype = C.c_int
+        lib_.ref_seqbuf.argtypes = [C.c_char_p, C.c_int, C.c_void_p, C.c_int64, C.c_void_p,
+                                    C.c_int64, C.c_void_p, C.c_void_p]
         lib_.ref_sketch_seqs.restype = None
         lib_.ref_sketch_seqs.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
                                          C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
@@ -348,6 +351,23 @@ class RefSketcher:
                                          int(use_rc), int(min_count), int(exact),
                                          words.ctypes.data, inv.ctypes.data, dens.ctypes.data)
         return words, inv, bool(dens[0]), bool(reads)
+
+
+    def seqbuf(self, path, kmer_len, cap=1 << 26, cap_seqs=1 << 20):
+        """What the reference's SeqBuf(files, kmer_len) keeps of one file:
+        dict(seqs, total, missing_bases, reads, max_length, base_freq)."""
+        bases = np.zeros(cap, np.uint8)
+        off = np.zeros(cap_seqs + 1, np.int64)
+        info = np.zeros(5, np.int64)
+        freq = np.zeros(4, np.float64)
+        rc = self.lib.ref_seqbuf(str(path).encode(), int(kmer_len), bases.ctypes.data, cap,
+                                 off.ctypes.data, cap_seqs, info.ctypes.data, freq.ctypes.data)
+        if rc != 0:
+            raise ValueError("ref_seqbuf capacity too small")
+        n = int(info[0])
+        seqs = [bytes(bases[off[i]:off[i + 1]]).decode() for i in range(n)]
+        return {"seqs": seqs, "total": int(info[1]), "missing_bases": int(info[2]),
+                "reads": bool(info[3]), "max_length": int(info[4]), "base_freq": freq.tolist()}
 
 
 def sketcher_available() -> bool:

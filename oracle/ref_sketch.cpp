@@ -150,4 +150,35 @@ int ref_sketch_file(const char *path, const int32_t *kmers, int K, int sketchsiz
   return buf.is_reads() ? 1 : 0;
 }
 
+// What the reference's SeqBuf(files, kmer_len) keeps of one file
+// (src/sketch/seqio.cpp:55-100): the kept sequences back to back in `bases`
+// (capacity cap bytes) with their offsets in `off` (capacity cap_seqs + 1),
+// and info = {n_seqs, total bases, N count, reads, max_length}, freq = base
+// composition A, C, G, T.  Returns 0, or -1 when a capacity is too small.
+int ref_seqbuf(const char *path, int kmer_len, char *bases, int64_t cap, int64_t *off,
+               int64_t cap_seqs, int64_t *info, double *freq) {
+  SeqBuf buf(std::vector<std::string>{std::string(path)}, static_cast<size_t>(kmer_len));
+  int64_t n = 0, used = 0;
+  off[0] = 0;
+  while (buf.nseqs() > 0 && !buf.eof()) {
+    const std::string &q = *buf.getseq();
+    if (n >= cap_seqs || used + static_cast<int64_t>(q.size()) > cap) return -1;
+    std::memcpy(bases + used, q.data(), q.size());
+    used += static_cast<int64_t>(q.size());
+    off[++n] = used;
+    buf.move_next_seq();
+  }
+  const BaseComp<double> c = buf.get_composition();
+  info[0] = n;
+  info[1] = static_cast<int64_t>(c.total);
+  info[2] = static_cast<int64_t>(buf.missing_bases());
+  info[3] = buf.is_reads() ? 1 : 0;
+  info[4] = static_cast<int64_t>(buf.max_length());
+  freq[0] = c.a;
+  freq[1] = c.c;
+  freq[2] = c.g;
+  freq[3] = c.t;
+  return 0;
+}
+
 }  // extern "C"

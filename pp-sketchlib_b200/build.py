@@ -76,7 +76,7 @@ def build_module(force: bool = False) -> Path | None:
           "-I", pybind11.get_include(), "-I", sysconfig.get_paths()["include"],
           "-I", INCLUDE, "-I", CSRC, src, *host_srcs, "-o", out,
           "-L", LIB.parent, "-lsketchlib_b200", "-Wl,-rpath,$ORIGIN/../sketchlib_b200",
-          "-lpthread"])
+          "-lpthread", "-lz"])
     return out
 
 

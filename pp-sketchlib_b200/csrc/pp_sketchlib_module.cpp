@@ -14,8 +14,12 @@
 //     refuses both, sketchlib_bindings.cpp:98-101, 144-147);
 //   * fewer than two k-mer lengths with core/accessory output raises instead
 //     of exiting the process (linear_regression.cpp:51-58);
-//   * sketch creation (constructDatabase, addRandom) is outside this path and
-//     raises NotImplementedError.
+//   * constructDatabase sketches on the GPU (sk_sketch) and writes the
+//     database with the built-in HDF5 writer (host_h5_write.cpp); it computes
+//     no Monte Carlo random-match table (calc_random only prints a note), and
+//     a read filter (min_count) counts k-mers exactly; codon-phased seeds
+//     raise, as in the reference's GPU sketcher.  addRandom raises
+//     NotImplementedError.
 #include <pybind11/numpy.h>
 #include <pybind11/pybind11.h>
 #include <pybind11/stl.h>
@@ -31,8 +35,16 @@
 #include <tuple>
 #include <vector>
 
+#include <algorithm>
+#include <array>
+#include <cstdio>
+#include <iostream>
+#include <sys/stat.h>
+
 #include "host_db.h"
 #include "host_h5.h"
+#include "host_h5_write.h"
+#include "host_seqio.h"
 #include "sketchlib_b200.h"
 
 namespace py = pybind11;
@@ -384,10 +396,204 @@ sparse_coo sparsifyDists(const FloatArray &, const float, const int, const size_
       "Downgrade to v2.0.0, or update the calling package");
 }
 
+// What constructDatabase stores per sample besides the sketch words.
+struct SampleInfo {
+  std::string name;
+  uint64_t length = 0, missing = 0;
+  bool reads = false, densified = false;
+  std::array<double, 4> bases{};
+};
+
+// Writes sketches [n][K][s64 * 14] in the reference's database layout
+// (src/database/database.cpp:40-96, 235-258): /sketches with codon_phased and
+// reverse_complement, one group per sample with its attributes and one
+// uint64 dataset per k.  The sketch_version string is left out (the
+// reference reads it only when present).
+void save_sketch_db(const std::string &path, const std::vector<SampleInfo> &info,
+                    const std::vector<uint64_t> &words, const std::vector<int32_t> &kmers, int s64,
+                    bool use_rc, bool codon_phased) {
+  const size_t K = kmers.size(), W = static_cast<size_t>(s64) * 14;
+  h5w::Group root, sk;
+  sk.name = "sketches";
+  sk.attrs = {h5w::Attr::u8("codon_phased", codon_phased ? 1 : 0),
+              h5w::Attr::u8("reverse_complement", use_rc ? 1 : 0)};
+  for (size_t i = 0; i < info.size(); ++i) {
+    h5w::Group g;
+    g.name = info[i].name;
+    g.attrs = {h5w::Attr::u64("sketchsize64", static_cast<uint64_t>(s64)),
+               h5w::Attr::u64("bbits", 14),
+               h5w::Attr::u64("length", info[i].length),
+               h5w::Attr::u64("missing_bases", info[i].missing),
+               h5w::Attr::u8("reads", info[i].reads ? 1 : 0),
+               h5w::Attr::f64_vec("base_freq", std::vector<double>(info[i].bases.begin(), info[i].bases.end())),
+               h5w::Attr::i32_vec("kmers", kmers)};
+    for (size_t k = 0; k < K; ++k) {
+      h5w::Dataset d;
+      d.name = std::to_string(kmers[k]);
+      d.data = words.data() + (i * K + k) * W;
+      d.count = W;
+      d.attrs = {h5w::Attr::i32("kmer-size", kmers[k])};
+      g.datasets.push_back(std::move(d));
+    }
+    sk.groups.push_back(std::move(g));
+  }
+  root.groups.push_back(std::move(sk));
+  h5w::write_file(path, root);
+}
+
+bool file_exists(const std::string &path) {
+  struct stat st {};
+  return stat(path.c_str(), &st) == 0;
+}
+
+// constructDatabase (src/sketchlib_bindings.cpp:47-87, src/api.cpp:39-135):
+// reads each sample's files as the reference's SeqBuf does, sketches every
+// sample on the GPU (sk_sketch) and writes the database.  An existing
+// database that already holds every sample at these k-mer lengths is kept,
+// as the reference keeps it.  Read sets (FASTQ input) with min_count > 0 are
+// filtered by exact k-mer counts (the reference's `exact = true`).
+void constructDatabase(const std::string &db_name, const std::vector<std::string> &names,
+                       const std::vector<std::vector<std::string>> &files,
+                       std::vector<size_t> kmer_lengths, const size_t sketch_size,
+                       const bool codon_phased, const bool calc_random, const bool use_rc,
+                       size_t min_count, const bool exact, const size_t num_threads,
+                       const bool /*use_gpu*/, const int device_id) {
+  if (codon_phased) throw std::runtime_error("Codon phased seeds not yet implemented for GPU sketching");
+  if (names.size() != files.size()) throw std::runtime_error("Sample names and file lists differ in length");
+  if (kmer_lengths.empty()) throw std::runtime_error("No k-mer lengths given");
+  const std::string path = db_name + ".h5";
+  std::vector<int32_t> kmers = to_kmers(kmer_lengths);
+  std::sort(kmers.begin(), kmers.end());
+  if (file_exists(path)) {
+    try {
+      skhost::load_sketches(db_name, names, kmers);
+      return;   // every sample is already sketched
+    } catch (const std::exception &) {
+    }
+  }
+  const size_t min_len = kmer_lengths.back();   // SeqBuf(files, kmer_lengths.back())
+  const size_t n = names.size();
+  std::vector<skhost::SampleSeqs> seqs(n);
+  {
+    py::gil_scoped_release release;
+    std::atomic<size_t> next{0};
+    std::vector<std::string> errors(n);
+    auto work = [&] {
+      for (size_t i; (i = next++) < n;) {
+        try {
+          seqs[i] = skhost::read_sample(files[i], min_len);
+          if (seqs[i].seqs.empty()) errors[i] = names[i] + " contains no sequence";
+        } catch (const std::exception &e) {
+          errors[i] = e.what();
+        }
+      }
+    };
+    std::vector<std::thread> pool;
+    for (size_t t = 1; t < std::max<size_t>(1, num_threads) && t < n; ++t) pool.emplace_back(work);
+    work();
+    for (auto &t : pool) t.join();
+    for (const std::string &e : errors)
+      if (!e.empty()) throw std::runtime_error(e);
+  }
+  if (min_count > 0 && !exact)
+    std::cerr << "NOTE: min_count uses exact k-mer counts on the GPU (the count-min "
+                 "approximation of the CPU sketcher is not reproduced)" << std::endl;
+  if (min_count > 255) min_count = 255;
+  const int s64 = static_cast<int>(sketch_size);
+  const size_t K = kmers.size(), W = static_cast<size_t>(s64) * 14;
+  std::vector<uint64_t> words(n * K * W);
+  std::vector<SampleInfo> info(n);
+  sk_ctx *ctx = context(device_id);
+  for (int pass = 0; pass < 2; ++pass) {   // assemblies, then read sets
+    std::vector<size_t> idx;
+    for (size_t i = 0; i < n; ++i)
+      if (seqs[i].reads == (pass == 1)) idx.push_back(i);
+    if (idx.empty()) continue;
+    std::string bases;
+    std::vector<int64_t> off{0}, first{0};
+    for (size_t i : idx) {
+      for (const std::string &q : seqs[i].seqs) {
+        bases += q;
+        off.push_back(static_cast<int64_t>(bases.size()));
+      }
+      first.push_back(static_cast<int64_t>(off.size() - 1));
+    }
+    std::vector<uint64_t> w(idx.size() * K * W);
+    std::vector<double> inv(idx.size() * K);
+    std::vector<uint8_t> dens(idx.size());
+    const int32_t mc = pass == 1 ? static_cast<int32_t>(min_count) : 0;
+    run_gpu(ctx, [&] {
+      return sk_sketch(ctx, bases.data(), off.data(), first.data(), static_cast<int64_t>(idx.size()),
+                       kmers.data(), static_cast<int32_t>(K), s64, use_rc ? 1 : 0, mc, w.data(),
+                       inv.data(), dens.data());
+    });
+    for (size_t j = 0; j < idx.size(); ++j) {
+      const size_t i = idx[j];
+      std::copy(w.begin() + j * K * W, w.begin() + (j + 1) * K * W, words.begin() + i * K * W);
+      SampleInfo &si = info[i];
+      si.name = names[i];
+      si.reads = seqs[i].reads;
+      si.missing = seqs[i].missing_bases;
+      si.densified = dens[j] != 0;
+      std::copy(seqs[i].base_freq, seqs[i].base_freq + 4, si.bases.begin());
+      if (si.reads) {   // 1/N ~ E(minhash) over the k-mer lengths (src/reference.cpp:47-54)
+        double sum = 0;
+        for (size_t k = 0; k < K; ++k) sum += inv[j * K + k];
+        si.length = static_cast<uint64_t>(static_cast<double>(K) / sum);
+      } else {
+        si.length = seqs[i].total;
+      }
+    }
+  }
+  std::cerr << "Writing sketches to file" << std::endl;
+  save_sketch_db(path, info, words, kmers, s64, use_rc, false);
+  for (const SampleInfo &si : info)
+    if (si.densified) std::cerr << "NOTE: " << si.name << " required densification" << std::endl;
+  if (calc_random) {
+    if (n >= 3)   // default_n_clusters (src/random/random_match.hpp)
+      std::cerr << "NOTE: random match chances were not calculated (the Monte Carlo random "
+                   "genomes are not part of this library); queries use the equal-base "
+                   "random-match formula" << std::endl;
+    else
+      std::cerr << "Too few input genomes to calculate random match chances" << std::endl;
+  }
+}
+
+// Test hook: the SeqBuf view of one sample's files.
+py::dict read_sequences(const std::vector<std::string> &files, size_t min_len) {
+  skhost::SampleSeqs s = skhost::read_sample(files, min_len);
+  py::dict d;
+  d["seqs"] = s.seqs;
+  d["reads"] = s.reads;
+  d["missing_bases"] = s.missing_bases;
+  d["total"] = s.total;
+  d["base_freq"] = std::vector<double>(s.base_freq, s.base_freq + 4);
+  d["max_length"] = s.max_length;
+  return d;
+}
+
+// Test hook: writes a database from sketch words (save_sketch_db).
+void save_sketch_db_py(const std::string &db_name, const std::vector<std::string> &names,
+                       py::array_t<uint64_t, py::array::c_style | py::array::forcecast> words,
+                       std::vector<size_t> kmer_lengths, int sketchsize64,
+                       std::vector<uint64_t> lengths, bool use_rc) {
+  const std::vector<int32_t> kmers = to_kmers(kmer_lengths);
+  const size_t need = names.size() * kmers.size() * static_cast<size_t>(sketchsize64) * 14;
+  if (static_cast<size_t>(words.size()) != need) throw std::runtime_error("words have the wrong size");
+  std::vector<SampleInfo> info(names.size());
+  for (size_t i = 0; i < names.size(); ++i) {
+    info[i].name = names[i];
+    info[i].length = i < lengths.size() ? lengths[i] : 0;
+    info[i].bases = {0.25, 0.25, 0.25, 0.25};
+  }
+  std::vector<uint64_t> w(words.data(), words.data() + need);
+  save_sketch_db(db_name + ".h5", info, w, kmers, sketchsize64, use_rc, false);
+}
+
 void not_in_path(const char *what) {
   const std::string msg = std::string(what) +
-                          " creates sketches; sketching is not part of this library's GPU "
-                          "distance path (use the reference pp-sketchlib to build databases)";
+                          " computes random-match chances from Monte Carlo random genomes, "
+                          "which this library does not build (use the reference pp-sketchlib)";
   PyErr_SetString(PyExc_NotImplementedError, msg.c_str());
   throw py::error_already_set();
 }
@@ -463,8 +669,19 @@ PYBIND11_MODULE(_pp_sketchlib, m) {
         py::arg("distMat"), py::arg("distCutoff") = 0, py::arg("kNN") = 0,
         py::arg("num_threads") = 1);
 
-  m.def("constructDatabase", [](py::args, py::kwargs) { not_in_path("constructDatabase"); });
+  m.def("constructDatabase", &constructDatabase, "Create and save sketches", py::arg("db_name"),
+        py::arg("samples"), py::arg("files"), py::arg("klist"), py::arg("sketch_size"),
+        py::arg("codon_phased") = false, py::arg("calc_random") = true, py::arg("use_rc") = true,
+        py::arg("min_count") = 0, py::arg("exact") = false, py::arg("num_threads") = 1,
+        py::arg("use_gpu") = false, py::arg("device_id") = 0);
   m.def("addRandom", [](py::args, py::kwargs) { not_in_path("addRandom"); });
+
+  // not in the reference module: the sequence reader and database writer
+  // behind constructDatabase (tests)
+  m.def("_read_sequences", &read_sequences, py::arg("files"), py::arg("min_len"));
+  m.def("_save_sketch_db", &save_sketch_db_py, py::arg("db_name"), py::arg("names"),
+        py::arg("words"), py::arg("klist"), py::arg("sketchsize64"),
+        py::arg("lengths") = std::vector<uint64_t>{}, py::arg("use_rc") = true);
 
   // not in the reference module: reads a database's sketches (tests, tools)
   m.def("_load_sketch_db", &load_sketch_db, py::arg("db_name"),

@@ -191,8 +191,10 @@ def test_api_errors(small_mass):
         pp_sketchlib.queryDatabase(s["ref"], s["ref"], r, r, [15, 21])
     with pytest.raises(RuntimeError, match="deprecated"):
         pp_sketchlib.sparsifyDists(np.zeros((3, 3), np.float32))
+    with pytest.raises(RuntimeError, match="Could not open"):
+        pp_sketchlib.constructDatabase("x", ["a"], [["missing_file.fa"]], [15], 156)
     with pytest.raises(NotImplementedError):
-        pp_sketchlib.constructDatabase("x", ["a"], [["a.fa"]], [15], 10000)
+        pp_sketchlib.addRandom("x", ["a"], [15])
     with pytest.raises(RuntimeError, match="dist_col out of range"):
         pp_sketchlib.querySelfSparse(s["ref"], r, s["kmers"], kNN=2, dist_col=3)
 
