@@ -633,7 +633,7 @@ sk_status upload(sk_ctx *ctx, void *dst, const void *src, size_t bytes) {
 }
 
 sk_status launch_hash(sk_ctx *ctx, const SketchCall &c, SketchArgs args, const SketchItem *d_items,
-                      size_t n_items) {
+                      size_t n_items, cudaStream_t stream) {
   if (n_items == 0) return SK_OK;
   args.items = d_items;
   const bool shared = bins_fit_shared(ctx->device, c.nbins);
@@ -643,29 +643,29 @@ sk_status launch_hash(sk_ctx *ctx, const SketchCall &c, SketchArgs args, const S
   if (shared) {
     auto kern = c.use_rc ? sketch_kernel<true, true> : sketch_kernel<true, false>;
     e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    if (e == cudaSuccess) kern<<<grid, kSketchThreads, smem, ctx->stream>>>(args);
+    if (e == cudaSuccess) kern<<<grid, kSketchThreads, smem, stream>>>(args);
   } else {
     auto kern = c.use_rc ? sketch_kernel<false, true> : sketch_kernel<false, false>;
-    kern<<<grid, kSketchThreads, 0, ctx->stream>>>(args);
+    kern<<<grid, kSketchThreads, 0, stream>>>(args);
   }
   if (e == cudaSuccess) e = cudaGetLastError();
   return e == cudaSuccess ? SK_OK : cuda_fail(ctx, e, "sketch kernel");
 }
 
 // Codes of bytes [a, b) of the caller's buffer (offsets relative to the
-// batch) and start flags of sequences [q0, q1), on the context's stream.
-sk_status make_codes(SketchCall &c, const Batch &batch, const Batch &part) {
+// batch) and start flags of sequences [q0, q1), on `stream`.
+sk_status make_codes(SketchCall &c, const Batch &batch, const Batch &part, cudaStream_t stream) {
   sk_ctx *ctx = c.ctx;
   const int64_t bytes = part.b1 - part.b0;
   uint8_t *dst = c.d_codes + (part.b0 - batch.b0);
   const uint8_t *src = c.device_in ? reinterpret_cast<const uint8_t *>(c.bases) + part.b0 : dst;
   const unsigned g = static_cast<unsigned>(
       std::max<int64_t>(1, std::min<int64_t>(ctx->sm_count * 8, (bytes / 16 + 255) / 256)));
-  if (bytes > 0) codes_kernel<<<g, 256, 0, ctx->stream>>>(src, dst, bytes);
+  if (bytes > 0) codes_kernel<<<g, 256, 0, stream>>>(src, dst, bytes);
   const int64_t n_seqs = part.q1 - part.q0;
   if (n_seqs > 0)
     mark_starts_kernel<<<static_cast<unsigned>(std::min<int64_t>(ctx->sm_count * 8, (n_seqs + 255) / 256)),
-                         256, 0, ctx->stream>>>(c.d_codes, c.d_seq_off + (part.q0 - batch.q0), n_seqs,
+                         256, 0, stream>>>(c.d_codes, c.d_seq_off + (part.q0 - batch.q0), n_seqs,
                                                 batch.b0);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? SK_OK : cuda_fail(ctx, e, "sketch codes");
@@ -732,8 +732,11 @@ sk_status count_batch(SketchCall &c, const Batch &b, SketchArgs &args, std::vect
 }
 
 // Bins rows of one batch without a count filter.  Host bases go up in sample
-// chunks on the copy stream; each chunk's codes and items run on the
-// context's stream as soon as it has landed, while later chunks copy.
+// chunks on the copy stream; each chunk's codes and items run as soon as it
+// has landed, while later chunks copy, on two compute streams in turn (so
+// one chunk's last wave is filled by the next chunk's CTAs; chunks touch
+// disjoint bins rows and codes, and no emitted window reads another chunk's
+// bytes).
 sk_status hash_batch(SketchCall &c, const Batch &b, SketchArgs &args, std::vector<SketchItem> &items) {
   sk_ctx *ctx = c.ctx;
   const std::vector<Batch> parts = c.device_in ? std::vector<Batch>{b} : upload_chunks(c, b);
@@ -752,12 +755,14 @@ sk_status hash_batch(SketchCall &c, const Batch &b, SketchArgs &args, std::vecto
   }
   const SketchItem *d_items = static_cast<const SketchItem *>(p);
   if (c.device_in) {
-    st = make_codes(c, b, b);
-    return st == SK_OK ? launch_hash(ctx, c, args, d_items, items.size()) : st;
+    st = make_codes(c, b, b, ctx->stream);
+    return st == SK_OK ? launch_hash(ctx, c, args, d_items, items.size(), ctx->stream) : st;
   }
   st = ensure_copy_stream(ctx);
   if (st != SK_OK) return st;
   cudaError_t e = cudaSuccess;
+  if (!ctx->stream_b) e = cudaStreamCreateWithFlags(&ctx->stream_b, cudaStreamNonBlocking);
+  if (e == cudaSuccess && !ctx->ev_join) e = cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming);
   while (e == cudaSuccess && ctx->ev_chunk.size() < parts.size()) {
     cudaEvent_t ev = nullptr;
     e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
@@ -774,14 +779,19 @@ sk_status hash_batch(SketchCall &c, const Batch &b, SketchArgs &args, std::vecto
     if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_chunk[i], ctx->copy_stream);
   }
   if (e != cudaSuccess) return cuda_fail(ctx, e, "sketch upload");
+  cudaStream_t compute[2] = {ctx->stream, ctx->stream_b};
   for (size_t i = 0; i < parts.size(); ++i) {
-    e = cudaStreamWaitEvent(ctx->stream, ctx->ev_chunk[i], 0);
+    cudaStream_t s = compute[i & 1];
+    e = cudaStreamWaitEvent(s, ctx->ev_chunk[i], 0);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "sketch upload");
-    st = make_codes(c, b, parts[i]);
-    if (st == SK_OK) st = launch_hash(ctx, c, args, d_items + first[i], first[i + 1] - first[i]);
+    st = make_codes(c, b, parts[i], s);
+    if (st == SK_OK) st = launch_hash(ctx, c, args, d_items + first[i], first[i + 1] - first[i], s);
     if (st != SK_OK) return st;
   }
-  return SK_OK;
+  // the context's stream (finishing, copies back) waits for the second one
+  e = cudaEventRecord(ctx->ev_join, ctx->stream_b);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0);
+  return e == cudaSuccess ? SK_OK : cuda_fail(ctx, e, "stream join");
 }
 
 // Sketches the samples of one batch into d_words / d_inv / d_dens (rows of the
@@ -819,7 +829,7 @@ sk_status sketch_batch(SketchCall &c, const Batch &b, std::vector<SketchItem> &i
   args.status = ctx->status_dev;
   if (c.min_count > 0) {
     if (!c.device_in) st = upload(ctx, c.d_codes, c.bases + b.b0, static_cast<size_t>(bytes));
-    if (st == SK_OK) st = make_codes(c, b, b);
+    if (st == SK_OK) st = make_codes(c, b, b, ctx->stream);
     if (st == SK_OK) st = count_batch(c, b, args, items);
   } else {
     st = hash_batch(c, b, args, items);
