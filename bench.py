@@ -371,6 +371,56 @@ def run_sketch(ctx, dev, steps, warmup, cpu=True):
                                "kind": kind, "sample": f"the whole workload ({n} genomes, "
                                                        f"{ct:.2f} s)"}
         out["matches_cpu_sketcher"] = bool(np.array_equal(want, words_dev))
+    out["reads"] = run_sketch_reads(ctx, steps, warmup, cpu)
+    return out
+
+
+def run_sketch_reads(ctx, steps, warmup, cpu):
+    """A read set (2 Mb genome, 10x coverage of 150 bp reads, 1% errors; 20
+    Mbases) sketched with min_count = 3 (exact k-mer counts), against the
+    reference's CPU sketcher with exact = true on the same reads as FASTQ."""
+    import tempfile
+    from sketchlib_b200 import capi
+    rng = np.random.default_rng(SKETCH_SEED + 1)
+    G, cov, RL = 2_000_000, 10, 150
+    genome = np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, G)]
+    n_reads = cov * G // RL
+    starts = rng.integers(0, G - RL, n_reads)
+    reads = genome[starts[:, None] + np.arange(RL)[None, :]]
+    err = rng.random(reads.shape) < 0.01
+    reads[err] = np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, int(err.sum()))]
+    off = np.arange(n_reads + 1, dtype=np.int64) * RL
+    ss = np.array([0, n_reads], np.int64)
+    bases = reads.reshape(-1)
+    for _ in range(warmup):
+        words, _, _ = capi.sketch(ctx, bases, off, ss, KMERS, S64, min_count=3)
+    ms = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        words, _, _ = capi.sketch(ctx, bases, off, ss, KMERS, S64, min_count=3)
+        ms.append(1e3 * (time.perf_counter() - t0))
+    out = {"workload": f"{n_reads:,} reads of {RL} bp (10x of a 2 Mb genome, 1% errors), "
+                       "k = 15..29 odd, sketchsize64 156, min_count 3 (exact counts)",
+           "bases": int(bases.size), "ms": statistics.median(ms),
+           "call": "sk_sketch from host memory (count table per k, then the bins)"}
+    if cpu:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle
+        if oracle.sketcher_available():
+            with tempfile.TemporaryDirectory() as tmp:
+                fq = Path(tmp) / "reads.fq"
+                q = b"\n+\n" + b"I" * RL + b"\n"
+                with open(fq, "wb") as f:
+                    for r in reads:
+                        f.write(b"@r\n" + r.tobytes() + q)
+                t0 = time.perf_counter()
+                want, _, _, _ = oracle.RefSketcher().sketch_file(fq, KMERS, S64, True, 3, True)
+                ct = time.perf_counter() - t0
+            out["cpu_baseline"] = {"seconds": ct, "cores": 1, "kind": "reference",
+                                   "sample": "the whole read set: the reference's SeqBuf + "
+                                             "sketch() with exact counting (one sample is one "
+                                             "thread in the reference)"}
+            out["matches_cpu_sketcher"] = bool(np.array_equal(want, words[0]))
     return out
 
 
