@@ -8,9 +8,10 @@
 // from a probe sequence (densifybin, :93-118) and the low 14 bits of every
 // bin become bit planes, 64 bins per word (fillusigs, :82-91).  Here:
 //
-//   codes      the bases go up as they are and are rewritten in place as one
-//              byte per base: 0..3 for A, C, G, T/U in either case, 4 for any
-//              other byte, plus kCodeStart on the first base of each sequence.
+//   codes      the bases go up as they are (or are read where they lie in
+//              device memory) and become one byte per base: 0..3 for A, C, G,
+//              T/U in either case, 4 for any other byte, plus kCodeStart on
+//              the first base of each sequence.
 //   hashing    a work item is (sample, k, range of window starts).  Its CTA
 //              keeps the item's bin minima in shared memory; each thread rolls
 //              the forward and reverse hashes over its share of the range.  A
@@ -44,7 +45,7 @@ constexpr uint64_t kLo33 = 0x1FFFFFFFFULL;
 constexpr uint8_t kCodeInvalid = 4;
 constexpr uint8_t kCodeStart = 8;
 constexpr int kSketchThreads = 512;
-constexpr int kPerThread = 512;                    // window starts per thread
+constexpr int kPerThread = 512;                    // window starts per thread, at most
 constexpr int64_t kItemWindows = static_cast<int64_t>(kSketchThreads) * kPerThread;
 constexpr int kFinishThreads = 512;
 constexpr int kMinK = 3;                           // generate_seeds (src/sketch/sketch.cpp:33-40)
@@ -684,7 +685,11 @@ uint64_t next_pow2(uint64_t v) {
 sk_status count_batch(SketchCall &c, const Batch &b, SketchArgs &args, std::vector<SketchItem> &items) {
   sk_ctx *ctx = c.ctx;
   const int K = static_cast<int>(c.kmers.size());
-  constexpr uint64_t kTableBudget = 1ULL << 31;   // bytes of keys + counts per pass
+  // bytes of keys + counts per pass: a quarter of the context's memory limit
+  // when one is set, else 2 GiB
+  const uint64_t kTableBudget =
+      ctx->mem_limit > 0 ? std::max<uint64_t>(1ULL << 16, static_cast<uint64_t>(ctx->mem_limit) / 4)
+                         : (1ULL << 31);
   for (int64_t s = b.s0; s < b.s1; ++s) {
     const int64_t windows = c.seq_off[c.sample_seqs[s + 1]] - c.seq_off[c.sample_seqs[s]];
     if (windows <= 0) continue;

@@ -189,3 +189,38 @@ def test_device_entry_point_matches_host_one(gpu_ctx, min_count, shift):
     np.testing.assert_array_equal(inv.cpu().numpy(), want[1])
     np.testing.assert_array_equal(dens.cpu().numpy().astype(bool), want[2])
     np.testing.assert_array_equal(buf[shift:shift + bases.size].cpu().numpy(), bases)
+
+
+def test_read_filter_in_many_counting_passes():
+    """A 1 MiB memory limit shrinks the count table to 256 KB per pass, so a
+    read set is counted in about two dozen bin-range passes; the sketch is
+    unchanged."""
+    from sketchlib_b200 import capi
+    rng = np.random.default_rng(77)
+    genome = np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, 50_000)]
+    reads = []
+    for _ in range(3 * 50_000 // 100):
+        s = int(rng.integers(0, 50_000 - 100))
+        r = genome[s:s + 100].copy()
+        e = rng.random(100) < 0.01
+        r[e] = np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, int(e.sum()))]
+        reads.append(r.tobytes())
+    bases, off, ss = capi.pack_sequences([reads])
+    kmers = [15, 21, 27]
+    with capi.Context(0) as ctx:
+        ctx.set_memory_limit(1 << 20)
+        got = capi.sketch(ctx, bases, off, ss, kmers, 64, min_count=2)
+    check(got, oracle.sketch(bases, off, ss, kmers, 64, True, min_count=2))
+
+
+def test_many_samples_split_into_batches(gpu_ctx):
+    """300 samples at 64,000 bins and 8 k-mer lengths: 1.2 GB of bins rows,
+    more than one batch holds, and bins too large for shared memory."""
+    from sketchlib_b200 import capi
+    rng = np.random.default_rng(78)
+    samples = [[np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, 100_000)].tobytes()]
+               for _ in range(300)]
+    bases, off, ss = capi.pack_sequences(samples)
+    kmers = list(range(15, 31, 2))
+    check(capi.sketch(gpu_ctx, bases, off, ss, kmers, 1000),
+          oracle.sketch(bases, off, ss, kmers, 1000, True))
