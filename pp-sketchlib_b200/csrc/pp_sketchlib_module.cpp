@@ -473,28 +473,6 @@ void constructDatabase(const std::string &db_name, const std::vector<std::string
   }
   const size_t min_len = kmer_lengths.back();   // SeqBuf(files, kmer_lengths.back())
   const size_t n = names.size();
-  std::vector<skhost::SampleSeqs> seqs(n);
-  {
-    py::gil_scoped_release release;
-    std::atomic<size_t> next{0};
-    std::vector<std::string> errors(n);
-    auto work = [&] {
-      for (size_t i; (i = next++) < n;) {
-        try {
-          seqs[i] = skhost::read_sample(files[i], min_len);
-          if (seqs[i].seqs.empty()) errors[i] = names[i] + " contains no sequence";
-        } catch (const std::exception &e) {
-          errors[i] = e.what();
-        }
-      }
-    };
-    std::vector<std::thread> pool;
-    for (size_t t = 1; t < std::max<size_t>(1, num_threads) && t < n; ++t) pool.emplace_back(work);
-    work();
-    for (auto &t : pool) t.join();
-    for (const std::string &e : errors)
-      if (!e.empty()) throw std::runtime_error(e);
-  }
   if (min_count > 0 && !exact)
     std::cerr << "NOTE: min_count uses exact k-mer counts on the GPU (the count-min "
                  "approximation of the CPU sketcher is not reproduced)" << std::endl;
@@ -504,46 +482,94 @@ void constructDatabase(const std::string &db_name, const std::vector<std::string
   std::vector<uint64_t> words(n * K * W);
   std::vector<SampleInfo> info(n);
   sk_ctx *ctx = context(device_id);
-  for (int pass = 0; pass < 2; ++pass) {   // assemblies, then read sets
-    std::vector<size_t> idx;
-    for (size_t i = 0; i < n; ++i)
-      if (seqs[i].reads == (pass == 1)) idx.push_back(i);
-    if (idx.empty()) continue;
-    std::string bases;
-    std::vector<int64_t> off{0}, first{0};
-    for (size_t i : idx) {
-      for (const std::string &q : seqs[i].seqs) {
-        bases += q;
-        off.push_back(static_cast<int64_t>(bases.size()));
-      }
-      first.push_back(static_cast<int64_t>(off.size() - 1));
+  // samples are read (num_threads at a time) and sketched in chunks of about
+  // kChunkBases bases, so only one chunk's sequences are held at once
+  constexpr uint64_t kChunkBases = 2ULL << 30;
+  size_t start = 0;
+  while (start < n) {
+    std::vector<skhost::SampleSeqs> seqs;
+    size_t end = start;
+    {
+      py::gil_scoped_release release;
+      std::mutex mu;
+      size_t next = start;
+      uint64_t held = 0;
+      std::vector<std::pair<size_t, skhost::SampleSeqs>> done;
+      std::vector<std::string> errors;
+      auto work = [&] {
+        for (;;) {
+          size_t i;
+          {
+            std::lock_guard<std::mutex> g(mu);
+            if (next >= n || (held >= kChunkBases && next > start)) return;
+            i = next++;
+          }
+          skhost::SampleSeqs got;
+          std::string err;
+          try {
+            got = skhost::read_sample(files[i], min_len);
+            if (got.seqs.empty()) err = names[i] + " contains no sequence";
+          } catch (const std::exception &e) {
+            err = e.what();
+          }
+          std::lock_guard<std::mutex> g(mu);
+          held += got.total;
+          if (!err.empty()) errors.push_back(err);
+          done.emplace_back(i, std::move(got));
+        }
+      };
+      std::vector<std::thread> pool;
+      for (size_t t = 1; t < std::max<size_t>(1, num_threads); ++t) pool.emplace_back(work);
+      work();
+      for (auto &t : pool) t.join();
+      if (!errors.empty()) throw std::runtime_error(errors.front());
+      end = next;
+      seqs.resize(end - start);
+      for (auto &d : done) seqs[d.first - start] = std::move(d.second);
     }
-    std::vector<uint64_t> w(idx.size() * K * W);
-    std::vector<double> inv(idx.size() * K);
-    std::vector<uint8_t> dens(idx.size());
-    const int32_t mc = pass == 1 ? static_cast<int32_t>(min_count) : 0;
-    run_gpu(ctx, [&] {
-      return sk_sketch(ctx, bases.data(), off.data(), first.data(), static_cast<int64_t>(idx.size()),
-                       kmers.data(), static_cast<int32_t>(K), s64, use_rc ? 1 : 0, mc, w.data(),
-                       inv.data(), dens.data());
-    });
-    for (size_t j = 0; j < idx.size(); ++j) {
-      const size_t i = idx[j];
-      std::copy(w.begin() + j * K * W, w.begin() + (j + 1) * K * W, words.begin() + i * K * W);
-      SampleInfo &si = info[i];
-      si.name = names[i];
-      si.reads = seqs[i].reads;
-      si.missing = seqs[i].missing_bases;
-      si.densified = dens[j] != 0;
-      std::copy(seqs[i].base_freq, seqs[i].base_freq + 4, si.bases.begin());
-      if (si.reads) {   // 1/N ~ E(minhash) over the k-mer lengths (src/reference.cpp:47-54)
-        double sum = 0;
-        for (size_t k = 0; k < K; ++k) sum += inv[j * K + k];
-        si.length = static_cast<uint64_t>(static_cast<double>(K) / sum);
-      } else {
-        si.length = seqs[i].total;
+    for (int pass = 0; pass < 2; ++pass) {   // assemblies, then read sets
+      std::vector<size_t> idx;
+      for (size_t i = start; i < end; ++i)
+        if (seqs[i - start].reads == (pass == 1)) idx.push_back(i);
+      if (idx.empty()) continue;
+      std::string bases;
+      std::vector<int64_t> off{0}, first{0};
+      for (size_t i : idx) {
+        for (const std::string &q : seqs[i - start].seqs) {
+          bases += q;
+          off.push_back(static_cast<int64_t>(bases.size()));
+        }
+        first.push_back(static_cast<int64_t>(off.size() - 1));
+      }
+      std::vector<uint64_t> w(idx.size() * K * W);
+      std::vector<double> inv(idx.size() * K);
+      std::vector<uint8_t> dens(idx.size());
+      const int32_t mc = pass == 1 ? static_cast<int32_t>(min_count) : 0;
+      run_gpu(ctx, [&] {
+        return sk_sketch(ctx, bases.data(), off.data(), first.data(), static_cast<int64_t>(idx.size()),
+                         kmers.data(), static_cast<int32_t>(K), s64, use_rc ? 1 : 0, mc, w.data(),
+                         inv.data(), dens.data());
+      });
+      for (size_t j = 0; j < idx.size(); ++j) {
+        const size_t i = idx[j];
+        const skhost::SampleSeqs &sq = seqs[i - start];
+        std::copy(w.begin() + j * K * W, w.begin() + (j + 1) * K * W, words.begin() + i * K * W);
+        SampleInfo &si = info[i];
+        si.name = names[i];
+        si.reads = sq.reads;
+        si.missing = sq.missing_bases;
+        si.densified = dens[j] != 0;
+        std::copy(sq.base_freq, sq.base_freq + 4, si.bases.begin());
+        if (si.reads) {   // 1/N ~ E(minhash) over the k-mer lengths (src/reference.cpp:47-54)
+          double sum = 0;
+          for (size_t k = 0; k < K; ++k) sum += inv[j * K + k];
+          si.length = static_cast<uint64_t>(static_cast<double>(K) / sum);
+        } else {
+          si.length = sq.total;
+        }
       }
     }
+    start = end;
   }
   std::cerr << "Writing sketches to file" << std::endl;
   save_sketch_db(path, info, words, kmers, s64, use_rc, false);

@@ -872,6 +872,15 @@ sk_status sketch_to_device(SketchCall &c) {
   return SK_OK;
 }
 
+// After a failed call: waits for the copy and second compute streams, so no
+// copy still reads the caller's host buffer once the call has returned.
+sk_status drain(sk_ctx *ctx, sk_status st) {
+  if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+  if (ctx->stream_b) cudaStreamSynchronize(ctx->stream_b);
+  cudaStreamSynchronize(ctx->stream);
+  return st;
+}
+
 // Call set-up; d_words / d_inv given by the caller are written directly,
 // else they are context scratch.
 sk_status setup_call(SketchCall &c, sk_ctx *ctx, const char *bases, bool device_in,
@@ -928,7 +937,7 @@ sk_status sk_sketch(sk_ctx *ctx, const char *bases, const int64_t *seq_offsets,
   st = setup_call(c, ctx, bases, false, seq_offsets, sample_seqs, n_samples, kmers, n_kmers,
                   sketchsize64, use_rc, min_count, nullptr, nullptr);
   if (st == SK_OK) st = sketch_to_device(c);
-  if (st != SK_OK) return st;
+  if (st != SK_OK) return drain(ctx, st);
   const size_t n_words = static_cast<size_t>(n_samples) * n_kmers * sketchsize64 * kBbits;
   const size_t rows = static_cast<size_t>(n_samples) * n_kmers;
   std::vector<int8_t> dens(rows);
@@ -936,7 +945,7 @@ sk_status sk_sketch(sk_ctx *ctx, const char *bases, const int64_t *seq_offsets,
   if (e == cudaSuccess && inv_minhash)
     e = cudaMemcpyAsync(inv_minhash, c.d_inv, rows * 8, cudaMemcpyDeviceToHost, ctx->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(dens.data(), c.d_dens, rows, cudaMemcpyDeviceToHost, ctx->stream);
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "sketch download");
+  if (e != cudaSuccess) return drain(ctx, cuda_fail(ctx, e, "sketch download"));
   st = finish_call(ctx);
   if (st != SK_OK) return st;
   if (densified)
@@ -965,7 +974,7 @@ sk_status sk_sketch_device(sk_ctx *ctx, const char *d_bases, const int64_t *seq_
   st = setup_call(c, ctx, d_bases, true, seq_offsets, sample_seqs, n_samples, kmers, n_kmers,
                   sketchsize64, use_rc, min_count, d_words, d_inv_minhash);
   if (st == SK_OK) st = sketch_to_device(c);
-  if (st != SK_OK) return st;
+  if (st != SK_OK) return drain(ctx, st);
   if (d_densified) {
     densified_kernel<<<static_cast<unsigned>((n_samples + 255) / 256), 256, 0, ctx->stream>>>(
         c.d_dens, n_samples, n_kmers, d_densified);

@@ -67,7 +67,7 @@ def test_construct_database_matches_reference_sketcher(tmp_path):
         files.append([str(p)])
     db = str(tmp_path / "db")
     pp_sketchlib.constructDatabase(db, names, files, KMERS, S64, calc_random=False,
-                                   min_count=2, exact=True)
+                                   min_count=2, exact=True, num_threads=4)
     got = pp_sketchlib._load_sketch_db(db, names=names, klist=KMERS)
     rs = oracle.RefSketcher()
     for i, (name, f) in enumerate(zip(names, files)):
