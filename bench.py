@@ -375,13 +375,8 @@ def run_sketch(ctx, dev, steps, warmup, cpu=True):
     return out
 
 
-def run_sketch_reads(ctx, steps, warmup, cpu):
-    """A read set (2 Mb genome, 10x coverage of 150 bp reads, 1% errors; 20
-    Mbases) sketched with min_count = 3 (exact k-mer counts), against the
-    reference's CPU sketcher with exact = true on the same reads as FASTQ."""
-    import tempfile
-    from sketchlib_b200 import capi
-    rng = np.random.default_rng(SKETCH_SEED + 1)
+def read_set(rng):
+    """133,333 reads of 150 bp: 10x coverage of a 2 Mb genome, 1% errors."""
     G, cov, RL = 2_000_000, 10, 150
     genome = np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, G)]
     n_reads = cov * G // RL
@@ -389,6 +384,18 @@ def run_sketch_reads(ctx, steps, warmup, cpu):
     reads = genome[starts[:, None] + np.arange(RL)[None, :]]
     err = rng.random(reads.shape) < 0.01
     reads[err] = np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, int(err.sum()))]
+    return reads
+
+
+def run_sketch_reads(ctx, steps, warmup, cpu):
+    """A read set (2 Mb genome, 10x coverage of 150 bp reads, 1% errors; 20
+    Mbases) sketched with min_count = 3 (exact k-mer counts), against the
+    reference's CPU sketcher with exact = true on the same reads as FASTQ."""
+    import tempfile
+    from sketchlib_b200 import capi
+    rng = np.random.default_rng(SKETCH_SEED + 1)
+    reads = read_set(rng)
+    n_reads, RL = reads.shape
     off = np.arange(n_reads + 1, dtype=np.int64) * RL
     ss = np.array([0, n_reads], np.int64)
     bases = reads.reshape(-1)
@@ -859,6 +866,21 @@ def run_profile_sketch(n: int, launches: int):
     ctx.close()
 
 
+def run_profile_sketch_reads(launches: int):
+    """A small case for ncu: the bench's 20 Mbase read set through sk_sketch
+    with min_count 3, `launches` times, nothing else."""
+    from sketchlib_b200 import capi
+    ctx = capi.Context(0)
+    reads = read_set(np.random.default_rng(SKETCH_SEED + 1))
+    n_reads, RL = reads.shape
+    off = np.arange(n_reads + 1, dtype=np.int64) * RL
+    ss = np.array([0, n_reads], np.int64)
+    for _ in range(launches):
+        capi.sketch(ctx, reads.reshape(-1), off, ss, KMERS, S64, min_count=3)
+    print(json.dumps({"profile_sketch_reads": int(reads.size), "launches": launches}))
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -884,9 +906,14 @@ def main():
     ap.add_argument("--profile-launches", type=int, default=2)
     ap.add_argument("--profile-sketch", type=int, default=0,
                     help="run only N genomes through sk_sketch_device (for ncu)")
+    ap.add_argument("--profile-sketch-reads", action="store_true",
+                    help="run only the 20 Mbase read set through sk_sketch (for ncu)")
     args = ap.parse_args()
     if args.profile_sketch:
         run_profile_sketch(args.profile_sketch, args.profile_launches)
+        return
+    if args.profile_sketch_reads:
+        run_profile_sketch_reads(args.profile_launches)
         return
     if args.profile:
         run_profile_case(args.profile, args.profile_launches)

@@ -38,9 +38,8 @@ enum ScratchSlot : int {
   kSlotSketchTables = 14, // rolling-hash tables per k
   kSlotSketchBins = 15,   // bin minima per (sample, k)
   kSlotSketchWords = 16,  // finished sketches, inverse minhashes, densify flags
-  kSlotSketchKeys = 17,   // hash-count table of read sets (keys, counts)
-  kSlotSketchCounts = 18,
-  kSlotCount = 19
+  kSlotSketchTable = 17,  // k-mer count table of read sets
+  kSlotCount = 18
 };
 
 struct sk_ctx {

@@ -287,6 +287,21 @@ __device__ __forceinline__ void roll_windows(const uint8_t *__restrict__ codes, 
   roll_span<false, true, kRc>(base, inner1, n_chunks, c, D, sh, k, lo, hi, t, st, emit);
 }
 
+// One slot of the k-mer count table: key and count share a 16-byte slot, so
+// an insertion touches one memory sector.
+struct __align__(16) TableSlot {
+  unsigned long long key;
+  unsigned int count;
+  unsigned int pad;
+};
+
+__global__ void table_clear_kernel(TableSlot *__restrict__ t, uint64_t n, unsigned int *max_key_count) {
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n; i += stride)
+    reinterpret_cast<uint4 *>(t)[i] = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *max_key_count = 0;
+}
+
 struct SketchArgs {
   const uint8_t *codes;
   const SketchItem *items;
@@ -296,8 +311,7 @@ struct SketchArgs {
   int use_rc;
   uint64_t binsize, magic;
   // counting mode
-  unsigned long long *keys;      // hash table keys (kEmptyKey = free)
-  unsigned int *counts;
+  struct TableSlot *table;       // hash-count table (key kEmptyKey = free)
   uint64_t table_mask;
   unsigned int *max_key_count;   // occurrences of the one hash equal to kEmptyKey
   uint32_t bin_lo, bin_hi;       // bins this pass counts
@@ -370,13 +384,14 @@ count_kernel(SketchArgs a) {
     }
     uint64_t slot = table_slot(h, a.table_mask);
     for (uint64_t probe = 0; probe <= a.table_mask; ++probe) {
-      unsigned long long cur = a.keys[slot];
+      TableSlot *t = a.table + slot;
+      unsigned long long cur = t->key;
       if (cur == kEmptyKey) {
-        cur = atomicCAS(a.keys + slot, kEmptyKey, static_cast<unsigned long long>(h));
+        cur = atomicCAS(&t->key, kEmptyKey, static_cast<unsigned long long>(h));
         if (cur == kEmptyKey) cur = h;
       }
       if (cur == h) {
-        atomicAdd(a.counts + slot, 1u);
+        atomicAdd(&t->count, 1u);
         return;
       }
       slot = (slot + 1) & a.table_mask;
@@ -391,8 +406,9 @@ __global__ void table_bins_kernel(SketchArgs a, int row_index, unsigned min_coun
   const uint64_t n = a.table_mask + 1;
   const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
   for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n; i += stride) {
-    const unsigned long long h = a.keys[i];
-    if (h == kEmptyKey || a.counts[i] < min_count) continue;
+    const TableSlot t = a.table[i];
+    const unsigned long long h = t.key;
+    if (h == kEmptyKey || t.count < min_count) continue;
     const uint64_t sign = mod_sign(h);
     const uint32_t q = bin_of(sign, a.binsize, a.magic);
     if (sign < row[q]) atomicMin(row + q, static_cast<unsigned long long>(sign));
@@ -602,11 +618,11 @@ std::vector<Batch> upload_chunks(const SketchCall &c, const Batch &b) {
 // (they read the same bases).  Windows end inside their sample, so a sample's
 // items read no other sample's codes that they depend on.
 void make_items(const SketchCall &c, const Batch &b, int64_t s0, int64_t s1, int k_only,
-                std::vector<SketchItem> &items) {
+                std::vector<SketchItem> &items, int64_t max_windows = kItemWindows) {
   const int K = static_cast<int>(c.kmers.size());
   for (int64_t s = s0; s < s1; ++s) {
     const int64_t a = c.seq_off[c.sample_seqs[s]] - b.b0, e = c.seq_off[c.sample_seqs[s + 1]] - b.b0;
-    const int64_t pieces = std::max<int64_t>(1, (e - a + kItemWindows - 1) / kItemWindows);
+    const int64_t pieces = std::max<int64_t>(1, (e - a + max_windows - 1) / max_windows);
     const int64_t piece = (e - a + pieces - 1) / pieces;
     const int32_t per = static_cast<int32_t>(
         std::max<int64_t>(16, ((piece + kSketchThreads - 1) / kSketchThreads + 15) / 16 * 16));
@@ -681,7 +697,11 @@ uint64_t next_pow2(uint64_t v) {
 // Bins rows of one batch with the exact count filter: per sample and k, the
 // hashes are counted in a table of twice the sample's windows (in bin-range
 // passes when that exceeds the table budget), then the ones counted
-// min_count times enter the bins.
+// min_count times enter the bins.  The counting items are an eighth of the
+// hashing ones (no per-CTA bins to amortise; more CTAs in flight hide the
+// table's memory latency).
+constexpr int64_t kCountItemWindows = kItemWindows / 8;
+
 sk_status count_batch(SketchCall &c, const Batch &b, SketchArgs &args, std::vector<SketchItem> &items) {
   sk_ctx *ctx = c.ctx;
   const int K = static_cast<int>(c.kmers.size());
@@ -694,19 +714,17 @@ sk_status count_batch(SketchCall &c, const Batch &b, SketchArgs &args, std::vect
     const int64_t windows = c.seq_off[c.sample_seqs[s + 1]] - c.seq_off[c.sample_seqs[s]];
     if (windows <= 0) continue;
     const uint64_t want = next_pow2(static_cast<uint64_t>(windows) * 2);
-    const uint64_t passes = std::max<uint64_t>(1, (want * 12 + kTableBudget - 1) / kTableBudget);
+    const uint64_t passes = std::max<uint64_t>(1, (want * sizeof(TableSlot) + kTableBudget - 1) / kTableBudget);
     const uint64_t slots = std::max<uint64_t>(1024, next_pow2((want + passes - 1) / passes));
-    void *tk = nullptr, *tc = nullptr;
-    sk_status st = scratch(ctx, kSlotSketchKeys, slots * 8, &tk);
-    if (st == SK_OK) st = scratch(ctx, kSlotSketchCounts, slots * 4 + 16, &tc);
+    void *tk = nullptr;
+    sk_status st = scratch(ctx, kSlotSketchTable, slots * sizeof(TableSlot) + 16, &tk);
     if (st != SK_OK) return st;
-    args.keys = static_cast<unsigned long long *>(tk);
-    args.counts = static_cast<unsigned int *>(tc);
-    args.max_key_count = reinterpret_cast<unsigned int *>(static_cast<char *>(tc) + slots * 4);
+    args.table = static_cast<TableSlot *>(tk);
+    args.max_key_count = reinterpret_cast<unsigned int *>(static_cast<char *>(tk) + slots * sizeof(TableSlot));
     args.table_mask = slots - 1;
     for (int k = 0; k < K; ++k) {
       items.clear();
-      make_items(c, b, s, s + 1, k, items);
+      make_items(c, b, s, s + 1, k, items, kCountItemWindows);
       if (items.empty()) continue;
       void *p = nullptr;
       st = scratch(ctx, kSlotSketchItems, items.size() * sizeof(SketchItem), &p);
@@ -716,8 +734,9 @@ sk_status count_batch(SketchCall &c, const Batch &b, SketchArgs &args, std::vect
       for (uint64_t pass = 0; pass < passes; ++pass) {
         args.bin_lo = static_cast<uint32_t>(c.nbins * pass / passes);
         args.bin_hi = static_cast<uint32_t>(c.nbins * (pass + 1) / passes);
-        cudaError_t e = cudaMemsetAsync(tk, 0xFF, slots * 8, ctx->stream);
-        if (e == cudaSuccess) e = cudaMemsetAsync(tc, 0, slots * 4 + 16, ctx->stream);
+        table_clear_kernel<<<static_cast<unsigned>(std::min<uint64_t>(4096, (slots + 255) / 256)), 256, 0,
+                             ctx->stream>>>(args.table, slots, args.max_key_count);
+        cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) {
           auto kern = c.use_rc ? count_kernel<true> : count_kernel<false>;
           kern<<<static_cast<unsigned>(items.size()), kSketchThreads, 0, ctx->stream>>>(args);
