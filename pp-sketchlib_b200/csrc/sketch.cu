@@ -23,11 +23,11 @@
 //   finishing  one CTA per (sample, k) records bin 0 (inverse_minhash), fills
 //              empty bins in the reference's order and writes the bit planes
 //              with warp ballots.
-//   counting   with min_count > 0 (read sets), hashes are first counted in a
-//              device hash table and only those seen min_count times enter
-//              the bins: the reference's exact counter (HashCounter,
-//              src/sketch/countmin.cpp:55-72, `exact = true`), whose answer
-//              does not depend on read order.
+//   counting   with min_count > 0 (read sets), hashes are counted in a device
+//              hash table and the insertion that brings a hash's count to
+//              min_count enters it in its bin: the reference's exact counter
+//              (HashCounter, src/sketch/countmin.cpp:55-72, `exact = true`),
+//              whose answer does not depend on read order.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -315,6 +315,7 @@ struct SketchArgs {
   uint64_t table_mask;
   unsigned int *max_key_count;   // occurrences of the one hash equal to kEmptyKey
   uint32_t bin_lo, bin_hi;       // bins this pass counts
+  unsigned int min_count;        // a hash enters its bin when its count reaches this
   DevStatus *status;
 };
 
@@ -361,7 +362,10 @@ __device__ __forceinline__ uint64_t table_slot(uint64_t h, uint64_t mask) {
   return h & mask;
 }
 
-// Counting pass: every hash whose bin lies in [bin_lo, bin_hi) is counted.
+// Counting pass: every hash whose bin lies in [bin_lo, bin_hi) is counted,
+// and the insertion that brings a hash's count to min_count puts it in its
+// bin (the reference's counter adds a k-mer at the occurrence whose count
+// reaches min_count, src/sketch/sketch.cpp:143-148).
 template <bool kRc>
 __global__ void __launch_bounds__(kSketchThreads)
 count_kernel(SketchArgs a) {
@@ -375,49 +379,37 @@ count_kernel(SketchArgs a) {
   const int64_t s = it.begin + static_cast<int64_t>(threadIdx.x) * it.per;
   const int64_t e = min(s + it.per, it.end);
   if (s >= e) return;
+  unsigned long long *row = a.signs + static_cast<int64_t>(it.row) * a.nbins;
   roll_windows<kRc>(a.codes, s, e, it.k, tab, [&](uint64_t h) {
-    const uint32_t q = bin_of(mod_sign(h), a.binsize, a.magic);
-    if (q < a.bin_lo || q >= a.bin_hi) return;
-    if (h == kEmptyKey) {
-      atomicAdd(a.max_key_count, 1u);
-      return;
-    }
-    uint64_t slot = table_slot(h, a.table_mask);
-    for (uint64_t probe = 0; probe <= a.table_mask; ++probe) {
-      TableSlot *t = a.table + slot;
-      unsigned long long cur = t->key;
-      if (cur == kEmptyKey) {
-        cur = atomicCAS(&t->key, kEmptyKey, static_cast<unsigned long long>(h));
-        if (cur == kEmptyKey) cur = h;
-      }
-      if (cur == h) {
-        atomicAdd(&t->count, 1u);
-        return;
-      }
-      slot = (slot + 1) & a.table_mask;
-    }
-    atomicOr(&a.status->error, kErrTable);   // table full (sized at twice the windows: not reached)
-  });
-}
-
-// Hashes counted at least min_count times enter the bins of `row`.
-__global__ void table_bins_kernel(SketchArgs a, int row_index, unsigned min_count) {
-  unsigned long long *row = a.signs + static_cast<int64_t>(row_index) * a.nbins;
-  const uint64_t n = a.table_mask + 1;
-  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n; i += stride) {
-    const TableSlot t = a.table[i];
-    const unsigned long long h = t.key;
-    if (h == kEmptyKey || t.count < min_count) continue;
     const uint64_t sign = mod_sign(h);
     const uint32_t q = bin_of(sign, a.binsize, a.magic);
-    if (sign < row[q]) atomicMin(row + q, static_cast<unsigned long long>(sign));
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0 && *a.max_key_count >= min_count && *a.max_key_count > 0) {
-    const uint64_t sign = mod_sign(kEmptyKey);
-    const uint32_t q = bin_of(sign, a.binsize, a.magic);
-    atomicMin(row + q, static_cast<unsigned long long>(sign));
-  }
+    if (q < a.bin_lo || q >= a.bin_hi) return;
+    unsigned int old = 0;
+    if (h == kEmptyKey) {
+      old = atomicAdd(a.max_key_count, 1u);
+    } else {
+      uint64_t slot = table_slot(h, a.table_mask);
+      uint64_t probe = 0;
+      for (; probe <= a.table_mask; ++probe) {
+        TableSlot *t = a.table + slot;
+        unsigned long long cur = t->key;
+        if (cur == kEmptyKey) {
+          cur = atomicCAS(&t->key, kEmptyKey, static_cast<unsigned long long>(h));
+          if (cur == kEmptyKey) cur = h;
+        }
+        if (cur == h) {
+          old = atomicAdd(&t->count, 1u);
+          break;
+        }
+        slot = (slot + 1) & a.table_mask;
+      }
+      if (probe > a.table_mask) {
+        atomicOr(&a.status->error, kErrTable);   // table full (sized at twice the windows: not reached)
+        return;
+      }
+    }
+    if (old + 1 == a.min_count && sign < row[q]) atomicMin(row + q, static_cast<unsigned long long>(sign));
+  });
 }
 
 __device__ __forceinline__ uint64_t univhash(uint64_t s, uint64_t t) {
@@ -696,8 +688,8 @@ uint64_t next_pow2(uint64_t v) {
 
 // Bins rows of one batch with the exact count filter: per sample and k, the
 // hashes are counted in a table of twice the sample's windows (in bin-range
-// passes when that exceeds the table budget), then the ones counted
-// min_count times enter the bins.  The counting items are an eighth of the
+// passes when that exceeds the table budget), a hash entering its bin when
+// its count reaches min_count.  The counting items are an eighth of the
 // hashing ones (no per-CTA bins to amortise; more CTAs in flight hide the
 // table's memory latency).
 constexpr int64_t kCountItemWindows = kItemWindows / 8;
@@ -722,6 +714,7 @@ sk_status count_batch(SketchCall &c, const Batch &b, SketchArgs &args, std::vect
     args.table = static_cast<TableSlot *>(tk);
     args.max_key_count = reinterpret_cast<unsigned int *>(static_cast<char *>(tk) + slots * sizeof(TableSlot));
     args.table_mask = slots - 1;
+    args.min_count = static_cast<unsigned int>(c.min_count);
     for (int k = 0; k < K; ++k) {
       items.clear();
       make_items(c, b, s, s + 1, k, items, kCountItemWindows);
@@ -740,12 +733,6 @@ sk_status count_batch(SketchCall &c, const Batch &b, SketchArgs &args, std::vect
         if (e == cudaSuccess) {
           auto kern = c.use_rc ? count_kernel<true> : count_kernel<false>;
           kern<<<static_cast<unsigned>(items.size()), kSketchThreads, 0, ctx->stream>>>(args);
-          e = cudaGetLastError();
-        }
-        if (e == cudaSuccess) {
-          const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(4096, (slots + 255) / 256));
-          table_bins_kernel<<<grid, 256, 0, ctx->stream>>>(args, static_cast<int>((s - b.s0) * K + k),
-                                                           static_cast<unsigned>(c.min_count));
           e = cudaGetLastError();
         }
         if (e != cudaSuccess) return cuda_fail(ctx, e, "sketch counting");
