@@ -141,8 +141,8 @@ sk_status sk_ctx_set_semantics(sk_ctx *ctx, int32_t semantics);
  * into chunks (query_db_cuda, src/gpu/gpu_api.cpp:357-389); query-vs-reference
  * outputs are blocked the same way (the reference refuses them).  The same
  * limit bounds sk_sketch's k-mer count table for read sets: a quarter of it
- * (default 2 GiB) per counting pass, more passes over bin ranges when a
- * sample's table would be larger. */
+ * (default: a quarter of the free memory less 2 GiB) per counting pass, more
+ * passes over bin ranges when a sample's table would be larger. */
 sk_status sk_ctx_set_memory_limit(sk_ctx *ctx, int64_t bytes);
 int32_t sk_tile_config_count(void);
 /* Describes shape `config_id`: rows x cols of the CTA tile and per-thread block. */

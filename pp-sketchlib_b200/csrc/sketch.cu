@@ -33,6 +33,7 @@
 #include <algorithm>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "sk_runtime.h"
@@ -63,15 +64,11 @@ constexpr uint64_t kNtSeed[4] = {0x3c8bfbb395c60474ULL, 0x3193c18562a02b4cULL,
                                  0x20323ed082572324ULL, 0x295549f54be24456ULL};
 
 // ntHash's split rotation: the low 33 bits and the high 31 bits of the hash
-// rotate independently (src/sketch/nthash.hpp:17-55).
+// rotate independently (src/sketch/nthash.hpp:17-55); used on the host to
+// build the rolling tables.
 __host__ __device__ __forceinline__ uint64_t srol1(uint64_t v) {
   const uint64_t lo = v & kLo33, hi = v & ~kLo33;
   return (((lo << 1) | (lo >> 32)) & kLo33) | ((hi << 1) & ~kLo33) | ((hi >> 30) & (1ULL << 33));
-}
-
-__host__ __device__ __forceinline__ uint64_t sror1(uint64_t v) {
-  const uint64_t lo = v & kLo33, hi = v & ~kLo33;
-  return (((lo >> 1) | (lo << 32)) & kLo33) | ((hi >> 1) & ~kLo33) | ((hi << 30) & (1ULL << 63));
 }
 
 // The same rotations on the two 32-bit halves of the hash: low word L holds
@@ -209,6 +206,13 @@ __global__ void densified_kernel(const int8_t *__restrict__ rows, int64_t n, int
 // the first k positions, where a leaving position before the range start
 // contributes nothing.  kRange: some windows ending in the chunk start outside
 // [lo, hi).  kRc: canonical hashes (the reverse strand is rolled too).
+// An emitter with a kBatch member takes the hashes of kBatch steps at a time
+// (put, then flush): its table probes can then be issued together.
+template <typename T, typename = void>
+struct is_batched : std::false_type {};
+template <typename T>
+struct is_batched<T, std::void_t<decltype(T::kBatch)>> : std::true_type {};
+
 template <bool kMask, bool kRange, bool kRc, typename Emit>
 __device__ __forceinline__ void roll_chunk(const uint4 &in, const uint4 &oa, const uint4 &ob, int D,
                                            int sh, int p0, int k, int lo, int hi,
@@ -236,7 +240,13 @@ __device__ __forceinline__ void roll_chunk(const uint4 &in, const uint4 &oa, con
     if (kRc) rh = sror1_w(rh ^ v.y);
     run = (ci & 7) == kCodeInvalid ? 0 : ((ci & kCodeStart) ? 1 : min(run + 1, k));
     const int w = p - k + 1;   // start of the window ending at p
-    if (run >= k && (!kRange || (w >= lo && w < hi))) emit(kRc && rh < fh ? rh : fh);
+    const bool valid = run >= k && (!kRange || (w >= lo && w < hi));
+    if constexpr (is_batched<Emit>::value) {
+      emit.put(i % Emit::kBatch, kRc && rh < fh ? rh : fh, valid);
+      if (i % Emit::kBatch == Emit::kBatch - 1) emit.flush();
+    } else {
+      if (valid) emit(kRc && rh < fh ? rh : fh);
+    }
   }
 }
 
@@ -362,12 +372,77 @@ __device__ __forceinline__ uint64_t table_slot(uint64_t h, uint64_t mask) {
   return h & mask;
 }
 
-// Counting pass: every hash whose bin lies in [bin_lo, bin_hi) is counted,
-// and the insertion that brings a hash's count to min_count puts it in its
-// bin (the reference's counter adds a k-mer at the occurrence whose count
-// reaches min_count, src/sketch/sketch.cpp:143-148).
+// The counting pass's emitter: 8 hashes at a time, their first table slots
+// loaded together so that 8 independent memory requests per thread are in
+// flight, then each insertion resolved (probe, compare-and-swap, count).  The
+// insertion that brings a hash's count to min_count puts it in its bin (the
+// reference's counter adds a k-mer at the occurrence whose count reaches
+// min_count, src/sketch/sketch.cpp:143-148).
+struct CountBatch {
+  static constexpr int kBatch = 8;
+  const SketchArgs &a;
+  unsigned long long *row;
+  uint64_t h[kBatch];
+  bool v[kBatch];
+
+  __device__ __forceinline__ void put(int i, uint64_t hash, bool valid) {
+    h[i] = hash;
+    v[i] = valid;
+  }
+
+  __device__ __forceinline__ void insert(uint64_t hh, uint64_t slot, unsigned long long cur) {
+    unsigned int old = 0;
+    if (hh == kEmptyKey) {
+      old = atomicAdd(a.max_key_count, 1u);
+    } else {
+      uint64_t probe = 0;
+      for (; probe <= a.table_mask; ++probe) {
+        TableSlot *t = a.table + slot;
+        if (probe > 0) cur = t->key;
+        if (cur == kEmptyKey) {
+          cur = atomicCAS(&t->key, kEmptyKey, static_cast<unsigned long long>(hh));
+          if (cur == kEmptyKey) cur = hh;
+        }
+        if (cur == hh) {
+          old = atomicAdd(&t->count, 1u);
+          break;
+        }
+        slot = (slot + 1) & a.table_mask;
+      }
+      if (probe > a.table_mask) {
+        atomicOr(&a.status->error, kErrTable);   // table full (sized at twice the windows: not reached)
+        return;
+      }
+    }
+    if (old + 1 == a.min_count) {
+      const uint64_t sign = mod_sign(hh);
+      const uint32_t q = bin_of(sign, a.binsize, a.magic);
+      if (sign < row[q]) atomicMin(row + q, static_cast<unsigned long long>(sign));
+    }
+  }
+
+  __device__ __forceinline__ void flush() {
+    uint64_t slot[kBatch];
+    unsigned long long cur[kBatch];
+#pragma unroll
+    for (int j = 0; j < kBatch; ++j) {
+      if (v[j]) {   // the pass's bin range
+        const uint32_t q = bin_of(mod_sign(h[j]), a.binsize, a.magic);
+        v[j] = q >= a.bin_lo && q < a.bin_hi;
+      }
+      slot[j] = table_slot(h[j], a.table_mask);
+    }
+#pragma unroll
+    for (int j = 0; j < kBatch; ++j) cur[j] = v[j] && h[j] != kEmptyKey ? a.table[slot[j]].key : kEmptyKey;
+#pragma unroll
+    for (int j = 0; j < kBatch; ++j)
+      if (v[j]) insert(h[j], slot[j], cur[j]);
+  }
+};
+
+// Counting pass: every hash whose bin lies in [bin_lo, bin_hi) is counted.
 template <bool kRc>
-__global__ void __launch_bounds__(kSketchThreads)
+__global__ void __launch_bounds__(kSketchThreads, 1)
 count_kernel(SketchArgs a) {
   __shared__ RollTable tab;
   const SketchItem it = a.items[blockIdx.x];
@@ -379,37 +454,8 @@ count_kernel(SketchArgs a) {
   const int64_t s = it.begin + static_cast<int64_t>(threadIdx.x) * it.per;
   const int64_t e = min(s + it.per, it.end);
   if (s >= e) return;
-  unsigned long long *row = a.signs + static_cast<int64_t>(it.row) * a.nbins;
-  roll_windows<kRc>(a.codes, s, e, it.k, tab, [&](uint64_t h) {
-    const uint64_t sign = mod_sign(h);
-    const uint32_t q = bin_of(sign, a.binsize, a.magic);
-    if (q < a.bin_lo || q >= a.bin_hi) return;
-    unsigned int old = 0;
-    if (h == kEmptyKey) {
-      old = atomicAdd(a.max_key_count, 1u);
-    } else {
-      uint64_t slot = table_slot(h, a.table_mask);
-      uint64_t probe = 0;
-      for (; probe <= a.table_mask; ++probe) {
-        TableSlot *t = a.table + slot;
-        unsigned long long cur = t->key;
-        if (cur == kEmptyKey) {
-          cur = atomicCAS(&t->key, kEmptyKey, static_cast<unsigned long long>(h));
-          if (cur == kEmptyKey) cur = h;
-        }
-        if (cur == h) {
-          old = atomicAdd(&t->count, 1u);
-          break;
-        }
-        slot = (slot + 1) & a.table_mask;
-      }
-      if (probe > a.table_mask) {
-        atomicOr(&a.status->error, kErrTable);   // table full (sized at twice the windows: not reached)
-        return;
-      }
-    }
-    if (old + 1 == a.min_count && sign < row[q]) atomicMin(row + q, static_cast<unsigned long long>(sign));
-  });
+  CountBatch emit{a, a.signs + static_cast<int64_t>(it.row) * a.nbins, {}, {}};
+  roll_windows<kRc>(a.codes, s, e, it.k, tab, emit);
 }
 
 __device__ __forceinline__ uint64_t univhash(uint64_t s, uint64_t t) {
@@ -697,11 +743,16 @@ constexpr int64_t kCountItemWindows = kItemWindows / 8;
 sk_status count_batch(SketchCall &c, const Batch &b, SketchArgs &args, std::vector<SketchItem> &items) {
   sk_ctx *ctx = c.ctx;
   const int K = static_cast<int>(c.kmers.size());
-  // bytes of keys + counts per pass: a quarter of the context's memory limit
-  // when one is set, else 2 GiB
-  const uint64_t kTableBudget =
-      ctx->mem_limit > 0 ? std::max<uint64_t>(1ULL << 16, static_cast<uint64_t>(ctx->mem_limit) / 4)
-                         : (1ULL << 31);
+  // bytes of table per pass: a quarter of the context's memory limit when one
+  // is set, else a quarter of the free device memory less 2 GiB (at least 1 GiB)
+  uint64_t kTableBudget = 0;
+  if (ctx->mem_limit > 0) {
+    kTableBudget = std::max<uint64_t>(1ULL << 16, static_cast<uint64_t>(ctx->mem_limit) / 4);
+  } else {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = 0;
+    kTableBudget = std::max<uint64_t>(1ULL << 30, free_b > (2ULL << 30) ? (free_b - (2ULL << 30)) / 4 : 0);
+  }
   for (int64_t s = b.s0; s < b.s1; ++s) {
     const int64_t windows = c.seq_off[c.sample_seqs[s + 1]] - c.seq_off[c.sample_seqs[s]];
     if (windows <= 0) continue;
