@@ -440,6 +440,11 @@ sk_status sk_synth_device(sk_ctx *ctx, const int32_t *parent,
  * count-min filter is an approximation whose answer depends on read order
  * (and, in its GPU sketcher, on a data race); it is not reproduced.
  *
+ * codon_phased = 1 uses the reference's codon-phased spaced seeds
+ * (generate_seeds, src/sketch/sketch.cpp:30-61): for each k a window of 3k-2
+ * bases of which positions 0, 3, ..., 3(k-1) are hashed, every base of the
+ * window valid (the reference's GPU sketcher refuses these seeds).
+ *
  * Outputs (host): words [n_samples][n_kmers][sketchsize64 * 14] in the
  * reference layout; inv_minhash [n_samples][n_kmers] (bin 0's value over
  * 2^61-1 before densifying, whose per-sample sum gives the reference's read-set
@@ -447,8 +452,8 @@ sk_status sk_synth_device(sk_ctx *ctx, const int32_t *parent,
  * or NULL. */
 sk_status sk_sketch(sk_ctx *ctx, const char *bases, const int64_t *seq_offsets,
                     const int64_t *sample_seqs, int64_t n_samples, const int32_t *kmers,
-                    int32_t n_kmers, int32_t sketchsize64, int32_t use_rc, int32_t min_count,
-                    uint64_t *words, double *inv_minhash, uint8_t *densified);
+                    int32_t n_kmers, int32_t sketchsize64, int32_t use_rc, int32_t codon_phased,
+                    int32_t min_count, uint64_t *words, double *inv_minhash, uint8_t *densified);
 
 /* sk_sketch with the bases already in device memory (d_bases, not modified)
  * and device outputs: d_words [n_samples][n_kmers][sketchsize64 * 14],
@@ -459,8 +464,8 @@ sk_status sk_sketch(sk_ctx *ctx, const char *bases, const int64_t *seq_offsets,
 sk_status sk_sketch_device(sk_ctx *ctx, const char *d_bases, const int64_t *seq_offsets,
                            const int64_t *sample_seqs, int64_t n_samples, const int32_t *kmers,
                            int32_t n_kmers, int32_t sketchsize64, int32_t use_rc,
-                           int32_t min_count, uint64_t *d_words, double *d_inv_minhash,
-                           uint8_t *d_densified);
+                           int32_t codon_phased, int32_t min_count, uint64_t *d_words,
+                           double *d_inv_minhash, uint8_t *d_densified);
 
 /* ---- measurement ---------------------------------------------------------- */
 

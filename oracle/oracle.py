@@ -60,8 +60,8 @@ def _load():
     lib.sko_square_to_long.restype = None
     lib.sko_square_to_long.argtypes = [vp, i64, vp]
     lib.sko_sketch_samples.restype = None
-    lib.sko_sketch_samples.argtypes = [vp, vp, vp, i64, vp, i32, i32, i32, i32, i32, vp, vp, vp,
-                                       i32]
+    lib.sko_sketch_samples.argtypes = [vp, vp, vp, i64, vp, i32, i32, i32, i32, i32, i32, vp, vp,
+                                       vp, i32]
     return lib
 
 
@@ -259,10 +259,11 @@ def pack_samples(samples):
 
 
 def sketch(bases, seq_off, sample_seqs, kmers, s64, use_rc=True, min_count=0, threads=NTHREADS,
-           bbits=14):
+           bbits=14, codon_phased=False):
     """The oracle's sketcher (sko_sketch_samples): words [n][K][s64*bbits],
     inv_minhash [n][K], densified [n]; min_count > 0 keeps hashes seen that
-    many times (exact counting)."""
+    many times (exact counting); codon_phased uses the reference's spaced
+    seeds."""
     b = np.ascontiguousarray(bases, np.uint8)
     so = np.ascontiguousarray(seq_off, np.int64)
     ss = np.ascontiguousarray(sample_seqs, np.int64)
@@ -272,8 +273,8 @@ def sketch(bases, seq_off, sample_seqs, kmers, s64, use_rc=True, min_count=0, th
     inv = np.zeros((n, len(km)), np.float64)
     dens = np.zeros(n, np.uint8)
     lib.sko_sketch_samples(b.ctypes.data, so.ctypes.data, ss.ctypes.data, n, km.ctypes.data,
-                           len(km), s64, bbits, int(use_rc), int(min_count), words.ctypes.data,
-                           inv.ctypes.data, dens.ctypes.data, threads)
+                           len(km), s64, bbits, int(use_rc), int(codon_phased), int(min_count),
+                           words.ctypes.data, inv.ctypes.data, dens.ctypes.data, threads)
     return words, inv, dens.astype(bool)
 
 
@@ -305,7 +306,7 @@ class RefSketcher:
                                     C.c_int64, C.c_void_p, C.c_void_p]
         lib_.ref_sketch_seqs.restype = None
         lib_.ref_sketch_seqs.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
-                                         C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                         C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
                                          C.c_void_p, C.c_void_p]
         self.lib = lib_
 
@@ -323,7 +324,8 @@ class RefSketcher:
         return out
 
 
-    def sketch_seqs(self, bases, seq_off, sample_seqs, kmers, s64, use_rc=True, threads=NTHREADS):
+    def sketch_seqs(self, bases, seq_off, sample_seqs, kmers, s64, use_rc=True, threads=NTHREADS,
+                    codon_phased=False):
         """The reference's sketch() over samples of several sequences:
         words [n][K][s64*14], inv_minhash [n][K], densified [n]."""
         b = np.ascontiguousarray(bases, np.uint8)
@@ -335,8 +337,8 @@ class RefSketcher:
         inv = np.zeros((n, len(km)), np.float64)
         dens = np.zeros(n, np.uint8)
         self.lib.ref_sketch_seqs(b.ctypes.data, so.ctypes.data, ss.ctypes.data, n, km.ctypes.data,
-                                 len(km), s64, int(use_rc), threads, words.ctypes.data,
-                                 inv.ctypes.data, dens.ctypes.data)
+                                 len(km), s64, int(use_rc), int(codon_phased), threads,
+                                 words.ctypes.data, inv.ctypes.data, dens.ctypes.data)
         return words, inv, dens.astype(bool)
 
 

@@ -102,11 +102,12 @@ int ref_sketch_genomes(const char *seqs, int n, int64_t length, const int32_t *k
 // inv_minhash [n][K] (bin 0 over 2^61-1 before densifying) and densified [n]
 // (any k densified).  The sequences go in as given (no case change, no length
 // filter): the reference's SeqBuf(std::vector<std::string>) constructor.
+// codon_phased selects the reference's spaced seeds (generate_seeds).
 void ref_sketch_seqs(const char *bases, const int64_t *seq_off, const int64_t *sample_seqs, int n,
-                     const int32_t *kmers, int K, int sketchsize64, int use_rc, int threads,
-                     uint64_t *out, double *inv_minhash, uint8_t *densified) {
+                     const int32_t *kmers, int K, int sketchsize64, int use_rc, int codon_phased,
+                     int threads, uint64_t *out, double *inv_minhash, uint8_t *densified) {
   std::vector<size_t> kl(kmers, kmers + K);
-  const KmerSeeds seeds = generate_seeds(kl, false);
+  const KmerSeeds seeds = generate_seeds(kl, codon_phased != 0);
   const int64_t W = static_cast<int64_t>(sketchsize64) * 14;
 #pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
   for (int s = 0; s < n; ++s) {
@@ -116,8 +117,8 @@ void ref_sketch_seqs(const char *bases, const int64_t *seq_off, const int64_t *s
     SeqBuf buf(seqs);
     bool any = false;
     for (int k = 0; k < K; ++k) {
-      auto res = sketch(buf, static_cast<uint64_t>(sketchsize64), seeds.at(kl[k]), 14, false,
-                        use_rc != 0, 0, false);
+      auto res = sketch(buf, static_cast<uint64_t>(sketchsize64), seeds.at(kl[k]), 14,
+                        codon_phased != 0, use_rc != 0, 0, false);
       std::memcpy(out + (static_cast<int64_t>(s) * K + k) * W, std::get<0>(res).data(), W * 8);
       inv_minhash[static_cast<int64_t>(s) * K + k] = std::get<1>(res);
       any = any || std::get<2>(res);

@@ -407,9 +407,25 @@ static void sko_binsign(uint64_t *signs, uint64_t h, uint64_t binsize) {
  * sample enter the bins -- the reference's exact counter (HashCounter,
  * src/sketch/countmin.cpp:55-72, counting full 64-bit hash values; its uint8
  * saturation at 255 never changes the answer for min_count <= 255). */
+/* Codon-phased spaced-seed hash of the window at s (generate_seeds,
+ * src/sketch/sketch.cpp:30-61: k kept positions 0, 3, ..., 3(k-1) of a
+ * window of 3k-2 bases; NTMSMC64 / NTMSM64, src/sketch/nthash.hpp:553-722:
+ * the dense hash with the masked positions' terms XORed out, i.e. the XOR of
+ * the kept positions' terms).  Every base of the window must be valid. */
+static uint64_t sko_phased_hash(const unsigned char *s, int k, int use_rc) {
+  const int kw = 3 * k - 2;
+  uint64_t fs = 0, rs = 0;
+  for (int m = 0; m < k; m++) {
+    const int i = 3 * m, c = sko_base(s[i]);
+    fs ^= sko_srol(kNtSeed[c], (unsigned)(kw - 1 - i));
+    rs ^= sko_srol(kNtSeed[3 - c], (unsigned)i);
+  }
+  return (use_rc && rs < fs) ? rs : fs;
+}
+
 int sko_sketch(const char *bases, const int64_t *seq_off, int64_t first, int64_t last, int k,
-               int s64, int bbits, int use_rc, int min_count, uint64_t *signs, uint64_t *words,
-               double *inv_minhash) {
+               int s64, int bbits, int use_rc, int codon_phased, int min_count, uint64_t *signs,
+               uint64_t *words, double *inv_minhash) {
   const uint64_t nbins = (uint64_t)s64 * 64;
   const uint64_t binsize = (SKO_SIGN_MOD + nbins - 1) / nbins;
   uint64_t rk[4];
@@ -418,7 +434,20 @@ int sko_sketch(const char *bases, const int64_t *seq_off, int64_t first, int64_t
   if (min_count > 0) hashes = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)(seq_off[last] - seq_off[first] + 1));
   for (int c = 0; c < 4; c++) rk[c] = sko_srol(kNtSeed[c], (unsigned)k);
   for (uint64_t b = 0; b < nbins; b++) signs[b] = UINT64_MAX;
-  for (int64_t sq = first; sq < last; sq++) {
+  for (int64_t sq = first; sq < last && codon_phased; sq++) {   /* spaced seeds */
+    const unsigned char *s = (const unsigned char *)bases + seq_off[sq];
+    const int64_t len = seq_off[sq + 1] - seq_off[sq], kw = 3 * (int64_t)k - 2;
+    int64_t run = 0;
+    for (int64_t p = 0; p < len; p++) {
+      run = sko_base(s[p]) < 0 ? 0 : run + 1;
+      if (run >= kw) {
+        const uint64_t h = sko_phased_hash(s + p - kw + 1, k, use_rc);
+        if (hashes) hashes[n_hashes++] = h;
+        else sko_binsign(signs, h, binsize);
+      }
+    }
+  }
+  for (int64_t sq = first; sq < last && !codon_phased; sq++) {
     const unsigned char *s = (const unsigned char *)bases + seq_off[sq];
     const int64_t len = seq_off[sq + 1] - seq_off[sq];
     uint64_t fh = 0, rh = 0;
@@ -489,8 +518,8 @@ int sko_sketch(const char *bases, const int64_t *seq_off, int64_t first, int64_t
  * inv_minhash [n][K], densified [n] (any k with a nonzero densify result). */
 void sko_sketch_samples(const char *bases, const int64_t *seq_off, const int64_t *sample_seqs,
                         int64_t n, const int *kmers, int K, int s64, int bbits, int use_rc,
-                        int min_count, uint64_t *words, double *inv_minhash, uint8_t *densified,
-                        int threads) {
+                        int codon_phased, int min_count, uint64_t *words, double *inv_minhash,
+                        uint8_t *densified, int threads) {
   const int64_t W = (int64_t)s64 * bbits;
 #pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
   for (int64_t s = 0; s < n; s++) {
@@ -498,7 +527,8 @@ void sko_sketch_samples(const char *bases, const int64_t *seq_off, const int64_t
     uint8_t any = 0;
     for (int k = 0; k < K; k++) {
       const int d = sko_sketch(bases, seq_off, sample_seqs[s], sample_seqs[s + 1], kmers[k], s64,
-                               bbits, use_rc, min_count, signs, words + (s * K + k) * W,
+                               bbits, use_rc, codon_phased, min_count, signs,
+                               words + (s * K + k) * W,
                                inv_minhash ? inv_minhash + s * K + k : NULL);
       if (d != 0) any = 1;
     }

@@ -17,8 +17,7 @@
 //   * constructDatabase sketches on the GPU (sk_sketch) and writes the
 //     database with the built-in HDF5 writer (host_h5_write.cpp); it computes
 //     no Monte Carlo random-match table (calc_random only prints a note), and
-//     a read filter (min_count) counts k-mers exactly; codon-phased seeds
-//     raise, as in the reference's GPU sketcher.  addRandom raises
+//     a read filter (min_count) counts k-mers exactly.  addRandom raises
 //     NotImplementedError.
 #include <pybind11/numpy.h>
 #include <pybind11/pybind11.h>
@@ -458,7 +457,6 @@ void constructDatabase(const std::string &db_name, const std::vector<std::string
                        const bool codon_phased, const bool calc_random, const bool use_rc,
                        size_t min_count, const bool exact, const size_t num_threads,
                        const bool /*use_gpu*/, const int device_id) {
-  if (codon_phased) throw std::runtime_error("Codon phased seeds not yet implemented for GPU sketching");
   if (names.size() != files.size()) throw std::runtime_error("Sample names and file lists differ in length");
   if (kmer_lengths.empty()) throw std::runtime_error("No k-mer lengths given");
   const std::string path = db_name + ".h5";
@@ -547,8 +545,8 @@ void constructDatabase(const std::string &db_name, const std::vector<std::string
       const int32_t mc = pass == 1 ? static_cast<int32_t>(min_count) : 0;
       run_gpu(ctx, [&] {
         return sk_sketch(ctx, bases.data(), off.data(), first.data(), static_cast<int64_t>(idx.size()),
-                         kmers.data(), static_cast<int32_t>(K), s64, use_rc ? 1 : 0, mc, w.data(),
-                         inv.data(), dens.data());
+                         kmers.data(), static_cast<int32_t>(K), s64, use_rc ? 1 : 0,
+                         codon_phased ? 1 : 0, mc, w.data(), inv.data(), dens.data());
       });
       for (size_t j = 0; j < idx.size(); ++j) {
         const size_t i = idx[j];
@@ -572,7 +570,7 @@ void constructDatabase(const std::string &db_name, const std::vector<std::string
     start = end;
   }
   std::cerr << "Writing sketches to file" << std::endl;
-  save_sketch_db(path, info, words, kmers, s64, use_rc, false);
+  save_sketch_db(path, info, words, kmers, s64, use_rc, codon_phased);
   for (const SampleInfo &si : info)
     if (si.densified) std::cerr << "NOTE: " << si.name << " required densification" << std::endl;
   if (calc_random) {

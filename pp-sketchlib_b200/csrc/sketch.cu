@@ -23,6 +23,10 @@
 //   finishing  one CTA per (sample, k) records bin 0 (inverse_minhash), fills
 //              empty bins in the reference's order and writes the bit planes
 //              with warp ballots.
+//   phased     codon-phased spaced seeds (k bases at positions 0, 3, ...,
+//              3(k-1) of a 3k-2 window) are a rolling hash along each of the
+//              three phase subsequences: three states rotate, each stepping
+//              by a split rotation of three with the base 3k back leaving.
 //   counting   with min_count > 0 (read sets), hashes are counted in a device
 //              hash table and the insertion that brings a hash's count to
 //              min_count enters it in its bin: the reference's exact counter
@@ -53,8 +57,10 @@ constexpr int kMinK = 3;                           // generate_seeds (src/sketch
 constexpr int kMaxK = 255;
 constexpr unsigned long long kEmptyKey = ~0ULL;
 // Invalid codes before and after a batch's bases: the roll reads up to
-// 16 * ceil(k / 16) bytes before a range and k + 31 bytes after it.
-constexpr int64_t kCodePad = 512;
+// 16 * ceil(k_out / 16) bytes before a range and its window length + 31
+// bytes after it (k_out and the window length are 3k and 3k - 2 for
+// codon-phased seeds, k <= 255).
+constexpr int64_t kCodePad = 1024;
 constexpr unsigned kErrDensify = 4u;               // DevStatus.error bits of the sketcher
 constexpr unsigned kErrTable = 8u;
 
@@ -90,6 +96,17 @@ __device__ __forceinline__ uint64_t sror1_w(uint64_t v) {
   return (static_cast<uint64_t>(hi) << 32) | lo;
 }
 
+// Split rotation by three positions (one step of a codon phase).
+__device__ __forceinline__ uint64_t srol3(uint64_t v) {
+  const uint64_t lo = v & kLo33, hi = v >> 33;
+  return ((((hi << 3) | (hi >> 28)) & 0x7FFFFFFFULL) << 33) | (((lo << 3) | (lo >> 30)) & kLo33);
+}
+
+__device__ __forceinline__ uint64_t sror3(uint64_t v) {
+  const uint64_t lo = v & kLo33, hi = v >> 33;
+  return ((((hi >> 3) | (hi << 28)) & 0x7FFFFFFFULL) << 33) | (((lo >> 3) | (lo << 30)) & kLo33);
+}
+
 uint64_t srol_n(uint64_t v, unsigned n) {
   for (unsigned i = 0; i < n % (33ULL * 31ULL); ++i) v = srol1(v);
   return v;
@@ -104,19 +121,22 @@ struct SketchItem {
 };
 
 // Rolling table of one k, indexed by (entering base | leaving base << 3):
-// the XOR of seed[in] and srol^k(seed[out]) for the forward hash and of
-// srol^k(seed[3-in]) and seed[3-out] for the reverse one; a code of 4 (not a
-// base) contributes zero.
+// the XOR of seed[in] and srol^n(seed[out]) for the forward hash and of
+// srol^n(seed[3-in]) and seed[3-out] for the reverse one, n = k (dense
+// seeds) or 3k (codon-phased seeds: the hash of one phase's subsequence
+// rolls three positions per step); a code of 4 (not a base) contributes
+// zero.
 struct RollTable {
   ulonglong2 v[64];
 };
 
-RollTable make_table(int k) {
+RollTable make_table(int k, bool phased) {
+  const unsigned n = static_cast<unsigned>(phased ? 3 * k : k);
   uint64_t fin[8] = {}, rin[8] = {}, fout[8] = {}, rout[8] = {};
   for (int c = 0; c < 4; ++c) {
     fin[c] = kNtSeed[c];
-    rin[c] = srol_n(kNtSeed[3 - c], k);
-    fout[c] = srol_n(kNtSeed[c], k);
+    rin[c] = srol_n(kNtSeed[3 - c], n);
+    fout[c] = srol_n(kNtSeed[c], n);
     rout[c] = kNtSeed[3 - c];
   }
   RollTable t{};
@@ -199,13 +219,6 @@ __global__ void densified_kernel(const int8_t *__restrict__ rows, int64_t n, int
   out[s] = any;
 }
 
-// Sixteen roll steps over one aligned chunk of codes.  `in` holds the bases
-// entering at relative positions p0 .. p0+15; the bases leaving (k earlier)
-// are bytes d .. d+15 of the 32-byte pair (oa, ob), d = (-k) mod 16, picked
-// with a uniform word select and funnel shift.  kMask: the chunk lies within
-// the first k positions, where a leaving position before the range start
-// contributes nothing.  kRange: some windows ending in the chunk start outside
-// [lo, hi).  kRc: canonical hashes (the reverse strand is rolled too).
 // An emitter with a kBatch member takes the hashes of kBatch steps at a time
 // (put, then flush): its table probes can then be issued together.
 template <typename T, typename = void>
@@ -213,19 +226,36 @@ struct is_batched : std::false_type {};
 template <typename T>
 struct is_batched<T, std::void_t<decltype(T::kBatch)>> : std::true_type {};
 
-template <bool kMask, bool kRange, bool kRc, typename Emit>
-__device__ __forceinline__ void roll_chunk(const uint4 &in, const uint4 &oa, const uint4 &ob, int D,
-                                           int sh, int p0, int k, int lo, int hi,
-                                           const RollTable &t, uint64_t &fh, uint64_t &rh, int &run,
-                                           Emit &emit) {
-  const uint32_t X[8] = {oa.x, oa.y, oa.z, oa.w, ob.x, ob.y, ob.z, ob.w};
+// Rolling state: forward and reverse hashes (three of each, one per codon
+// phase, for spaced seeds), the count of bases since the last break, and the
+// loaded chunks.
+struct RollState {
+  uint64_t f[3], r[3];
+  int run;
+  uint4 oa, ob, in;
+};
+
+// Sixteen roll steps over one aligned chunk of codes.  `in` holds the bases
+// entering at relative positions p0 .. p0+15; the bases leaving (k_out
+// earlier) are bytes d .. d+15 of the 32-byte pair (oa, ob), d = (-k_out)
+// mod 16, picked with a uniform word select and funnel shift.  kMask: the
+// chunk lies within the first k_out positions, where a leaving position
+// before the range start contributes nothing.  kRange: some windows ending in
+// the chunk start outside [lo, hi).  kRc: canonical hashes (the reverse
+// strand is rolled too).  kPhased: codon-phased spaced seeds -- the state of
+// the current base's phase takes the step (rotation by three, k_out = 3k)
+// and the three states rotate; windows are k_win = 3k - 2 bases.
+template <bool kMask, bool kRange, bool kRc, bool kPhased, typename Emit>
+__device__ __forceinline__ void roll_chunk(int D, int sh, int p0, int k_out, int k_win, int lo, int hi,
+                                           const RollTable &t, RollState &st, Emit &emit) {
+  const uint32_t X[8] = {st.oa.x, st.oa.y, st.oa.z, st.oa.w, st.ob.x, st.ob.y, st.ob.z, st.ob.w};
   uint32_t Y[5];
 #pragma unroll
   for (int m = 0; m < 5; ++m) Y[m] = D == 0 ? X[m] : D == 1 ? X[m + 1] : D == 2 ? X[m + 2] : X[m + 3];
   uint32_t O[4];
 #pragma unroll
   for (int w = 0; w < 4; ++w) O[w] = __funnelshift_r(Y[w], Y[w + 1], sh);
-  const uint32_t I[4] = {in.x, in.y, in.z, in.w};
+  const uint32_t I[4] = {st.in.x, st.in.y, st.in.z, st.in.w};
   uint32_t IX[4];   // table indices of the 16 steps, four per word
 #pragma unroll
   for (int w = 0; w < 4; ++w) IX[w] = (I[w] & 0x07070707u) | ((O[w] & 0x07070707u) << 3);
@@ -234,67 +264,76 @@ __device__ __forceinline__ void roll_chunk(const uint4 &in, const uint4 &oa, con
     const uint32_t ci = (I[i >> 2] >> (8 * (i & 3))) & 0xFF;
     uint32_t idx = (IX[i >> 2] >> (8 * (i & 3))) & 0x3F;
     const int p = p0 + i;
-    if (kMask && p < k) idx = (idx & 7) | (kCodeInvalid << 3);
+    if (kMask && p < k_out) idx = (idx & 7) | (kCodeInvalid << 3);
     const ulonglong2 v = t.v[idx];
-    fh = srol1_w(fh) ^ v.x;
-    if (kRc) rh = sror1_w(rh ^ v.y);
-    run = (ci & 7) == kCodeInvalid ? 0 : ((ci & kCodeStart) ? 1 : min(run + 1, k));
-    const int w = p - k + 1;   // start of the window ending at p
-    const bool valid = run >= k && (!kRange || (w >= lo && w < hi));
+    uint64_t hf, hr = 0;
+    if (!kPhased) {
+      st.f[0] = hf = srol1_w(st.f[0]) ^ v.x;
+      if (kRc) st.r[0] = hr = sror1_w(st.r[0] ^ v.y);
+    } else {
+      hf = srol3(st.f[0]) ^ v.x;
+      st.f[0] = st.f[1];
+      st.f[1] = st.f[2];
+      st.f[2] = hf;
+      if (kRc) {
+        hr = sror3(st.r[0] ^ v.y);
+        st.r[0] = st.r[1];
+        st.r[1] = st.r[2];
+        st.r[2] = hr;
+      }
+    }
+    st.run = (ci & 7) == kCodeInvalid ? 0 : ((ci & kCodeStart) ? 1 : min(st.run + 1, k_win));
+    const int w = p - k_win + 1;   // start of the window ending at p
+    const bool valid = st.run >= k_win && (!kRange || (w >= lo && w < hi));
     if constexpr (is_batched<Emit>::value) {
-      emit.put(i % Emit::kBatch, kRc && rh < fh ? rh : fh, valid);
+      emit.put(i % Emit::kBatch, kRc && hr < hf ? hr : hf, valid);
       if (i % Emit::kBatch == Emit::kBatch - 1) emit.flush();
     } else {
-      if (valid) emit(kRc && rh < fh ? rh : fh);
+      if (valid) emit(kRc && hr < hf ? hr : hf);
     }
   }
 }
 
-struct RollState {
-  uint64_t fh, rh;
-  int run;
-  uint4 oa, ob, in;
-};
-
 // Chunks j0 .. j1-1 of a range, each chunk's loads issued one chunk ahead.
-template <bool kMask, bool kRange, bool kRc, typename Emit>
+template <bool kMask, bool kRange, bool kRc, bool kPhased, typename Emit>
 __device__ __forceinline__ void roll_span(const uint4 *base, int j0, int j1, int c, int D, int sh,
-                                          int k, int lo, int hi, const RollTable &t, RollState &st,
-                                          Emit &emit) {
+                                          int k_out, int k_win, int lo, int hi, const RollTable &t,
+                                          RollState &st, Emit &emit) {
   for (int j = j0; j < j1; ++j) {
     const uint4 in_n = base[j + 1], ob_n = base[j + 2 - c];
-    roll_chunk<kMask, kRange, kRc>(st.in, st.oa, st.ob, D, sh, 16 * j, k, lo, hi, t, st.fh, st.rh,
-                                   st.run, emit);
+    roll_chunk<kMask, kRange, kRc, kPhased>(D, sh, 16 * j, k_out, k_win, lo, hi, t, st, emit);
     st.oa = st.ob;
     st.ob = ob_n;
     st.in = in_n;
   }
 }
 
-// Calls emit(hash) for every window of k bases inside one sequence whose
-// start lies in [s, e).  Rolls from s rounded down to 16 with a zero state (a
-// non-base contributes zero, so the state after k positions is the window's
-// hash whatever came before); reads the 16-byte chunks of codes from 16 * c
-// bytes before that through e + k + 31 (the code buffer's pads cover both).
-// Chunks whose windows all start inside [s, e) skip the range test.
-template <bool kRc, typename Emit>
+// Calls emit(hash) for every window of k bases (3k - 2 for codon-phased
+// seeds) inside one sequence whose start lies in [s, e).  Rolls from s
+// rounded down to 16 with a zero state (a non-base contributes zero, so the
+// state after k_out positions is the window's hash whatever came before);
+// reads the 16-byte chunks of codes from 16 * c bytes before that through
+// e + k_win + 31 (the code buffer's pads cover both).  Chunks whose windows
+// all start inside [s, e) skip the range test.
+template <bool kRc, bool kPhased, typename Emit>
 __device__ __forceinline__ void roll_windows(const uint8_t *__restrict__ codes, int64_t s, int64_t e,
                                              int k, const RollTable &t, Emit emit) {
+  const int k_out = kPhased ? 3 * k : k, k_win = kPhased ? 3 * k - 2 : k;
   const int64_t s0 = s & ~static_cast<int64_t>(15);
   const int lo = static_cast<int>(s - s0), hi = static_cast<int>(e - s0);
-  const int n_chunks = (hi + k - 1 + 15) >> 4;
-  const int d = (-k) & 15, D = d >> 2, sh = 8 * (d & 3);
-  const int c = (k + d) >> 4;            // the leaving bytes start in chunk j - c
+  const int n_chunks = (hi + k_win - 1 + 15) >> 4;
+  const int d = (-k_out) & 15, D = d >> 2, sh = 8 * (d & 3);
+  const int c = (k_out + d) >> 4;        // the leaving bytes start in chunk j - c
   const uint4 *base = reinterpret_cast<const uint4 *>(codes + s0);
-  RollState st{0, 0, 0, base[-c], base[1 - c], base[0]};
+  RollState st{{0, 0, 0}, {0, 0, 0}, 0, base[-c], base[1 - c], base[0]};
   const int masked = min(n_chunks, c);
-  // chunk j ends windows starting at 16j - k + 1 .. 16j + 16 - k
-  const int inner0 = max(masked, (lo + k - 1 + 15) >> 4);
-  const int inner1 = max(inner0, min(n_chunks, (hi + k - 1) >> 4));
-  roll_span<true, true, kRc>(base, 0, masked, c, D, sh, k, lo, hi, t, st, emit);
-  roll_span<false, true, kRc>(base, masked, inner0, c, D, sh, k, lo, hi, t, st, emit);
-  roll_span<false, false, kRc>(base, inner0, inner1, c, D, sh, k, lo, hi, t, st, emit);
-  roll_span<false, true, kRc>(base, inner1, n_chunks, c, D, sh, k, lo, hi, t, st, emit);
+  // chunk j ends windows starting at 16j - k_win + 1 .. 16j + 16 - k_win
+  const int inner0 = max(masked, (lo + k_win - 1 + 15) >> 4);
+  const int inner1 = max(inner0, min(n_chunks, (hi + k_win - 1) >> 4));
+  roll_span<true, true, kRc, kPhased>(base, 0, masked, c, D, sh, k_out, k_win, lo, hi, t, st, emit);
+  roll_span<false, true, kRc, kPhased>(base, masked, inner0, c, D, sh, k_out, k_win, lo, hi, t, st, emit);
+  roll_span<false, false, kRc, kPhased>(base, inner0, inner1, c, D, sh, k_out, k_win, lo, hi, t, st, emit);
+  roll_span<false, true, kRc, kPhased>(base, inner1, n_chunks, c, D, sh, k_out, k_win, lo, hi, t, st, emit);
 }
 
 // One slot of the k-mer count table: key and count share a 16-byte slot, so
@@ -331,7 +370,7 @@ struct SketchArgs {
 
 // Bin minima of one item; kShared keeps them in shared memory (nbins * 8
 // bytes of dynamic shared memory), else the CTA updates the global row.
-template <bool kShared, bool kRc>
+template <bool kShared, bool kRc, bool kPhased>
 __global__ void __launch_bounds__(kSketchThreads, 1)
 sketch_kernel(SketchArgs a) {
   extern __shared__ unsigned long long sh_bins[];
@@ -350,7 +389,7 @@ sketch_kernel(SketchArgs a) {
   const int64_t e = min(s + it.per, it.end);
   if (s < e) {
     const uint64_t binsize = a.binsize, magic = a.magic;
-    roll_windows<kRc>(a.codes, s, e, it.k, tab, [&](uint64_t h) {
+    roll_windows<kRc, kPhased>(a.codes, s, e, it.k, tab, [&](uint64_t h) {
       const uint64_t sign = mod_sign(h);
       const uint32_t q = bin_of(sign, binsize, magic);
       if (sign < bins[q]) atomicMin(bins + q, static_cast<unsigned long long>(sign));
@@ -441,7 +480,7 @@ struct CountBatch {
 };
 
 // Counting pass: every hash whose bin lies in [bin_lo, bin_hi) is counted.
-template <bool kRc>
+template <bool kRc, bool kPhased>
 __global__ void __launch_bounds__(kSketchThreads, 1)
 count_kernel(SketchArgs a) {
   __shared__ RollTable tab;
@@ -455,7 +494,7 @@ count_kernel(SketchArgs a) {
   const int64_t e = min(s + it.per, it.end);
   if (s >= e) return;
   CountBatch emit{a, a.signs + static_cast<int64_t>(it.row) * a.nbins, {}, {}};
-  roll_windows<kRc>(a.codes, s, e, it.k, tab, emit);
+  roll_windows<kRc, kPhased>(a.codes, s, e, it.k, tab, emit);
 }
 
 __device__ __forceinline__ uint64_t univhash(uint64_t s, uint64_t t) {
@@ -564,7 +603,7 @@ struct SketchCall {
   const int64_t *sample_seqs;
   int64_t n;
   std::vector<int32_t> kmers;
-  int s64, use_rc, min_count;
+  int s64, use_rc, codon_phased, min_count;
   int nbins;
   uint64_t binsize, magic;
   // device buffers (context scratch unless the caller gave them)
@@ -579,7 +618,7 @@ struct SketchCall {
 
 sk_status check_inputs(sk_ctx *ctx, const char *bases, const int64_t *seq_off,
                        const int64_t *sample_seqs, int64_t n, const int32_t *kmers, int32_t K,
-                       int32_t s64, int32_t use_rc, int32_t min_count) {
+                       int32_t s64, int32_t use_rc, int32_t codon_phased, int32_t min_count) {
   if (n < 0) return fail(ctx, SK_EINVAL, "negative sample count");
   if (n == 0) return SK_OK;
   if (!seq_off || !sample_seqs || !kmers) return fail(ctx, SK_EINVAL, "null argument");
@@ -591,6 +630,7 @@ sk_status check_inputs(sk_ctx *ctx, const char *bases, const int64_t *seq_off,
   if (s64 < 1 || s64 > kMaxSketch64)
     return fail(ctx, SK_ERANGE, "sketchsize64 %d outside [1, %d]", s64, kMaxSketch64);
   if (use_rc != 0 && use_rc != 1) return fail(ctx, SK_EINVAL, "use_rc must be 0 or 1");
+  if (codon_phased != 0 && codon_phased != 1) return fail(ctx, SK_EINVAL, "codon_phased must be 0 or 1");
   if (min_count < 0 || min_count > 255) return fail(ctx, SK_EINVAL, "min_count %d outside [0, 255]", min_count);
   if (sample_seqs[0] < 0) return fail(ctx, SK_EINVAL, "negative sequence index");
   for (int64_t s = 0; s < n; ++s)
@@ -671,7 +711,8 @@ void make_items(const SketchCall &c, const Batch &b, int64_t s0, int64_t s1, int
         SketchItem it{};
         it.begin = p;
         it.per = per;
-        it.end = std::min(p + step, e - c.kmers[k] + 1);
+        const int64_t window = c.codon_phased ? 3 * static_cast<int64_t>(c.kmers[k]) - 2 : c.kmers[k];
+        it.end = std::min(p + step, e - window + 1);
         if (it.end <= it.begin) continue;
         it.row = static_cast<int32_t>((s - b.s0) * K + k);
         it.k = c.kmers[k];
@@ -696,11 +737,13 @@ sk_status launch_hash(sk_ctx *ctx, const SketchCall &c, SketchArgs args, const S
   cudaError_t e = cudaSuccess;
   const unsigned grid = static_cast<unsigned>(n_items);
   if (shared) {
-    auto kern = c.use_rc ? sketch_kernel<true, true> : sketch_kernel<true, false>;
+    auto kern = c.codon_phased ? (c.use_rc ? sketch_kernel<true, true, true> : sketch_kernel<true, false, true>)
+                               : (c.use_rc ? sketch_kernel<true, true, false> : sketch_kernel<true, false, false>);
     e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e == cudaSuccess) kern<<<grid, kSketchThreads, smem, stream>>>(args);
   } else {
-    auto kern = c.use_rc ? sketch_kernel<false, true> : sketch_kernel<false, false>;
+    auto kern = c.codon_phased ? (c.use_rc ? sketch_kernel<false, true, true> : sketch_kernel<false, false, true>)
+                               : (c.use_rc ? sketch_kernel<false, true, false> : sketch_kernel<false, false, false>);
     kern<<<grid, kSketchThreads, 0, stream>>>(args);
   }
   if (e == cudaSuccess) e = cudaGetLastError();
@@ -782,7 +825,8 @@ sk_status count_batch(SketchCall &c, const Batch &b, SketchArgs &args, std::vect
                              ctx->stream>>>(args.table, slots, args.max_key_count);
         cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) {
-          auto kern = c.use_rc ? count_kernel<true> : count_kernel<false>;
+          auto kern = c.codon_phased ? (c.use_rc ? count_kernel<true, true> : count_kernel<false, true>)
+                                     : (c.use_rc ? count_kernel<true, false> : count_kernel<false, false>);
           kern<<<static_cast<unsigned>(items.size()), kSketchThreads, 0, ctx->stream>>>(args);
           e = cudaGetLastError();
         }
@@ -910,7 +954,7 @@ sk_status sketch_to_device(SketchCall &c) {
   sk_ctx *ctx = c.ctx;
   const int K = static_cast<int>(c.kmers.size());
   std::vector<RollTable> tables(K);
-  for (int k = 0; k < K; ++k) tables[k] = make_table(c.kmers[k]);
+  for (int k = 0; k < K; ++k) tables[k] = make_table(c.kmers[k], c.codon_phased != 0);
   void *p = nullptr;
   sk_status st = scratch(ctx, kSlotSketchTables, tables.size() * sizeof(RollTable), &p);
   if (st == SK_OK) st = upload(ctx, p, tables.data(), tables.size() * sizeof(RollTable));
@@ -942,8 +986,8 @@ sk_status drain(sk_ctx *ctx, sk_status st) {
 // else they are context scratch.
 sk_status setup_call(SketchCall &c, sk_ctx *ctx, const char *bases, bool device_in,
                      const int64_t *seq_offsets, const int64_t *sample_seqs, int64_t n,
-                     const int32_t *kmers, int32_t K, int32_t s64, int32_t use_rc, int32_t min_count,
-                     uint64_t *d_words, double *d_inv) {
+                     const int32_t *kmers, int32_t K, int32_t s64, int32_t use_rc,
+                     int32_t codon_phased, int32_t min_count, uint64_t *d_words, double *d_inv) {
   c.ctx = ctx;
   c.bases = bases;
   c.device_in = device_in;
@@ -953,6 +997,7 @@ sk_status setup_call(SketchCall &c, sk_ctx *ctx, const char *bases, bool device_
   c.kmers.assign(kmers, kmers + K);
   c.s64 = s64;
   c.use_rc = use_rc;
+  c.codon_phased = codon_phased;
   c.min_count = min_count;
   c.nbins = s64 * 64;
   c.binsize = (kSignMod + static_cast<uint64_t>(c.nbins) - 1) / static_cast<uint64_t>(c.nbins);
@@ -979,20 +1024,20 @@ extern "C" {
 
 sk_status sk_sketch(sk_ctx *ctx, const char *bases, const int64_t *seq_offsets,
                     const int64_t *sample_seqs, int64_t n_samples, const int32_t *kmers,
-                    int32_t n_kmers, int32_t sketchsize64, int32_t use_rc, int32_t min_count,
-                    uint64_t *words, double *inv_minhash, uint8_t *densified) {
+                    int32_t n_kmers, int32_t sketchsize64, int32_t use_rc, int32_t codon_phased,
+                    int32_t min_count, uint64_t *words, double *inv_minhash, uint8_t *densified) {
   if (!ctx) return SK_EINVAL;
   std::lock_guard<std::recursive_mutex> lock(ctx->mu);
   DeviceGuard dev(ctx->device);
   sk_status st = begin_call(ctx);
   if (st != SK_OK) return st;
   st = check_inputs(ctx, bases, seq_offsets, sample_seqs, n_samples, kmers, n_kmers, sketchsize64,
-                    use_rc, min_count);
+                    use_rc, codon_phased, min_count);
   if (st != SK_OK || n_samples == 0) return st;
   if (!words) return fail(ctx, SK_EINVAL, "null output words");
   SketchCall c{};
   st = setup_call(c, ctx, bases, false, seq_offsets, sample_seqs, n_samples, kmers, n_kmers,
-                  sketchsize64, use_rc, min_count, nullptr, nullptr);
+                  sketchsize64, use_rc, codon_phased, min_count, nullptr, nullptr);
   if (st == SK_OK) st = sketch_to_device(c);
   if (st != SK_OK) return drain(ctx, st);
   const size_t n_words = static_cast<size_t>(n_samples) * n_kmers * sketchsize64 * kBbits;
@@ -1016,20 +1061,21 @@ sk_status sk_sketch(sk_ctx *ctx, const char *bases, const int64_t *seq_offsets,
 
 sk_status sk_sketch_device(sk_ctx *ctx, const char *d_bases, const int64_t *seq_offsets,
                            const int64_t *sample_seqs, int64_t n_samples, const int32_t *kmers,
-                           int32_t n_kmers, int32_t sketchsize64, int32_t use_rc, int32_t min_count,
-                           uint64_t *d_words, double *d_inv_minhash, uint8_t *d_densified) {
+                           int32_t n_kmers, int32_t sketchsize64, int32_t use_rc,
+                           int32_t codon_phased, int32_t min_count, uint64_t *d_words,
+                           double *d_inv_minhash, uint8_t *d_densified) {
   if (!ctx) return SK_EINVAL;
   std::lock_guard<std::recursive_mutex> lock(ctx->mu);
   DeviceGuard dev(ctx->device);
   sk_status st = begin_call(ctx);
   if (st != SK_OK) return st;
   st = check_inputs(ctx, d_bases, seq_offsets, sample_seqs, n_samples, kmers, n_kmers, sketchsize64,
-                    use_rc, min_count);
+                    use_rc, codon_phased, min_count);
   if (st != SK_OK || n_samples == 0) return st;
   if (!d_words) return fail(ctx, SK_EINVAL, "null output words");
   SketchCall c{};
   st = setup_call(c, ctx, d_bases, true, seq_offsets, sample_seqs, n_samples, kmers, n_kmers,
-                  sketchsize64, use_rc, min_count, d_words, d_inv_minhash);
+                  sketchsize64, use_rc, codon_phased, min_count, d_words, d_inv_minhash);
   if (st == SK_OK) st = sketch_to_device(c);
   if (st != SK_OK) return drain(ctx, st);
   if (d_densified) {

@@ -87,8 +87,9 @@ _SIGNATURES = {
     "sk_server_release": (_i32, [_p, _i64]),
     "sk_server_stats": (_i32, [_p, C.POINTER(_i64), C.POINTER(C.c_double), C.POINTER(_i64)]),
     "sk_server_destroy": (_i32, [_p]),
-    "sk_sketch": (_i32, [_p, _p, _p, _p, _i64, _p, _i32, _i32, _i32, _i32, _p, _p, _p]),
-    "sk_sketch_device": (_i32, [_p, _p, _p, _p, _i64, _p, _i32, _i32, _i32, _i32, _p, _p, _p]),
+    "sk_sketch": (_i32, [_p, _p, _p, _p, _i64, _p, _i32, _i32, _i32, _i32, _i32, _p, _p, _p]),
+    "sk_sketch_device": (_i32, [_p, _p, _p, _p, _i64, _p, _i32, _i32, _i32, _i32, _i32, _p, _p,
+                                _p]),
 }
 
 
@@ -535,12 +536,13 @@ def pack_sequences(samples):
 
 
 def sketch(ctx: Context, bases, seq_offsets, sample_seqs, kmers, sketchsize64: int,
-           use_rc: bool = True, min_count: int = 0, words=None):
+           use_rc: bool = True, min_count: int = 0, words=None, codon_phased: bool = False):
     """MinHash sketches of sequences on the device (sk_sketch).  `bases`
     uint8 (or bytes) holding every sequence back to back; sequence i is
     bases[seq_offsets[i]:seq_offsets[i+1]]; sample s owns sequences
-    sample_seqs[s] .. sample_seqs[s+1]-1.  Returns (words uint64
-    [n][K][sketchsize64 * 14], inv_minhash float64 [n][K], densified bool [n])."""
+    sample_seqs[s] .. sample_seqs[s+1]-1; codon_phased selects the reference's
+    spaced seeds.  Returns (words uint64 [n][K][sketchsize64 * 14],
+    inv_minhash float64 [n][K], densified bool [n])."""
     b = np.frombuffer(bases, np.uint8) if isinstance(bases, (bytes, bytearray)) else \
         np.ascontiguousarray(bases, np.uint8)
     so = np.ascontiguousarray(seq_offsets, np.int64)
@@ -553,13 +555,14 @@ def sketch(ctx: Context, bases, seq_offsets, sample_seqs, kmers, sketchsize64: i
     dens = np.empty(n, np.uint8)
     _check(lib.sk_sketch(ctx.handle, b.ctypes.data if b.size else None, so.ctypes.data,
                          ss.ctypes.data, n, km.ctypes.data, len(km), sketchsize64, int(use_rc),
-                         int(min_count), words.ctypes.data, inv.ctypes.data, dens.ctypes.data), ctx)
+                         int(codon_phased), int(min_count), words.ctypes.data, inv.ctypes.data,
+                         dens.ctypes.data), ctx)
     return words, inv, dens.astype(bool)
 
 
 def sketch_device(ctx: Context, d_bases: int, seq_offsets, sample_seqs, kmers, sketchsize64: int,
                   d_words: int, use_rc: bool = True, min_count: int = 0, d_inv_minhash: int = 0,
-                  d_densified: int = 0) -> None:
+                  d_densified: int = 0, codon_phased: bool = False) -> None:
     """sk_sketch_device: device bases in (address d_bases), device outputs
     (addresses d_words [n][K][sketchsize64 * 14] uint64, d_inv_minhash [n][K]
     float64 and d_densified [n] uint8, 0 to skip); e.g. torch tensors'
@@ -569,7 +572,7 @@ def sketch_device(ctx: Context, d_bases: int, seq_offsets, sample_seqs, kmers, s
     km = np.ascontiguousarray(kmers, np.int32)
     _check(lib.sk_sketch_device(ctx.handle, d_bases or None, so.ctypes.data, ss.ctypes.data,
                                 len(ss) - 1, km.ctypes.data, len(km), sketchsize64, int(use_rc),
-                                int(min_count), d_words, d_inv_minhash or None,
+                                int(codon_phased), int(min_count), d_words, d_inv_minhash or None,
                                 d_densified or None), ctx)
 
 

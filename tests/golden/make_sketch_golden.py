@@ -10,8 +10,9 @@ nor its build:
              bases, seq_off, sample_seqs) covering several sequences per
              sample, N runs, lower case, U, IUPAC letters, sequences shorter
              than k, an all-N sample and a sample of one k-mer;
-             sketched for three (kmers, sketchsize64, use_rc) settings through
-             SeqBuf(std::vector<std::string>) -- sequences as given.
+             sketched for five (kmers, sketchsize64, use_rc, codon_phased)
+             settings through SeqBuf(std::vector<std::string>) -- sequences as
+             given; the last two use the codon-phased spaced seeds.
   reads_*    a read set (FASTQ with N-containing and short reads) sketched
              through SeqBuf(files, largest k) with min_count = 2 and 3 and the
              exact counter (`exact = true`); the fixture keeps the reads as
@@ -54,14 +55,17 @@ samples = [
     [genome[:3000], genome[2500:6000].lower()],
 ]
 bases, seq_off, sample_seqs = oracle.pack_samples(samples)
-settings = [([3, 15, 31, 33], 4, True), ([15, 17, 63, 64, 101], 4, False), ([21, 29], 156, True)]
+settings = [([3, 15, 31, 33], 4, True, False), ([15, 17, 63, 64, 101], 4, False, False),
+            ([21, 29], 156, True, False), ([3, 9, 15], 4, True, True), ([5, 11, 17], 16, False, True)]
 rs = oracle.RefSketcher()
 out = {"seqs_bases": bases, "seqs_seq_off": seq_off, "seqs_sample_seqs": sample_seqs}
-for i, (kmers, s64, rc) in enumerate(settings):
-    words, inv, dens = rs.sketch_seqs(bases, seq_off, sample_seqs, kmers, s64, rc)
+for i, (kmers, s64, rc, phased) in enumerate(settings):
+    words, inv, dens = rs.sketch_seqs(bases, seq_off, sample_seqs, kmers, s64, rc,
+                                      codon_phased=phased)
     out[f"seqs{i}_kmers"] = np.asarray(kmers, np.int32)
     out[f"seqs{i}_s64"] = np.int32(s64)
     out[f"seqs{i}_use_rc"] = np.int32(rc)
+    out[f"seqs{i}_codon_phased"] = np.int32(phased)
     out[f"seqs{i}_words"] = words
     out[f"seqs{i}_inv_minhash"] = inv
     out[f"seqs{i}_densified"] = dens

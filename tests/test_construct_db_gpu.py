@@ -88,12 +88,33 @@ def test_construct_database_matches_reference_sketcher(tmp_path):
     assert (tmp_path / "db.h5").read_bytes() == before
 
 
+def test_construct_database_codon_phased(tmp_path):
+    """codon_phased=True sketches with the reference's spaced seeds (the
+    reference's CPU sketcher does; its GPU sketcher refuses)."""
+    import pp_sketchlib
+    rng = np.random.default_rng(4)
+    names, files = [], []
+    for i, g in enumerate(genomes(rng, 3, 100_000)):
+        p = tmp_path / f"g{i}.fa"
+        write_fasta(p, g, rng)
+        names.append(f"g{i}")
+        files.append([str(p)])
+    db = str(tmp_path / "phased")
+    kmers = [15, 19]
+    pp_sketchlib.constructDatabase(db, names, files, kmers, S64, codon_phased=True,
+                                   calc_random=False)
+    got = pp_sketchlib._load_sketch_db(db, names=names, klist=kmers)
+    rs = oracle.RefSketcher()
+    for i, f in enumerate(files):
+        info = rs.seqbuf(f[0], kmers[-1])
+        bases, off, ss = oracle.pack_samples([[q.encode() for q in info["seqs"]]])
+        want = rs.sketch_seqs(bases, off, ss, kmers, S64, True, codon_phased=True)[0]
+        np.testing.assert_array_equal(got["words"][i], want[0])
+
+
 def test_construct_database_errors(tmp_path):
     import pp_sketchlib
     empty = tmp_path / "empty.fa"
     empty.write_bytes(b">x\nACGT\n")          # shorter than the largest k: nothing kept
     with pytest.raises(RuntimeError, match="contains no sequence"):
         pp_sketchlib.constructDatabase(str(tmp_path / "e"), ["e"], [[str(empty)]], KMERS, S64)
-    with pytest.raises(RuntimeError, match="Codon phased"):
-        pp_sketchlib.constructDatabase(str(tmp_path / "c"), ["e"], [[str(empty)]], KMERS, S64,
-                                       codon_phased=True)

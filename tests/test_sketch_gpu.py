@@ -18,12 +18,13 @@ def check(got, want):
         np.testing.assert_array_equal(a, b)
 
 
-@pytest.mark.parametrize("setting", [0, 1, 2])
+@pytest.mark.parametrize("setting", [0, 1, 2, 3, 4])
 def test_sketch_matches_reference_goldens(gpu_ctx, setting):
     from sketchlib_b200 import capi
     got = capi.sketch(gpu_ctx, G["seqs_bases"], G["seqs_seq_off"], G["seqs_sample_seqs"],
                       G[f"seqs{setting}_kmers"], int(G[f"seqs{setting}_s64"]),
-                      use_rc=bool(G[f"seqs{setting}_use_rc"]))
+                      use_rc=bool(G[f"seqs{setting}_use_rc"]),
+                      codon_phased=bool(G[f"seqs{setting}_codon_phased"]))
     check(got, (G[f"seqs{setting}_words"], G[f"seqs{setting}_inv_minhash"],
                 G[f"seqs{setting}_densified"]))
 
@@ -224,3 +225,42 @@ def test_many_samples_split_into_batches(gpu_ctx):
     kmers = list(range(15, 31, 2))
     check(capi.sketch(gpu_ctx, bases, off, ss, kmers, 1000),
           oracle.sketch(bases, off, ss, kmers, 1000, True))
+
+
+@pytest.mark.parametrize("seed,kmers,s64,rc,min_count", [
+    (31, [3, 15, 17], 16, True, 0),
+    (32, [9, 21, 29], 156, False, 0),
+    (33, [15, 85, 255], 64, True, 0),     # windows of 253, 763 bases
+    (34, [15, 21], 64, True, 2),          # read filter with spaced seeds
+])
+def test_codon_phased_matches_oracle(gpu_ctx, seed, kmers, s64, rc, min_count):
+    from sketchlib_b200 import capi
+    rng = np.random.default_rng(seed)
+    if min_count:
+        genome = np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, 30_000)]
+        reads = []
+        for _ in range(4 * 30_000 // 150):
+            s = int(rng.integers(0, 30_000 - 150))
+            reads.append(genome[s:s + 150].tobytes())
+        samples = [reads]
+    else:
+        samples = random_samples(rng, 8, 80_000)
+    bases, off, ss = capi.pack_sequences(samples)
+    got = capi.sketch(gpu_ctx, bases, off, ss, kmers, s64, use_rc=rc, min_count=min_count,
+                      codon_phased=True)
+    check(got, oracle.sketch(bases, off, ss, kmers, s64, rc, min_count=min_count,
+                             codon_phased=True))
+
+
+def test_codon_phased_device_entry_point(gpu_ctx):
+    import torch
+    from sketchlib_b200 import capi
+    rng = np.random.default_rng(35)
+    bases, off, ss = capi.pack_sequences(random_samples(rng, 5, 100_000))
+    kmers = [15, 21]
+    want = capi.sketch(gpu_ctx, bases, off, ss, kmers, 64, codon_phased=True)
+    buf = torch.from_numpy(bases.copy()).cuda()
+    words = torch.empty((5, 2, 64 * 14), dtype=torch.int64, device="cuda")
+    capi.sketch_device(gpu_ctx, buf.data_ptr(), off, ss, kmers, 64, words.data_ptr(),
+                       codon_phased=True)
+    np.testing.assert_array_equal(words.cpu().numpy().view(np.uint64), want[0])

@@ -19,11 +19,12 @@ def reads_as_seqbuf(max_k):
     return oracle.pack_samples([[q for q in seqs if len(q) >= max_k]])
 
 
-@pytest.mark.parametrize("setting", [0, 1, 2])
+@pytest.mark.parametrize("setting", [0, 1, 2, 3, 4])
 def test_oracle_sketch_matches_reference_goldens(setting):
     kmers = G[f"seqs{setting}_kmers"]
     w, inv, dens = oracle.sketch(G["seqs_bases"], G["seqs_seq_off"], G["seqs_sample_seqs"], kmers,
-                                 int(G[f"seqs{setting}_s64"]), bool(G[f"seqs{setting}_use_rc"]))
+                                 int(G[f"seqs{setting}_s64"]), bool(G[f"seqs{setting}_use_rc"]),
+                                 codon_phased=bool(G[f"seqs{setting}_codon_phased"]))
     np.testing.assert_array_equal(w, G[f"seqs{setting}_words"])
     np.testing.assert_array_equal(inv, G[f"seqs{setting}_inv_minhash"])
     np.testing.assert_array_equal(dens, G[f"seqs{setting}_densified"])
@@ -53,7 +54,7 @@ def test_golden_cases_cover_the_edges():
 
 
 @pytest.mark.skipif(not oracle.sketcher_available(), reason="oracle/_ref/libref_sketch.so not built")
-@pytest.mark.parametrize("seed", [1, 2])
+@pytest.mark.parametrize("seed", [1, 2, 3])
 def test_oracle_sketch_matches_reference_random(seed):
     rng = np.random.default_rng(seed)
     alphabet = np.frombuffer(b"ACGTacgtNNRU", np.uint8)
@@ -66,7 +67,8 @@ def test_oracle_sketch_matches_reference_random(seed):
     kmers = sorted(rng.choice(np.arange(3, 80), 4, replace=False).tolist())
     s64 = int(rng.choice([1, 3, 16]))
     rc = bool(seed % 2)
-    want = oracle.RefSketcher().sketch_seqs(bases, off, ss, kmers, s64, rc)
-    got = oracle.sketch(bases, off, ss, kmers, s64, rc)
+    phased = seed == 3
+    want = oracle.RefSketcher().sketch_seqs(bases, off, ss, kmers, s64, rc, codon_phased=phased)
+    got = oracle.sketch(bases, off, ss, kmers, s64, rc, codon_phased=phased)
     for a, b in zip(got, want):
         np.testing.assert_array_equal(a, b)
