@@ -458,6 +458,9 @@ void constructDatabase(const std::string &db_name, const std::vector<std::string
                        size_t min_count, const bool exact, const size_t num_threads,
                        const bool /*use_gpu*/, const int device_id) {
   if (names.size() != files.size()) throw std::runtime_error("Sample names and file lists differ in length");
+  for (const std::string &nm : names)   // HDF5 link names: no path separator, not empty
+    if (nm.empty() || nm.find('/') != std::string::npos || nm == "." || nm == "..")
+      throw std::runtime_error("Sample name '" + nm + "' cannot name a database group");
   if (kmer_lengths.empty()) throw std::runtime_error("No k-mer lengths given");
   const std::string path = db_name + ".h5";
   std::vector<int32_t> kmers = to_kmers(kmer_lengths);

@@ -118,3 +118,5 @@ def test_construct_database_errors(tmp_path):
     empty.write_bytes(b">x\nACGT\n")          # shorter than the largest k: nothing kept
     with pytest.raises(RuntimeError, match="contains no sequence"):
         pp_sketchlib.constructDatabase(str(tmp_path / "e"), ["e"], [[str(empty)]], KMERS, S64)
+    with pytest.raises(RuntimeError, match="cannot name a database group"):
+        pp_sketchlib.constructDatabase(str(tmp_path / "s"), ["a/b"], [[str(empty)]], KMERS, S64)
