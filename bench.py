@@ -550,7 +550,7 @@ def run_serving(ctx, dev, n_requests=120, rate_hz=10.0):
     sizes = np.exp(rng.uniform(0, np.log(2000), n_requests)).astype(int).clip(1, 2000)
     starts = rng.integers(0, pool - sizes + 1)
     gaps = rng.exponential(1.0 / rate_hz, n_requests)
-    server = capi.Server(ctx, ref, slots=4, slice_queries=128, kNN=5)
+    server = capi.Server(ctx, ref, slots=4, slice_queries=128, kNN=5, large_slice_queries=64)
     # warm-up request
     t = server.submit(qwords[:64])
     server.wait(t)
@@ -591,6 +591,8 @@ def run_serving(ctx, dev, n_requests=120, rate_hz=10.0):
     pairs = int(sizes.sum()) * n_ref
     mid = (sizes >= 50) & (sizes <= 200)
     small = sizes <= 64
+    one_slice = sizes <= 128                      # one slice: the 100-query class
+    near100 = (sizes > 64) & (sizes <= 128)       # a full 128-row tile of queries
     pct = lambda a, q: float(np.percentile(a, q) * 1e3) if len(a) else None
     return {
         "workload": "50,000 resident references, 10 k x 10k bins; seeded Poisson arrivals "
@@ -601,7 +603,11 @@ def run_serving(ctx, dev, n_requests=120, rate_hz=10.0):
         "p50_ms_batches_50_200": pct(lat[mid], 50), "p99_ms_batches_50_200": pct(lat[mid], 99),
         "n_batches_50_200": int(mid.sum()),
         "p50_ms_batches_le_64": pct(lat[small], 50), "n_batches_le_64": int(small.sum()),
-        "slots": 4, "slice_queries": 128,
+        "p50_ms_batches_65_128": pct(lat[near100], 50), "p99_ms_batches_65_128": pct(lat[near100], 99),
+        "n_batches_65_128": int(near100.sum()),
+        "p99_ms_batches_le_128": pct(lat[one_slice], 99), "n_batches_le_128": int(one_slice.sum()),
+        "max_ms": float(lat.max() * 1e3),
+        "slots": 4, "slice_queries": 128, "large_slice_queries": 64,
         "alone_vs_mixed_equal": alone_equal, "alone_vs_mixed_requests": len(check),
     }
 

@@ -337,15 +337,22 @@ typedef struct sk_server sk_server;
 
 typedef struct sk_server_params {
   int32_t slots;          /* slices on the device at once (one stream each), 1..16 */
-  int32_t slice_queries;  /* largest number of queries per slice */
+  int32_t slice_queries;  /* largest number of queries per slice; a request of at
+                             most this many runs as one slice at high priority */
   int32_t kNN;            /* nearest references returned per query, 0..800 */
   int32_t dist_col;       /* distance the kNN ranks by: 0 core, 1 accessory */
   int32_t keep_rows;      /* 1: also return each query's core/accessory row */
+  int32_t large_slice_queries;  /* slice size for larger requests, 1..slice_queries
+                                   (0: slice_queries); smaller slices shorten the wait
+                                   of a one-slice request behind a large one */
 } sk_server_params;
 
 /* Starts a server over `ref` (kept resident; it must outlive the server).
- * Every slot's buffers are allocated here, so the HBM footprint is fixed and
- * requests are admitted as slots free up.  The context's tile shape, tuning
+ * Every slot's buffers and kernel scratch are allocated here, so the HBM
+ * footprint is fixed and requests are admitted as slots free up.  Free slots
+ * go to the request with the fewest queries left (a request waiting over 2 s
+ * first); one-slice requests run on a high-priority stream, and slices of
+ * larger requests hold at most half the slots.  The context's tile shape, tuning
  * and semantics at this moment apply to every request.  No reference
  * counterpart: the reference answers one query_db_cuda call at a time
  * (src/gpu/gpu_api.cpp:352). */

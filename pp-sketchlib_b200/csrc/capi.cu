@@ -380,16 +380,26 @@ void split_tail(std::vector<WorkItem> &items, size_t begin, int grid, int32_t *n
 
 // Device buffers for a plan: job table, work list, control block (queue
 // counter + split arrival counters, zeroed per launch) and count scratch.
+MetaLayout meta_layout(size_t n_jobs, size_t n_items, int32_t n_splits, int threads) {
+  MetaLayout m;
+  m.items_off = (n_jobs * sizeof(JobParams) + 255) & ~static_cast<size_t>(255);
+  m.ctrl_off = (m.items_off + n_items * sizeof(WorkItem) + 255) & ~static_cast<size_t>(255);
+  m.ctrl_bytes = 8 + static_cast<size_t>(n_splits) * threads * 4;
+  m.bytes = m.ctrl_off + m.ctrl_bytes;
+  return m;
+}
+
 sk_status upload_plan(sk_ctx *ctx, const std::vector<JobParams> &jobs, Plan &plan,
                       LaunchBuffers &buf, bool owned) {
   const TileConfig &cfg = *plan.cfg;
   const size_t jobs_bytes = jobs.size() * sizeof(JobParams);
   const size_t items_bytes = plan.items.size() * sizeof(WorkItem);
-  const size_t ctrl_bytes = 8 + static_cast<size_t>(plan.n_splits) * cfg.threads * 4;
+  const MetaLayout ml = meta_layout(jobs.size(), plan.items.size(), plan.n_splits, cfg.threads);
+  const size_t ctrl_bytes = ml.ctrl_bytes;
   const size_t jobs_off = 0;
-  const size_t items_off = (jobs_bytes + 255) & ~static_cast<size_t>(255);
-  const size_t ctrl_off = (items_off + items_bytes + 255) & ~static_cast<size_t>(255);
-  const size_t meta_bytes = ctrl_off + ctrl_bytes;
+  const size_t items_off = ml.items_off;
+  const size_t ctrl_off = ml.ctrl_off;
+  const size_t meta_bytes = ml.bytes;
   const size_t slot = count_slot_bytes(cfg, plan.k_slots);
   const size_t cta_bytes = static_cast<size_t>(plan.grid) * slot;
   const size_t split_bytes = std::max<size_t>(static_cast<size_t>(plan.n_splits) * slot, 16);

@@ -282,7 +282,7 @@ Attr Attr::i32_vec(const std::string &n, const std::vector<int32_t> &v) {
   a.scalar = false;
   a.count = v.size();
   a.data.resize(4 * v.size());
-  std::memcpy(a.data.data(), v.data(), a.data.size());
+  std::memcpy(a.data.data(), v.data(), v.size() * sizeof(int32_t));
   return a;
 }
 

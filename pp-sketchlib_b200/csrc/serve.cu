@@ -9,9 +9,23 @@
 // the server's HBM footprint is fixed (slots x slot bytes + the reference).
 // Slices of different requests run on different streams and overlap on the
 // device: a slot's persistent kernel takes SMs as another slot's kernel
-// releases them.  Scheduling is round-robin over requests with work
-// conservation: a request holds at most one slot while others wait, so a
-// 2,000-query request cannot delay a 10-query one by more than a slice.
+// releases them.
+//
+// Scheduling.  The distance kernel is persistent and fills every SM, so
+// slices queued on several streams run one after another; what decides a
+// small request's latency is how many slices the block scheduler starts
+// before its own.  So:
+//   * free slots go to the request with the fewest queries left (shortest
+//     remaining work first), FIFO among equals; a request older than
+//     kStarveSeconds goes ahead of every younger one, so a stream of small
+//     requests cannot hold a large one back for good;
+//   * a request that fits in one slice runs on a high-priority stream: its
+//     kernels start as soon as the slice on the SMs ends, ahead of slices of
+//     larger requests already queued;
+//   * slices of requests larger than one slice hold at most half the slots
+//     (at least one), so a request of one slice finds a slot free and waits
+//     at most for the slice already running, and the device still always has
+//     a large slice queued behind the running one.
 //
 // Per slice: pinned staging copy of the query words, H2D, pack, the distance
 // kernel (core or accessory column vs all references, optionally the full
@@ -71,10 +85,16 @@ struct Slot {
   float *h_knn_d = nullptr;
   float *h_rows = nullptr;
   cudaEvent_t done_ev = nullptr;
+  cudaStream_t lo_stream = nullptr;  // the slot context's own stream
+  cudaStream_t hi_stream = nullptr;  // greatest priority, for one-slice requests
   std::shared_ptr<Request> req;
   int64_t q0 = 0, nq = 0;
   bool busy = false;
+  bool high = false;                 // the running slice is on hi_stream
 };
+
+// A request waiting longer than this goes ahead of every younger request.
+constexpr double kStarveSeconds = 2.0;
 
 }  // namespace
 
@@ -103,6 +123,8 @@ struct sk_server {
 namespace {
 
 void free_slot(Slot &s) {
+  if (s.ctx && s.lo_stream) s.ctx->stream = s.lo_stream;   // the context destroys its own
+  if (s.hi_stream) cudaStreamDestroy(s.hi_stream);
   if (s.done_ev) cudaEventDestroy(s.done_ev);
   if (s.d_words) cudaFree(s.d_words);
   if (s.h_words) cudaFreeHost(s.h_words);
@@ -118,6 +140,45 @@ void free_slot(Slot &s) {
   s = Slot{};
 }
 
+// Reserves, at start-up, the kernel scratch of the largest slice under every
+// tile shape a slice can take (the default shape and the 64-row one of small
+// batches).  Growing a scratch buffer mid-request would free the old one, and
+// cudaFree waits for the whole device: every slot's work would stall behind
+// it.  build_job on a full-size slice also creates the lazily built
+// per-query random-match factors here.
+sk_status reserve_slice_scratch(sk_server *sv, Slot &s) {
+  sk_ctx *ctx = s.ctx;
+  const sk_db *ref = sv->ref;
+  const int64_t sq = sv->params.slice_queries;
+  s.qdb.n = sq;
+  s.qdb.jv_rc = -1;
+  s.qdb.seq_len.assign(sq, 0);
+  JobParams jp;
+  const TileConfig *cfg = nullptr;
+  sk_status st = build_job(ctx, ref, &s.qdb, sv->random, kOutColumn, sv->params.dist_col,
+                           s.d_col, &cfg, &jp);
+  if (st != SK_OK) return st;
+  size_t meta = 0, cta = 16, split = 16;
+  for (const TileConfig *c : {choose_config(ctx, ref->K, ref->s64), tile_config(kSmallQueryConfig)}) {
+    if (!c || c->max_kmers < ref->K) continue;
+    const int grid = resident_grid(ctx, *c);
+    if (grid < 1) continue;
+    const int64_t tiles = ((sq + c->tile_rows - 1) / c->tile_rows) *
+                          ((ref->n + c->tile_cols - 1) / c->tile_cols);
+    // the tail tiles (fewer than the grid) may each be cut into K parts
+    const int64_t items = tiles + static_cast<int64_t>(grid) * ref->K;
+    meta = std::max(meta, meta_layout(1, static_cast<size_t>(items), grid, c->threads).bytes);
+    const size_t slot = count_slot_bytes(*c, ref->K);
+    cta = std::max(cta, static_cast<size_t>(grid) * slot);
+    split = std::max(split, static_cast<size_t>(grid) * slot);
+  }
+  void *p = nullptr;
+  st = scratch(ctx, kSlotLaunchMeta, meta, &p);
+  if (st == SK_OK) st = scratch(ctx, kSlotCounts, cta, &p);
+  if (st == SK_OK) st = scratch(ctx, kSlotSplitCounts, split, &p);
+  return st;
+}
+
 // Queues one slice on its slot's stream.  Called by the scheduler thread only.
 sk_status start_slice(sk_server *sv, Slot &s) {
   sk_ctx *ctx = s.ctx;
@@ -125,6 +186,7 @@ sk_status start_slice(sk_server *sv, Slot &s) {
   const size_t wps = sv->words_per_sample;
   Request &r = *s.req;
   DeviceGuard g(ctx->device);
+  ctx->stream = s.high ? s.hi_stream : s.lo_stream;
   sk_status st = begin_call(ctx);
   if (st != SK_OK) return st;
   std::memcpy(s.h_words, r.words + s.q0 * wps, static_cast<size_t>(s.nq) * wps * 8);
@@ -201,9 +263,23 @@ void finish_slice(sk_server *sv, Slot &s) {
   s.busy = false;
 }
 
+// Admission order: a request waiting longer than kStarveSeconds first (FIFO
+// among those), then the fewest queries left, then FIFO.
+bool goes_before(const Request &a, const Request &b, Clock::time_point now) {
+  const bool sa = std::chrono::duration<double>(now - a.t_submit).count() > kStarveSeconds;
+  const bool sb = std::chrono::duration<double>(now - b.t_submit).count() > kStarveSeconds;
+  if (sa != sb) return sa;
+  if (!sa) {
+    const int64_t ra = a.n - a.dispatched, rb = b.n - b.dispatched;
+    if (ra != rb) return ra < rb;
+  }
+  return a.id < b.id;
+}
+
 void scheduler(sk_server *sv) {
   std::unique_lock<std::mutex> lock(sv->mu);
-  size_t rr = 0;   // round-robin cursor over pending requests
+  const int64_t sq = sv->params.slice_queries;
+  const int large_cap = std::max<int>(1, static_cast<int>(sv->slots.size()) / 2);
   while (true) {
     bool progressed = false;
     // completions
@@ -223,26 +299,24 @@ void scheduler(sk_server *sv) {
       progressed = true;
     }
     if (progressed) sv->done_cv.notify_all();
-    // admissions: give free slots to requests, one slice per request per round
+    // admissions
     for (Slot &s : sv->slots) {
       if (s.busy || sv->pending.empty()) continue;
-      // prefer the next request with nothing in flight; else any with work left
+      int large_busy = 0;
+      for (const Slot &o : sv->slots) large_busy += (o.busy && !o.high) ? 1 : 0;
+      const auto now = Clock::now();
       std::shared_ptr<Request> pick;
-      const size_t np = sv->pending.size();
-      for (int pass = 0; pass < 2 && !pick; ++pass) {
-        for (size_t i = 0; i < np; ++i) {
-          auto &cand = sv->pending[(rr + i) % np];
-          if (cand->dispatched >= cand->n) continue;
-          if (pass == 0 && cand->inflight > 0) continue;
-          pick = cand;
-          rr = (rr + i + 1) % np;
-          break;
-        }
+      for (auto &cand : sv->pending) {
+        if (cand->dispatched >= cand->n) continue;
+        if (cand->n > sq && large_busy >= large_cap) continue;
+        if (!pick || goes_before(*cand, *pick, now)) pick = cand;
       }
       if (!pick) break;
       s.req = pick;
+      s.high = pick->n <= sq;
       s.q0 = pick->dispatched;
-      s.nq = std::min<int64_t>(sv->params.slice_queries, pick->n - pick->dispatched);
+      s.nq = std::min<int64_t>(s.high ? sq : sv->params.large_slice_queries,
+                               pick->n - pick->dispatched);
       pick->dispatched += s.nq;
       pick->inflight += 1;
       s.busy = true;
@@ -289,6 +363,7 @@ sk_status sk_server_create(sk_ctx *ctx, const sk_db *ref, const sk_random *rando
   if (ref->n < 1) return fail(ctx, SK_EINVAL, "Query with empty ref or query list!");
   const sk_server_params &p = *params;
   if (p.slots < 1 || p.slots > 16 || p.slice_queries < 1 || p.slice_queries > 65536 ||
+      p.large_slice_queries < 0 || p.large_slice_queries > p.slice_queries ||
       p.kNN < 0 || p.kNN > 800 || p.kNN > ref->n || (p.dist_col != 0 && p.dist_col != 1))
     return fail(ctx, SK_EINVAL, "bad server parameters");
   if (random && random->kmers != ref->kmers)
@@ -302,6 +377,7 @@ sk_status sk_server_create(sk_ctx *ctx, const sk_db *ref, const sk_random *rando
   sv->ref = ref;
   sv->random = random;
   sv->params = p;
+  if (sv->params.large_slice_queries == 0) sv->params.large_slice_queries = p.slice_queries;
   sv->words_per_sample = static_cast<size_t>(ref->K) * ref->s64 * kBbits;
   sv->slots.resize(p.slots);
   const int64_t sq = p.slice_queries;
@@ -310,6 +386,17 @@ sk_status sk_server_create(sk_ctx *ctx, const sk_db *ref, const sk_random *rando
   for (Slot &s : sv->slots) {
     st = sk_ctx_create(ctx->device, &s.ctx);
     if (st != SK_OK) break;
+    s.lo_stream = s.ctx->stream;
+    {
+      int least = 0, greatest = 0;
+      cudaError_t e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+      if (e == cudaSuccess)
+        e = cudaStreamCreateWithPriority(&s.hi_stream, cudaStreamNonBlocking, greatest);
+      if (e != cudaSuccess) {
+        st = cuda_fail(ctx, e, "server stream");
+        break;
+      }
+    }
     s.ctx->tile_cfg = ctx->tile_cfg;
     s.ctx->tuning = ctx->tuning;
     s.ctx->semantics = ctx->semantics;   // fixed for the server's lifetime
@@ -341,6 +428,11 @@ sk_status sk_server_create(sk_ctx *ctx, const sk_db *ref, const sk_random *rando
     if (p.kNN > 0) {
       s.d_knn_d = reinterpret_cast<float *>(s.d_knn + sq * p.kNN);
       s.h_knn_d = reinterpret_cast<float *>(s.h_knn + sq * p.kNN);
+    }
+    st = reserve_slice_scratch(sv, s);
+    if (st != SK_OK) {
+      fail(ctx, st, "server slot scratch: %s", sk_last_error(s.ctx));
+      break;
     }
   }
   if (st != SK_OK) {

@@ -114,6 +114,13 @@ struct Plan {
   int32_t k_slots = 1;
 };
 
+// Byte layout of a launch's meta buffer: job table at 0, then the work list
+// and the control block (queue counter, split arrival counters), 256-aligned.
+struct MetaLayout {
+  size_t items_off = 0, ctrl_off = 0, ctrl_bytes = 0, bytes = 0;
+};
+MetaLayout meta_layout(size_t n_jobs, size_t n_items, int32_t n_splits, int threads);
+
 struct LaunchBuffers {
   void *meta = nullptr, *cta = nullptr, *split = nullptr;
   void *ctrl = nullptr;

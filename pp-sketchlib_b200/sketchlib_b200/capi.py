@@ -95,7 +95,7 @@ _SIGNATURES = {
 
 class ServerParams(C.Structure):
     _fields_ = [("slots", _i32), ("slice_queries", _i32), ("kNN", _i32), ("dist_col", _i32),
-                ("keep_rows", _i32)]
+                ("keep_rows", _i32), ("large_slice_queries", _i32)]
 
 BATCH_AUTOTUNE = 1
 
@@ -387,13 +387,14 @@ class Server:
 
     def __init__(self, ctx: Context, ref: Database, random: Random | None = None, slots: int = 3,
                  slice_queries: int = 128, kNN: int = 5, dist_col: int = 0,
-                 keep_rows: bool = False):
+                 keep_rows: bool = False, large_slice_queries: int = 0):
         self.ctx = ctx
         self.ref = ref
         self.kNN = kNN
         self.keep_rows = keep_rows
         self._inputs = {}
-        prm = ServerParams(slots, slice_queries, kNN, dist_col, int(keep_rows))
+        prm = ServerParams(slots, slice_queries, kNN, dist_col, int(keep_rows),
+                           large_slice_queries)
         h = _p()
         _check(lib.sk_server_create(ctx.handle, ref.handle, _h(random), C.byref(prm), C.byref(h)),
                ctx)

@@ -114,3 +114,43 @@ def test_server_keeps_the_context_semantics(setup):
         assert np.any(cpu_rows != rows)
     finally:
         server.close()
+
+
+def test_priority_slicing_with_equal_base(setup):
+    """Requests larger than slice_queries run in large_slice_queries slices
+    (low priority, at most half the slots), the others as one high-priority
+    slice; free slots go to the fewest queries left.  Under the equal-base
+    random-match model with per-sample lengths, every result equals the direct
+    query-vs-reference computation whatever order the scheduler chose."""
+    ctx, _, queries, kmers = setup
+    rng = np.random.default_rng(5)
+    ref_words, q_words = queries[:500], queries[500:700]
+    ref_len = rng.integers(1_000_000, 5_000_000, 500).astype(np.uint64)
+    q_len = rng.integers(1_000_000, 5_000_000, 200).astype(np.uint64)
+    ref = capi.Database(ctx, ref_words, kmers, 156, seq_len=ref_len)
+    rnd = capi.Random(ctx, capi.RANDOM_EQUAL_BASE, kmers)
+    with pytest.raises(capi.SketchlibError):
+        capi.Server(ctx, ref, random=rnd, slots=2, slice_queries=16, kNN=3,
+                    large_slice_queries=17)
+    server = capi.Server(ctx, ref, random=rnd, slots=4, slice_queries=64, kNN=4,
+                         keep_rows=True, large_slice_queries=24)
+    try:
+        sizes = [100, 3, 64, 1, 20, 12]
+        offs = np.cumsum([0] + sizes)
+        tickets = [server.submit(q_words[offs[i]:offs[i + 1]], seq_len=q_len[offs[i]:offs[i + 1]])
+                   for i in range(len(sizes))]
+        for i, t in enumerate(tickets):
+            server.wait(t)
+            idx, dist, rows, _ = server.result(t)
+            q = q_words[offs[i]:offs[i + 1]]
+            qdb = capi.Database(ctx, q, kmers, 156, seq_len=q_len[offs[i]:offs[i + 1]])
+            e_rows = capi.dists_dense(ctx, ref, qdb, random=rnd).reshape(len(q), ref.n, 2)
+            e_idx, e_dist = capi.query_knn(ctx, ref, qdb, 4, dist_col=0, random=rnd)
+            qdb.close()
+            np.testing.assert_array_equal(rows, e_rows)
+            np.testing.assert_array_equal(idx, e_idx)
+            np.testing.assert_array_equal(dist, e_dist)
+    finally:
+        server.close()
+        rnd.close()
+        ref.close()
