@@ -409,7 +409,8 @@ def run_sketch_reads(ctx, steps, warmup, cpu):
     out = {"workload": f"{n_reads:,} reads of {RL} bp (10x of a 2 Mb genome, 1% errors), "
                        "k = 15..29 odd, sketchsize64 156, min_count 3 (exact counts)",
            "bases": int(bases.size), "ms": statistics.median(ms),
-           "call": "sk_sketch from host memory (count table per k, then the bins)"}
+           "call": "sk_sketch from host memory (per k: the hashes grouped by range, each "
+                   "group counted in shared memory, then the bins)"}
     if cpu:
         sys.path.insert(0, str(ROOT / "oracle"))
         import oracle

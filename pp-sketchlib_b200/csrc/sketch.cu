@@ -497,6 +497,148 @@ count_kernel(SketchArgs a) {
   roll_windows<kRc, kPhased>(a.codes, s, e, it.k, tab, emit);
 }
 
+// ---- partitioned exact counting
+//
+// The hashes of one (sample, k) are grouped by the top log2p bits of their
+// 61-bit sign (a contiguous range of bins per group) in two rolls over the
+// windows: the first counts each group, the second reserves each CTA's range
+// of every group and writes the hashes there.  Then one CTA per group counts
+// its hashes in a shared-memory table; the occurrence that brings a hash's
+// count to min_count puts it in its bin, as in the table pass above.  Every
+// occurrence of a hash lands in the same group, so the counts are exact and
+// the result does not depend on the order of the writes.
+struct PartArgs {
+  unsigned int *count;          // [P] hashes per group
+  unsigned int *cursor;         // [P] next free position of each group
+  unsigned int *start;          // [P + 1] first position of each group
+  unsigned long long *hashes;   // the hashes, grouped
+  int log2p;                    // P = 2^log2p groups
+  int table_slots;              // slots of one group's counting table (a power of two)
+};
+
+// kScatter false: per-group counts; true: the hashes into their groups (the
+// cursors start at the groups' first positions).
+template <bool kRc, bool kPhased, bool kScatter>
+__global__ void __launch_bounds__(kSketchThreads, 1)
+part_kernel(SketchArgs a, PartArgs pa) {
+  extern __shared__ unsigned int sh_part[];   // [P]
+  __shared__ RollTable tab;
+  const SketchItem it = a.items[blockIdx.x];
+  const int P = 1 << pa.log2p;
+  const int shift = 61 - pa.log2p;
+  for (int i = threadIdx.x; i < P; i += kSketchThreads) sh_part[i] = 0;
+  if (threadIdx.x < 64) {
+    const ulonglong2 *src = reinterpret_cast<const ulonglong2 *>(a.tables + it.tab);
+    reinterpret_cast<ulonglong2 *>(&tab)[threadIdx.x] = src[threadIdx.x];
+  }
+  __syncthreads();
+  const int64_t s = it.begin + static_cast<int64_t>(threadIdx.x) * it.per;
+  const int64_t e = min(s + it.per, it.end);
+  if (s < e)
+    roll_windows<kRc, kPhased>(a.codes, s, e, it.k, tab, [&](uint64_t h) {
+      atomicAdd(&sh_part[mod_sign(h) >> shift], 1u);
+    });
+  __syncthreads();
+  if constexpr (!kScatter) {
+    for (int i = threadIdx.x; i < P; i += kSketchThreads)
+      if (sh_part[i]) atomicAdd(pa.count + i, sh_part[i]);
+  } else {
+    for (int i = threadIdx.x; i < P; i += kSketchThreads) {
+      const unsigned int n = sh_part[i];
+      if (n) sh_part[i] = atomicAdd(pa.cursor + i, n);
+    }
+    __syncthreads();
+    if (s < e)
+      roll_windows<kRc, kPhased>(a.codes, s, e, it.k, tab, [&](uint64_t h) {
+        const unsigned int pos = atomicAdd(&sh_part[mod_sign(h) >> shift], 1u);
+        pa.hashes[pos] = h;
+      });
+  }
+}
+
+// Exclusive prefix sum of the group counts (one CTA of kScanThreads): the
+// groups' first positions, also the scatter's starting cursors.
+constexpr int kScanThreads = 1024;
+__global__ void __launch_bounds__(kScanThreads) part_scan_kernel(PartArgs pa) {
+  __shared__ unsigned int warp_sums[kScanThreads / 32];
+  const int P = 1 << pa.log2p;
+  const int per = (P + kScanThreads - 1) / kScanThreads;
+  const int i0 = min(P, threadIdx.x * per), i1 = min(P, i0 + per);
+  unsigned int sum = 0;
+  for (int i = i0; i < i1; ++i) sum += pa.count[i];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned int incl = sum;
+  for (int d = 1; d < 32; d <<= 1) {
+    const unsigned int v = __shfl_up_sync(0xffffffffu, incl, d);
+    if (lane >= d) incl += v;
+  }
+  if (lane == 31) warp_sums[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    unsigned int w = warp_sums[lane];
+    for (int d = 1; d < 32; d <<= 1) {
+      const unsigned int v = __shfl_up_sync(0xffffffffu, w, d);
+      if (lane >= d) w += v;
+    }
+    warp_sums[lane] = w;   // inclusive sums of the warps
+  }
+  __syncthreads();
+  unsigned int run = incl - sum + (warp > 0 ? warp_sums[warp - 1] : 0u);
+  for (int i = i0; i < i1; ++i) {
+    pa.start[i] = run;
+    pa.cursor[i] = run;
+    run += pa.count[i];
+  }
+  if (threadIdx.x == kScanThreads - 1) pa.start[P] = run;
+}
+
+// One CTA per group: the group's hashes counted in a shared-memory table of
+// table_slots keys and counts.
+constexpr int kPartCountThreads = 512;
+__global__ void __launch_bounds__(kPartCountThreads)
+part_count_kernel(SketchArgs a, PartArgs pa, unsigned long long *__restrict__ row) {
+  extern __shared__ unsigned long long sh_keys[];   // [C] keys, then [C] counts
+  __shared__ unsigned int empty_count;               // occurrences of the hash equal to kEmptyKey
+  const int C = pa.table_slots;
+  unsigned int *sh_counts = reinterpret_cast<unsigned int *>(sh_keys + C);
+  for (int i = threadIdx.x; i < C; i += kPartCountThreads) {
+    sh_keys[i] = kEmptyKey;
+    sh_counts[i] = 0;
+  }
+  if (threadIdx.x == 0) empty_count = 0;
+  __syncthreads();
+  const unsigned int b0 = pa.start[blockIdx.x], b1 = pa.start[blockIdx.x + 1];
+  for (unsigned int i = b0 + threadIdx.x; i < b1; i += kPartCountThreads) {
+    const unsigned long long h = pa.hashes[i];
+    unsigned int old;
+    if (h == kEmptyKey) {
+      old = atomicAdd(&empty_count, 1u);
+    } else {
+      uint32_t slot = static_cast<uint32_t>(table_slot(h, static_cast<uint64_t>(C - 1)));
+      int probe = 0;
+      for (; probe < C; ++probe) {
+        unsigned long long cur = *reinterpret_cast<volatile unsigned long long *>(sh_keys + slot);
+        if (cur == kEmptyKey) {
+          cur = atomicCAS(sh_keys + slot, kEmptyKey, h);
+          if (cur == kEmptyKey) cur = h;
+        }
+        if (cur == h) break;
+        slot = (slot + 1) & static_cast<uint32_t>(C - 1);
+      }
+      if (probe == C) {   // more distinct hashes than slots (sized at twice the expected: not reached)
+        atomicOr(&a.status->error, kErrTable);
+        continue;
+      }
+      old = atomicAdd(sh_counts + slot, 1u);
+    }
+    if (old + 1 == a.min_count) {
+      const uint64_t sign = mod_sign(h);
+      const uint32_t q = bin_of(sign, a.binsize, a.magic);
+      if (sign < row[q]) atomicMin(row + q, static_cast<unsigned long long>(sign));
+    }
+  }
+}
+
 __device__ __forceinline__ uint64_t univhash(uint64_t s, uint64_t t) {
   const uint64_t x = 1009ULL * s + (1000ULL * 1000ULL + 3ULL) * t;
   return (48271ULL * x + 11ULL) % ((1ULL << 31) - 1ULL);
@@ -775,12 +917,62 @@ uint64_t next_pow2(uint64_t v) {
   return p;
 }
 
-// Bins rows of one batch with the exact count filter: per sample and k, the
-// hashes are counted in a table of twice the sample's windows (in bin-range
-// passes when that exceeds the table budget), a hash entering its bin when
-// its count reaches min_count.  The counting items are an eighth of the
-// hashing ones (no per-CTA bins to amortise; more CTAs in flight hide the
-// table's memory latency).
+// Groups of the partitioned count: about kPartHashes hashes each, at most
+// 2^kMaxLog2Parts groups, tables of 2048..kMaxPartSlots slots (twice the
+// expected hashes of a group).
+constexpr int64_t kPartHashes = 4096;
+constexpr int kMaxLog2Parts = 15;
+constexpr int kMaxPartSlots = 16384;
+
+// The exact count of one (sample, k) by groups of hashes (part_kernel,
+// part_scan_kernel, part_count_kernel); `windows` bounds the sample's hashes.
+sk_status count_partitioned(SketchCall &c, const Batch &b, SketchArgs &args, std::vector<SketchItem> &items,
+                            int64_t s, int k, const PartArgs &pa) {
+  sk_ctx *ctx = c.ctx;
+  const int K = static_cast<int>(c.kmers.size());
+  items.clear();
+  make_items(c, b, s, s + 1, k, items);
+  if (items.empty()) return SK_OK;
+  void *p = nullptr;
+  sk_status st = scratch(ctx, kSlotSketchItems, items.size() * sizeof(SketchItem), &p);
+  if (st == SK_OK) st = upload(ctx, p, items.data(), items.size() * sizeof(SketchItem));
+  if (st != SK_OK) return st;
+  args.items = static_cast<SketchItem *>(p);
+  const int P = 1 << pa.log2p;
+  const size_t part_smem = static_cast<size_t>(P) * 4;
+  const size_t table_smem = static_cast<size_t>(pa.table_slots) * 12;
+  auto hist = c.codon_phased ? (c.use_rc ? part_kernel<true, true, false> : part_kernel<false, true, false>)
+                             : (c.use_rc ? part_kernel<true, false, false> : part_kernel<false, false, false>);
+  auto scat = c.codon_phased ? (c.use_rc ? part_kernel<true, true, true> : part_kernel<false, true, true>)
+                             : (c.use_rc ? part_kernel<true, false, true> : part_kernel<false, false, true>);
+  cudaError_t e = cudaFuncSetAttribute(hist, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(part_smem));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(scat, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(part_smem));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(part_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(table_smem));
+  if (e == cudaSuccess) e = cudaMemsetAsync(pa.count, 0, part_smem, ctx->stream);
+  const unsigned grid = static_cast<unsigned>(items.size());
+  if (e == cudaSuccess) {
+    hist<<<grid, kSketchThreads, part_smem, ctx->stream>>>(args, pa);
+    part_scan_kernel<<<1, kScanThreads, 0, ctx->stream>>>(pa);
+    scat<<<grid, kSketchThreads, part_smem, ctx->stream>>>(args, pa);
+    unsigned long long *row = args.signs + ((s - b.s0) * K + k) * static_cast<int64_t>(c.nbins);
+    part_count_kernel<<<static_cast<unsigned>(P), kPartCountThreads, table_smem, ctx->stream>>>(args, pa, row);
+    e = cudaGetLastError();
+  }
+  return e == cudaSuccess ? SK_OK : cuda_fail(ctx, e, "sketch counting");
+}
+
+// Bins rows of one batch with the exact count filter, a hash entering its bin
+// when its count reaches min_count.  Per sample and k the hashes are counted
+// by groups (count_partitioned) when the sample's hash buffer fits the table
+// budget and its groups fit shared memory; otherwise in a global table of
+// twice the sample's windows (in bin-range passes when that exceeds the
+// budget).  The table pass's items are an eighth of the hashing ones (no
+// per-CTA bins to amortise; more CTAs in flight hide the table's memory
+// latency).
 constexpr int64_t kCountItemWindows = kItemWindows / 8;
 
 sk_status count_batch(SketchCall &c, const Batch &b, SketchArgs &args, std::vector<SketchItem> &items) {
@@ -796,9 +988,33 @@ sk_status count_batch(SketchCall &c, const Batch &b, SketchArgs &args, std::vect
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = 0;
     kTableBudget = std::max<uint64_t>(1ULL << 30, free_b > (2ULL << 30) ? (free_b - (2ULL << 30)) / 4 : 0);
   }
+  args.min_count = static_cast<unsigned int>(c.min_count);
   for (int64_t s = b.s0; s < b.s1; ++s) {
     const int64_t windows = c.seq_off[c.sample_seqs[s + 1]] - c.seq_off[c.sample_seqs[s]];
     if (windows <= 0) continue;
+    int log2p = 0;
+    while (log2p < kMaxLog2Parts && (kPartHashes << log2p) < windows) ++log2p;
+    const int64_t per_part = (windows + (int64_t(1) << log2p) - 1) >> log2p;
+    const int part_slots =
+        static_cast<int>(std::max<uint64_t>(2048, next_pow2(static_cast<uint64_t>(per_part) * 2)));
+    const uint64_t part_bytes = static_cast<uint64_t>(windows) * 8 + ((uint64_t(3) << log2p) + 1) * 4 + 256;
+    if (part_slots <= kMaxPartSlots && windows < (int64_t(1) << 32) && part_bytes <= kTableBudget) {
+      void *tk = nullptr;
+      sk_status st = scratch(ctx, kSlotSketchTable, part_bytes, &tk);
+      if (st != SK_OK) return st;
+      PartArgs pa{};
+      pa.hashes = static_cast<unsigned long long *>(tk);
+      pa.count = reinterpret_cast<unsigned int *>(pa.hashes + windows);
+      pa.cursor = pa.count + (1 << log2p);
+      pa.start = pa.cursor + (1 << log2p);
+      pa.log2p = log2p;
+      pa.table_slots = part_slots;
+      for (int k = 0; k < K; ++k) {
+        st = count_partitioned(c, b, args, items, s, k, pa);
+        if (st != SK_OK) return st;
+      }
+      continue;
+    }
     const uint64_t want = next_pow2(static_cast<uint64_t>(windows) * 2);
     const uint64_t passes = std::max<uint64_t>(1, (want * sizeof(TableSlot) + kTableBudget - 1) / kTableBudget);
     const uint64_t slots = std::max<uint64_t>(1024, next_pow2((want + passes - 1) / passes));

@@ -264,3 +264,28 @@ def test_codon_phased_device_entry_point(gpu_ctx):
     capi.sketch_device(gpu_ctx, buf.data_ptr(), off, ss, kmers, 64, words.data_ptr(),
                        codon_phased=True)
     np.testing.assert_array_equal(words.cpu().numpy().view(np.uint64), want[0])
+
+
+@pytest.mark.parametrize("min_count", [2, 40])
+def test_read_filter_with_skewed_hash_groups(gpu_ctx, min_count):
+    """Counting groups hashes by range of their sign; low-complexity reads
+    (homopolymers, short tandem repeats, thousands of copies of one read) pile
+    most occurrences into a few groups, next to ordinary reads spread over all
+    of them.  The sketch equals the oracle's exact count."""
+    from sketchlib_b200 import capi
+    rng = np.random.default_rng(91 + min_count)
+    genome = np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, 40_000)]
+    reads = []
+    for _ in range(6 * 40_000 // 100):
+        s = int(rng.integers(0, 40_000 - 100))
+        r = genome[s:s + 100].copy()
+        e = rng.random(100) < 0.01
+        r[e] = np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, int(e.sum()))]
+        reads.append(r.tobytes())
+    copy = genome[1000:1100].tobytes()
+    reads += [b"A" * 100, b"CA" * 50, b"GGT" * 33 + b"G"] * 300 + [copy] * 3000
+    order = rng.permutation(len(reads))
+    bases, off, ss = capi.pack_sequences([[reads[i] for i in order]])
+    kmers = [15, 21, 27]
+    check(capi.sketch(gpu_ctx, bases, off, ss, kmers, 64, min_count=min_count),
+          oracle.sketch(bases, off, ss, kmers, 64, True, min_count=min_count))
