@@ -516,6 +516,32 @@ struct PartArgs {
   int table_slots;              // slots of one group's counting table (a power of two)
 };
 
+// The scatter roll's emitter: 8 hashes at a time, their ranks in their
+// groups taken by 8 independent shared-memory atomics before the 8 stores, so
+// no store waits on its own atomic alone.
+struct ScatterBatch {
+  static constexpr int kBatch = 8;
+  unsigned int *rank;           // [P] next position of each group for this CTA
+  unsigned long long *out;
+  int shift;
+  uint64_t h[kBatch];
+  bool v[kBatch];
+
+  __device__ __forceinline__ void put(int i, uint64_t hash, bool valid) {
+    h[i] = hash;
+    v[i] = valid;
+  }
+  __device__ __forceinline__ void flush() {
+    unsigned int pos[kBatch];
+#pragma unroll
+    for (int j = 0; j < kBatch; ++j)
+      if (v[j]) pos[j] = atomicAdd(rank + (mod_sign(h[j]) >> shift), 1u);
+#pragma unroll
+    for (int j = 0; j < kBatch; ++j)
+      if (v[j]) out[pos[j]] = h[j];
+  }
+};
+
 // kScatter false: per-group counts; true: the hashes into their groups (the
 // cursors start at the groups' first positions).
 template <bool kRc, bool kPhased, bool kScatter>
@@ -548,11 +574,10 @@ part_kernel(SketchArgs a, PartArgs pa) {
       if (n) sh_part[i] = atomicAdd(pa.cursor + i, n);
     }
     __syncthreads();
-    if (s < e)
-      roll_windows<kRc, kPhased>(a.codes, s, e, it.k, tab, [&](uint64_t h) {
-        const unsigned int pos = atomicAdd(&sh_part[mod_sign(h) >> shift], 1u);
-        pa.hashes[pos] = h;
-      });
+    if (s < e) {
+      ScatterBatch emit{sh_part, pa.hashes, shift, {}, {}};
+      roll_windows<kRc, kPhased>(a.codes, s, e, it.k, tab, emit);
+    }
   }
 }
 
@@ -927,11 +952,16 @@ constexpr int kMaxPartSlots = 16384;
 // The exact count of one (sample, k) by groups of hashes (part_kernel,
 // part_scan_kernel, part_count_kernel); `windows` bounds the sample's hashes.
 sk_status count_partitioned(SketchCall &c, const Batch &b, SketchArgs &args, std::vector<SketchItem> &items,
-                            int64_t s, int k, const PartArgs &pa) {
+                            int64_t s, int k, int64_t windows, const PartArgs &pa) {
   sk_ctx *ctx = c.ctx;
   const int K = static_cast<int>(c.kmers.size());
+  // items: two per SM where the sample allows, but at least 4 P windows each,
+  // so that a CTA's P group counters (added to the global ones once per CTA)
+  // stay few against its windows
+  const int64_t per_item = std::min<int64_t>(
+      kItemWindows, std::max<int64_t>(int64_t(4) << pa.log2p, (windows + 2 * ctx->sm_count - 1) / (2 * ctx->sm_count)));
   items.clear();
-  make_items(c, b, s, s + 1, k, items);
+  make_items(c, b, s, s + 1, k, items, per_item);
   if (items.empty()) return SK_OK;
   void *p = nullptr;
   sk_status st = scratch(ctx, kSlotSketchItems, items.size() * sizeof(SketchItem), &p);
@@ -1010,7 +1040,7 @@ sk_status count_batch(SketchCall &c, const Batch &b, SketchArgs &args, std::vect
       pa.log2p = log2p;
       pa.table_slots = part_slots;
       for (int k = 0; k < K; ++k) {
-        st = count_partitioned(c, b, args, items, s, k, pa);
+        st = count_partitioned(c, b, args, items, s, k, windows, pa);
         if (st != SK_OK) return st;
       }
       continue;
