@@ -140,9 +140,11 @@ sk_status sk_ctx_set_semantics(sk_ctx *ctx, int32_t semantics);
  * computes, as the reference splits an all-vs-all that exceeds device memory
  * into chunks (query_db_cuda, src/gpu/gpu_api.cpp:357-389); query-vs-reference
  * outputs are blocked the same way (the reference refuses them).  The same
- * limit bounds sk_sketch's k-mer count table for read sets: a quarter of it
- * (default: a quarter of the free memory less 2 GiB) per counting pass, more
- * passes over bin ranges when a sample's table would be larger. */
+ * limit bounds sk_sketch's k-mer counting for read sets: a quarter of it
+ * (default: a quarter of the free memory less 2 GiB) holds a sample's hashes
+ * grouped by range (8 bytes per base); a sample larger than that is counted
+ * in a global table, in passes over bin ranges when the table would exceed
+ * the quarter. */
 sk_status sk_ctx_set_memory_limit(sk_ctx *ctx, int64_t bytes);
 int32_t sk_tile_config_count(void);
 /* Describes shape `config_id`: rows x cols of the CTA tile and per-thread block. */
