@@ -508,6 +508,7 @@ count_kernel(SketchArgs a) {
 // occurrence of a hash lands in the same group, so the counts are exact and
 // the result does not depend on the order of the writes.
 struct PartArgs {
+  unsigned int *cta_count;      // [items][P] hashes per group of each CTA (count roll)
   unsigned int *count;          // [P] hashes per group
   unsigned int *cursor;         // [P] next free position of each group
   unsigned int *start;          // [P + 1] first position of each group
@@ -542,8 +543,10 @@ struct ScatterBatch {
   }
 };
 
-// kScatter false: per-group counts; true: the hashes into their groups (the
-// cursors start at the groups' first positions).
+// kScatter false: the count roll, per-group counts of the CTA (kept) and of
+// the sample; true: the scatter roll, the hashes into their groups (the
+// cursors start at the groups' first positions), each CTA reserving its
+// ranges from the counts its item's count roll kept.
 template <bool kRc, bool kPhased, bool kScatter>
 __global__ void __launch_bounds__(kSketchThreads, 1)
 part_kernel(SketchArgs a, PartArgs pa) {
@@ -552,26 +555,30 @@ part_kernel(SketchArgs a, PartArgs pa) {
   const SketchItem it = a.items[blockIdx.x];
   const int P = 1 << pa.log2p;
   const int shift = 61 - pa.log2p;
-  for (int i = threadIdx.x; i < P; i += kSketchThreads) sh_part[i] = 0;
+  unsigned int *mine = pa.cta_count + static_cast<int64_t>(blockIdx.x) * P;
   if (threadIdx.x < 64) {
     const ulonglong2 *src = reinterpret_cast<const ulonglong2 *>(a.tables + it.tab);
     reinterpret_cast<ulonglong2 *>(&tab)[threadIdx.x] = src[threadIdx.x];
   }
-  __syncthreads();
   const int64_t s = it.begin + static_cast<int64_t>(threadIdx.x) * it.per;
   const int64_t e = min(s + it.per, it.end);
-  if (s < e)
-    roll_windows<kRc, kPhased>(a.codes, s, e, it.k, tab, [&](uint64_t h) {
-      atomicAdd(&sh_part[mod_sign(h) >> shift], 1u);
-    });
-  __syncthreads();
   if constexpr (!kScatter) {
-    for (int i = threadIdx.x; i < P; i += kSketchThreads)
-      if (sh_part[i]) atomicAdd(pa.count + i, sh_part[i]);
-  } else {
+    for (int i = threadIdx.x; i < P; i += kSketchThreads) sh_part[i] = 0;
+    __syncthreads();
+    if (s < e)
+      roll_windows<kRc, kPhased>(a.codes, s, e, it.k, tab, [&](uint64_t h) {
+        atomicAdd(&sh_part[mod_sign(h) >> shift], 1u);
+      });
+    __syncthreads();
     for (int i = threadIdx.x; i < P; i += kSketchThreads) {
       const unsigned int n = sh_part[i];
-      if (n) sh_part[i] = atomicAdd(pa.cursor + i, n);
+      mine[i] = n;
+      if (n) atomicAdd(pa.count + i, n);
+    }
+  } else {
+    for (int i = threadIdx.x; i < P; i += kSketchThreads) {
+      const unsigned int n = mine[i];
+      sh_part[i] = n ? atomicAdd(pa.cursor + i, n) : 0u;
     }
     __syncthreads();
     if (s < e) {
@@ -952,14 +959,9 @@ constexpr int kMaxPartSlots = 16384;
 // The exact count of one (sample, k) by groups of hashes (part_kernel,
 // part_scan_kernel, part_count_kernel); `windows` bounds the sample's hashes.
 sk_status count_partitioned(SketchCall &c, const Batch &b, SketchArgs &args, std::vector<SketchItem> &items,
-                            int64_t s, int k, int64_t windows, const PartArgs &pa) {
+                            int64_t s, int k, int64_t per_item, const PartArgs &pa) {
   sk_ctx *ctx = c.ctx;
   const int K = static_cast<int>(c.kmers.size());
-  // items: two per SM where the sample allows, but at least 4 P windows each,
-  // so that a CTA's P group counters (added to the global ones once per CTA)
-  // stay few against its windows
-  const int64_t per_item = std::min<int64_t>(
-      kItemWindows, std::max<int64_t>(int64_t(4) << pa.log2p, (windows + 2 * ctx->sm_count - 1) / (2 * ctx->sm_count)));
   items.clear();
   make_items(c, b, s, s + 1, k, items, per_item);
   if (items.empty()) return SK_OK;
@@ -1027,7 +1029,12 @@ sk_status count_batch(SketchCall &c, const Batch &b, SketchArgs &args, std::vect
     const int64_t per_part = (windows + (int64_t(1) << log2p) - 1) >> log2p;
     const int part_slots =
         static_cast<int>(std::max<uint64_t>(2048, next_pow2(static_cast<uint64_t>(per_part) * 2)));
-    const uint64_t part_bytes = static_cast<uint64_t>(windows) * 8 + ((uint64_t(3) << log2p) + 1) * 4 + 256;
+    // items of the grouped count: two per SM, at least 4 P windows each
+    const int64_t per_item = std::min<int64_t>(
+        kItemWindows, std::max<int64_t>(int64_t(4) << log2p, (windows + 2 * ctx->sm_count - 1) / (2 * ctx->sm_count)));
+    const int64_t max_items = (windows + per_item - 1) / per_item + 1;   // items of one k
+    const uint64_t part_bytes = static_cast<uint64_t>(windows) * 8 + ((uint64_t(3) << log2p) + 1) * 4 +
+                                (static_cast<uint64_t>(max_items) << log2p) * 4 + 256;
     if (part_slots <= kMaxPartSlots && windows < (int64_t(1) << 32) && part_bytes <= kTableBudget) {
       void *tk = nullptr;
       sk_status st = scratch(ctx, kSlotSketchTable, part_bytes, &tk);
@@ -1037,10 +1044,11 @@ sk_status count_batch(SketchCall &c, const Batch &b, SketchArgs &args, std::vect
       pa.count = reinterpret_cast<unsigned int *>(pa.hashes + windows);
       pa.cursor = pa.count + (1 << log2p);
       pa.start = pa.cursor + (1 << log2p);
+      pa.cta_count = pa.start + (1 << log2p) + 1;
       pa.log2p = log2p;
       pa.table_slots = part_slots;
       for (int k = 0; k < K; ++k) {
-        st = count_partitioned(c, b, args, items, s, k, windows, pa);
+        st = count_partitioned(c, b, args, items, s, k, per_item, pa);
         if (st != SK_OK) return st;
       }
       continue;
