@@ -640,8 +640,10 @@ part_count_kernel(SketchArgs a, PartArgs pa, unsigned long long *__restrict__ ro
   if (threadIdx.x == 0) empty_count = 0;
   __syncthreads();
   const unsigned int b0 = pa.start[blockIdx.x], b1 = pa.start[blockIdx.x + 1];
+  unsigned long long next = b0 + threadIdx.x < b1 ? pa.hashes[b0 + threadIdx.x] : 0ULL;
   for (unsigned int i = b0 + threadIdx.x; i < b1; i += kPartCountThreads) {
-    const unsigned long long h = pa.hashes[i];
+    const unsigned long long h = next;   // this hash; the next one loads meanwhile
+    if (i + kPartCountThreads < b1) next = pa.hashes[i + kPartCountThreads];
     unsigned int old;
     if (h == kEmptyKey) {
       old = atomicAdd(&empty_count, 1u);
@@ -657,7 +659,7 @@ part_count_kernel(SketchArgs a, PartArgs pa, unsigned long long *__restrict__ ro
         if (cur == h) break;
         slot = (slot + 1) & static_cast<uint32_t>(C - 1);
       }
-      if (probe == C) {   // more distinct hashes than slots (sized at twice the expected: not reached)
+      if (probe == C) {   // more distinct hashes than slots (1.5 per base of the group: not reached)
         atomicOr(&a.status->error, kErrTable);
         continue;
       }
@@ -949,9 +951,9 @@ uint64_t next_pow2(uint64_t v) {
   return p;
 }
 
-// Groups of the partitioned count: about kPartHashes hashes each, at most
-// 2^kMaxLog2Parts groups, tables of 2048..kMaxPartSlots slots (twice the
-// expected hashes of a group).
+// Groups of the partitioned count: at most kPartHashes bases per group (while
+// there are at most 2^kMaxLog2Parts groups), tables of 2048..kMaxPartSlots
+// slots (1.5 times the bases of a group, the hashes' upper bound).
 constexpr int64_t kPartHashes = 4096;
 constexpr int kMaxLog2Parts = 15;
 constexpr int kMaxPartSlots = 16384;
@@ -1027,8 +1029,10 @@ sk_status count_batch(SketchCall &c, const Batch &b, SketchArgs &args, std::vect
     int log2p = 0;
     while (log2p < kMaxLog2Parts && (kPartHashes << log2p) < windows) ++log2p;
     const int64_t per_part = (windows + (int64_t(1) << log2p) - 1) >> log2p;
+    // 1.5 slots per base of a group: the distinct hashes (at most the
+    // bases) fill at most two thirds of a table
     const int part_slots =
-        static_cast<int>(std::max<uint64_t>(2048, next_pow2(static_cast<uint64_t>(per_part) * 2)));
+        static_cast<int>(std::max<uint64_t>(2048, next_pow2(static_cast<uint64_t>(per_part) * 3 / 2)));
     // items of the grouped count: two per SM, at least 4 P windows each
     const int64_t per_item = std::min<int64_t>(
         kItemWindows, std::max<int64_t>(int64_t(4) << log2p, (windows + 2 * ctx->sm_count - 1) / (2 * ctx->sm_count)));
