@@ -959,7 +959,8 @@ constexpr int kMaxLog2Parts = 15;
 constexpr int kMaxPartSlots = 16384;
 
 // The exact count of one (sample, k) by groups of hashes (part_kernel,
-// part_scan_kernel, part_count_kernel); `windows` bounds the sample's hashes.
+// part_scan_kernel, part_count_kernel), in items of at most per_item window
+// starts; pa's buffers hold the sample's hashes and its groups.
 sk_status count_partitioned(SketchCall &c, const Batch &b, SketchArgs &args, std::vector<SketchItem> &items,
                             int64_t s, int k, int64_t per_item, const PartArgs &pa) {
   sk_ctx *ctx = c.ctx;
