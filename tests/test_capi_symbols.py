@@ -41,3 +41,37 @@ def test_no_device_needed_for_metadata():
     cfgs = capi.tile_configs()
     assert cfgs and all(c["tile_rows"] % c["tile_cols"] == 0 for c in cfgs)
     assert capi.lib.sk_tile_config_info(999, *([None] * 5)) != 0
+
+
+def header_structs():
+    """Field names, offsets and sizes of the header's plain structs, laid out
+    with the x86-64 C rules (each field aligned to its size)."""
+    text = (ROOT / "include" / "sketchlib_b200.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    sizes = {"int32_t": 4, "uint32_t": 4, "int64_t": 8, "uint64_t": 8, "uint16_t": 2, "double": 8}
+    out = {}
+    for name, body in re.findall(r"typedef struct (\w+) \{(.*?)\} \1;", text, flags=re.S):
+        fields, off = [], 0
+        for typ, ptr, field in re.findall(r"(?:const\s+)?(\w+)\s*(\*?)\s*(\w+);", body):
+            size = 8 if ptr else sizes[typ]
+            off = (off + size - 1) // size * size
+            fields.append((field, off))
+            off += size
+        align = max(8 if p else sizes[t] for t, p, _ in
+                    re.findall(r"(?:const\s+)?(\w+)\s*(\*?)\s*(\w+);", body))
+        out[name] = (fields, (off + align - 1) // align * align)
+    return out
+
+
+@pytest.mark.parametrize("c_name,py_name", [("sk_host_sketches", "HostSketches"),
+                                            ("sk_job", "Job"),
+                                            ("sk_server_params", "ServerParams")])
+def test_ctypes_structs_match_header(c_name, py_name):
+    """The Python binding's ctypes mirrors have the header's fields, in order,
+    at the same offsets, and the same size."""
+    from sketchlib_b200 import capi
+    fields, size = header_structs()[c_name]
+    cls = getattr(capi, py_name)
+    assert [f for f, _ in fields] == [f[0] for f in cls._fields_]
+    assert [o for _, o in fields] == [getattr(cls, f).offset for f, _ in fields]
+    assert ctypes.sizeof(cls) == size
