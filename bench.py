@@ -52,8 +52,10 @@ def n_pairs(n: int) -> int:
     return n * (n - 1) // 2
 
 
-def workload_config(extra=None):
-    cfg = {
+def workload_config():
+    """The workload both arms report (identical dicts: per-arm details such as
+    thread counts and tile shapes sit outside `config`)."""
+    return {
         "workload": "plain all-vs-all, 4,096 bin-level synthetic samples (seeded random tree), "
                     "8 k-mer lengths x 10,000 bins (sketchsize64 156 x 14 planes), float32 "
                     "core/accessory long form",
@@ -61,9 +63,6 @@ def workload_config(extra=None):
         "pairs": n_pairs(N_SAMPLES), "seed": SEED,
         "l2": "inputs larger than L2 (573 MB of packed sketches vs 126 MB L2)",
     }
-    if extra:
-        cfg.update(extra)
-    return cfg
 
 
 # ------------------------------------------------------------------ ranks
@@ -160,16 +159,37 @@ class ClockSampler:
 
 # -------------------------------------------------------------- baselines
 
+def synth_module():
+    """The numpy tree generator (pp-sketchlib_b200/sketchlib_b200/synth.py),
+    loaded from its file alone: importing it through its package would load
+    the library under test, which the reference arm must not map."""
+    import importlib.util
+    path = ROOT / "pp-sketchlib_b200" / "sketchlib_b200" / "synth.py"
+    spec = importlib.util.spec_from_file_location("_bench_synth", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def reference_inputs(threads: int):
+    """The workload's sketches, built by the oracle's restatement of the
+    generator (bit-identical to the library's, tests/test_synth.py)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    synth = synth_module()
+    parent, thresh = synth.random_tree(N_SAMPLES, kmers=KMERS, seed=SEED)
+    return oracle.synth_words(parent, thresh, S64, SEED, threads=threads)
+
+
 def cpu_reference_rate(target_s: float = 15.0, threads: int | None = None):
     """The reference's CPU path (oracle/_ref) on a bounded row sample of the
-    workload; falls back to the oracle port when _ref was not built."""
+    workload; falls back to the oracle port when _ref was not built.  Uses
+    nothing from the library under test."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import numpy as np
     import oracle
-    from sketchlib_b200 import capi, synth
     threads = threads or os.cpu_count() or 1
-    parent, thresh = synth.random_tree(N_SAMPLES, kmers=KMERS, seed=SEED)
-    words = capi.synth_host(parent, thresh, S64, seed=SEED, threads=threads)
+    words = reference_inputs(threads)
     out = np.zeros((n_pairs(N_SAMPLES), 2), np.float32)
     if oracle.ref_available():
         kind = "reference"
@@ -250,7 +270,7 @@ def run_reference_arm(args, rank, world):
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * total_t / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded bin-level tree)",
-        "config": workload_config({"threads": threads}),
+        "config": workload_config(),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -798,9 +818,10 @@ def run_ours(args, rank, world, local):
         "higher_is_better": True, "scaling": "weak",
         "vs_baseline": value / PUBLISHED_GPU,
         "dtype": "u32", "data": "synthetic (seeded bin-level tree, generated on device)",
-        "config": workload_config({"tile_config": args.tile_config or "auto",
-                                   "vs_baseline_ref": "reference README.md:137,140 GPU figure, "
-                                                      "6.0e6 distances/s (RTX 2080 Ti)"}),
+        "config": workload_config(),
+        "tile_config": args.tile_config or "auto",
+        "vs_baseline_source": "reference README.md:137,140 GPU figure, 6.0e6 distances/s "
+                              "(RTX 2080 Ti)",
         "roofline": {"bound": "alu", "achieved": achieved / 1e12, "peak": lop3_peak / 1e12,
                      "unit": "T LOP3/s", "frac": achieved / lop3_peak,
                      "traffic": traffic,

@@ -59,6 +59,8 @@ def _load():
     lib.sko_long_to_square.argtypes = [vp, i64, vp, vp, i64, vp]
     lib.sko_square_to_long.restype = None
     lib.sko_square_to_long.argtypes = [vp, i64, vp]
+    lib.sko_synth_words.restype = i32
+    lib.sko_synth_words.argtypes = [vp, vp, i64, i32, i32, C.c_uint64, vp, i32]
     lib.sko_sketch_samples.restype = None
     lib.sko_sketch_samples.argtypes = [vp, vp, vp, i64, vp, i32, i32, i32, i32, i32, i32, vp, vp,
                                        vp, i32]
@@ -123,6 +125,21 @@ def dists_self_rows(words, kmers, s64, row_begin, row_end, out, threads=NTHREADS
     km = np.ascontiguousarray(kmers, np.int32)
     return lib.sko_dists_self_rows(w.ctypes.data, w.shape[0], len(km), km.ctypes.data, s64, bbits,
                                    row_begin, row_end, out.ctypes.data, threads)
+
+
+def synth_words(parent, thresh, s64, seed, threads=NTHREADS):
+    """Reference-layout words [n][K][s64 * 14] of the seeded bin-level tree
+    generator (parent / thresh from synth.random_tree and friends), computed
+    here so a caller needs nothing from the library under test."""
+    parent = np.ascontiguousarray(parent, np.int32)
+    thresh = np.ascontiguousarray(thresh, np.uint32)
+    n, K = thresh.shape
+    words = np.empty((n, K, s64 * 14), np.uint64)
+    rc = lib.sko_synth_words(parent.ctypes.data, thresh.ctypes.data, n, K, s64,
+                             C.c_uint64(seed & (2 ** 64 - 1)), words.ctypes.data, threads)
+    if rc != 0:
+        raise ValueError("parents must precede their children")
+    return words
 
 
 def intersize(a, b, s64, bbits=14):

@@ -339,6 +339,72 @@ void sko_square_to_long(const float *square, int64_t n, float *long_out) {
     for (int64_t j = i + 1; j < n; j++) long_out[condensed(i, j, n)] = square[i * n + j];
 }
 
+/* ------------------------------------------------------ synthetic inputs */
+
+/* The seeded bin-level tree generator of the benchmarks, restated so the
+ * timed reference arm can build its inputs without the library under test.
+ * Sample s at k-mer index k, bin `bin`: h = splitmix64 finaliser of
+ *   seed ^ s * 0x9E3779B97F4A7C15 ^ ((k << 32 | bin) * 0xC2B2AE3D27D4EB4F);
+ * a root, or a sample whose (h >> 32) < thresh[s][k], takes the 14-bit value
+ * h & 0x3FFF, every other sample its parent's value.  Samples are filled
+ * level by level (parents first), a bin being inherited by copying its bit
+ * from the parent's plane words; the result is the reference word layout
+ * [n][K][s64][bbits] (src/sketch/sketch.cpp:82-92).  Returns -1 when a
+ * parent does not precede its child. */
+static uint64_t sko_mix(uint64_t x) {
+  x ^= x >> 30;
+  x *= 0xBF58476D1CE4E5B9ULL;
+  x ^= x >> 27;
+  x *= 0x94D049BB133111EBULL;
+  x ^= x >> 31;
+  return x;
+}
+
+int sko_synth_words(const int32_t *parent, const uint32_t *thresh, int64_t n, int K, int s64,
+                    uint64_t seed, uint64_t *words, int threads) {
+  const int bbits = 14;
+  int32_t *depth = (int32_t *)malloc((size_t)(n > 0 ? n : 1) * sizeof(int32_t));
+  int32_t max_depth = 0;
+  for (int64_t s = 0; s < n; s++) {
+    if (parent[s] >= s) {
+      free(depth);
+      return -1;
+    }
+    depth[s] = parent[s] < 0 ? 0 : depth[parent[s]] + 1;
+    if (depth[s] > max_depth) max_depth = depth[s];
+  }
+  const int64_t W = (int64_t)s64 * bbits;
+  for (int32_t level = 0; level <= max_depth; level++) {
+#pragma omp parallel for schedule(dynamic, 4) num_threads(threads)
+    for (int64_t s = 0; s < n; s++) {
+      if (depth[s] != level) continue;
+      const int32_t par = parent[s];
+      for (int k = 0; k < K; k++) {
+        const uint32_t th = thresh[s * K + k];
+        uint64_t *o = words + (s * K + k) * W;
+        const uint64_t *po = par < 0 ? NULL : words + ((int64_t)par * K + k) * W;
+        for (int b = 0; b < s64; b++) {
+          uint64_t w[14] = {0}, fresh = 0;
+          for (int i = 0; i < 64; i++) {
+            const uint64_t bin = (uint64_t)b * 64u + (uint64_t)i;
+            const uint64_t h = sko_mix(seed ^ ((uint64_t)s * 0x9E3779B97F4A7C15ULL) ^
+                                       ((((uint64_t)k << 32) | bin) * 0xC2B2AE3D27D4EB4FULL));
+            if (par < 0 || (uint32_t)(h >> 32) < th) {
+              const uint32_t v = (uint32_t)h & 0x3FFFu;
+              fresh |= 1ULL << i;
+              for (int p = 0; p < bbits; p++) w[p] |= (uint64_t)((v >> p) & 1u) << i;
+            }
+          }
+          for (int p = 0; p < bbits; p++)
+            o[b * bbits + p] = po ? (po[b * bbits + p] & ~fresh) | w[p] : w[p];
+        }
+      }
+    }
+  }
+  free(depth);
+  return 0;
+}
+
 /* -------------------------------------------------------------- sketching */
 
 /* ntHash (Mohamadi et al., Bioinformatics 2016) as the reference uses it:

@@ -36,3 +36,16 @@ def test_synth_host_deterministic_and_related():
     s = 5
     shares = [oracle.intersize(w1[s, k], w1[p[s], k], 16) for k in range(8)]
     assert shares[0] >= shares[-1]
+
+
+def test_oracle_generator_matches_library():
+    """The reference arm of the benchmark builds its inputs with the oracle's
+    restatement of the generator; it must give the library's words bit for bit."""
+    for n, K, s64, seed in ((40, 8, 16, 11), (300, 3, 5, 0x5EED0002), (1, 2, 4, 7)):
+        kmers = list(range(15, 15 + 2 * K, 2))
+        p, t = synth.random_tree(n, kmers=kmers, seed=seed)
+        np.testing.assert_array_equal(oracle.synth_words(p, t, s64, seed, threads=3),
+                                      capi.synth_host(p, t, s64, seed=seed, threads=2))
+    p, t = synth.clade_tree(500, n_clades=7, seed=5)
+    np.testing.assert_array_equal(oracle.synth_words(p, t, 8, 99),
+                                  capi.synth_host(p, t, 8, seed=99))
