@@ -207,6 +207,12 @@ sk_status sk_random_destroy(sk_random *random);
  * sk_server_submit. */
 sk_status sk_closest_cluster(const float *centroids, int32_t n_clusters, int32_t use_rc,
                              const double *base_freq, int64_t n, uint16_t *cluster_out);
+/* Gives a table model its base-composition centroids [n_clusters][4] (the
+ * /random/centroids of a database, Database::load_random,
+ * src/database/database.cpp:195-227), from which the query server assigns
+ * clusters with sk_closest_cluster under the model's use_rc. */
+sk_status sk_random_set_centroids(sk_random *random, const float *centroids,
+                                  int32_t n_clusters);
 
 /* ---- dense distances ---------------------------------------------------- */
 
@@ -347,24 +353,42 @@ typedef struct sk_server_params {
   int32_t large_slice_queries;  /* slice size for larger requests, 1..slice_queries
                                    (0: slice_queries); smaller slices shorten the wait
                                    of a one-slice request behind a large one */
+  int64_t device_bytes;   /* HBM the slots may take (0: no budget, `slots` slots).
+                             With a budget the server makes as many slots as fit in
+                             it, at most `slots`; a budget below one slot is
+                             refused with SK_ENOMEM (sk_server_info reports the
+                             bytes one slot holds) */
 } sk_server_params;
 
 /* Starts a server over `ref` (kept resident; it must outlive the server).
  * Every slot's buffers and kernel scratch are allocated here, so the HBM
- * footprint is fixed and requests are admitted as slots free up.  Free slots
- * go to the request with the fewest queries left (a request waiting over 2 s
- * first); one-slice requests run on a high-priority stream, and slices of
- * larger requests hold at most half the slots.  The context's tile shape, tuning
- * and semantics at this moment apply to every request.  No reference
- * counterpart: the reference answers one query_db_cuda call at a time
- * (src/gpu/gpu_api.cpp:352). */
+ * footprint is fixed (slots x slot bytes, bounded by device_bytes) and
+ * queries are admitted onto the device as slots, i.e. their memory, free up.
+ * A slot runs one slice: up to slice_queries queries, which may come from
+ * several requests.  Free slots go to the request with the fewest queries left
+ * (a request waiting over 2 s first); whole requests of at most slice_queries
+ * queries are packed together into one slice on a high-priority stream, and
+ * slices of larger requests (large_slice_queries each, the tail of one request
+ * packed with the head of the next) hold at most half the slots.  Free rows
+ * of a slice's last query tile are filled with queries of larger requests.
+ * The context's tile shape, tuning and semantics at this moment apply to
+ * every request.  No reference counterpart: the reference answers one
+ * query_db_cuda call at a time (src/gpu/gpu_api.cpp:352). */
 sk_status sk_server_create(sk_ctx *ctx, const sk_db *ref, const sk_random *random,
                            const sk_server_params *params, sk_server **out);
 /* Queues a request: n_queries sketches in the reference word layout (host
- * memory that must stay valid until the request is done), optional per-query
- * random-match cluster ids and sequence lengths.  Thread-safe. */
+ * memory that must stay valid until the request is done), and optional
+ * per-query random-match inputs: cluster ids, sequence lengths and base
+ * compositions base_freq [n][4] (A, C, G, T).  Under a table random model
+ * with centroids (sk_random_set_centroids), queries without cluster ids get
+ * the nearest centroid of their base composition, as the reference assigns
+ * queries missing from its cluster table (RandomMC::lookup_array /
+ * closest_cluster, src/random/random_match.cpp:222-227, 254-273).  Queries
+ * with neither get cluster 0 and length 0, as sk_db_set_sample_info with
+ * NULL.  Thread-safe. */
 sk_status sk_server_submit(sk_server *server, const uint64_t *query_words, int64_t n_queries,
-                           const uint16_t *cluster, const uint64_t *seq_len, int64_t *ticket);
+                           const uint16_t *cluster, const uint64_t *seq_len,
+                           const double *base_freq, int64_t *ticket);
 /* Waits for a request (bounded by timeout_s; SK_ETIMEDOUT when it runs out). */
 sk_status sk_server_wait(sk_server *server, int64_t ticket, double timeout_s);
 /* Copies a finished request's results: knn_idx / knn_dist [n_queries][kNN]
@@ -376,6 +400,11 @@ sk_status sk_server_result(sk_server *server, int64_t ticket, int64_t *knn_idx, 
 sk_status sk_server_release(sk_server *server, int64_t ticket);
 sk_status sk_server_stats(sk_server *server, int64_t *pairs_done, double *uptime_s,
                           int64_t *queued_queries);
+/* Slots the server made, HBM one slot holds, and slices run so far with the
+ * number of requests they carried (slices_shared: slices holding queries of
+ * more than one request). */
+sk_status sk_server_info(sk_server *server, int32_t *slots, int64_t *slot_bytes,
+                         int64_t *slices, int64_t *slices_shared);
 /* Finishes the queued work, stops the scheduler thread and frees the slots. */
 sk_status sk_server_destroy(sk_server *server);
 

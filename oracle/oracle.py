@@ -59,6 +59,8 @@ def _load():
     lib.sko_long_to_square.argtypes = [vp, i64, vp, vp, i64, vp]
     lib.sko_square_to_long.restype = None
     lib.sko_square_to_long.argtypes = [vp, i64, vp]
+    lib.sko_closest_cluster.restype = None
+    lib.sko_closest_cluster.argtypes = [vp, i32, i32, vp, i64, vp]
     lib.sko_synth_words.restype = i32
     lib.sko_synth_words.argtypes = [vp, vp, i64, i32, i32, C.c_uint64, vp, i32]
     lib.sko_sketch_samples.restype = None
@@ -125,6 +127,16 @@ def dists_self_rows(words, kmers, s64, row_begin, row_end, out, threads=NTHREADS
     km = np.ascontiguousarray(kmers, np.int32)
     return lib.sko_dists_self_rows(w.ctypes.data, w.shape[0], len(km), km.ctypes.data, s64, bbits,
                                    row_begin, row_end, out.ctypes.data, threads)
+
+
+def closest_cluster(centroids, base_freq, use_rc=True):
+    """Cluster ids [n] of compositions base_freq [n][4] against centroids [C][4]."""
+    c = np.ascontiguousarray(centroids, np.float32)
+    b = np.ascontiguousarray(base_freq, np.float64).reshape(-1, 4)
+    out = np.zeros(b.shape[0], np.uint16)
+    lib.sko_closest_cluster(c.ctypes.data, c.shape[0], int(use_rc), b.ctypes.data, b.shape[0],
+                            out.ctypes.data)
+    return out
 
 
 def synth_words(parent, thresh, s64, seed, threads=NTHREADS):

@@ -18,6 +18,8 @@
  *   sko_sparsify       sparsify_dists_by_threshold src/dist/matrix_ops.cpp:38-69
  *   sko_long_to_square long_to_square            src/dist/matrix_ops.cpp:71-126
  *   sko_square_to_long square_to_long            src/dist/matrix_ops.cpp:130-150
+ *   sko_closest_cluster closest_cluster / nearest_neighbour
+ *                                                src/random/random_match.cpp:222-227, 338-359
  *   sko_sketch         sketch (one sample, one k) src/sketch/sketch.cpp:120-168
  *                      stHashIterator / NTMC64   src/sketch/stHashIterator.hpp:63-120,
  *                                                src/sketch/nthash.hpp:57-126, 341-372
@@ -337,6 +339,43 @@ void sko_long_to_square(const float *rr, int64_t n_rr, const float *qr, const fl
 void sko_square_to_long(const float *square, int64_t n, float *long_out) {
   for (int64_t i = 0; i < n; i++)
     for (int64_t j = i + 1; j < n; j++) long_out[condensed(i, j, n)] = square[i * n + j];
+}
+
+/* ------------------------------------------------- query cluster lookup */
+
+/* Cluster of a query missing from the Monte Carlo model's table
+ * (RandomMC::lookup_array -> closest_cluster -> nearest_neighbour,
+ * src/random/random_match.cpp:254-273, 222-227, 351-359; apply_rc :338-349):
+ * with use_rc the A/T and C/G frequencies are averaged; the composition is
+ * cast to float and the centroid [C][4] with the smallest squared distance,
+ * summed over A, C, G, T in order, is taken, the first on a tie; 0 without
+ * clusters. */
+void sko_closest_cluster(const float *centroids, int n_clusters, int use_rc,
+                         const double *base_freq, int64_t n, uint16_t *out) {
+  for (int64_t i = 0; i < n; i++) {
+    double b[4] = {base_freq[4 * i], base_freq[4 * i + 1], base_freq[4 * i + 2],
+                   base_freq[4 * i + 3]};
+    if (use_rc) {
+      b[0] = 0.5 * (b[0] + b[3]);
+      b[1] = 0.5 * (b[1] + b[2]);
+      b[2] = b[1];
+      b[3] = b[0];
+    }
+    int best = 0;
+    float best_d = INFINITY;
+    for (int c = 0; c < n_clusters; c++) {
+      float d = 0.0f;
+      for (int j = 0; j < 4; j++) {
+        const float diff = centroids[c * 4 + j] - (float)b[j];
+        d += diff * diff;
+      }
+      if (d < best_d) {
+        best_d = d;
+        best = c;
+      }
+    }
+    out[i] = (uint16_t)best;
+  }
 }
 
 /* ------------------------------------------------------ synthetic inputs */

@@ -1065,6 +1065,20 @@ sk_status sk_random_create(sk_ctx *ctx, int32_t mode, int32_t use_rc, const int3
   return SK_OK;
 }
 
+sk_status sk_random_set_centroids(sk_random *random, const float *centroids,
+                                  int32_t n_clusters) {
+  if (!random) return SK_EINVAL;
+  sk_ctx *ctx = random->ctx;
+  std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+  ctx->err.clear();
+  if (random->mode != kRandTable)
+    return fail(ctx, SK_EINVAL, "Centroids belong to a Monte Carlo (table) random-match model");
+  if (n_clusters != random->n_clusters || !centroids)
+    return fail(ctx, SK_EINVAL, "Expected %d centroids of 4 base frequencies", random->n_clusters);
+  random->centroids.assign(centroids, centroids + static_cast<size_t>(n_clusters) * 4);
+  return SK_OK;
+}
+
 sk_status sk_closest_cluster(const float *centroids, int32_t n_clusters, int32_t use_rc,
                              const double *base_freq, int64_t n, uint16_t *cluster_out) {
   if (n < 0 || n_clusters < 0 || (n > 0 && (!base_freq || !cluster_out)) ||

@@ -1,15 +1,23 @@
 // serve.cu -- a query server over a reference database resident in HBM.
 //
 // Requests (a batch of query sketches each) arrive at any time from any host
-// thread.  A scheduler thread cuts every request into slices of at most
-// `slice_queries` queries and runs slices on `slots`: each slot owns a
-// context (its own stream and kernel scratch), a packed query buffer, a
-// distance column for the slice against every reference and the kNN result
-// buffers, all allocated once at start-up, so admission is by free slot and
-// the server's HBM footprint is fixed (slots x slot bytes + the reference).
-// Slices of different requests run on different streams and overlap on the
-// device: a slot's persistent kernel takes SMs as another slot's kernel
-// releases them.
+// thread.  A scheduler thread packs waiting queries into slices and runs the
+// slices on `slots`: each slot owns a context (its own stream and kernel
+// scratch), a packed query buffer, a distance column for one slice against
+// every reference and the kNN result buffers, all allocated once at start-up,
+// so admission is by free slot, i.e. by free HBM, and the server's footprint
+// is fixed (slots x slot bytes + the reference; `device_bytes` caps it).
+// Slices run on different streams and overlap on the device: a slot's
+// persistent kernel takes SMs as another slot's kernel releases them.
+//
+// Continuous batching.  A slice is a list of segments, each a run of one
+// request's queries; the slice's queries go up, are packed and are scored as
+// one query database in one launch, and each segment's results go back to its
+// request.  Queries that arrive while the device is busy therefore share the
+// next launch and its query tiles instead of each paying for a whole tile of
+// their own.  Every query's result depends only on that query (its sketch,
+// cluster id and length) and the references, so a request gets bit-identical
+// results alone or in any mix.
 //
 // Scheduling.  The distance kernel is persistent and fills every SM, so
 // slices queued on several streams run one after another; what decides a
@@ -19,19 +27,22 @@
 //     remaining work first), FIFO among equals; a request older than
 //     kStarveSeconds goes ahead of every younger one, so a stream of small
 //     requests cannot hold a large one back for good;
-//   * a request that fits in one slice runs on a high-priority stream: its
-//     kernels start as soon as the slice on the SMs ends, ahead of slices of
-//     larger requests already queued;
-//   * slices of requests larger than one slice hold at most half the slots
-//     (at least one), so a request of one slice finds a slot free and waits
-//     at most for the slice already running, and the device still always has
-//     a large slice queued behind the running one.
+//   * requests of at most slice_queries queries (small) run whole in one
+//     slice on a high-priority stream, packed with other small requests in
+//     that order while they fit: their kernels start as soon as the slice on
+//     the SMs ends, ahead of slices of larger requests already queued;
+//   * slices of larger requests (large_slice_queries queries, the tail of one
+//     request continued by the head of the next) hold at most half the slots
+//     (at least one), so a small request finds a slot free and waits at most
+//     for the slice already running, and the device still always has a large
+//     slice queued behind the running one;
+//   * rows left free in a slice's last query tile are filled with queries of
+//     larger requests: the kernel computes whole tiles anyway.
 //
-// Per slice: pinned staging copy of the query words, H2D, pack, the distance
-// kernel (core or accessory column vs all references, optionally the full
-// core/accessory rows), per-query top-kNN, D2H of the kNN lists (and rows).
-// Results of each query depend only on that query and the references, so a
-// request gets bit-identical results alone or in any mix.
+// Per slice: pinned staging copy of the query words, cluster ids and
+// lengths, H2D, pack, the distance kernel (core or accessory column vs all
+// references, optionally the full core/accessory rows), per-query top-kNN,
+// D2H of the kNN lists (and rows).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -58,8 +69,8 @@ struct Request {
   int64_t id = 0;
   const uint64_t *words = nullptr;   // caller's host buffer, kept alive until done
   int64_t n = 0;
-  std::vector<uint16_t> cluster;
-  std::vector<uint64_t> seq_len;
+  std::vector<uint16_t> cluster;     // [n] random-match cluster per query
+  std::vector<uint64_t> seq_len;     // [n] sequence length per query
   int64_t dispatched = 0;            // queries handed to slots
   int64_t completed = 0;             // queries finished
   int inflight = 0;                  // slices on the device
@@ -72,11 +83,19 @@ struct Request {
   bool done = false;
 };
 
+// A run of one request's queries inside a slice: queries q0 .. q0+nq-1 of
+// the request are slice rows row0 .. row0+nq-1.
+struct Segment {
+  std::shared_ptr<Request> req;
+  int64_t q0 = 0, nq = 0, row0 = 0;
+};
+
 struct Slot {
   sk_ctx *ctx = nullptr;
   sk_db qdb;                         // packed query buffer (pre-allocated)
   uint64_t *d_words = nullptr;       // staging of the reference-layout words
   uint64_t *h_words = nullptr;       // pinned host staging
+  uint16_t *h_cluster = nullptr;     // pinned cluster ids of the slice's queries
   float *d_col = nullptr;            // [slice][n_ref] distance column
   float *d_rows = nullptr;           // [slice][n_ref][2] core/accessory (optional)
   int64_t *d_knn = nullptr;
@@ -86,9 +105,9 @@ struct Slot {
   float *h_rows = nullptr;
   cudaEvent_t done_ev = nullptr;
   cudaStream_t lo_stream = nullptr;  // the slot context's own stream
-  cudaStream_t hi_stream = nullptr;  // greatest priority, for one-slice requests
-  std::shared_ptr<Request> req;
-  int64_t q0 = 0, nq = 0;
+  cudaStream_t hi_stream = nullptr;  // greatest priority, for slices of small requests
+  std::vector<Segment> segs;         // the running slice
+  int64_t nq = 0;                    // queries in the running slice
   bool busy = false;
   bool high = false;                 // the running slice is on hi_stream
 };
@@ -104,6 +123,7 @@ struct sk_server {
   const sk_random *random = nullptr;
   sk_server_params params{};
   size_t words_per_sample = 0;
+  int64_t slot_bytes = 0;            // device bytes one slot holds
   std::vector<Slot> slots;
   std::mutex mu;
   std::condition_variable cv;        // wakes the scheduler
@@ -115,9 +135,8 @@ struct sk_server {
   std::thread worker;
   // statistics
   int64_t pairs_done = 0;
-  double busy_s = 0;
+  int64_t slices = 0, slices_shared = 0;
   Clock::time_point t_start;
-  std::string fatal;
 };
 
 namespace {
@@ -128,6 +147,7 @@ void free_slot(Slot &s) {
   if (s.done_ev) cudaEventDestroy(s.done_ev);
   if (s.d_words) cudaFree(s.d_words);
   if (s.h_words) cudaFreeHost(s.h_words);
+  if (s.h_cluster) cudaFreeHost(s.h_cluster);
   if (s.d_col) cudaFree(s.d_col);
   if (s.d_rows) cudaFree(s.d_rows);
   if (s.d_knn) cudaFree(s.d_knn);
@@ -140,13 +160,28 @@ void free_slot(Slot &s) {
   s = Slot{};
 }
 
+// Device bytes of one slot's own buffers (kernel scratch comes on top and is
+// measured when it is reserved).
+int64_t slot_buffer_bytes(const sk_db *ref, const sk_server_params &p, size_t words_per_sample) {
+  const int64_t sq = p.slice_queries;
+  const int64_t npad = ((sq + kSamplePad - 1) / kSamplePad) * kSamplePad;
+  int64_t b = static_cast<int64_t>(ref->K) * 2 * ref->s64 * (npad / kGranule) * kStripeWords * 4;
+  b += npad * 2;                                          // cluster ids
+  b += static_cast<int64_t>(ref->K) * npad * 8;           // equal-base factors
+  b += sq * static_cast<int64_t>(words_per_sample) * 8;   // word staging
+  b += sq * ref->n * 4;                                   // distance column
+  if (p.keep_rows) b += sq * ref->n * 8;
+  if (p.kNN > 0) b += sq * p.kNN * 12;
+  return b;
+}
+
 // Reserves, at start-up, the kernel scratch of the largest slice under every
 // tile shape a slice can take (the default shape and the 64-row one of small
 // batches).  Growing a scratch buffer mid-request would free the old one, and
 // cudaFree waits for the whole device: every slot's work would stall behind
 // it.  build_job on a full-size slice also creates the lazily built
-// per-query random-match factors here.
-sk_status reserve_slice_scratch(sk_server *sv, Slot &s) {
+// per-query random-match factors here.  Adds the scratch bytes to *bytes.
+sk_status reserve_slice_scratch(sk_server *sv, Slot &s, int64_t *bytes) {
   sk_ctx *ctx = s.ctx;
   const sk_db *ref = sv->ref;
   const int64_t sq = sv->params.slice_queries;
@@ -176,6 +211,7 @@ sk_status reserve_slice_scratch(sk_server *sv, Slot &s) {
   st = scratch(ctx, kSlotLaunchMeta, meta, &p);
   if (st == SK_OK) st = scratch(ctx, kSlotCounts, cta, &p);
   if (st == SK_OK) st = scratch(ctx, kSlotSplitCounts, split, &p);
+  *bytes += static_cast<int64_t>(meta + cta + split);
   return st;
 }
 
@@ -184,26 +220,30 @@ sk_status start_slice(sk_server *sv, Slot &s) {
   sk_ctx *ctx = s.ctx;
   const sk_db *ref = sv->ref;
   const size_t wps = sv->words_per_sample;
-  Request &r = *s.req;
   DeviceGuard g(ctx->device);
   ctx->stream = s.high ? s.hi_stream : s.lo_stream;
   sk_status st = begin_call(ctx);
   if (st != SK_OK) return st;
-  std::memcpy(s.h_words, r.words + s.q0 * wps, static_cast<size_t>(s.nq) * wps * 8);
-  // the query database of this slice: same packed buffer, new samples
+  // the query database of this slice: same packed buffer, new samples, and
+  // every query's cluster id and length set again (nothing is kept from the
+  // slot's previous slice)
   s.qdb.n = s.nq;
   s.qdb.jv_rc = -1;   // equal-base factors depend on the samples
-  if (!r.cluster.empty()) {
-    cudaError_t e = cudaMemcpyAsync(s.qdb.cluster, r.cluster.data() + s.q0, s.nq * 2,
-                                    cudaMemcpyHostToDevice, ctx->stream);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "query clusters");
+  s.qdb.seq_len.resize(s.nq);
+  for (const Segment &seg : s.segs) {
+    const Request &r = *seg.req;
+    std::memcpy(s.h_words + seg.row0 * wps, r.words + seg.q0 * wps,
+                static_cast<size_t>(seg.nq) * wps * 8);
+    std::copy(r.cluster.begin() + seg.q0, r.cluster.begin() + seg.q0 + seg.nq,
+              s.h_cluster + seg.row0);
+    std::copy(r.seq_len.begin() + seg.q0, r.seq_len.begin() + seg.q0 + seg.nq,
+              s.qdb.seq_len.begin() + seg.row0);
   }
-  if (!r.seq_len.empty())
-    s.qdb.seq_len.assign(r.seq_len.begin() + s.q0, r.seq_len.begin() + s.q0 + s.nq);
-  else
-    s.qdb.seq_len.assign(s.nq, 0);
-  cudaError_t e = cudaMemcpyAsync(s.d_words, s.h_words, static_cast<size_t>(s.nq) * wps * 8,
-                                  cudaMemcpyHostToDevice, ctx->stream);
+  cudaError_t e = cudaMemcpyAsync(s.qdb.cluster, s.h_cluster, s.nq * 2, cudaMemcpyHostToDevice,
+                                  ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(s.d_words, s.h_words, static_cast<size_t>(s.nq) * wps * 8,
+                        cudaMemcpyHostToDevice, ctx->stream);
   if (e == cudaSuccess)
     e = launch_pack(s.d_words, s.nq, ref->K, ref->s64, s.qdb.ng, s.qdb.packed, ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "query upload");
@@ -234,32 +274,38 @@ sk_status start_slice(sk_server *sv, Slot &s) {
 }
 
 void finish_slice(sk_server *sv, Slot &s) {
-  Request &r = *s.req;
   const int knn = sv->params.kNN;
+  const int64_t n_ref = sv->ref->n;
   DevStatus dst{};
   {
     DeviceGuard g(s.ctx->device);
     cudaMemcpy(&dst, s.ctx->status_dev, sizeof(dst), cudaMemcpyDeviceToHost);
   }
-  if (dst.error) {
-    r.failed = true;
-    r.error = (dst.error & 2u) ? "cancelled" : "device-side error";
+  for (const Segment &seg : s.segs) {
+    Request &r = *seg.req;
+    if (dst.error) {
+      r.failed = true;
+      r.error = (dst.error & 2u) ? "cancelled" : "device-side error";
+    }
+    if (knn > 0) {
+      std::memcpy(r.knn_idx.data() + seg.q0 * knn, s.h_knn + seg.row0 * knn,
+                  static_cast<size_t>(seg.nq) * knn * 8);
+      std::memcpy(r.knn_dist.data() + seg.q0 * knn, s.h_knn_d + seg.row0 * knn,
+                  static_cast<size_t>(seg.nq) * knn * 4);
+    }
+    if (sv->params.keep_rows)
+      std::memcpy(r.rows.data() + seg.q0 * n_ref * 2, s.h_rows + seg.row0 * n_ref * 2,
+                  static_cast<size_t>(seg.nq) * n_ref * 8);
+    r.completed += seg.nq;
+    r.inflight -= 1;
+    if (r.completed == r.n) {
+      r.done = true;
+      r.t_done = Clock::now();
+    }
   }
-  if (knn > 0) {
-    std::memcpy(r.knn_idx.data() + s.q0 * knn, s.h_knn, static_cast<size_t>(s.nq) * knn * 8);
-    std::memcpy(r.knn_dist.data() + s.q0 * knn, s.h_knn_d, static_cast<size_t>(s.nq) * knn * 4);
-  }
-  if (sv->params.keep_rows)
-    std::memcpy(r.rows.data() + s.q0 * sv->ref->n * 2, s.h_rows,
-                static_cast<size_t>(s.nq) * sv->ref->n * 8);
-  r.completed += s.nq;
-  r.inflight -= 1;
-  sv->pairs_done += s.nq * sv->ref->n;
-  if (r.completed == r.n) {
-    r.done = true;
-    r.t_done = Clock::now();
-  }
-  s.req.reset();
+  sv->pairs_done += s.nq * n_ref;
+  s.segs.clear();
+  s.nq = 0;
   s.busy = false;
 }
 
@@ -276,10 +322,66 @@ bool goes_before(const Request &a, const Request &b, Clock::time_point now) {
   return a.id < b.id;
 }
 
+// Appends up to `room` queries of request r (from its next undispatched one)
+// to the slot's slice.  Returns the number taken.
+int64_t take(Slot &s, const std::shared_ptr<Request> &r, int64_t room) {
+  const int64_t nq = std::min(room, r->n - r->dispatched);
+  if (nq <= 0) return 0;
+  s.segs.push_back(Segment{r, r->dispatched, nq, s.nq});
+  r->dispatched += nq;
+  r->inflight += 1;
+  s.nq += nq;
+  return nq;
+}
+
+// Rows of the query tile(s) a slice of nq queries occupies: the 64-row tile
+// of at most 64 queries, else 128-row tiles (build_job's choice).
+int64_t tile_rows_for(int64_t nq) { return nq <= 64 ? 64 : ((nq + 127) / 128) * 128; }
+
+// Fills a free slot with the next slice, or leaves it empty when nothing may
+// start now.  `order` is the pending requests in admission order.
+void compose_slice(sk_server *sv, Slot &s, const std::vector<std::shared_ptr<Request>> &order,
+                   int large_busy, int large_cap) {
+  const int64_t sq = sv->params.slice_queries;
+  auto small = [&](const Request &r) { return r.n <= sq && r.dispatched == 0; };
+  auto open = [](const Request &r) { return r.dispatched < r.n; };
+  std::shared_ptr<Request> first;
+  for (const auto &r : order) {
+    if (!open(*r)) continue;
+    if (small(*r) || large_busy < large_cap) {
+      first = r;
+      break;
+    }
+  }
+  if (!first) return;
+  s.segs.clear();
+  s.nq = 0;
+  if (small(*first)) {
+    // whole small requests, in admission order, while they fit
+    s.high = true;
+    for (const auto &r : order)
+      if (small(*r) && s.nq + r->n <= sq) take(s, r, r->n);
+  } else {
+    // large_slice_queries queries of the large requests, in admission order
+    s.high = false;
+    const int64_t cap = sv->params.large_slice_queries;
+    for (const auto &r : order) {
+      if (s.nq >= cap) break;
+      if (open(*r) && !small(*r)) take(s, r, cap - s.nq);
+    }
+  }
+  // free rows of the last query tile: queries of large requests ride along
+  const int64_t fill = std::min(tile_rows_for(s.nq), sq);
+  for (const auto &r : order) {
+    if (s.nq >= fill) break;
+    if (open(*r) && !small(*r)) take(s, r, fill - s.nq);
+  }
+}
+
 void scheduler(sk_server *sv) {
   std::unique_lock<std::mutex> lock(sv->mu);
-  const int64_t sq = sv->params.slice_queries;
   const int large_cap = std::max<int>(1, static_cast<int>(sv->slots.size()) / 2);
+  std::vector<std::shared_ptr<Request>> order;
   while (true) {
     bool progressed = false;
     // completions
@@ -292,8 +394,10 @@ void scheduler(sk_server *sv) {
       }
       if (q == cudaErrorNotReady) continue;
       if (q != cudaSuccess) {
-        s.req->failed = true;
-        s.req->error = cudaGetErrorString(q);
+        for (Segment &seg : s.segs) {
+          seg.req->failed = true;
+          seg.req->error = cudaGetErrorString(q);
+        }
       }
       finish_slice(sv, s);
       progressed = true;
@@ -305,25 +409,22 @@ void scheduler(sk_server *sv) {
       int large_busy = 0;
       for (const Slot &o : sv->slots) large_busy += (o.busy && !o.high) ? 1 : 0;
       const auto now = Clock::now();
-      std::shared_ptr<Request> pick;
-      for (auto &cand : sv->pending) {
-        if (cand->dispatched >= cand->n) continue;
-        if (cand->n > sq && large_busy >= large_cap) continue;
-        if (!pick || goes_before(*cand, *pick, now)) pick = cand;
-      }
-      if (!pick) break;
-      s.req = pick;
-      s.high = pick->n <= sq;
-      s.q0 = pick->dispatched;
-      s.nq = std::min<int64_t>(s.high ? sq : sv->params.large_slice_queries,
-                               pick->n - pick->dispatched);
-      pick->dispatched += s.nq;
-      pick->inflight += 1;
+      order.assign(sv->pending.begin(), sv->pending.end());
+      std::stable_sort(order.begin(), order.end(),
+                       [now](const std::shared_ptr<Request> &a, const std::shared_ptr<Request> &b) {
+                         return goes_before(*a, *b, now);
+                       });
+      compose_slice(sv, s, order, large_busy, large_cap);
+      if (s.nq == 0) break;
       s.busy = true;
+      sv->slices += 1;
+      sv->slices_shared += s.segs.size() > 1 ? 1 : 0;
       sk_status st = start_slice(sv, s);
       if (st != SK_OK) {
-        pick->failed = true;
-        pick->error = sk_last_error(s.ctx);
+        for (Segment &seg : s.segs) {
+          seg.req->failed = true;
+          seg.req->error = sk_last_error(s.ctx);
+        }
         // the slice still completes through its event (recorded or not)
         DeviceGuard g(s.ctx->device);
         cudaEventRecord(s.done_ev, s.ctx->stream);
@@ -348,6 +449,61 @@ void scheduler(sk_server *sv) {
   }
 }
 
+// One slot: its context and streams, buffers, and reserved kernel scratch.
+// Adds the device bytes it holds to *bytes.
+sk_status make_slot(sk_server *sv, sk_ctx *ctx, Slot &s, int64_t *bytes) {
+  const sk_db *ref = sv->ref;
+  const sk_server_params &p = sv->params;
+  const int64_t sq = p.slice_queries;
+  const int64_t npad = ((sq + kSamplePad - 1) / kSamplePad) * kSamplePad;
+  sk_status st = sk_ctx_create(ctx->device, &s.ctx);
+  if (st != SK_OK) return st;
+  s.lo_stream = s.ctx->stream;
+  {
+    int least = 0, greatest = 0;
+    cudaError_t e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if (e == cudaSuccess)
+      e = cudaStreamCreateWithPriority(&s.hi_stream, cudaStreamNonBlocking, greatest);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "server stream");
+  }
+  s.ctx->tile_cfg = ctx->tile_cfg;
+  s.ctx->tuning = ctx->tuning;
+  s.ctx->semantics = ctx->semantics;   // fixed for the server's lifetime
+  s.qdb.ctx = s.ctx;
+  s.qdb.K = ref->K;
+  s.qdb.s64 = ref->s64;
+  s.qdb.bbits = ref->bbits;
+  s.qdb.kmers = ref->kmers;
+  s.qdb.ng = static_cast<int32_t>(npad / kGranule);
+  const size_t wps = sv->words_per_sample;
+  cudaError_t e = cudaMalloc(&s.qdb.packed, static_cast<size_t>(ref->K) * 2 * ref->s64 *
+                                                s.qdb.ng * kStripeWords * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&s.qdb.cluster, npad * 2);
+  if (e == cudaSuccess) e = cudaMemset(s.qdb.cluster, 0, npad * 2);
+  if (e == cudaSuccess) e = cudaMalloc(&s.d_words, sq * wps * 8);
+  if (e == cudaSuccess)
+    e = cudaHostAlloc(reinterpret_cast<void **>(&s.h_words), sq * wps * 8, cudaHostAllocDefault);
+  if (e == cudaSuccess)
+    e = cudaHostAlloc(reinterpret_cast<void **>(&s.h_cluster), sq * 2, cudaHostAllocDefault);
+  if (e == cudaSuccess) e = cudaMalloc(&s.d_col, sq * ref->n * 4);
+  if (e == cudaSuccess && p.keep_rows) e = cudaMalloc(&s.d_rows, sq * ref->n * 8);
+  if (e == cudaSuccess && p.keep_rows)
+    e = cudaHostAlloc(reinterpret_cast<void **>(&s.h_rows), sq * ref->n * 8, cudaHostAllocDefault);
+  if (e == cudaSuccess && p.kNN > 0) e = cudaMalloc(&s.d_knn, sq * p.kNN * 12);
+  if (e == cudaSuccess && p.kNN > 0)
+    e = cudaHostAlloc(reinterpret_cast<void **>(&s.h_knn), sq * p.kNN * 12, cudaHostAllocDefault);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.done_ev, cudaEventDisableTiming);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "server slot allocation");
+  if (p.kNN > 0) {
+    s.d_knn_d = reinterpret_cast<float *>(s.d_knn + sq * p.kNN);
+    s.h_knn_d = reinterpret_cast<float *>(s.h_knn + sq * p.kNN);
+  }
+  *bytes += slot_buffer_bytes(ref, p, wps);
+  st = reserve_slice_scratch(sv, s, bytes);
+  if (st != SK_OK) return fail(ctx, st, "server slot scratch: %s", sk_last_error(s.ctx));
+  return SK_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -364,7 +520,8 @@ sk_status sk_server_create(sk_ctx *ctx, const sk_db *ref, const sk_random *rando
   const sk_server_params &p = *params;
   if (p.slots < 1 || p.slots > 16 || p.slice_queries < 1 || p.slice_queries > 65536 ||
       p.large_slice_queries < 0 || p.large_slice_queries > p.slice_queries ||
-      p.kNN < 0 || p.kNN > 800 || p.kNN > ref->n || (p.dist_col != 0 && p.dist_col != 1))
+      p.kNN < 0 || p.kNN > 800 || p.kNN > ref->n || (p.dist_col != 0 && p.dist_col != 1) ||
+      p.device_bytes < 0)
     return fail(ctx, SK_EINVAL, "bad server parameters");
   if (random && random->kmers != ref->kmers)
     return fail(ctx, SK_EMISMATCH, "Random match table k-mer lengths differ from the sketches");
@@ -379,60 +536,25 @@ sk_status sk_server_create(sk_ctx *ctx, const sk_db *ref, const sk_random *rando
   sv->params = p;
   if (sv->params.large_slice_queries == 0) sv->params.large_slice_queries = p.slice_queries;
   sv->words_per_sample = static_cast<size_t>(ref->K) * ref->s64 * kBbits;
-  sv->slots.resize(p.slots);
-  const int64_t sq = p.slice_queries;
-  const int64_t npad = ((sq + kSamplePad - 1) / kSamplePad) * kSamplePad;
+  // Slots are made one at a time; under a budget, the first slot's measured
+  // bytes decide how many fit.
   sk_status st = SK_OK;
-  for (Slot &s : sv->slots) {
-    st = sk_ctx_create(ctx->device, &s.ctx);
+  int target = p.slots;
+  for (int i = 0; i < target; ++i) {
+    sv->slots.emplace_back();
+    int64_t bytes = 0;
+    st = make_slot(sv, ctx, sv->slots.back(), &bytes);
     if (st != SK_OK) break;
-    s.lo_stream = s.ctx->stream;
-    {
-      int least = 0, greatest = 0;
-      cudaError_t e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
-      if (e == cudaSuccess)
-        e = cudaStreamCreateWithPriority(&s.hi_stream, cudaStreamNonBlocking, greatest);
-      if (e != cudaSuccess) {
-        st = cuda_fail(ctx, e, "server stream");
-        break;
+    if (i == 0) {
+      sv->slot_bytes = bytes;
+      if (p.device_bytes > 0) {
+        if (p.device_bytes < bytes) {
+          st = fail(ctx, SK_ENOMEM, "server budget of %lld bytes is below one slot (%lld bytes)",
+                    static_cast<long long>(p.device_bytes), static_cast<long long>(bytes));
+          break;
+        }
+        target = static_cast<int>(std::min<int64_t>(p.slots, p.device_bytes / bytes));
       }
-    }
-    s.ctx->tile_cfg = ctx->tile_cfg;
-    s.ctx->tuning = ctx->tuning;
-    s.ctx->semantics = ctx->semantics;   // fixed for the server's lifetime
-    s.qdb.ctx = s.ctx;
-    s.qdb.K = ref->K;
-    s.qdb.s64 = ref->s64;
-    s.qdb.bbits = ref->bbits;
-    s.qdb.kmers = ref->kmers;
-    s.qdb.ng = static_cast<int32_t>(npad / kGranule);
-    cudaError_t e = cudaMalloc(&s.qdb.packed, static_cast<size_t>(ref->K) * 2 * ref->s64 *
-                                                  s.qdb.ng * kStripeWords * 4);
-    if (e == cudaSuccess) e = cudaMalloc(&s.qdb.cluster, npad * 2);
-    if (e == cudaSuccess) e = cudaMemset(s.qdb.cluster, 0, npad * 2);
-    if (e == cudaSuccess) e = cudaMalloc(&s.d_words, sq * sv->words_per_sample * 8);
-    if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void **>(&s.h_words),
-                                            sq * sv->words_per_sample * 8, cudaHostAllocDefault);
-    if (e == cudaSuccess) e = cudaMalloc(&s.d_col, sq * ref->n * 4);
-    if (e == cudaSuccess && p.keep_rows) e = cudaMalloc(&s.d_rows, sq * ref->n * 8);
-    if (e == cudaSuccess && p.keep_rows)
-      e = cudaHostAlloc(reinterpret_cast<void **>(&s.h_rows), sq * ref->n * 8, cudaHostAllocDefault);
-    if (e == cudaSuccess && p.kNN > 0) e = cudaMalloc(&s.d_knn, sq * p.kNN * 12);
-    if (e == cudaSuccess && p.kNN > 0)
-      e = cudaHostAlloc(reinterpret_cast<void **>(&s.h_knn), sq * p.kNN * 12, cudaHostAllocDefault);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.done_ev, cudaEventDisableTiming);
-    if (e != cudaSuccess) {
-      st = cuda_fail(ctx, e, "server slot allocation");
-      break;
-    }
-    if (p.kNN > 0) {
-      s.d_knn_d = reinterpret_cast<float *>(s.d_knn + sq * p.kNN);
-      s.h_knn_d = reinterpret_cast<float *>(s.h_knn + sq * p.kNN);
-    }
-    st = reserve_slice_scratch(sv, s);
-    if (st != SK_OK) {
-      fail(ctx, st, "server slot scratch: %s", sk_last_error(s.ctx));
-      break;
     }
   }
   if (st != SK_OK) {
@@ -448,13 +570,25 @@ sk_status sk_server_create(sk_ctx *ctx, const sk_db *ref, const sk_random *rando
 }
 
 sk_status sk_server_submit(sk_server *sv, const uint64_t *query_words, int64_t n_queries,
-                           const uint16_t *cluster, const uint64_t *seq_len, int64_t *ticket) {
+                           const uint16_t *cluster, const uint64_t *seq_len,
+                           const double *base_freq, int64_t *ticket) {
   if (!sv || !ticket || n_queries < 1 || !query_words) return SK_EINVAL;
   auto r = std::make_shared<Request>();
   r->words = query_words;
   r->n = n_queries;
-  if (cluster) r->cluster.assign(cluster, cluster + n_queries);
+  if (cluster) {
+    r->cluster.assign(cluster, cluster + n_queries);
+  } else {
+    r->cluster.assign(n_queries, 0);
+    const sk_random *rnd = sv->random;
+    if (base_freq && rnd && rnd->mode == kRandTable && !rnd->centroids.empty()) {
+      const sk_status st = sk_closest_cluster(rnd->centroids.data(), rnd->n_clusters, rnd->use_rc,
+                                              base_freq, n_queries, r->cluster.data());
+      if (st != SK_OK) return st;
+    }
+  }
   if (seq_len) r->seq_len.assign(seq_len, seq_len + n_queries);
+  else r->seq_len.assign(n_queries, 0);
   if (sv->params.kNN > 0) {
     r->knn_idx.assign(static_cast<size_t>(n_queries) * sv->params.kNN, -1);
     r->knn_dist.assign(static_cast<size_t>(n_queries) * sv->params.kNN, 0.0f);
@@ -522,6 +656,17 @@ sk_status sk_server_stats(sk_server *sv, int64_t *pairs_done, double *uptime_s,
     for (auto &r : sv->pending) q += r->n - r->dispatched;
     *queued_queries = q;
   }
+  return SK_OK;
+}
+
+sk_status sk_server_info(sk_server *sv, int32_t *slots, int64_t *slot_bytes, int64_t *slices,
+                         int64_t *slices_shared) {
+  if (!sv) return SK_EINVAL;
+  std::lock_guard<std::mutex> lock(sv->mu);
+  if (slots) *slots = static_cast<int32_t>(sv->slots.size());
+  if (slot_bytes) *slot_bytes = sv->slot_bytes;
+  if (slices) *slices = sv->slices;
+  if (slices_shared) *slices_shared = sv->slices_shared;
   return SK_OK;
 }
 

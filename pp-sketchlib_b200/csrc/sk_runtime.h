@@ -96,6 +96,7 @@ struct sk_random {
   std::vector<int32_t> kmers;
   int n_clusters = 0;
   float *table = nullptr;         // [K][C][C]
+  std::vector<float> centroids;   // [C][4] base-composition centroids (may be empty)
 };
 
 struct sk_sparse {

@@ -55,6 +55,7 @@ _SIGNATURES = {
     "sk_random_create": (_i32, [_p, _i32, _i32, _p, _i32, _i32, _p, C.POINTER(_p)]),
     "sk_random_destroy": (_i32, [_p]),
     "sk_closest_cluster": (_i32, [_p, _i32, _i32, _p, _i64, _p]),
+    "sk_random_set_centroids": (_i32, [_p, _p, _i32]),
     "sk_dists_rows": (_i64, [_p, _p]),
     "sk_dists_dense": (_i32, [_p, _p, _p, _p, _i32, _p, _i32]),
     "sk_query_db": (_i32, [_p, _p, _p, _p, _i32, _i32, _i32, _p, _i32, _p]),
@@ -81,11 +82,13 @@ _SIGNATURES = {
     "sk_ctx_save_tuning": (_i32, [_p, C.c_char_p]),
     "sk_dists_dense_noalloc": (_i32, [_p, _p, _p, _p, _i32, _p]),
     "sk_server_create": (_i32, [_p, _p, _p, _p, C.POINTER(_p)]),
-    "sk_server_submit": (_i32, [_p, _p, _i64, _p, _p, C.POINTER(_i64)]),
+    "sk_server_submit": (_i32, [_p, _p, _i64, _p, _p, _p, C.POINTER(_i64)]),
     "sk_server_wait": (_i32, [_p, _i64, C.c_double]),
     "sk_server_result": (_i32, [_p, _i64, _p, _p, _p, C.POINTER(C.c_double)]),
     "sk_server_release": (_i32, [_p, _i64]),
     "sk_server_stats": (_i32, [_p, C.POINTER(_i64), C.POINTER(C.c_double), C.POINTER(_i64)]),
+    "sk_server_info": (_i32, [_p, C.POINTER(_i32), C.POINTER(_i64), C.POINTER(_i64),
+                               C.POINTER(_i64)]),
     "sk_server_destroy": (_i32, [_p]),
     "sk_sketch": (_i32, [_p, _p, _p, _p, _i64, _p, _i32, _i32, _i32, _i32, _i32, _p, _p, _p]),
     "sk_sketch_device": (_i32, [_p, _p, _p, _p, _i64, _p, _i32, _i32, _i32, _i32, _i32, _p, _p,
@@ -95,7 +98,7 @@ _SIGNATURES = {
 
 class ServerParams(C.Structure):
     _fields_ = [("slots", _i32), ("slice_queries", _i32), ("kNN", _i32), ("dist_col", _i32),
-                ("keep_rows", _i32), ("large_slice_queries", _i32)]
+                ("keep_rows", _i32), ("large_slice_queries", _i32), ("device_bytes", _i64)]
 
 BATCH_AUTOTUNE = 1
 
@@ -325,6 +328,12 @@ class Random:
         self.handle = h.value
         self.mode = mode
 
+    def set_centroids(self, centroids):
+        """Base-composition centroids [C][4] (A, C, G, T) of a table model, for
+        the server's cluster assignment of queries."""
+        c = np.ascontiguousarray(centroids, dtype=np.float32)
+        _check(lib.sk_random_set_centroids(self.handle, c.ctypes.data, c.shape[0]), self.ctx)
+
     def close(self):
         if self.handle:
             lib.sk_random_destroy(self.handle)
@@ -387,26 +396,30 @@ class Server:
 
     def __init__(self, ctx: Context, ref: Database, random: Random | None = None, slots: int = 3,
                  slice_queries: int = 128, kNN: int = 5, dist_col: int = 0,
-                 keep_rows: bool = False, large_slice_queries: int = 0):
+                 keep_rows: bool = False, large_slice_queries: int = 0,
+                 device_bytes: int = 0):
         self.ctx = ctx
         self.ref = ref
         self.kNN = kNN
         self.keep_rows = keep_rows
         self._inputs = {}
         prm = ServerParams(slots, slice_queries, kNN, dist_col, int(keep_rows),
-                           large_slice_queries)
+                           large_slice_queries, device_bytes)
         h = _p()
         _check(lib.sk_server_create(ctx.handle, ref.handle, _h(random), C.byref(prm), C.byref(h)),
                ctx)
         self.handle = h.value
 
-    def submit(self, words, cluster=None, seq_len=None) -> int:
+    def submit(self, words, cluster=None, seq_len=None, base_freq=None) -> int:
         w = np.ascontiguousarray(words, dtype=np.uint64)
         cl = None if cluster is None else np.ascontiguousarray(cluster, np.uint16)
         ln = None if seq_len is None else np.ascontiguousarray(seq_len, np.uint64)
+        bf = None if base_freq is None else np.ascontiguousarray(base_freq, np.float64)
+        if bf is not None and bf.shape != (w.shape[0], 4):
+            raise ValueError("base_freq must be [n_queries][4]")
         t = _i64()
         st = lib.sk_server_submit(self.handle, w.ctypes.data, w.shape[0], _ptr(cl), _ptr(ln),
-                                  C.byref(t))
+                                  _ptr(bf), C.byref(t))
         if st != SK_OK:
             raise SketchlibError(st, "submit failed")
         self._inputs[t.value] = (w, cl, ln)       # the server reads them until done
@@ -436,6 +449,12 @@ class Server:
         p, u, q = _i64(), C.c_double(), _i64()
         _check(lib.sk_server_stats(self.handle, C.byref(p), C.byref(u), C.byref(q)), self.ctx)
         return dict(pairs_done=p.value, uptime_s=u.value, queued_queries=q.value)
+
+    def info(self):
+        n, b, sl, sh = _i32(), _i64(), _i64(), _i64()
+        _check(lib.sk_server_info(self.handle, C.byref(n), C.byref(b), C.byref(sl), C.byref(sh)),
+               self.ctx)
+        return dict(slots=n.value, slot_bytes=b.value, slices=sl.value, slices_shared=sh.value)
 
     def close(self):
         if self.handle:

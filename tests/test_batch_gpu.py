@@ -1,6 +1,6 @@
 """Batched persistent launch (one graph-captured launch over many uneven jobs)
-against the plain single-job path, pair for pair; tail splitting along k
-against unsplit tiles; the autotuner."""
+against the plain single-job path, pair for pair, and against the oracle;
+tail splitting along k against unsplit tiles; the autotuner."""
 import numpy as np
 import pytest
 
@@ -29,6 +29,12 @@ def _job_specs():
         (1000, 3, 8, 156, capi.OUT_CORE_ACC, "equal_base"),
         (64, 64, 11, 16, capi.OUT_JACCARD, "none"),
         (257, None, 6, 64, capi.OUT_CORE_ACC, "table"),
+        # the batched workload's widest shape: K = 14 over k = 13..39 at
+        # sketch_size 20,000 (sketchsize64 312), self and query
+        (400, None, 14, 312, capi.OUT_CORE_ACC, "equal_base"),
+        (350, 60, 14, 312, capi.OUT_CORE_ACC, "table"),
+        (200, 30, 14, 312, capi.OUT_JACCARD, "none"),
+        (330, None, 14, 312, capi.OUT_COUNTS, "table"),
     ]
 
 
@@ -43,21 +49,29 @@ def _make(ctx, spec, seed):
     ref = capi.Database(ctx, w[:n], kmers, s64, cluster=cl[:n], seq_len=lens[:n])
     qry = None if nq is None else capi.Database(ctx, w[n:], kmers, s64, cluster=cl[n:],
                                                  seq_len=lens[n:])
-    rnd = None
+    rnd, spec_o = None, None
+    rows_sl = slice(0, n) if nq is None else slice(n, n + nq)
     if rmode == "equal_base":
         rnd = capi.Random(ctx, capi.RANDOM_EQUAL_BASE, kmers)
+        spec_o = oracle.RandomSpec(mode=1, len_rows=lens[rows_sl], len_cols=lens[:n])
     elif rmode == "table":
-        rnd = capi.Random(ctx, capi.RANDOM_TABLE, kmers,
-                          table=rng.uniform(0, 0.01, (K, 3, 3)).astype(np.float32))
+        table = rng.uniform(0, 0.01, (K, 3, 3)).astype(np.float32)
+        rnd = capi.Random(ctx, capi.RANDOM_TABLE, kmers, table=table)
+        spec_o = oracle.RandomSpec(mode=2, table=table, cl_rows=cl[rows_sl], cl_cols=cl[:n])
     rows = capi.dists_rows(ref, qry)
     tdt = torch.int32 if mode == capi.OUT_COUNTS else torch.float32
     out = torch.full((max(rows, 1), _width(mode, K)), -7, dtype=tdt, device="cuda")
-    return ref, qry, rnd, mode, out
+    want = oracle.dists(w[:n], kmers, s64, query_words=None if nq is None else w[n:],
+                        random=spec_o, out_mode=mode)
+    return (ref, qry, rnd, mode, out), want
 
 
-def test_batch_equals_plain(gpu_ctx):
+def test_batch_equals_plain_and_oracle(gpu_ctx):
+    """Every job of one batched launch equals the plain single-job path pair
+    for pair and the oracle: counts and Jaccards exactly, core/accessory
+    within 1e-6 of its double fit (tolerance per database: 5 / (64 s64))."""
     specs = _job_specs()
-    made = [_make(gpu_ctx, sp, 100 + i) for i, sp in enumerate(specs)]
+    made, wants = zip(*[_make(gpu_ctx, sp, 100 + i) for i, sp in enumerate(specs)])
     batch = capi.Batch(gpu_ctx, [(r, q, rnd, m, o.data_ptr()) for r, q, rnd, m, o in made])
     info = batch.info()
     assert info["n_pairs"] == sum(capi.dists_rows(r, q) for r, q, *_ in made)
@@ -65,12 +79,16 @@ def test_batch_equals_plain(gpu_ctx):
         for *_, o in made:
             o.fill_(-7)
         batch.run()
-        for (ref, qry, rnd, mode, out), sp in zip(made, specs):
+        for (ref, qry, rnd, mode, out), want, sp in zip(made, wants, specs):
             plain = capi.dists_dense(gpu_ctx, ref, qry, rnd, out_mode=mode)
             got = out.cpu().numpy()[: plain.shape[0]]
             if mode == capi.OUT_COUNTS:
                 got = got.view(np.uint32)
             np.testing.assert_array_equal(got, plain, err_msg=f"job {sp} replay {rep}")
+            if mode == capi.OUT_CORE_ACC:
+                np.testing.assert_allclose(got, want, rtol=0, atol=1e-6, err_msg=f"job {sp}")
+            else:
+                np.testing.assert_array_equal(got, want, err_msg=f"job {sp}")
     batch.close()
 
 

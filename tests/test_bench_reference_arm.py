@@ -12,7 +12,7 @@ import json, sys
 sys.path.insert(0, %r)
 import numpy as np
 import bench
-kind, threads, run, words = bench.cpu_reference_rate(threads=2)
+kind, threads, run, words = bench.cpu_reference_rate()
 out_pairs = run(0, 2)
 maps = [l.split()[-1] for l in open('/proc/self/maps') if l.rstrip().endswith('.so')]
 print(json.dumps({"kind": kind, "pairs": int(out_pairs), "shape": list(words.shape),

@@ -1,9 +1,13 @@
 """Cluster assignment of new queries for the Monte Carlo random-match model
 (RandomMC::closest_cluster, src/random/random_match.cpp:222-227, 338-360),
-a host-only C-ABI function (no GPU needed)."""
+a host-only C-ABI function (no GPU needed).  The reference's test databases
+(test/small_mass*.h5) hold no /random group and its nearest_neighbour needs
+Eigen, so no reference output pins this step: the oracle's C restatement and
+an independent numpy one do."""
 import numpy as np
 import pytest
 
+import oracle
 from sketchlib_b200 import capi
 
 
@@ -24,6 +28,7 @@ def test_matches_nearest_centroid(use_rc):
     bases = rng.dirichlet(np.ones(4) * 10, 2000)
     got = capi.closest_cluster(centroids, bases, use_rc=use_rc)
     np.testing.assert_array_equal(got, _restated(centroids, bases, use_rc))
+    np.testing.assert_array_equal(got, oracle.closest_cluster(centroids, bases, use_rc))
     assert len(np.unique(got)) > 1
 
 
