@@ -276,9 +276,8 @@ sk_status sk_query_knn(sk_ctx *ctx, const sk_db *ref, const sk_db *query,
 
 /* No counterpart in the reference.  Dense distances (as sk_dists_dense with
  * out_on_device = 1) for callers that cannot allocate device memory at call
- * time: services whose device memory is partitioned once at start-up, code
- * inside a CUDA stream capture (where cudaMalloc breaks the capture), hosts
- * that share the device with an allocator they do not control.  The call
+ * time: services whose device memory is partitioned once at start-up, and
+ * hosts that share the device with an allocator they do not control.  The call
  * makes no cudaMalloc, cudaFree or other allocating call: the kernel's scratch
  * (job descriptor, work list, queue counter, per-CTA count slots, equal-base
  * random-match factors) lives in one static device array of
@@ -287,9 +286,12 @@ sk_status sk_query_knn(sk_ctx *ctx, const sk_db *ref, const sk_db *query,
  * `d_out` (caller-allocated device memory, sk_dists_rows(ref, query) rows) the
  * output.  A job whose work list and one count slot do not fit the buffer is
  * rejected with SK_ERANGE; when the count slots of all resident CTAs do not
- * fit, fewer CTAs run.  The first call on a device looks up the buffer's
- * device address (cudaGetSymbolAddress) and should come before any stream
- * capture.  Every call shares the buffer and leaves its contents behind (the
+ * fit, fewer CTAs run.  The first call on each context looks up the buffer's
+ * device address (cudaGetSymbolAddress, with the context's device current)
+ * and keeps it on the context, so that first call should come before any
+ * stream capture; a context created after a device reset looks it up again.
+ * Its small uploads (job descriptor, work list, equal-base factors) are
+ * copied from host memory owned by the call.  Every call shares the buffer and leaves its contents behind (the
  * work counter is cleared by each call): calls that overlap on the GPU, from
  * different contexts or streams of one device, race; calls queued on one
  * stream do not.  Returns once the work is queued on the context's stream;

@@ -191,9 +191,8 @@ std::vector<float> equal_base_gpu(const sk_db *db, int use_rc) {
 
 // Equal-base random-match factors j(k, len) = 1 - (1 - 4^-k')^len per sample
 // (csrs, src/random/random_match.cpp:318-336), computed with std::pow on the
-// host exactly as the reference does and cached on the database.
-sk_status ensure_jv(sk_ctx *ctx, sk_db *db, int use_rc) {
-  if (db->jv && db->jv_rc == use_rc) return SK_OK;
+// host exactly as the reference does: [K][padded samples] doubles.
+std::vector<double> equal_base_factors(const sk_db *db, int use_rc) {
   const int64_t ld = static_cast<int64_t>(db->ng) * kGranule;
   std::vector<double> jv(static_cast<size_t>(db->K) * ld, 0.0);
   for (int k = 0; k < db->K; ++k) {
@@ -204,6 +203,13 @@ sk_status ensure_jv(sk_ctx *ctx, sk_db *db, int use_rc) {
       jv[k * ld + s] = 1 - std::pow(1 - (double)1 / match_chance, len);
     }
   }
+  return jv;
+}
+
+// The same factors, uploaded and cached on the database.
+sk_status ensure_jv(sk_ctx *ctx, sk_db *db, int use_rc) {
+  if (db->jv && db->jv_rc == use_rc) return SK_OK;
+  const std::vector<double> jv = equal_base_factors(db, use_rc);
   if (!db->jv) {
     cudaError_t e = cudaMalloc(&db->jv, jv.size() * sizeof(double));
     if (e != cudaSuccess) return cuda_fail(ctx, e, "random-match factors");

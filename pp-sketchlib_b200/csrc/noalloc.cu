@@ -2,9 +2,8 @@
 //
 // Some callers cannot allocate device memory when they compute distances: a
 // service whose device memory is carved up once at start-up and must not
-// grow, code running inside a CUDA stream capture (cudaMalloc is not a stream
-// operation and breaks the capture), or a host program that links this
-// library next to an allocator it does not control.  For them
+// grow, or a host program that links this library next to an allocator it
+// does not control.  For them
 // sk_dists_dense_noalloc runs the same persistent distance kernel as
 // sk_dists_dense, but every byte the kernel needs beyond its inputs (the
 // databases) and its output (the caller's device buffer) comes from one
@@ -32,21 +31,18 @@ constexpr size_t kNoAllocBytes = static_cast<size_t>(SK_NOALLOC_SCRATCH_BYTES);
 // is only a stand-in); its device address comes from cudaGetSymbolAddress.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
-std::mutex g_addr_mu;
-void *g_addr[64] = {nullptr};   // device address of the array, per device ordinal
-
-// Looks up the array's device address once per device, with that device
-// current (the caller's DeviceGuard has made it current).
+// Looks up the array's device address on the context's first call, with the
+// context's device current (the caller's DeviceGuard has made it current),
+// and keeps it on the context: a context made after a device reset looks it
+// up again instead of reusing an address from before the reset.
 sk_status scratch_address(sk_ctx *ctx, unsigned char **out) {
-  if (ctx->device < 0 || ctx->device >= 64) return fail(ctx, SK_EINVAL, "device ordinal too large");
-  std::lock_guard<std::mutex> lock(g_addr_mu);
-  if (!g_addr[ctx->device]) {
+  if (!ctx->noalloc_scratch) {
     void *p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGetSymbolAddress of the no-alloc scratch");
-    g_addr[ctx->device] = p;
+    ctx->noalloc_scratch = p;
   }
-  *out = static_cast<unsigned char *>(g_addr[ctx->device]);
+  *out = static_cast<unsigned char *>(ctx->noalloc_scratch);
   return SK_OK;
 }
 
@@ -85,19 +81,8 @@ extern "C" sk_status sk_dists_dense_noalloc(sk_ctx *ctx, const sk_db *ref, const
   if (random && random->mode == kRandEqualBase && jp.semantics == kSemRefGpu) {
     jgpu = equal_base_gpu(ref, random->use_rc);
   } else if (random && random->mode == kRandEqualBase) {
-    auto factors = [&](const sk_db *db, std::vector<double> &jv) {
-      const int64_t ld = static_cast<int64_t>(db->ng) * kGranule;
-      jv.assign(static_cast<size_t>(db->K) * ld, 0.0);
-      for (int k = 0; k < db->K; ++k) {
-        const double match_chance = std::ldexp(1.0, (db->kmers[k] - 1) * 2 + (random->use_rc ? 1 : 0));
-        for (int64_t s = 0; s < db->n; ++s) {
-          const double len = static_cast<double>(db->seq_len.empty() ? 0 : db->seq_len[s]);
-          jv[k * ld + s] = 1 - std::pow(1 - (double)1 / match_chance, len);
-        }
-      }
-    };
-    factors(ref, jv_cols);
-    if (query) factors(rows, jv_rows);
+    jv_cols = equal_base_factors(ref, random->use_rc);
+    if (query) jv_rows = equal_base_factors(rows, random->use_rc);
   }
   int grid = resident_grid(ctx, *cfg);
   if (grid < 1) return fail(ctx, SK_ECUDA, "Tile configuration %d does not fit the device", cfg->id);

@@ -66,6 +66,7 @@ struct sk_ctx {
   int semantics = 0;                              // sk::Semantics of later calls
   std::map<std::pair<int, int>, int> tuning;      // (K, s64) -> shape id
   Scratch scratch[kSlotCount];                    // reusable device buffers
+  void *noalloc_scratch = nullptr;                // device address of the static no-alloc buffer
   std::recursive_mutex mu;
   // Databases and random models keep their context alive: sk_ctx_destroy only
   // marks it, the last dependent handle to go frees it.
@@ -168,6 +169,7 @@ sk_status dense_to_device(sk_ctx *ctx, const sk_db *ref, const sk_db *query,
                           const sk_random *random, int out_mode, int out_col, void *d_out);
 int64_t n_pairs(const sk_db *ref, const sk_db *query);
 sk_status ensure_jv(sk_ctx *ctx, sk_db *db, int use_rc);
+std::vector<double> equal_base_factors(const sk_db *db, int use_rc);
 std::vector<float> equal_base_gpu(const sk_db *db, int use_rc);
 sk_status ensure_copy_stream(sk_ctx *ctx);
 size_t dense_budget(sk_ctx *ctx);

@@ -14,14 +14,15 @@ for name in {unphased (k = 15,19,23,27; `sketch -k 15,29,4`, test/run_test.py:28
              phased (k = 15,19,23,27,31; the CLI default -k 15,31,4)},
 all at sketch size 10000 (sketchsize64 156).
 
-Usage: python tests/golden/make_golden.py [path/to/reference]
+Usage: python tests/golden/make_golden.py [path/to/reference]  (default: $PP_SKETCHLIB_REF)
 """
+import os
 import sys
 from pathlib import Path
 
 import numpy as np
 
-ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference") / "test"
+ref = Path(sys.argv[1] if len(sys.argv) > 1 else os.environ["PP_SKETCHLIB_REF"]) / "test"
 out = {}
 for name, stem, kmers in [("unphased", "ppsketch_ref", [15, 19, 23, 27]),
                           ("phased", "ppsketch_ref_phased", [15, 19, 23, 27, 31])]:

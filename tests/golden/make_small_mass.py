@@ -13,8 +13,9 @@ run on real bacterial sketches without the reference tree:
   length  (7,) u64          sequence lengths (database default where absent)
   n_small ()                samples belonging to small_mass.h5 (the first 6)
 
-Usage: python tests/golden/make_small_mass.py [path/to/reference]
+Usage: python tests/golden/make_small_mass.py [path/to/reference]  (default: $PP_SKETCHLIB_REF)
 """
+import os
 import sys
 from pathlib import Path
 
@@ -24,7 +25,7 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT / "pp-sketchlib_b200"))
 import pp_sketchlib  # noqa: E402
 
-ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference") / "test"
+ref = Path(sys.argv[1] if len(sys.argv) > 1 else os.environ["PP_SKETCHLIB_REF"]) / "test"
 kmers = [14, 17, 20, 23, 26, 29]
 plus1 = pp_sketchlib._load_sketch_db(str(ref / "small_mass_plus1"), [], kmers)
 small = pp_sketchlib._load_sketch_db(str(ref / "small_mass"), [], kmers)

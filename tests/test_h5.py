@@ -2,6 +2,8 @@
 tables written in the reference's on-disk layout read back exactly."""
 from pathlib import Path
 
+import os
+
 import numpy as np
 import pytest
 
@@ -10,7 +12,8 @@ from conftest import GOLDEN
 
 pp_sketchlib = pytest.importorskip("pp_sketchlib")
 
-REF_TEST = Path("/root/reference/test")
+# the reference's own test databases, when its tree is named by PP_SKETCHLIB_REF
+REF_TEST = Path(os.environ.get("PP_SKETCHLIB_REF", "/nonexistent")) / "test"
 
 
 def _db(tmp_path, n=300, K=3, s64=16, random=None, seed=0):

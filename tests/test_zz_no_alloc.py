@@ -1,9 +1,8 @@
 """sk_dists_dense_noalloc: dense distances with no device allocation.
 
 Callers that cannot allocate device memory when they ask for distances (a
-service whose device memory is partitioned at start-up, code inside a CUDA
-stream capture, a host sharing the GPU with an allocator it does not control)
-use this entry point; its scratch is a static device buffer inside the
+service whose device memory is partitioned at start-up, a host sharing the
+GPU with an allocator it does not control) use this entry point; its scratch is a static device buffer inside the
 library.  Checked here through the C ABI against the allocating entry point,
 sk_dists_dense, on two calls in a row, with the tolerances of the parity tests
 (counts and Jaccard exact, core/accessory 1e-6).  The file is named to be
@@ -30,7 +29,7 @@ def _noalloc(ctx, ref, query, rnd, mode, out):
 
 
 @pytest.mark.parametrize("case", ["self_coreacc", "query_equal_base", "self_table_jaccard",
-                                  "self_counts"])
+                                  "self_counts", "query_table", "self_equal_base_refgpu"])
 def test_noalloc_matches_allocating_entry_point(case):
     import torch
     ctx = capi.Context(0)
@@ -52,6 +51,15 @@ def test_noalloc_matches_allocating_entry_point(case):
         mode = capi.OUT_JACCARD
     elif case == "self_counts":
         mode = capi.OUT_COUNTS
+    elif case == "query_table":
+        query = qry
+        rnd = capi.Random(ctx, capi.RANDOM_TABLE, kmers,
+                          table=rng.uniform(0, 0.01, (K, 3, 3)).astype(np.float32))
+    elif case == "self_equal_base_refgpu":
+        # the reference GPU path's equal-base branch: one chance per k from
+        # the first reference's length
+        ctx.set_semantics(capi.SEMANTICS_REFERENCE_GPU)
+        rnd = capi.Random(ctx, capi.RANDOM_EQUAL_BASE, kmers)
     want = capi.dists_dense(ctx, ref, query, rnd, out_mode=mode)
     dtype = torch.int32 if mode == capi.OUT_COUNTS else torch.float32
     out = torch.empty(want.shape, dtype=dtype, device="cuda")
