@@ -49,6 +49,9 @@ def _load():
     lib.sko_dists.restype = None
     lib.sko_dists.argtypes = [vp, i64, vp, i64, i32, i32, vp, i32, i32, C.POINTER(_Random), i32,
                               i32, vp, i32]
+    lib.sko_dists_multi.restype = i64
+    lib.sko_dists_multi.argtypes = [vp, i64, vp, i64, i32, i32, vp, i32, i32, C.POINTER(_Random),
+                                    i64, i64, vp, vp, vp, i32]
     lib.sko_dists_self_rows.restype = i64
     lib.sko_dists_self_rows.argtypes = [vp, i64, i32, vp, i32, i32, i64, i64, vp, i32]
     lib.sko_knn_self.restype = None
@@ -118,6 +121,35 @@ def dists(ref_words, kmers, s64, query_words=None, random: RandomSpec | None = N
                   km.ctypes.data, s64, bbits, C.byref(rs), out_mode, regress, out.ctypes.data,
                   threads)
     return out
+
+
+def dists_multi(ref_words, kmers, s64, query_words=None, random: RandomSpec | None = None,
+                row_begin=0, row_end=None, threads=NTHREADS, bbits=14):
+    """Jaccard (pairs, K), double fit and float-LDLT fit (pairs, 2) of rows
+    [row_begin, row_end) from one intersection pass, long-form order."""
+    cols = np.ascontiguousarray(ref_words, dtype=np.uint64)
+    self_ = query_words is None
+    rows = cols if self_ else np.ascontiguousarray(query_words, dtype=np.uint64)
+    n_cols, n_rows = cols.shape[0], rows.shape[0]
+    outer = n_cols if self_ else n_rows
+    row_end = outer if row_end is None else row_end
+    K = len(kmers)
+    km = np.ascontiguousarray(kmers, dtype=np.int32)
+    if self_:
+        def first(i):
+            return n_cols * i - i * (i + 1) // 2
+        pairs = first(row_end) - first(row_begin)
+    else:
+        pairs = (row_end - row_begin) * n_cols
+    jac = np.zeros((pairs, K), np.float32)
+    f64 = np.zeros((pairs, 2), np.float32)
+    f32 = np.zeros((pairs, 2), np.float32)
+    rs = (random or RandomSpec()).struct()
+    done = lib.sko_dists_multi(rows.ctypes.data, n_rows, cols.ctypes.data, n_cols, int(self_), K,
+                               km.ctypes.data, s64, bbits, C.byref(rs), row_begin, row_end,
+                               jac.ctypes.data, f64.ctypes.data, f32.ctypes.data, threads)
+    assert done == pairs
+    return jac, f64, f32
 
 
 def dists_self_rows(words, kmers, s64, row_begin, row_end, out, threads=NTHREADS, bbits=14):

@@ -52,7 +52,7 @@ int64_t ref_query_db_self(void *h, int64_t n, int K, const int *kmers, int s64, 
   int64_t done = 0;
 #pragma omp parallel for schedule(dynamic, 5) num_threads(threads) reduction(+ : done)
   for (int64_t i = row_begin; i < row_end; i++) {
-    float J[64];
+    float J[128];
     for (int64_t j = i + 1; j < n; j++) {
       for (int k = 0; k < K; k++) {
         const size_t inter = calc_intersize(&sk[i][k], &sk[j][k], s64, bbits);

@@ -14,6 +14,7 @@
  *   sko_fit_slope_f64  fit_slope (semantics)     src/dist/linear_regression.cpp:16-60
  *   sko_fit_slope_f32  fit_slope (float LDLT arithmetic of Eigen's pivoted LDLT)
  *   sko_dists          query_db loops            src/api.cpp:195-283
+ *   sko_dists_multi    the same, every float output of one pass
  *   sko_knn_self       query_db_sparse           src/api.cpp:332-432
  *   sko_sparsify       sparsify_dists_by_threshold src/dist/matrix_ops.cpp:38-69
  *   sko_long_to_square long_to_square            src/dist/matrix_ops.cpp:71-126
@@ -202,7 +203,7 @@ void sko_dists(const uint64_t *rows, int64_t n_rows, const uint64_t *cols, int64
 #pragma omp parallel for schedule(dynamic, 5) num_threads(threads)
 #endif
   for (int64_t i = 0; i < outer; i++) {
-    float J[64];
+    float J[128];
     const int64_t j0 = self ? i + 1 : 0;
     for (int64_t j = j0; j < n_cols; j++) {
       const int64_t pos = self ? condensed(i, j, n_cols) : i * n_cols + j;
@@ -229,6 +230,43 @@ void sko_dists(const uint64_t *rows, int64_t n_rows, const uint64_t *cols, int64
   }
 }
 
+/* The query_db loops for rows [row_begin, row_end) with every float output of
+ * one intersection pass: the Jaccards (pairs, K), the double fit and the
+ * float-LDLT fit (pairs, 2); any output may be NULL.  Outputs hold only the
+ * rows asked for, in long-form order starting at the first pair of
+ * row_begin (self: condensed(row_begin, row_begin + 1); query:
+ * row_begin * n_cols).  Returns the pairs computed. */
+int64_t sko_dists_multi(const uint64_t *rows, int64_t n_rows, const uint64_t *cols, int64_t n_cols,
+                        int self, int K, const int *kmers, int s64, int bbits,
+                        const sko_random *random, int64_t row_begin, int64_t row_end, float *jac,
+                        float *fit64, float *fit32, int threads) {
+  const int64_t W = (int64_t)s64 * bbits;
+  const int64_t base = self ? (row_begin < n_cols - 1 ? condensed(row_begin, row_begin + 1, n_cols) : 0)
+                            : row_begin * n_cols;
+  int64_t done = 0;
+#ifdef _OPENMP
+  if (threads < 1) threads = 1;
+#pragma omp parallel for schedule(dynamic, 5) num_threads(threads) reduction(+ : done)
+#endif
+  for (int64_t i = row_begin; i < row_end; i++) {
+    float J[128];
+    const int64_t j0 = self ? i + 1 : 0;
+    const uint64_t *si = (self ? cols : rows) + i * K * W;
+    for (int64_t j = j0; j < n_cols; j++) {
+      const int64_t pos = (self ? condensed(i, j, n_cols) : i * n_cols + j) - base;
+      const uint64_t *sj = cols + j * K * W;
+      for (int k = 0; k < K; k++)
+        J[k] = (float)sko_jaccard(sko_intersize(si + k * W, sj + k * W, s64, bbits), s64,
+                                  random_for(random, self, k, kmers[k], i, j));
+      if (jac) memcpy(jac + pos * K, J, sizeof(float) * K);
+      if (fit64) sko_fit_slope_f64(J, kmers, K, s64, &fit64[pos * 2], &fit64[pos * 2 + 1]);
+      if (fit32) sko_fit_slope_f32(J, kmers, K, s64, &fit32[pos * 2], &fit32[pos * 2 + 1]);
+      done++;
+    }
+  }
+  return done;
+}
+
 /* All-vs-all core/accessory (double fit) for rows [row_begin, row_end) only;
  * out is the full (n(n-1)/2, 2) long form.  Returns the pairs computed. */
 int64_t sko_dists_self_rows(const uint64_t *words, int64_t n, int K, const int *kmers, int s64,
@@ -241,7 +279,7 @@ int64_t sko_dists_self_rows(const uint64_t *words, int64_t n, int K, const int *
 #pragma omp parallel for schedule(dynamic, 5) num_threads(threads) reduction(+ : done)
 #endif
   for (int64_t i = row_begin; i < row_end; i++) {
-    float J[64];
+    float J[128];
     for (int64_t j = i + 1; j < n; j++) {
       for (int k = 0; k < K; k++)
         J[k] = (float)sko_jaccard(sko_intersize(words + (i * K + k) * W, words + (j * K + k) * W,

@@ -251,8 +251,8 @@ sk_status build_job(sk_ctx *ctx, const sk_db *ref, const sk_db *query, const sk_
     if (small && small->tile_rows == 64 && small->max_kmers >= ref->K) cfg = small;
   }
   if (!cfg || cfg->max_kmers < ref->K)
-    return fail(ctx, SK_ENOTSUP, "No tile configuration holds %d k-mer lengths (at most 16)",
-                ref->K);
+    return fail(ctx, SK_ENOTSUP, "No tile configuration holds %d k-mer lengths (at most %d)",
+                ref->K, cfg ? cfg->max_kmers : kMaxKmers);
   std::memset(jp, 0, sizeof(*jp));
   const sk_db *rows = query ? query : ref;
   jp->self = query ? 0 : 1;
@@ -264,6 +264,8 @@ sk_status build_job(sk_ctx *ctx, const sk_db *ref, const sk_db *query, const sk_
   jp->ng_cols = ref->ng;
   jp->n_kmers = ref->K;
   jp->nb = 2 * ref->s64;
+  jp->nchunk = (jp->nb + kMaxChunkBlocks - 1) / kMaxChunkBlocks;
+  jp->chunk_nb = jp->nchunk == 1 ? jp->nb : kMaxChunkBlocks;
   jp->out_mode = out_mode;
   jp->out_col = out_col;
   jp->out = d_out;
@@ -339,7 +341,7 @@ void plan_items(const std::vector<JobParams> &jobs, int grid, Plan &plan) {
            static_cast<int64_t>(jobs[b].n_kmers) * jobs[b].nb;
   });
   for (int j : order) {
-    plan.k_slots = std::max(plan.k_slots, jobs[j].n_kmers);
+    plan.k_slots = std::max(plan.k_slots, job_slots(jobs[j]));
     for (int64_t t = 0; t < jobs[j].n_tiles; ++t)
       plan.items.push_back(WorkItem{t, j, 0, static_cast<int16_t>(jobs[j].n_kmers), -1, 1});
   }
@@ -447,6 +449,8 @@ sk_status upload_plan(sk_ctx *ctx, const std::vector<JobParams> &jobs, Plan &pla
   lp.cta_scratch = static_cast<uint16_t *>(cta);
   lp.split_scratch = static_cast<uint16_t *>(split);
   lp.k_slots = plan.k_slots;
+  lp.wide = 0;
+  for (const JobParams &jp : jobs) lp.wide |= needs_wide(jp) ? 1 : 0;
   lp.status = ctx->status_dev;
   lp.cancel = ctx->cancel_dev;
   return SK_OK;
@@ -603,7 +607,7 @@ sk_status dense_blocked_to_host(sk_ctx *ctx, const sk_db *ref, const sk_db *quer
     ctrl_at[c] = meta_bytes;
     meta_bytes += (8 + static_cast<size_t>(splits[c]) * cfg->threads * 4 + 255) & ~static_cast<size_t>(255);
   }
-  const size_t slot = count_slot_bytes(*cfg, base.n_kmers);
+  const size_t slot = count_slot_bytes(*cfg, job_slots(base));
   void *meta = nullptr, *cta = nullptr, *split = nullptr, *obuf = nullptr;
   st = scratch(ctx, kSlotLaunchMeta, meta_bytes, &meta);
   if (st == SK_OK) st = scratch(ctx, kSlotCounts, static_cast<size_t>(grid) * slot, &cta);
@@ -625,7 +629,8 @@ sk_status dense_blocked_to_host(sk_ctx *ctx, const sk_db *ref, const sk_db *quer
   lp.jobs = reinterpret_cast<const JobParams *>(mt);
   lp.cta_scratch = static_cast<uint16_t *>(cta);
   lp.split_scratch = static_cast<uint16_t *>(split);
-  lp.k_slots = base.n_kmers;
+  lp.k_slots = job_slots(base);
+  lp.wide = needs_wide(base) ? 1 : 0;
   lp.status = ctx->status_dev;
   lp.cancel = ctx->cancel_dev;
   // block c computes into buf[c & 1] once the copy of block c - 2 has left it;
@@ -875,7 +880,8 @@ sk_status db_alloc(sk_ctx *ctx, int64_t n, const int32_t *kmers, int32_t K, int3
   if (K < 1 || K > kMaxKmers || !kmers)
     return fail(ctx, SK_ERANGE, "n_kmers %d outside [1, %d]", K, kMaxKmers);
   for (int k = 0; k < K; ++k)
-    if (kmers[k] < 1 || kmers[k] > 64) return fail(ctx, SK_EINVAL, "bad k-mer length %d", kmers[k]);
+    if (kmers[k] < 1 || kmers[k] > kMaxKmerLength)
+      return fail(ctx, SK_EINVAL, "bad k-mer length %d", kmers[k]);
   sk_db *db = new sk_db();
   db->ctx = ctx;
   ctx_retain(ctx);

@@ -22,6 +22,7 @@
 // stripes here.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 
@@ -37,8 +38,8 @@ constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s bounded waits
 struct StepMeta {
   int32_t job;
   int32_t ti, tj;     // tile coordinates within the job
-  int32_t kidx;       // k-mer index of this step
-  int32_t flags;      // kStepEnd / kStepLastOfK / kStepLastOfItem
+  int32_t kidx;       // count slot of this step: k-mer index x nchunk + chunk
+  int32_t flags;      // kStepEnd / kStepLastOfK (last step of a count slot) / kStepLastOfItem
   int32_t split;      // split slot of the item, -1 for whole tiles
   int32_t nparts;
   int32_t pad;
@@ -101,7 +102,11 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 // ROT: the refill duty (wait for every warp on the stage barrier, then issue
 // the next copies) moves round-robin over warps 0..ROT-1, one per SM
 // sub-partition for ROT = 4, so no scheduler carries all of it.
-template <int QT, int RT, int TQ, int TR, int STAGES, int MINB, int ROT>
+// WIDE: the instance for jobs with more than kNarrowKmers k-mer lengths or
+// sketches counted in chunks (one count slot per chunk of kMaxChunkBlocks
+// blocks); the narrow instance keeps one slot per k and the unrolled
+// epilogues, whose code size the hot loop is sensitive to.
+template <int QT, int RT, int TQ, int TR, int STAGES, int MINB, int ROT, bool WIDE>
 __global__ void __launch_bounds__((QT / TQ) * (RT / TR), MINB)
     dist_items_kernel(const LaunchParams lp) {
   using S = TileShape<QT, RT, TQ, TR, STAGES>;
@@ -141,6 +146,7 @@ __global__ void __launch_bounds__((QT / TQ) * (RT / TR), MINB)
   struct Producer {
     const uint32_t *rows, *cols;
     int32_t done, have, job, ti, tj, k, k1, split, nparts, b0, nb, ngr, ngc;
+    int32_t slot, slot_end, chunk_nb;   // count slot of the step, its last block + 1
   };
   __shared__ Producer ps;
   if (tid == 0) {
@@ -184,17 +190,25 @@ __global__ void __launch_bounds__((QT / TQ) * (RT / TR), MINB)
       ps.cols = jp.col_words;
       ps.ngr = jp.ng_rows;
       ps.ngc = jp.ng_cols;
+      if constexpr (WIDE) {
+        ps.slot = it.k0 * jp.nchunk;
+        ps.chunk_nb = jp.chunk_nb;
+        ps.slot_end = jp.chunk_nb;   // chunk_nb == nb when one slot holds a whole k
+      }
       ps.have = 1;
       atomicAdd(&lp.status->tiles_done, 1ull);
     }
-    const bool last_of_k = ps.b0 + kBlocksPerStage >= ps.nb;
+    // slot ends fall on step boundaries (chunk_nb and nb are even)
+    const bool last_of_slot = WIDE ? ps.b0 + kBlocksPerStage >= ps.slot_end
+                                   : ps.b0 + kBlocksPerStage >= ps.nb;
+    const bool last_of_k = WIDE ? last_of_slot && ps.slot_end >= ps.nb : last_of_slot;
     const bool last_of_item = last_of_k && ps.k + 1 >= ps.k1;
     StepMeta &m = meta[s];
     m.job = ps.job;
     m.ti = ps.ti;
     m.tj = ps.tj;
-    m.kidx = ps.k;
-    m.flags = (last_of_k ? kStepLastOfK : 0) | (last_of_item ? kStepLastOfItem : 0);
+    m.kidx = WIDE ? ps.slot : ps.k;
+    m.flags = (last_of_slot ? kStepLastOfK : 0) | (last_of_item ? kStepLastOfItem : 0);
     m.split = ps.split;
     m.nparts = ps.nparts;
     mbar_arrive_expect_tx(&full_bar[s], S::kStageBytes);
@@ -211,7 +225,19 @@ __global__ void __launch_bounds__((QT / TQ) * (RT / TR), MINB)
                S::kRG * kStripeBytes, &full_bar[s]);
     }
     ps.b0 += kBlocksPerStage;
-    if (last_of_k) {
+    if constexpr (WIDE) {
+      if (last_of_slot) {
+        ++ps.slot;
+        if (last_of_k) {
+          ps.b0 = 0;
+          ++ps.k;
+          ps.slot_end = ps.chunk_nb;
+          if (last_of_item) ps.have = 0;
+        } else {
+          ps.slot_end = min(ps.slot_end + ps.chunk_nb, ps.nb);
+        }
+      }
+    } else if (last_of_k) {
       ps.b0 = 0;
       ++ps.k;
       if (last_of_item) ps.have = 0;
@@ -306,7 +332,7 @@ __global__ void __launch_bounds__((QT / TQ) * (RT / TR), MINB)
     }
 
     if (m.flags & kStepLastOfK) {
-      // counts of k-mer index m.kidx done: park them (own slot or split slot)
+      // counts of count slot m.kidx done: park them (own slot or split slot)
       uint16_t *base = m.split >= 0
                            ? lp.split_scratch + m.split * slot_size + static_cast<int64_t>(tid) * PT
                            : my_counts;
@@ -340,7 +366,8 @@ __global__ void __launch_bounds__((QT / TQ) * (RT / TR), MINB)
           __threadfence();
           const uint4 *src = reinterpret_cast<const uint4 *>(
               lp.split_scratch + m.split * slot_size + static_cast<int64_t>(tid) * PT);
-          for (int k = 0; k < jp.n_kmers; ++k)
+          const int slots = WIDE ? job_slots(jp) : jp.n_kmers;
+          for (int k = 0; k < slots; ++k)
 #pragma unroll
             for (int w = 0; w < PT / 8; ++w)
               reinterpret_cast<uint4 *>(my_counts + k * slot_k_stride)[w] =
@@ -356,7 +383,8 @@ __global__ void __launch_bounds__((QT / TQ) * (RT / TR), MINB)
           const int64_t gj = gj0 + q % TR;
           const bool valid =
               jp.self ? (gj > gi && gj < jp.n_cols) : (gi < jp.n_rows && gj < jp.n_cols);
-          if (valid) finish_pair_any(jp, gi, gj, my_counts + q, static_cast<int>(slot_k_stride));
+          if (valid)
+            finish_pair_any<WIDE>(jp, gi, gj, my_counts + q, static_cast<int>(slot_k_stride));
         }
       }
     }
@@ -369,11 +397,11 @@ namespace {
 
 // Raises the instance's dynamic shared memory limit once (before any launch,
 // so never inside a stream capture).
-template <int QT, int RT, int TQ, int TR, int STAGES, int MINB, int ROT>
+template <int QT, int RT, int TQ, int TR, int STAGES, int MINB, int ROT, bool WIDE>
 cudaError_t ensure_smem_attr() {
   using S = TileShape<QT, RT, TQ, TR, STAGES>;
   static cudaError_t status = cudaFuncSetAttribute(
-      dist_items_kernel<QT, RT, TQ, TR, STAGES, MINB, ROT>,
+      dist_items_kernel<QT, RT, TQ, TR, STAGES, MINB, ROT, WIDE>,
       cudaFuncAttributeMaxDynamicSharedMemorySize, S::kSmemBytes);
   return status;
 }
@@ -381,23 +409,37 @@ cudaError_t ensure_smem_attr() {
 template <int QT, int RT, int TQ, int TR, int STAGES, int MINB, int ROT>
 cudaError_t launch_cfg(const LaunchParams &lp, int grid, cudaStream_t stream) {
   using S = TileShape<QT, RT, TQ, TR, STAGES>;
-  cudaError_t e = ensure_smem_attr<QT, RT, TQ, TR, STAGES, MINB, ROT>();
-  if (e != cudaSuccess) return e;
-  dist_items_kernel<QT, RT, TQ, TR, STAGES, MINB, ROT>
-      <<<grid, S::kThreads, S::kSmemBytes, stream>>>(lp);
+  if (lp.wide) {
+    cudaError_t e = ensure_smem_attr<QT, RT, TQ, TR, STAGES, MINB, ROT, true>();
+    if (e != cudaSuccess) return e;
+    dist_items_kernel<QT, RT, TQ, TR, STAGES, MINB, ROT, true>
+        <<<grid, S::kThreads, S::kSmemBytes, stream>>>(lp);
+  } else {
+    cudaError_t e = ensure_smem_attr<QT, RT, TQ, TR, STAGES, MINB, ROT, false>();
+    if (e != cudaSuccess) return e;
+    dist_items_kernel<QT, RT, TQ, TR, STAGES, MINB, ROT, false>
+        <<<grid, S::kThreads, S::kSmemBytes, stream>>>(lp);
+  }
   return cudaGetLastError();
 }
 
-template <int QT, int RT, int TQ, int TR, int STAGES, int MINB, int ROT>
-int occupancy_cfg() {
+template <int QT, int RT, int TQ, int TR, int STAGES, int MINB, int ROT, bool WIDE>
+int occupancy_one() {
   using S = TileShape<QT, RT, TQ, TR, STAGES>;
-  if (ensure_smem_attr<QT, RT, TQ, TR, STAGES, MINB, ROT>() != cudaSuccess) return 0;
+  if (ensure_smem_attr<QT, RT, TQ, TR, STAGES, MINB, ROT, WIDE>() != cudaSuccess) return 0;
   int blocks = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-          &blocks, dist_items_kernel<QT, RT, TQ, TR, STAGES, MINB, ROT>, S::kThreads,
+          &blocks, dist_items_kernel<QT, RT, TQ, TR, STAGES, MINB, ROT, WIDE>, S::kThreads,
           S::kSmemBytes) != cudaSuccess)
     return 0;
   return blocks;
+}
+
+// Resident CTAs per SM of both instances (a grid sized by it suits either).
+template <int QT, int RT, int TQ, int TR, int STAGES, int MINB, int ROT>
+int occupancy_cfg() {
+  return std::min(occupancy_one<QT, RT, TQ, TR, STAGES, MINB, ROT, false>(),
+                  occupancy_one<QT, RT, TQ, TR, STAGES, MINB, ROT, true>());
 }
 
 template <int QT, int RT, int TQ, int TR, int STAGES, int MINB, int ROT = 1>

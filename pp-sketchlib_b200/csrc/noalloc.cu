@@ -97,7 +97,7 @@ extern "C" sk_status sk_dists_dense_noalloc(sk_ctx *ctx, const sk_db *ref, const
   const size_t off_jv_rows = align256(off_jv_cols + jv_cols.size() * sizeof(double));
   const size_t off_jgpu = align256(off_jv_rows + jv_rows.size() * sizeof(double));
   const size_t off_counts = align256(off_jgpu + jgpu.size() * sizeof(float));
-  const size_t slot = count_slot_bytes(*cfg, jp.n_kmers);
+  const size_t slot = count_slot_bytes(*cfg, job_slots(jp));
   const size_t fixed = off_counts;
   if (fixed + slot > kNoAllocBytes)
     return fail(ctx, SK_ERANGE,
@@ -160,7 +160,8 @@ extern "C" sk_status sk_dists_dense_noalloc(sk_ctx *ctx, const sk_db *ref, const
   lp.split_done = nullptr;       // no tile is split here
   lp.cta_scratch = reinterpret_cast<uint16_t *>(base + off_counts);
   lp.split_scratch = nullptr;
-  lp.k_slots = jp.n_kmers;
+  lp.k_slots = job_slots(jp);
+  lp.wide = needs_wide(jp) ? 1 : 0;
   lp.status = ctx->status_dev;
   lp.cancel = ctx->cancel_dev;
   e = cfg->launch(lp, grid, ctx->stream);

@@ -187,7 +187,7 @@ extern "C" sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
     ctrl_at[c] = meta_bytes;
     meta_bytes += (8 + static_cast<size_t>(splits[c]) * cfg->threads * 4 + 255) & ~static_cast<size_t>(255);
   }
-  const size_t slot = count_slot_bytes(*cfg, jp.n_kmers);
+  const size_t slot = count_slot_bytes(*cfg, job_slots(jp));
   const int64_t wps = static_cast<int64_t>(n_kmers) * sketchsize64 * bbits;   // words per sample
   void *meta = nullptr, *staging = nullptr, *cta[2] = {}, *split[2] = {};
   const size_t split_bytes = std::max<size_t>(static_cast<size_t>(max_splits) * slot, 16);
@@ -210,7 +210,8 @@ extern "C" sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
   if (e != cudaSuccess) return cuda_fail(ctx, e, "work list upload");
   LaunchParams base{};
   base.jobs = reinterpret_cast<const JobParams *>(m);
-  base.k_slots = jp.n_kmers;
+  base.k_slots = job_slots(jp);
+  base.wide = needs_wide(jp) ? 1 : 0;
   base.status = ctx->status_dev;
   base.cancel = ctx->cancel_dev;
   const WorkItem *d_items = reinterpret_cast<const WorkItem *>(m + items_off);

@@ -203,7 +203,7 @@ sk_status reserve_slice_scratch(sk_server *sv, Slot &s, int64_t *bytes) {
     // the tail tiles (fewer than the grid) may each be cut into K parts
     const int64_t items = tiles + static_cast<int64_t>(grid) * ref->K;
     meta = std::max(meta, meta_layout(1, static_cast<size_t>(items), grid, c->threads).bytes);
-    const size_t slot = count_slot_bytes(*c, ref->K);
+    const size_t slot = count_slot_bytes(*c, job_slots(jp));
     cta = std::max(cta, static_cast<size_t>(grid) * slot);
     split = std::max(split, static_cast<size_t>(grid) * slot);
   }

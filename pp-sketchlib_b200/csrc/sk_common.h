@@ -21,8 +21,14 @@ constexpr int kGranule = 64;            // samples per packed granule
 constexpr int kStripeWords = kBbits * kGranule;       // 896 uint32
 constexpr int kStripeBytes = kStripeWords * 4;        // 3584 bytes
 constexpr int kSamplePad = 256;         // databases are padded to this many samples
-constexpr int kMaxKmers = 32;           // k-mer lengths per database
-constexpr int kMaxSketch64 = 1023;      // 64 * s64 must fit the uint16 tile counters
+constexpr int kMaxKmers = 128;          // k-mer lengths per database
+constexpr int kNarrowKmers = 32;        // k-mer lengths the narrow kernel instance finishes
+constexpr int kMaxKmerLength = 255;     // longest k (the sketcher's limit)
+constexpr int kMaxSketch64 = 1 << 16;   // sketchsize64 accepted (4.2 M bins per k)
+// 32-bin blocks of one k whose bin matches fit a uint16 tile counter
+// (2046 * 32 = 65,472): a k with more blocks is counted in chunks of this
+// many blocks, each in its own count slot, summed by the epilogue.
+constexpr int kMaxChunkBlocks = 2046;
 
 // Output modes (public values in sketchlib_b200.h) plus internal single-column modes.
 enum OutMode : int {
@@ -51,6 +57,8 @@ struct JobParams {
   int32_t ng_rows, ng_cols;    // granules in each packed array
   int32_t n_kmers;             // K
   int32_t nb;                  // 2 * sketchsize64
+  int32_t nchunk;              // count slots per k: ceil(nb / kMaxChunkBlocks)
+  int32_t chunk_nb;            // blocks per count slot (even; the last may hold fewer)
   int32_t self;                // 1: all-vs-all upper triangle
   int32_t out_mode;            // OutMode
   int32_t out_col;             // column for kOutColumn
@@ -78,6 +86,19 @@ struct JobParams {
   int64_t row_base;
 };
 
+// Count slots one job's tile needs: one per (k, chunk of blocks).
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+inline int32_t job_slots(const JobParams &jp) { return jp.n_kmers * jp.nchunk; }
+
+// Jobs the wide kernel instance must run: more k-mer lengths than the narrow
+// instance finishes, or sketches counted in chunks.
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+inline bool needs_wide(const JobParams &jp) { return jp.n_kmers > kNarrowKmers || jp.nchunk > 1; }
+
 // One unit of work of the persistent distance kernel: k-mer indices
 // [k0, k1) of one tile of one job.  A tile whose k range is cut into several
 // items (the last wave's tiles, to even out the tail) shares a split slot; the
@@ -99,7 +120,8 @@ struct LaunchParams {
   unsigned int *split_done;           // [n_splits][threads], zeroed before each launch
   uint16_t *cta_scratch;              // [grid][k_slots][threads][pairs per thread]
   uint16_t *split_scratch;            // [n_splits][k_slots][threads][pairs per thread]
-  int32_t k_slots;                    // largest K over the jobs
+  int32_t k_slots;                    // largest K x nchunk over the jobs
+  int32_t wide;                       // 1: some job needs the wide kernel instance
   DevStatus *status;
   const volatile int *cancel;
 };

@@ -121,6 +121,26 @@ __device__ __forceinline__ void tile_coords(const JobParams &p, int64_t tile, in
 
 // -------------------------------------------------------------- pair epilogue
 
+// Intersection count of k-mer index k: its count slot, or (CHUNKED) the sum
+// of its chunks' slots when the sketch is wider than one uint16 counter holds
+// (counts[(k * nchunk + c) * stride]).
+template <bool CHUNKED>
+__device__ __forceinline__ uint32_t pair_count(const JobParams &p, const uint16_t *counts,
+                                               int stride, int k) {
+  if (!CHUNKED) return counts[k * stride];
+  uint32_t c = 0;
+  for (int q = 0; q < p.nchunk; ++q) c += counts[(k * p.nchunk + q) * stride];
+  return c;
+}
+
+// Loop bound over the k-mer lengths of a per-pair array of KMAX entries: the
+// constant KMAX (loops unroll, arrays stay in registers) for the narrow
+// instance's arrays, the job's K (loops stay loops) for the wide one.
+template <int KMAX>
+__device__ __forceinline__ int k_bound(const JobParams &p) {
+  return KMAX <= kNarrowKmers ? KMAX : p.n_kmers;
+}
+
 // Random match chance for (row gi, col gj) at k-mer index k
 // (RandomMC::random_match, src/random/random_match.cpp:185-206; csrs :318-336).
 __device__ __forceinline__ double random_match(const JobParams &p, int k, int64_t gi, int64_t gj) {
@@ -169,7 +189,7 @@ template <int KMAX>
 __device__ __forceinline__ float2 fit_core_acc(const float (&jf)[KMAX], const JobParams &p) {
   int first = -1, last = -1;
 #pragma unroll
-  for (int k = 0; k < KMAX; ++k) {
+  for (int k = 0; k < k_bound<KMAX>(p); ++k) {
     if (k < p.n_kmers && static_cast<double>(jf[k]) > p.tol) {
       if (first < 0) first = k;
       last = k;
@@ -181,18 +201,18 @@ __device__ __forceinline__ float2 fit_core_acc(const float (&jf)[KMAX], const Jo
   // solve turns it into NaN slopes, i.e. (0, 0).
   bool zero_inside = false;
 #pragma unroll
-  for (int k = 0; k < KMAX; ++k)
+  for (int k = 0; k < k_bound<KMAX>(p); ++k)
     if (k > first && k < last && jf[k] <= 0.0f) zero_inside = true;
   if (zero_inside) return res;
   const double n = static_cast<double>(last - first + 1);
   double sx = 0.0;
 #pragma unroll
-  for (int k = 0; k < KMAX; ++k)
+  for (int k = 0; k < k_bound<KMAX>(p); ++k)
     if (k >= first && k <= last) sx = __dadd_rn(sx, static_cast<double>(p.kmers[k]));
   const double xm = __ddiv_rn(sx, n);
   double sy = 0.0, sxx = 0.0, sxy = 0.0;
 #pragma unroll
-  for (int k = 0; k < KMAX; ++k) {
+  for (int k = 0; k < k_bound<KMAX>(p); ++k) {
     if (k >= first && k <= last) {
       const double y = log(static_cast<double>(jf[k]));
       const double dx = __dsub_rn(static_cast<double>(p.kmers[k]), xm);
@@ -222,6 +242,7 @@ __device__ __forceinline__ float2 fit_core_acc(const float (&jf)[KMAX], const Jo
 //   ybar - slope xbar (round-up FMA); core / accessory = 1 - __expf(.) when
 //   negative.  A pair whose Jaccards are all equal has sd_y = 0, r_xy = 0 / 0
 //   and so (0, 0), as in the reference kernel.
+template <bool CHUNKED>
 __device__ __forceinline__ float2 refgpu_core_acc(const JobParams &p, int64_t gi, int64_t gj,
                                                   const uint16_t *counts, int stride) {
   const int bins = static_cast<int>(p.union_bits);
@@ -231,7 +252,7 @@ __device__ __forceinline__ float2 refgpu_core_acc(const JobParams &p, int64_t gi
   float xsum = 0.0f, ysum = 0.0f, xysum = 0.0f, xsq = 0.0f, ysq = 0.0f;
   bool stop = false;
   for (int k = 0; k < p.n_kmers; ++k) {
-    const float obs = __fdiv_ru(static_cast<float>(counts[k * stride]), unionf);
+    const float obs = __fdiv_ru(static_cast<float>(pair_count<CHUNKED>(p, counts, stride, k)), unionf);
     const float r = static_cast<float>(random_match(p, k, gi, gj));
     const float diff = obs > r ? __fsub_rn(obs, r) : 0.0f;
     const float jac = __fdiv_rn(diff, __fsub_rn(1.0f, r));
@@ -276,41 +297,41 @@ __device__ __forceinline__ int64_t pair_row(const JobParams &p, int64_t gi, int6
 
 // Finishes one pair from its K intersection counts (counts[k * stride]) and
 // writes its long-form row.
-template <int KMAX>
+template <int KMAX, bool CHUNKED>
 __device__ __forceinline__ void finish_pair(const JobParams &p, int64_t gi, int64_t gj,
                                             const uint16_t *counts, int stride) {
   const int64_t row = pair_row(p, gi, gj);
   const int K = p.n_kmers;
   if (p.out_mode == kOutCounts) {
     uint32_t *o = static_cast<uint32_t *>(p.out) + row * K;
-    for (int k = 0; k < K; ++k) o[k] = counts[k * stride];
+    for (int k = 0; k < K; ++k) o[k] = pair_count<CHUNKED>(p, counts, stride, k);
     return;
   }
   if (p.semantics == kSemRefGpu &&
       (p.out_mode == kOutCoreAcc || (p.out_mode == kOutColumn && p.out_col < 2))) {
-    const float2 ca = refgpu_core_acc(p, gi, gj, counts, stride);
+    const float2 ca = refgpu_core_acc<CHUNKED>(p, gi, gj, counts, stride);
     if (p.out_mode == kOutCoreAcc) static_cast<float2 *>(p.out)[row] = ca;
     else static_cast<float *>(p.out)[row] = p.out_col == 0 ? ca.x : ca.y;
     return;
   }
   float jf[KMAX];
 #pragma unroll
-  for (int k = 0; k < KMAX; ++k) {
+  for (int k = 0; k < k_bound<KMAX>(p); ++k) {
     jf[k] = 0.0f;
-    if (k < K) jf[k] = corrected_jaccard(counts[k * stride], p.union_bits,
+    if (k < K) jf[k] = corrected_jaccard(pair_count<CHUNKED>(p, counts, stride, k), p.union_bits,
                                          random_match(p, k, gi, gj));
   }
   if (p.out_mode == kOutJaccard) {
     float *o = static_cast<float *>(p.out) + row * K;
 #pragma unroll
-    for (int k = 0; k < KMAX; ++k)
+    for (int k = 0; k < k_bound<KMAX>(p); ++k)
       if (k < K) o[k] = jf[k];
     return;
   }
   if (p.out_mode == kOutColumn && p.out_col >= 2) {  // Jaccard at k index out_col - 2
     float v = 0.0f;
 #pragma unroll
-    for (int k = 0; k < KMAX; ++k)
+    for (int k = 0; k < k_bound<KMAX>(p); ++k)
       if (k == p.out_col - 2) v = jf[k];
     static_cast<float *>(p.out)[row] = v;
     return;
@@ -324,12 +345,22 @@ __device__ __forceinline__ void finish_pair(const JobParams &p, int64_t gi, int6
 }
 
 // Dispatches on the number of k-mer lengths so the per-pair arrays stay in
-// registers for the common K <= 8 and K <= 16 cases.
+// registers for the common K <= 8 and K <= 16 cases.  The narrow kernel
+// instance finishes up to kNarrowKmers k-mer lengths with unrolled arrays;
+// the wide one finishes wider k sets, and sketches counted in chunks, with
+// loops over arrays in local memory.
+template <bool WIDE>
 __device__ __forceinline__ void finish_pair_any(const JobParams &p, int64_t gi, int64_t gj,
                                                 const uint16_t *counts, int stride) {
-  if (p.n_kmers <= 8) finish_pair<8>(p, gi, gj, counts, stride);
-  else if (p.n_kmers <= 16) finish_pair<16>(p, gi, gj, counts, stride);
-  else finish_pair<kMaxKmers>(p, gi, gj, counts, stride);
+  if constexpr (WIDE) {
+    if (p.nchunk == 1 && p.n_kmers <= 8) finish_pair<8, false>(p, gi, gj, counts, stride);
+    else if (p.nchunk == 1 && p.n_kmers <= 16) finish_pair<16, false>(p, gi, gj, counts, stride);
+    else finish_pair<kMaxKmers, true>(p, gi, gj, counts, stride);
+  } else {
+    if (p.n_kmers <= 8) finish_pair<8, false>(p, gi, gj, counts, stride);
+    else if (p.n_kmers <= 16) finish_pair<16, false>(p, gi, gj, counts, stride);
+    else finish_pair<kNarrowKmers, false>(p, gi, gj, counts, stride);
+  }
 }
 
 }  // namespace sk

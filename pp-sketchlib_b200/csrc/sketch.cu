@@ -54,7 +54,7 @@ constexpr int kPerThread = 512;                    // window starts per thread, 
 constexpr int64_t kItemWindows = static_cast<int64_t>(kSketchThreads) * kPerThread;
 constexpr int kFinishThreads = 512;
 constexpr int kMinK = 3;                           // generate_seeds (src/sketch/sketch.cpp:33-40)
-constexpr int kMaxK = 255;
+constexpr int kMaxK = kMaxKmerLength;
 constexpr unsigned long long kEmptyKey = ~0ULL;
 // Invalid codes before and after a batch's bases: the roll reads up to
 // 16 * ceil(k_out / 16) bytes before a range and its window length + 31
@@ -152,10 +152,11 @@ __device__ __forceinline__ uint64_t mod_sign(uint64_t h) {
 }
 
 // sign / binsize exactly: magic = floor((2^64-1) / binsize) under-estimates
-// the quotient by at most one for sign < 2^61.  magic < 2^20 (binsize >
-// 2^45 for at most 65,472 bins), so the high half of sign * magic is
-// (hi(sign) * magic + umulhi(lo(sign), magic)) >> 32, two multiplies; the
-// quotient is below 2^16, so q * binsize needs two more.
+// the quotient by less than one for sign < 2^61 (by under sign / 2^64 <= 1/8).
+// magic < 2^32 (the host refuses wider: it is about 8 x the bin count), so
+// the high half of sign * magic is (hi(sign) * magic + umulhi(lo(sign),
+// magic)) >> 32, two multiplies; the quotient is below the bin count and
+// q * hi(binsize) below 2^29, so q * binsize needs two more.
 __device__ __forceinline__ uint32_t bin_of(uint64_t sign, uint64_t binsize, uint64_t magic) {
   const uint32_t m = static_cast<uint32_t>(magic);
   const uint32_t s_lo = static_cast<uint32_t>(sign), s_hi = static_cast<uint32_t>(sign >> 32);
@@ -1261,7 +1262,7 @@ sk_status setup_call(SketchCall &c, sk_ctx *ctx, const char *bases, bool device_
   c.nbins = s64 * 64;
   c.binsize = (kSignMod + static_cast<uint64_t>(c.nbins) - 1) / static_cast<uint64_t>(c.nbins);
   c.magic = ~0ULL / c.binsize;
-  if (c.magic >> 32) return fail(ctx, SK_ERANGE, "bin divisor out of range");   // nbins <= 65,472 keeps it < 2^20
+  if (c.magic >> 32) return fail(ctx, SK_ERANGE, "bin divisor out of range");   // about 8 x nbins
   const size_t words = static_cast<size_t>(n) * K * s64 * kBbits;
   const size_t rows = static_cast<size_t>(n) * K;
   const size_t bytes = (d_words ? 0 : words * 8) + (d_inv ? 0 : rows * 8) + rows + 16;

@@ -46,3 +46,4 @@ def test_reference_gpu_harness_loads():
     launches run only in the GPU tests and the reference arm of the bench)."""
     k = oracle.RefGpuKernel()
     assert hasattr(k.lib, "refgpu_self_dists")
+

@@ -66,6 +66,7 @@ def random_samples(rng, n, max_len, n_frac=0.3, max_seqs=4):
     (4, [14, 101, 255], 312, True),
     (5, [21], 1, True),
     (6, [15, 29], 500, True),          # 32,000 bins: bins kept in global memory
+    (7, [17, 21], 1562, True),         # sketch_size 100,000: 99,968 bins per k
 ])
 def test_sketch_matches_oracle_random(gpu_ctx, seed, kmers, s64, rc):
     from sketchlib_b200 import capi
