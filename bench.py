@@ -246,11 +246,14 @@ def run_reference_arm(args, rank, world):
     if rank != 0:
         return
     kind, threads, run, words = cpu_reference_rate()
-    # calibrate the step size: ~2 s of CPU work per step
-    pairs, elapsed, _ = sample_rate(run, 1.0)
-    rate = pairs / elapsed
-    rows_per_step = 1
-    while rows_per_step < N_SAMPLES // 4 and rate * 2.0 > (N_SAMPLES - 1) * rows_per_step:
+    # A step is a block of consecutive rows: at least 16 per thread, so the
+    # loop's dynamic schedule (5 rows per chunk) keeps every thread busy, and
+    # about 1.5 s of work at the rate all threads reach on such a block.
+    rows_per_step = min(N_SAMPLES // 4, 16 * threads)
+    t0 = time.perf_counter()
+    pairs = run(0, rows_per_step)
+    rate = pairs / (time.perf_counter() - t0)
+    while rows_per_step * 2 <= N_SAMPLES // 4 and rate * 1.5 > (N_SAMPLES - 1) * rows_per_step * 2:
         rows_per_step *= 2
     total_pairs, total_t, row = 0, 0.0, 0
     for step in range(args.warmup + args.steps):
@@ -391,6 +394,15 @@ def run_sketch(ctx, dev, steps, warmup, cpu=True):
                                "kind": kind, "sample": f"the whole workload ({n} genomes, "
                                                        f"{ct:.2f} s)"}
         out["matches_cpu_sketcher"] = bool(np.array_equal(want, words_dev))
+        # distances of the genomes (the CPU-runnable case) against the oracle
+        gdb = capi.Database(ctx, words_dev, KMERS, S64)
+        jac = capi.dists_dense(ctx, gdb, out_mode=capi.OUT_JACCARD)
+        ca = capi.dists_dense(ctx, gdb)
+        gdb.close()
+        want_j, f64, f32 = oracle.dists_multi(want, KMERS, S64)
+        out["genomes_parity"] = parity_stats(jac, want_j, ca, f64, f32)
+        out["genomes_parity"]["sample"] = (f"all {n * (n - 1) // 2} pairs of the {n} genomes, "
+                                           "sketched by the reference's sketcher")
     out["reads"] = run_sketch_reads(ctx, steps, warmup, cpu)
     return out
 
@@ -407,18 +419,25 @@ def read_set(rng):
     return reads
 
 
-def run_sketch_reads(ctx, steps, warmup, cpu):
-    """A read set (2 Mb genome, 10x coverage of 150 bp reads, 1% errors; 20
-    Mbases) sketched with min_count = 3 (exact k-mer counts), against the
-    reference's CPU sketcher with exact = true on the same reads as FASTQ."""
+def run_sketch_reads(ctx, steps, warmup, cpu, n_samples=None):
+    """A batch of read sets, each a 2 Mb genome at 10x coverage of 150 bp reads
+    with 1% errors (20 Mbases), sketched with min_count = 3 (exact k-mer
+    counts): one sample per host core, as the reference sketches one sample
+    per thread.  The GPU sketches the whole batch in one sk_sketch call; the
+    reference's CPU sketcher (exact = true, the same reads as FASTQ) runs the
+    samples on that many threads."""
     import tempfile
+    from concurrent.futures import ThreadPoolExecutor
     from sketchlib_b200 import capi
+    cores = os.cpu_count() or 1
+    n = n_samples or cores
     rng = np.random.default_rng(SKETCH_SEED + 1)
     reads = read_set(rng)
     n_reads, RL = reads.shape
-    off = np.arange(n_reads + 1, dtype=np.int64) * RL
-    ss = np.array([0, n_reads], np.int64)
-    bases = reads.reshape(-1)
+    one = reads.reshape(-1)
+    bases = np.tile(one, n)
+    off = np.arange(n * n_reads + 1, dtype=np.int64) * RL
+    ss = np.arange(n + 1, dtype=np.int64) * n_reads
     for _ in range(warmup):
         words, _, _ = capi.sketch(ctx, bases, off, ss, KMERS, S64, min_count=3)
     ms = []
@@ -426,15 +445,18 @@ def run_sketch_reads(ctx, steps, warmup, cpu):
         t0 = time.perf_counter()
         words, _, _ = capi.sketch(ctx, bases, off, ss, KMERS, S64, min_count=3)
         ms.append(1e3 * (time.perf_counter() - t0))
-    out = {"workload": f"{n_reads:,} reads of {RL} bp (10x of a 2 Mb genome, 1% errors), "
-                       "k = 15..29 odd, sketchsize64 156, min_count 3 (exact counts)",
-           "bases": int(bases.size), "ms": statistics.median(ms),
-           "call": "sk_sketch from host memory (per k: the hashes grouped by range, each "
-                   "group counted in shared memory, then the bins)"}
+    sec = statistics.median(ms) / 1e3
+    out = {"workload": f"{n} read sets of {n_reads:,} reads x {RL} bp (10x of a 2 Mb genome, "
+                       "1% errors), k = 15..29 odd, sketchsize64 156, min_count 3 (exact counts)",
+           "samples": n, "bases": int(bases.size), "value": n / sec, "unit": "samples/s",
+           "ms": 1e3 * sec,
+           "call": "one sk_sketch call from host memory (per k: the hashes grouped by range, "
+                   "each group counted in shared memory, then the bins)"}
     if cpu:
         sys.path.insert(0, str(ROOT / "oracle"))
         import oracle
         if oracle.sketcher_available():
+            rs = oracle.RefSketcher()
             with tempfile.TemporaryDirectory() as tmp:
                 fq = Path(tmp) / "reads.fq"
                 q = b"\n+\n" + b"I" * RL + b"\n"
@@ -442,13 +464,17 @@ def run_sketch_reads(ctx, steps, warmup, cpu):
                     for r in reads:
                         f.write(b"@r\n" + r.tobytes() + q)
                 t0 = time.perf_counter()
-                want, _, _, _ = oracle.RefSketcher().sketch_file(fq, KMERS, S64, True, 3, True)
+                with ThreadPoolExecutor(cores) as pool:
+                    res = list(pool.map(lambda _: rs.sketch_file(fq, KMERS, S64, True, 3, True),
+                                        range(n)))
                 ct = time.perf_counter() - t0
-            out["cpu_baseline"] = {"seconds": ct, "cores": 1, "kind": "reference",
-                                   "sample": "the whole read set: the reference's SeqBuf + "
-                                             "sketch() with exact counting (one sample is one "
-                                             "thread in the reference)"}
-            out["matches_cpu_sketcher"] = bool(np.array_equal(want, words[0]))
+            out["cpu_baseline"] = {"value": n / ct, "unit": "samples/s", "cores": cores,
+                                   "kind": "reference", "seconds": ct,
+                                   "sample": f"the same {n} read sets as FASTQ, one per thread: "
+                                             "the reference's SeqBuf + sketch() with exact "
+                                             "counting"}
+            out["matches_cpu_sketcher"] = bool(all(np.array_equal(r[0], words[i])
+                                                   for i, r in enumerate(res)))
     return out
 
 
@@ -544,44 +570,49 @@ def run_batched(ctx, dev, lop3_peak, repeats=3, autotune=False):
 # ------------------------------------------------------- serving (config 5)
 
 SERVE_SEED = 0x5EED0005
+SERVE_KMERS = list(range(15, 34, 2))
+SERVE_N_REF, SERVE_POOL = 50_000, 4_000
+# The 100-query run: its rate is the highest of the swept rates (5, 7.5, 10,
+# 12.5 requests/s, 300 requests each) whose p99 stayed under 50 ms, on a
+# server of 2 slots x 256-query slices (which beat 4 x 128 at every rate).
+Q100_RATE = 7.5
+Q100_SLOTS, Q100_SLICE = 2, 256
 
 
-def run_serving(ctx, dev, n_requests=120, rate_hz=10.0):
-    """50,000 resident references (10 k-mer lengths, 15..33, sketchsize64 156);
-    query batches of 1..2000 (log-uniform) arriving as a seeded Poisson stream,
-    drawn from a pool of 4,000 query sketches of the same tree with 5% novel
-    clades; every query against every reference, top-5 kNN returned."""
-    import threading
+def serving_setup(ctx, dev):
+    """50,000 resident references (10 k-mer lengths, 15..33, sketchsize64 156)
+    and a pool of 4,000 query sketches from the same tree, 5% from novel
+    clades; the reference database is resident in HBM."""
     import torch
     from sketchlib_b200 import capi, synth
-    kmers = list(range(15, 34, 2))
-    n_ref, pool = 50_000, 4_000
-    rp, rt = synth.clade_tree(n_ref, n_clades=200, kmers=kmers, seed=SERVE_SEED)
-    parent, thresh, qidx = synth.query_population(rp, rt, pool, novel_frac=0.05, kmers=kmers,
-                                                  seed=SERVE_SEED + 1)
+    kmers = SERVE_KMERS
+    rp, rt = synth.clade_tree(SERVE_N_REF, n_clades=200, kmers=kmers, seed=SERVE_SEED)
+    parent, thresh, qidx = synth.query_population(rp, rt, SERVE_POOL, novel_frac=0.05,
+                                                  kmers=kmers, seed=SERVE_SEED + 1)
     n_all = len(parent)
     wps = len(kmers) * S64 * BBITS
     words = torch.empty(n_all * wps, dtype=torch.int64, device=dev)
     capi.synth_device(ctx, parent, thresh, S64, seed=SERVE_SEED, d_words=words.data_ptr())
-    ref = capi.Database(ctx, words.data_ptr(), kmers, S64, n_samples=n_ref)
-    qwords = words.view(n_all, wps)[torch.as_tensor(qidx, device=dev)].cpu().numpy().view(np.uint64)
-    qwords = np.ascontiguousarray(qwords.reshape(pool, len(kmers), S64 * BBITS))
+    ref = capi.Database(ctx, words.data_ptr(), kmers, S64, n_samples=SERVE_N_REF)
+    qwords = words.view(n_all, wps)[torch.as_tensor(qidx, device=dev)].cpu().numpy()
+    qwords = np.ascontiguousarray(qwords.view(np.uint64).reshape(SERVE_POOL, len(kmers),
+                                                                  S64 * BBITS))
     del words
-    rng = np.random.default_rng(SERVE_SEED + 2)
-    sizes = np.exp(rng.uniform(0, np.log(2000), n_requests)).astype(int).clip(1, 2000)
-    starts = rng.integers(0, pool - sizes + 1)
-    gaps = rng.exponential(1.0 / rate_hz, n_requests)
-    server = capi.Server(ctx, ref, slots=4, slice_queries=128, kNN=5, large_slice_queries=64)
-    # warm-up request
-    t = server.submit(qwords[:64])
-    server.wait(t)
-    server.result(t)
-    tickets = [None] * n_requests
+    return ref, qwords
+
+
+def serve_stream(server, qwords, sizes, starts, gaps, check=()):
+    """Submits requests as a Poisson stream (inter-arrival gaps in seconds)
+    from a separate thread; returns latencies (s), the makespan and the
+    results of the requests listed in `check`."""
+    import threading
+    n = len(sizes)
+    tickets = [None] * n
     t_begin = time.perf_counter()
 
     def arrivals():
         t_next = time.perf_counter()
-        for i in range(n_requests):
+        for i in range(n):
             t_next += gaps[i]
             d = t_next - time.perf_counter()
             if d > 0:
@@ -591,46 +622,95 @@ def run_serving(ctx, dev, n_requests=120, rate_hz=10.0):
     th = threading.Thread(target=arrivals)
     th.start()
     th.join()
-    lat = np.zeros(n_requests)
-    check = [i for i in range(n_requests) if sizes[i] <= 500][:8]
-    mixed = {}
-    for i in range(n_requests):
+    lat = np.zeros(n)
+    kept = {}
+    for i in range(n):
         server.wait(tickets[i], timeout=600)
         idx, dist, _, lat[i] = server.result(tickets[i])
         if i in check:
-            mixed[i] = (idx, dist)
-    makespan = time.perf_counter() - t_begin
-    # the same requests again, one at a time on an idle server
+            kept[i] = (idx, dist)
+    return lat, time.perf_counter() - t_begin, kept
+
+
+def pct_ms(a, q):
+    return round(float(np.percentile(a, q) * 1e3), 2) if len(a) else None
+
+
+def run_serving(ctx, dev, n_requests=120, rate_hz=10.0, q100_requests=1000, q100_rate=Q100_RATE,
+                sweep=(), q100_slots=Q100_SLOTS, q100_slice=Q100_SLICE, sweep_requests=400):
+    """(a) the mixed stream: batches of 1..2000 queries (log-uniform) at
+    rate_hz; (b) q100_requests batches of exactly 100 queries at q100_rate;
+    (c) optionally the same 100-query stream at each rate of `sweep`
+    (sweep_requests each).  The 100-query runs use their own server with
+    q100_slots slots of q100_slice queries.  Every query is scored against all
+    references, top-5 kNN returned."""
+    from sketchlib_b200 import capi
+    ref, qwords = serving_setup(ctx, dev)
+    n_ref, pool = SERVE_N_REF, SERVE_POOL
+    server = capi.Server(ctx, ref, slots=4, slice_queries=128, kNN=5, large_slice_queries=64)
+    t = server.submit(qwords[:64])       # warm-up request
+    server.wait(t)
+    server.result(t)
+    out = {"references": n_ref, "kmers": len(SERVE_KMERS), "kNN": 5, "slots": 4,
+           "slice_queries": 128, "large_slice_queries": 64}
+
+    # (a) mixed sizes
+    rng = np.random.default_rng(SERVE_SEED + 2)
+    sizes = np.exp(rng.uniform(0, np.log(2000), n_requests)).astype(int).clip(1, 2000)
+    starts = rng.integers(0, pool - sizes + 1)
+    gaps = rng.exponential(1.0 / rate_hz, n_requests)
+    check = [i for i in range(n_requests) if sizes[i] <= 500][:8]
+    info0 = server.info()
+    lat, makespan, mixed = serve_stream(server, qwords, sizes, starts, gaps, check)
+    info1 = server.info()
     alone_equal = True
-    for i in check:
+    for i in check:                      # the same requests again, alone on an idle server
         t = server.submit(qwords[starts[i]:starts[i] + sizes[i]])
         server.wait(t, timeout=600)
         idx, dist, _, _ = server.result(t)
         alone_equal &= bool(np.array_equal(idx, mixed[i][0]) and np.array_equal(dist, mixed[i][1]))
+    one = sizes <= 128
+    near100 = (sizes > 64) & (sizes <= 128)
+    out["mixed"] = {
+        "requests": n_requests, "rate_hz": rate_hz, "queries": int(sizes.sum()),
+        "value": int(sizes.sum()) * n_ref / makespan, "unit": UNIT,
+        "p50_ms": pct_ms(lat, 50), "p99_ms": pct_ms(lat, 99), "max_ms": pct_ms(lat, 100),
+        "n_le_128": int(one.sum()), "p99_ms_le_128": pct_ms(lat[one], 99),
+        "n_65_128": int(near100.sum()), "p99_ms_65_128": pct_ms(lat[near100], 99),
+        "slices": info1["slices"] - info0["slices"],
+        "slices_shared": info1["slices_shared"] - info0["slices_shared"],
+        "alone_vs_mixed_equal": alone_equal, "alone_vs_mixed_checked": len(check)}
+
+    server.close()
+    server = capi.Server(ctx, ref, slots=q100_slots, slice_queries=q100_slice, kNN=5)
+    t = server.submit(qwords[:100])      # warm-up request
+    server.wait(t)
+    server.result(t)
+    out["q100_server"] = {"slots": q100_slots, "slice_queries": q100_slice}
+
+    def q100(n_req, rate, seed):
+        r = np.random.default_rng(seed)
+        sz = np.full(n_req, 100)
+        st = r.integers(0, pool - 100 + 1, n_req)
+        gp = r.exponential(1.0 / rate, n_req)
+        i0 = server.info()
+        lt, mk, _ = serve_stream(server, qwords, sz, st, gp)
+        i1 = server.info()
+        return {"requests": n_req, "rate_hz": rate, "queries_per_request": 100,
+                "value": n_req * 100 * n_ref / mk, "unit": UNIT,
+                "p50_ms": pct_ms(lt, 50), "p99_ms": pct_ms(lt, 99), "max_ms": pct_ms(lt, 100),
+                "slices": i1["slices"] - i0["slices"],
+                "slices_shared": i1["slices_shared"] - i0["slices_shared"]}
+
+    if q100_requests:
+        out["q100"] = q100(q100_requests, q100_rate, SERVE_SEED + 3)
+        out["q100"]["p99_under_50ms"] = out["q100"]["p99_ms"] < 50.0
+    if sweep:
+        out["q100_sweep"] = [q100(sweep_requests, float(r), SERVE_SEED + 4 + k)
+                             for k, r in enumerate(sweep)]
     server.close()
     ref.close()
-    pairs = int(sizes.sum()) * n_ref
-    mid = (sizes >= 50) & (sizes <= 200)
-    small = sizes <= 64
-    one_slice = sizes <= 128                      # one slice: the 100-query class
-    near100 = (sizes > 64) & (sizes <= 128)       # a full 128-row tile of queries
-    pct = lambda a, q: float(np.percentile(a, q) * 1e3) if len(a) else None
-    return {
-        "workload": "50,000 resident references, 10 k x 10k bins; seeded Poisson arrivals "
-                    f"({rate_hz} req/s), batches log-uniform 1..2000, top-5 kNN per query",
-        "requests": n_requests, "queries": int(sizes.sum()),
-        "value": pairs / makespan, "unit": UNIT,
-        "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99),
-        "p50_ms_batches_50_200": pct(lat[mid], 50), "p99_ms_batches_50_200": pct(lat[mid], 99),
-        "n_batches_50_200": int(mid.sum()),
-        "p50_ms_batches_le_64": pct(lat[small], 50), "n_batches_le_64": int(small.sum()),
-        "p50_ms_batches_65_128": pct(lat[near100], 50), "p99_ms_batches_65_128": pct(lat[near100], 99),
-        "n_batches_65_128": int(near100.sum()),
-        "p99_ms_batches_le_128": pct(lat[one_slice], 99), "n_batches_le_128": int(one_slice.sum()),
-        "max_ms": float(lat.max() * 1e3),
-        "slots": 4, "slice_queries": 128, "large_slice_queries": 64,
-        "alone_vs_mixed_equal": alone_equal, "alone_vs_mixed_requests": len(check),
-    }
+    return out
 
 
 # ------------------------------------------------------------ large (config 3)
@@ -689,6 +769,94 @@ def run_large(ctx, dev, lop3_peak, launches=2, knn=10):
                           "2 GB column, top-k pass, D2H of the lists)"},
         "all_finite": finite,
     }
+
+
+# ----------------------------------------------------------- parity, drop-in
+
+WELL_CONDITIONED = 5e-6   # float-LDLT fit vs FP64 fit, both outputs
+
+
+def parity_stats(jac_got, jac_want, ca_got, ca_f64, ca_f32):
+    """Error of the CUDA path's outputs against the FP64 oracle and against the
+    float-LDLT restatement of the reference's fit_slope; `well_conditioned`
+    counts the pairs whose float fit agrees with the FP64 fit to 5e-6."""
+    dj = np.abs(jac_got.astype(np.float64) - jac_want)
+    d64 = np.abs(ca_got.astype(np.float64) - ca_f64)
+    d32 = np.abs(ca_got.astype(np.float64) - ca_f32)
+    well = (np.abs(ca_f32.astype(np.float64) - ca_f64) <= WELL_CONDITIONED).all(axis=1)
+    out = {"pairs": int(ca_got.shape[0]), "jaccard_max_vs_f64": float(dj.max()),
+           "well_conditioned": int(well.sum())}
+    for c, name in enumerate(("core", "accessory")):
+        out[name] = {"max_vs_f64": float(d64[:, c].max()),
+                     "p99.9_vs_f64": float(np.quantile(d64[:, c], 0.999)),
+                     "max_vs_f32": float(d32[:, c].max()),
+                     "p99.9_vs_f32": float(np.quantile(d32[:, c], 0.999)),
+                     "above_1e-5_vs_f32": int((d32[:, c] > 1e-5).sum()),
+                     "max_vs_f32_well_conditioned": float(d32[well, c].max()) if well.any()
+                     else 0.0}
+    return out
+
+
+def run_parity_rows(ctx, db, words, out_dev, rows=128):
+    """The first `rows` rows of the all-vs-all (the longest rows) against the
+    oracle: Jaccard, core and accessory, FP64 and float-LDLT fits."""
+    from sketchlib_b200 import capi
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    n = words.shape[0]
+    m = n * rows - rows * (rows + 1) // 2
+    jac = capi.dists_dense(ctx, db, out_mode=capi.OUT_JACCARD)[:m]
+    ca = out_dev[:m].cpu().numpy()
+    t0 = time.perf_counter()
+    want_j, f64, f32 = oracle.dists_multi(words, KMERS, S64, row_begin=0, row_end=rows)
+    out = parity_stats(jac, want_j, ca, f64, f32)
+    out["sample"] = f"all-vs-all rows 0..{rows - 1} ({m} pairs, oracle {time.perf_counter() - t0:.1f} s)"
+    return out
+
+
+def run_dropin(device, words, steps):
+    """The reference-facing call end to end: pp_sketchlib.queryDatabase on an
+    HDF5 sketch database of the 4,096 samples (written once, outside the timed
+    region), self query with random_correct = True (equal-base correction, the
+    reference's default without a /random group), use_gpu = True: read,
+    flatten, upload, distances, and the numpy result."""
+    import tempfile
+    import pp_sketchlib
+    n = words.shape[0]
+    names = [f"sample{i:05d}" for i in range(n)]
+    with tempfile.TemporaryDirectory() as tmp:
+        db = str(Path(tmp) / "samples4096")
+        pp_sketchlib._save_sketch_db(db, names, words, KMERS, S64, lengths=[2_500_000] * n)
+
+        def call():
+            return pp_sketchlib.queryDatabase(db, db, names, names, KMERS, random_correct=True,
+                                              use_gpu=True, device_id=device)
+
+        res = call()                      # warm-up (the module's context, scratch)
+        ms = []
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            res = call()
+            ms.append(1e3 * (time.perf_counter() - t0))
+        fsize = Path(db + ".h5").stat().st_size
+    sec = statistics.median(ms) / 1e3
+    return {"value": n_pairs(n) / sec, "unit": UNIT, "ms": round(1e3 * sec, 2), "steps": steps,
+            "file_bytes": int(fsize), "result_shape": list(res.shape),
+            "call": "pp_sketchlib.queryDatabase(db, db, names, names, klist, use_gpu=True) from "
+                    "an HDF5 file in the page cache (sketches read, uploaded, distances, numpy "
+                    "result)"}
+
+
+def rounded(x, digits=4):
+    """Floats rounded to `digits` significant digits, recursively (the bench
+    line stays one short line)."""
+    if isinstance(x, float):
+        return float(f"{x:.{digits}g}")
+    if isinstance(x, dict):
+        return {k: rounded(v, digits) for k, v in x.items()}
+    if isinstance(x, list):
+        return [rounded(v, digits) for v in x]
+    return x
 
 
 def run_ours(args, rank, world, local):
@@ -791,10 +959,16 @@ def run_ours(args, rank, world, local):
     ok = ok and bool(torch.equal(host_out, out.cpu()))
 
     extra = {}
+    if not args.skip_dropin:
+        extra["e2e_dropin"] = run_dropin(local, hw, max(1, min(args.steps, 3)))
     if not args.skip_batched:
         extra["batched"] = run_batched(ctx, dev, lop3_peak, autotune=args.batch_autotune)
     if not args.skip_serving:
-        extra["serving"] = run_serving(ctx, dev)
+        sweep = [float(r) for r in args.serving_sweep.split(",")] if args.serving_sweep else ()
+        extra["serving"] = run_serving(ctx, dev, q100_requests=args.q100_requests,
+                                       q100_rate=args.q100_rate, sweep=sweep,
+                                       q100_slots=args.q100_slots, q100_slice=args.q100_slice,
+                                       sweep_requests=args.sweep_requests)
     if world == 1 and not args.skip_large:
         extra["large"] = run_large(ctx, dev, lop3_peak)
     if not args.skip_sketch:
@@ -808,6 +982,10 @@ def run_ours(args, rank, world, local):
         cpu = {"value": cp / ct, "unit": UNIT, "cores": threads, "kind": kind,
                "sample": f"rows 0..{rows - 1} of the 4,096-sample all-vs-all ({cp} pairs, "
                          f"{ct:.1f} s)"}
+        # the oracle as the checker of this run's results (outside every timed region)
+        extra["parity"] = {"samples4096": run_parity_rows(ctx, db, hw, out)}
+        if "sketch" in extra and "genomes_parity" in extra["sketch"]:
+            extra["parity"]["genomes"] = extra["sketch"].pop("genomes_parity")
 
     achieved = pairs * LOP3_PER_PAIR / launch_s
     traffic = profiled_traffic()
@@ -854,9 +1032,76 @@ def run_ours(args, rank, world, local):
         line["cpu_baseline"] = cpu
     line.update(extra)
     if rank == 0:
-        print(json.dumps(line), flush=True)
+        if args.details:
+            Path(args.details).parent.mkdir(parents=True, exist_ok=True)
+            Path(args.details).write_text(json.dumps(line, indent=1))
+        print(json.dumps(compact_line(line)), flush=True)
     db.close()
     ctx.close()
+
+
+def compact_line(line):
+    """The bench line: the contract's keys and each section's headline numbers
+    (the full record goes to --details)."""
+    keep = ["metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
+            "higher_is_better", "scaling", "vs_baseline", "dtype", "data", "config",
+            "tile_config", "gpu_launches", "clocks", "cpu_baseline"]
+    out = {k: line[k] for k in keep if k in line}
+    rf = line["roofline"]
+    out["roofline"] = {k: rf[k] for k in ("bound", "achieved", "peak", "unit", "frac", "traffic",
+                                          "dram_gbs", "popc_frac")}
+    e = line["e2e"]
+    out["e2e"] = {k: e[k] for k in ("value", "unit", "h2d_bytes_per_step", "d2h_bytes_per_step",
+                                    "matches_resident_result")}
+    out["e2e"]["link_gbs"] = {k: e["link_gbs"][k] for k in ("h2d", "d2h")}
+    if "e2e_dropin" in line:
+        d = line["e2e_dropin"]
+        out["e2e_dropin"] = {k: d[k] for k in ("value", "unit", "ms")}
+    if "batched" in line:
+        b = line["batched"]
+        out["batched"] = {"value": b["value"], "lop3_frac": b["lop3_frac"],
+                          "ms": b["ms_per_batch"], "plain_sequential": b["plain_sequential"]["value"],
+                          "equal_to_plain": b["pair_for_pair_equal_to_plain"]}
+    if "serving" in line:
+        sv = line["serving"]
+        out["serving"] = {}
+        for key in ("mixed", "q100"):
+            if key in sv:
+                out["serving"][key] = {k: sv[key][k] for k in sv[key]
+                                       if k in ("requests", "rate_hz", "value", "p50_ms", "p99_ms",
+                                                "p99_ms_le_128", "n_le_128", "slices_shared",
+                                                "alone_vs_mixed_equal", "p99_under_50ms")}
+        if "q100_sweep" in sv:
+            out["serving"]["q100_sweep"] = [[r["rate_hz"], r["p50_ms"], r["p99_ms"]]
+                                            for r in sv["q100_sweep"]]
+        if "q100_server" in sv:
+            out["serving"]["q100_server"] = sv["q100_server"]
+    if "large" in line:
+        lg = line["large"]
+        out["large"] = {"value": lg["value"], "lop3_frac": lg["lop3_frac"],
+                        "knn_ms": lg["knn"]["ms"]}
+    if "sketch" in line:
+        sk = line["sketch"]
+        out["sketch"] = {"value": sk["value"], "unit": sk["unit"], "e2e": sk["e2e"]["value"]}
+        if "cpu_baseline" in sk:
+            out["sketch"]["cpu_baseline"] = sk["cpu_baseline"]["value"]
+        rd = sk.get("reads", {})
+        if rd:
+            out["sketch"]["reads"] = {"value": rd["value"], "unit": rd["unit"],
+                                      "samples": rd["samples"]}
+            if "cpu_baseline" in rd:
+                out["sketch"]["reads"]["cpu_baseline"] = rd["cpu_baseline"]["value"]
+    if "parity" in line:
+        out["parity"] = {}
+        for key, p in line["parity"].items():
+            out["parity"][key] = {"pairs": p["pairs"], "jaccard_max": p["jaccard_max_vs_f64"],
+                                  "core_max_f64": p["core"]["max_vs_f64"],
+                                  "acc_max_f64": p["accessory"]["max_vs_f64"],
+                                  "core_max_f32": p["core"]["max_vs_f32"],
+                                  "acc_max_f32": p["accessory"]["max_vs_f32"],
+                                  "acc_above_1e-5_f32": p["accessory"]["above_1e-5_vs_f32"],
+                                  "well_conditioned": p["well_conditioned"]}
+    return rounded(out)
 
 
 def run_profile_case(n: int, launches: int):
@@ -921,6 +1166,18 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-batched", action="store_true")
     ap.add_argument("--skip-serving", action="store_true")
+    ap.add_argument("--skip-dropin", action="store_true",
+                    help="skip timing pp_sketchlib.queryDatabase on an HDF5 database")
+    ap.add_argument("--q100-requests", type=int, default=1000,
+                    help="requests of exactly 100 queries in the serving run (0: none)")
+    ap.add_argument("--q100-rate", type=float, default=Q100_RATE)
+    ap.add_argument("--q100-slots", type=int, default=Q100_SLOTS)
+    ap.add_argument("--q100-slice", type=int, default=Q100_SLICE)
+    ap.add_argument("--sweep-requests", type=int, default=400)
+    ap.add_argument("--serving-sweep", default="",
+                    help="comma-separated arrival rates for 100-query streams of 400 requests")
+    ap.add_argument("--details", default="",
+                    help="also write the full record (every section) to this JSON file")
     ap.add_argument("--skip-sketch", action="store_true",
                     help="skip the sketching section (64 genomes x 2.5 Mb)")
     ap.add_argument("--batch-autotune", action="store_true",

@@ -254,6 +254,15 @@ sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
                       int32_t n_kmers, int32_t sketchsize64, int32_t bbits,
                       const sk_random *random, int32_t out_mode, void *out);
 
+/* Page-locked host memory (cudaHostAlloc, portable) for the sketch words a
+ * host program hands to sk_query_db, and its release.  No reference
+ * counterpart: query_db_cuda copies from pageable vectors
+ * (src/gpu/gpu_api.cpp:232-305), which both halves the copy rate and costs a
+ * first-touch page fault per 4 KiB of every freshly allocated buffer; a
+ * caller that keeps one such buffer across calls pays neither. */
+sk_status sk_host_alloc(int64_t bytes, void **out);
+sk_status sk_host_free(void *ptr);
+
 /* Self kNN (querySelfSparse with kNN > 0, src/sketchlib_bindings.cpp:136-187):
  * for every sample i, the kNN smallest distances d(i, j), j != i, of column
  * dist_col (0 = core, 1 = accessory; jaccard != 0 sorts on 1 - J at k-mer

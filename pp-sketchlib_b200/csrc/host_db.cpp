@@ -8,6 +8,7 @@
 #include <numeric>
 #include <sstream>
 #include <stdexcept>
+#include <thread>
 
 #include "host_h5.h"
 
@@ -34,61 +35,115 @@ std::vector<std::string> list_samples(const std::string &db_name) {
   return f.list(f.open("/sketches"));
 }
 
-SketchSet load_sketches(const std::string &db_name, const std::vector<std::string> &names,
-                        const std::vector<int32_t> &kmers) {
+int64_t sketch_words_per_k(const std::string &db_name, const std::string &first_name) {
   h5::File f(h5_path(db_name));
-  SketchSet out;
+  const h5::Object sketches = f.open("/sketches");
+  const auto samples = f.members(sketches);
+  const auto it = samples.find(first_name);
+  if (it == samples.end())
+    throw h5::Error("Missing sketch: Object /sketches/" + first_name + " does not exist in " +
+                    f.path());
+  const h5::Object g = f.object_at(it->second);
+  return f.attr_ints(g, "sketchsize64").at(0) * f.attr_ints(g, "bbits").at(0);
+}
+
+void load_sketches_into(const std::string &db_name, const std::vector<std::string> &names,
+                        const std::vector<int32_t> &kmers, SketchSet &out, uint64_t *dst,
+                        int threads) {
+  h5::File f(h5_path(db_name));
   out.names = names;
   out.kmers = kmers;
+  out.words.clear();
   const size_t n = names.size();
-  out.seq_len.resize(n);
-  out.bases.resize(n);
+  out.seq_len.assign(n, 0);
+  out.bases.assign(n, {});
+  std::vector<uint8_t> reads(n, 0);
+  // one walk of /sketches for every sample, one of each sample's group for its k
+  const h5::Object sketches = f.open("/sketches");
+  const auto samples = f.members(sketches);
+  std::vector<int32_t> req(kmers);
+  std::sort(req.begin(), req.end());
+  int32_t s64_0 = 0, bbits_0 = 0;
   size_t W = 0;
-  for (size_t i = 0; i < n; ++i) {
-    h5::Object g;
-    try {
-      g = f.open("/sketches/" + names[i]);
-    } catch (const h5::Error &e) {
-      throw h5::Error(std::string("Missing sketch: ") + e.what());
-    }
+  // the first sample fixes sketchsize64 and bbits (every other must match)
+  auto sample = [&](size_t i) {
+    const auto it = samples.find(names[i]);
+    if (it == samples.end())
+      throw h5::Error("Missing sketch: Object /sketches/" + names[i] + " does not exist in " +
+                      f.path());
+    const h5::Object g = f.object_at(it->second);
     std::vector<int64_t> have = f.attr_ints(g, "kmers");
     const int32_t s64 = static_cast<int32_t>(f.attr_ints(g, "sketchsize64").at(0));
     const int32_t bbits = static_cast<int32_t>(f.attr_ints(g, "bbits").at(0));
     if (i == 0) {
-      out.sketchsize64 = s64;
-      out.bbits = bbits;
+      s64_0 = s64;
+      bbits_0 = bbits;
       W = static_cast<size_t>(s64) * bbits;
-      out.words.assign(n * kmers.size() * W, 0);
-    } else if (s64 != out.sketchsize64) {
+    } else if (s64 != s64_0) {
       throw std::runtime_error("Mismatching sketchsize64 in sketches");
-    } else if (bbits != out.bbits) {
+    } else if (bbits != bbits_0) {
       throw std::runtime_error("Mismatching bbits in sketches");
     }
     // every requested k must be present (api.cpp:464-489)
     std::vector<int32_t> have32(have.begin(), have.end());
     std::sort(have32.begin(), have32.end());
     for (int32_t k : kmers) {
-      if (!std::binary_search(have32.begin(), have32.end(), k)) {
-        std::vector<int32_t> req(kmers);
-        std::sort(req.begin(), req.end());
+      if (!std::binary_search(have32.begin(), have32.end(), k))
         throw std::runtime_error("Mismatched data: k-mer lengths in old database (" + join(have32) +
                                  ") do not match those requested (" + join(req) + ")");
-      }
     }
     out.seq_len[i] = h5::File::has_attr(g, "length")
                          ? static_cast<uint64_t>(f.attr_ints(g, "length").at(0))
                          : kDefaultLength;
     out.bases[i] = h5::File::has_attr(g, "base_freq") ? f.attr_doubles(g, "base_freq")
                                                       : std::vector<double>{0.25, 0.25, 0.25, 0.25};
-    if (h5::File::has_attr(g, "reads")) out.reads = out.reads || f.attr_ints(g, "reads").at(0) != 0;
+    if (h5::File::has_attr(g, "reads")) reads[i] = f.attr_ints(g, "reads").at(0) != 0;
+    const auto ks = f.members(g);
     for (size_t ki = 0; ki < kmers.size(); ++ki) {
-      h5::Object ds = f.open("/sketches/" + names[i] + "/" + std::to_string(kmers[ki]));
+      const auto kt = ks.find(std::to_string(kmers[ki]));
+      if (kt == ks.end())
+        throw h5::Error("Object /sketches/" + names[i] + "/" + std::to_string(kmers[ki]) +
+                        " does not exist in " + f.path());
+      const h5::Object ds = f.object_at(kt->second);
       if (ds.space.count() != W)
         throw std::runtime_error("Sketch " + names[i] + " at k = " + std::to_string(kmers[ki]) +
                                  " has the wrong number of words");
-      f.read_u64(ds, out.words.data() + (i * kmers.size() + ki) * W);
+      f.read_u64(ds, dst + (i * kmers.size() + ki) * W);
     }
+  };
+  if (n == 0) return;
+  sample(0);
+  const int nt = std::max(1, std::min<int>(threads, static_cast<int>(n)));
+  std::vector<std::exception_ptr> errs(nt);
+  auto work = [&](int t) {
+    try {
+      for (size_t i = 1 + t; i < n; i += nt) sample(i);
+    } catch (...) {
+      errs[t] = std::current_exception();
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nt; ++t) pool.emplace_back(work, t);
+  work(0);
+  for (auto &th : pool) th.join();
+  for (auto &e : errs)
+    if (e) std::rethrow_exception(e);
+  out.sketchsize64 = s64_0;
+  out.bbits = bbits_0;
+  out.reads = std::any_of(reads.begin(), reads.end(), [](uint8_t r) { return r != 0; });
+}
+
+SketchSet load_sketches(const std::string &db_name, const std::vector<std::string> &names,
+                        const std::vector<int32_t> &kmers) {
+  SketchSet out;
+  if (names.empty()) {
+    out.kmers = kmers;
+    return out;
   }
+  const int64_t W = sketch_words_per_k(db_name, names[0]);
+  std::vector<uint64_t> words(names.size() * kmers.size() * static_cast<size_t>(W));
+  load_sketches_into(db_name, names, kmers, out, words.data(), 1);
+  out.words = std::move(words);
   return out;
 }
 

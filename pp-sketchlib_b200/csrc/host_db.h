@@ -33,6 +33,14 @@ struct SketchSet {
 // load_sketches (src/api.cpp:436-516): the named samples' sketches at the
 // requested k-mer lengths.  Throws std::runtime_error with the reference's
 // messages when a sample or k-mer length is missing.
+// The same into a caller's buffer of names.size() * kmers.size() * W words
+// (W = sketchsize64 * bbits, found in the file: `words_per_sample_k` gives it
+// before the buffer is sized): out.words stays empty.  Samples are read on up
+// to `threads` threads straight from the mapped file.
+int64_t sketch_words_per_k(const std::string &db_name, const std::string &first_name);
+void load_sketches_into(const std::string &db_name, const std::vector<std::string> &names,
+                        const std::vector<int32_t> &kmers, SketchSet &out, uint64_t *dst,
+                        int threads);
 SketchSet load_sketches(const std::string &db_name, const std::vector<std::string> &names,
                         const std::vector<int32_t> &kmers);
 

@@ -263,6 +263,20 @@ std::vector<std::string> File::list(const Object &group) const {
   return names;
 }
 
+std::unordered_map<std::string, uint64_t> File::members(const Object &group) const {
+  if (!group.is_group) throw Error("not an HDF5 group");
+  const uint8_t *h = at(group.heap, 8 + 2 * len_size_ + off_size_);
+  if (std::memcmp(h, "HEAP", 4) != 0) throw Error("bad HDF5 local heap");
+  const uint64_t heap_size = len(h + 8);
+  const uint8_t *heap = at(off(h + 8 + 2 * len_size_), heap_size);
+  std::vector<std::pair<std::string, uint64_t>> entries;
+  walk_btree(group.btree, heap, heap_size, entries, 0);
+  std::unordered_map<std::string, uint64_t> out;
+  out.reserve(entries.size());
+  for (auto &e : entries) out.emplace(std::move(e.first), e.second);
+  return out;
+}
+
 uint64_t File::lookup(const Object &group, const std::string &name, bool *found) const {
   *found = false;
   if (!group.is_group) return 0;

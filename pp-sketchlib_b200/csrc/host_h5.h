@@ -15,6 +15,7 @@
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 namespace h5 {
@@ -67,6 +68,11 @@ class File {
   bool exists(const std::string &path) const;
   // Names of a group's members, in the group's (name-sorted) B-tree order.
   std::vector<std::string> list(const Object &group) const;
+  // A group's members by name (one walk of its B-tree), and the object at a
+  // member's header address: opening many members of one large group costs
+  // one walk instead of one per member.
+  std::unordered_map<std::string, uint64_t> members(const Object &group) const;
+  Object object_at(uint64_t addr) const { return decode(addr); }
 
   // Attribute / dataset values converted to the requested element type.
   static bool has_attr(const Object &o, const std::string &name);

@@ -124,6 +124,34 @@ struct RandomHandle {
   }
 };
 
+// Page-locked staging for the sketch words of queryDatabase, kept between
+// calls and grown when a call needs more: the upload runs at the pinned copy
+// rate, and no call pays first-touch page faults on a fresh buffer of the
+// whole database.  Calls hold the lock while they use it.
+struct PinnedStage {
+  std::mutex mu;
+  void *ptr = nullptr;
+  size_t bytes = 0;
+  uint64_t *words(size_t n_words) {
+    const size_t need = n_words * sizeof(uint64_t);
+    if (need > bytes) {
+      if (ptr) sk_host_free(ptr);
+      ptr = nullptr;
+      bytes = 0;
+      if (sk_host_alloc(static_cast<int64_t>(need), &ptr) != SK_OK)
+        throw std::runtime_error("Unable to allocate page-locked host memory for the sketches");
+      bytes = need;
+    }
+    return static_cast<uint64_t *>(ptr);
+  }
+};
+PinnedStage g_stage;
+
+int loader_threads() {
+  const unsigned hw = std::thread::hardware_concurrency();
+  return static_cast<int>(std::min(16u, std::max(1u, hw)));
+}
+
 void upload(sk_ctx *ctx, const skhost::SketchSet &s, const std::vector<uint16_t> &clusters,
             DbHandle &db) {
   check(ctx, sk_db_create(ctx, s.words.data(), static_cast<int64_t>(s.size()), s.kmers.data(),
@@ -197,11 +225,20 @@ py::array_t<float> queryDatabase(const std::string &ref_db_name, const std::stri
   if (!jaccard && kmer_lengths.size() < 2)
     throw std::runtime_error("Core and accessory distances need at least two k-mer lengths");
   const std::vector<int32_t> kmers = to_kmers(kmer_lengths);
-  skhost::SketchSet ref = skhost::load_sketches(ref_db_name, ref_names, kmers);
   const bool self = ref_db_name == query_db_name && ref_names == query_names;
-  skhost::SketchSet query;
+  // the sketch words go straight from the mapped files into pinned staging
+  std::lock_guard<std::mutex> stage_lock(g_stage.mu);
+  const size_t w_ref = static_cast<size_t>(skhost::sketch_words_per_k(ref_db_name, ref_names[0]));
+  const size_t w_query =
+      self ? 0 : static_cast<size_t>(skhost::sketch_words_per_k(query_db_name, query_names[0]));
+  const size_t ref_words = ref_names.size() * kmers.size() * w_ref;
+  const size_t query_words = self ? 0 : query_names.size() * kmers.size() * w_query;
+  uint64_t *stage = g_stage.words(ref_words + query_words);
+  skhost::SketchSet ref, query;
+  skhost::load_sketches_into(ref_db_name, ref_names, kmers, ref, stage, loader_threads());
   if (!self) {
-    query = skhost::load_sketches(query_db_name, query_names, kmers);
+    skhost::load_sketches_into(query_db_name, query_names, kmers, query, stage + ref_words,
+                               loader_threads());
     // checkSketchParamsMatch (src/gpu/gpu_api.cpp:170-185)
     if (query.bbits != ref.bbits) throw std::runtime_error("Mismatching bbits in sketches");
     if (query.sketchsize64 != ref.sketchsize64)
@@ -217,9 +254,9 @@ py::array_t<float> queryDatabase(const std::string &ref_db_name, const std::stri
   // one sk_query_db call: the sketch upload overlaps the distance kernel
   const std::vector<uint16_t> ref_cl = random.lookup(ref, false);
   const std::vector<uint16_t> query_cl = self ? std::vector<uint16_t>() : random.lookup(query, true);
-  const sk_host_sketches r{ref.words.data(), static_cast<int64_t>(ref.size()), ref_cl.data(),
+  const sk_host_sketches r{stage, static_cast<int64_t>(ref.size()), ref_cl.data(),
                            ref.seq_len.data()};
-  const sk_host_sketches q{self ? nullptr : query.words.data(),
+  const sk_host_sketches q{self ? nullptr : stage + ref_words,
                            self ? 0 : static_cast<int64_t>(query.size()),
                            self ? nullptr : query_cl.data(), self ? nullptr : query.seq_len.data()};
   const int64_t n_ref = static_cast<int64_t>(ref.size());

@@ -315,3 +315,24 @@ extern "C" sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
   if (e != cudaSuccess) return cuda_fail(ctx, e, "result copy");
   return finish_call(ctx);
 }
+
+extern "C" {
+
+sk_status sk_host_alloc(int64_t bytes, void **out) {
+  if (!out || bytes < 0) return SK_EINVAL;
+  *out = nullptr;
+  if (bytes == 0) return SK_OK;
+  const cudaError_t e = cudaHostAlloc(out, static_cast<size_t>(bytes), cudaHostAllocPortable);
+  if (e != cudaSuccess) {
+    *out = nullptr;
+    return SK_ENOMEM;
+  }
+  return SK_OK;
+}
+
+sk_status sk_host_free(void *ptr) {
+  if (!ptr) return SK_OK;
+  return cudaFreeHost(ptr) == cudaSuccess ? SK_OK : SK_ECUDA;
+}
+
+}  // extern "C"

@@ -81,6 +81,8 @@ _SIGNATURES = {
     "sk_autotune": (_i32, [_p, _p, _p, _p, _i32, C.POINTER(_i32)]),
     "sk_ctx_save_tuning": (_i32, [_p, C.c_char_p]),
     "sk_dists_dense_noalloc": (_i32, [_p, _p, _p, _p, _i32, _p]),
+    "sk_host_alloc": (_i32, [_i64, C.POINTER(_p)]),
+    "sk_host_free": (_i32, [_p]),
     "sk_server_create": (_i32, [_p, _p, _p, _p, C.POINTER(_p)]),
     "sk_server_submit": (_i32, [_p, _p, _i64, _p, _p, _p, C.POINTER(_i64)]),
     "sk_server_wait": (_i32, [_p, _i64, C.c_double]),
