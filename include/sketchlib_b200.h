@@ -396,7 +396,9 @@ sk_status sk_server_create(sk_ctx *ctx, const sk_db *ref, const sk_random *rando
  * queries missing from its cluster table (RandomMC::lookup_array /
  * closest_cluster, src/random/random_match.cpp:222-227, 254-273).  Queries
  * with neither get cluster 0 and length 0, as sk_db_set_sample_info with
- * NULL.  Thread-safe. */
+ * NULL.  Query words in page-locked memory (sk_host_alloc, cudaHostAlloc)
+ * go to the device directly; pageable ones are staged by the server first.
+ * Thread-safe. */
 sk_status sk_server_submit(sk_server *server, const uint64_t *query_words, int64_t n_queries,
                            const uint16_t *cluster, const uint64_t *seq_len,
                            const double *base_freq, int64_t *ticket);

@@ -329,7 +329,10 @@ sk_status build_job(sk_ctx *ctx, const sk_db *ref, const sk_db *query, const sk_
 // The tiles of the last, partial wave are cut into p parts along k (p chosen to
 // minimise ceil(r p / W) * ceil(K / p), r tail tiles on W resident CTAs); the
 // per-k counts are independent, so the parts need no reduction, only a shared
-// count slot and an arrival counter.
+// count slot and an arrival counter.  When every part holds one k, narrow
+// jobs' parts are cut further into block ranges (about 32 parts per tile), so
+// the launch ends within a small fraction of a tile on every SM; the partial
+// counts of one k's ranges are summed by the tile's finishing thread.
 void plan_items(const std::vector<JobParams> &jobs, int grid, Plan &plan) {
   plan.items.clear();
   plan.n_splits = 0;
@@ -345,12 +348,29 @@ void plan_items(const std::vector<JobParams> &jobs, int grid, Plan &plan) {
     for (int64_t t = 0; t < jobs[j].n_tiles; ++t)
       plan.items.push_back(WorkItem{t, j, 0, static_cast<int16_t>(jobs[j].n_kmers), -1, 1});
   }
-  split_tail(plan.items, 0, grid, &plan.n_splits);
+  split_tail(plan.items, 0, grid, &plan.n_splits, &jobs);
+  plan.k_slots = items_slots(plan.items, plan.k_slots);
+}
+
+// Block ranges each k of a narrow job's tail tile is cut into: about 32 parts
+// per tile with the k parts, each range a whole number of 2-block steps.
+int32_t tail_block_parts(const JobParams &jp) {
+  if (needs_wide(jp)) return 1;
+  return std::max(1, std::min(32 / jp.n_kmers, jp.nb / 2));
+}
+
+// Count slots the items of a work list need: base (the jobs' K x nchunk), or
+// K x block ranges for tail tiles cut into block ranges.
+int32_t items_slots(const std::vector<WorkItem> &items, int32_t base) {
+  for (const WorkItem &it : items)
+    if (it.nbpart > 1) base = std::max<int32_t>(base, it.k1 * it.nbpart);
+  return base;
 }
 
 // Splits the last partial wave of items[begin..end) (whole tiles, k range
 // [0, K)) along k; split slots are numbered from 0 for this range.
-void split_tail(std::vector<WorkItem> &items, size_t begin, int grid, int32_t *n_splits) {
+void split_tail(std::vector<WorkItem> &items, size_t begin, int grid, int32_t *n_splits,
+                const std::vector<JobParams> *jobs) {
   *n_splits = 0;
   const int64_t T = static_cast<int64_t>(items.size() - begin);
   if (T == 0 || grid <= 0) return;
@@ -376,10 +396,28 @@ void split_tail(std::vector<WorkItem> &items, size_t begin, int grid, int32_t *n
   for (const WorkItem &it : tail) {
     const int K = it.k1;
     const int parts = std::min(best_p, K);
-    for (int q = 0; q < parts; ++q) {
-      const int k0 = K * q / parts, k1 = K * (q + 1) / parts;
-      items.push_back(WorkItem{it.tile, it.job, static_cast<int16_t>(k0),
-                               static_cast<int16_t>(k1), slot, parts});
+    // narrow jobs cut each k further into block ranges when the tile is
+    // already cut into single k: about 32 parts per tile
+    int q = 1, nb = 0;
+    if (jobs && parts == K) {
+      const JobParams &jp = (*jobs)[it.job];
+      q = tail_block_parts(jp);
+      nb = jp.nb;
+    }
+    for (int p = 0; p < parts; ++p) {
+      const int k0 = K * p / parts, k1 = K * (p + 1) / parts;
+      for (int b = 0; b < q; ++b) {
+        WorkItem w{it.tile, it.job, static_cast<int16_t>(k0), static_cast<int16_t>(k1), slot,
+                   parts * q};
+        if (q > 1) {
+          const int steps = nb / 2;
+          w.b0 = 2 * (steps * b / q);
+          w.b1 = 2 * (steps * (b + 1) / q);
+          w.bpart = static_cast<int16_t>(b);
+          w.nbpart = static_cast<int16_t>(q);
+        }
+        items.push_back(w);
+      }
     }
     ++slot;
   }
@@ -595,10 +633,11 @@ sk_status dense_blocked_to_host(sk_ctx *ctx, const sk_db *ref, const sk_db *quer
     start[c] = items.size();
     for (int64_t t = first_tile(cut[c]); t < first_tile(cut[c + 1]); ++t)
       items.push_back(WorkItem{t, c, 0, static_cast<int16_t>(base.n_kmers), -1, 1});
-    split_tail(items, start[c], grid, &splits[c]);
+    split_tail(items, start[c], grid, &splits[c], &jobs);
     count[c] = items.size() - start[c];
   }
   int32_t max_splits = *std::max_element(splits.begin(), splits.end());
+  const int32_t k_slots = items_slots(items, job_slots(base));
   const size_t items_off = (jobs.size() * sizeof(JobParams) + 255) & ~static_cast<size_t>(255);
   const size_t ctrl_off = (items_off + items.size() * sizeof(WorkItem) + 255) & ~static_cast<size_t>(255);
   std::vector<size_t> ctrl_at(nblk);
@@ -607,7 +646,7 @@ sk_status dense_blocked_to_host(sk_ctx *ctx, const sk_db *ref, const sk_db *quer
     ctrl_at[c] = meta_bytes;
     meta_bytes += (8 + static_cast<size_t>(splits[c]) * cfg->threads * 4 + 255) & ~static_cast<size_t>(255);
   }
-  const size_t slot = count_slot_bytes(*cfg, job_slots(base));
+  const size_t slot = count_slot_bytes(*cfg, k_slots);
   void *meta = nullptr, *cta = nullptr, *split = nullptr, *obuf = nullptr;
   st = scratch(ctx, kSlotLaunchMeta, meta_bytes, &meta);
   if (st == SK_OK) st = scratch(ctx, kSlotCounts, static_cast<size_t>(grid) * slot, &cta);
@@ -629,7 +668,7 @@ sk_status dense_blocked_to_host(sk_ctx *ctx, const sk_db *ref, const sk_db *quer
   lp.jobs = reinterpret_cast<const JobParams *>(mt);
   lp.cta_scratch = static_cast<uint16_t *>(cta);
   lp.split_scratch = static_cast<uint16_t *>(split);
-  lp.k_slots = job_slots(base);
+  lp.k_slots = k_slots;
   lp.wide = needs_wide(base) ? 1 : 0;
   lp.status = ctx->status_dev;
   lp.cancel = ctx->cancel_dev;

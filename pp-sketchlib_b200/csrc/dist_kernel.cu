@@ -42,7 +42,7 @@ struct StepMeta {
   int32_t flags;      // kStepEnd / kStepLastOfK (last step of a count slot) / kStepLastOfItem
   int32_t split;      // split slot of the item, -1 for whole tiles
   int32_t nparts;
-  int32_t pad;
+  int32_t nbpart;     // block ranges per k of the item's tile (count slots per k)
 };
 constexpr int32_t kStepEnd = 1, kStepLastOfK = 2, kStepLastOfItem = 4;
 
@@ -147,6 +147,7 @@ __global__ void __launch_bounds__((QT / TQ) * (RT / TR), MINB)
     const uint32_t *rows, *cols;
     int32_t done, have, job, ti, tj, k, k1, split, nparts, b0, nb, ngr, ngc;
     int32_t slot, slot_end, chunk_nb;   // count slot of the step, its last block + 1
+    int32_t bstart, bend, bpart, nbpart;  // the item's block range of each k
   };
   __shared__ Producer ps;
   if (tid == 0) {
@@ -184,8 +185,12 @@ __global__ void __launch_bounds__((QT / TQ) * (RT / TR), MINB)
       ps.k1 = it.k1;
       ps.split = it.split;
       ps.nparts = it.nparts;
-      ps.b0 = 0;
       ps.nb = jp.nb;
+      ps.bstart = it.b1 ? it.b0 : 0;
+      ps.bend = it.b1 ? it.b1 : jp.nb;
+      ps.bpart = it.bpart;
+      ps.nbpart = it.nbpart > 1 ? it.nbpart : 1;
+      ps.b0 = WIDE ? 0 : ps.bstart;
       ps.rows = jp.row_words;
       ps.cols = jp.col_words;
       ps.ngr = jp.ng_rows;
@@ -200,14 +205,15 @@ __global__ void __launch_bounds__((QT / TQ) * (RT / TR), MINB)
     }
     // slot ends fall on step boundaries (chunk_nb and nb are even)
     const bool last_of_slot = WIDE ? ps.b0 + kBlocksPerStage >= ps.slot_end
-                                   : ps.b0 + kBlocksPerStage >= ps.nb;
+                                   : ps.b0 + kBlocksPerStage >= ps.bend;
     const bool last_of_k = WIDE ? last_of_slot && ps.slot_end >= ps.nb : last_of_slot;
     const bool last_of_item = last_of_k && ps.k + 1 >= ps.k1;
     StepMeta &m = meta[s];
     m.job = ps.job;
     m.ti = ps.ti;
     m.tj = ps.tj;
-    m.kidx = WIDE ? ps.slot : ps.k;
+    m.kidx = WIDE ? ps.slot : ps.k * ps.nbpart + ps.bpart;
+    m.nbpart = WIDE ? 1 : ps.nbpart;
     m.flags = (last_of_slot ? kStepLastOfK : 0) | (last_of_item ? kStepLastOfItem : 0);
     m.split = ps.split;
     m.nparts = ps.nparts;
@@ -238,7 +244,7 @@ __global__ void __launch_bounds__((QT / TQ) * (RT / TR), MINB)
         }
       }
     } else if (last_of_k) {
-      ps.b0 = 0;
+      ps.b0 = ps.bstart;
       ++ps.k;
       if (last_of_item) ps.have = 0;
     }
@@ -366,12 +372,27 @@ __global__ void __launch_bounds__((QT / TQ) * (RT / TR), MINB)
           __threadfence();
           const uint4 *src = reinterpret_cast<const uint4 *>(
               lp.split_scratch + m.split * slot_size + static_cast<int64_t>(tid) * PT);
-          const int slots = WIDE ? job_slots(jp) : jp.n_kmers;
-          for (int k = 0; k < slots; ++k)
+          if (WIDE || m.nbpart == 1) {
+            const int slots = WIDE ? job_slots(jp) : jp.n_kmers;
+            for (int k = 0; k < slots; ++k)
 #pragma unroll
-            for (int w = 0; w < PT / 8; ++w)
-              reinterpret_cast<uint4 *>(my_counts + k * slot_k_stride)[w] =
-                  __ldcg(src + k * (slot_k_stride / 8) + w);
+              for (int w = 0; w < PT / 8; ++w)
+                reinterpret_cast<uint4 *>(my_counts + k * slot_k_stride)[w] =
+                    __ldcg(src + k * (slot_k_stride / 8) + w);
+          } else {
+            // block ranges of one k: partial counts add up (two 16-bit
+            // counts per word never carry: their sums fit 16 bits)
+            for (int k = 0; k < jp.n_kmers; ++k)
+#pragma unroll
+              for (int w = 0; w < PT / 8; ++w) {
+                uint4 acc = __ldcg(src + (k * m.nbpart) * (slot_k_stride / 8) + w);
+                for (int p = 1; p < m.nbpart; ++p) {
+                  const uint4 v = __ldcg(src + (k * m.nbpart + p) * (slot_k_stride / 8) + w);
+                  acc.x += v.x; acc.y += v.y; acc.z += v.z; acc.w += v.w;
+                }
+                reinterpret_cast<uint4 *>(my_counts + k * slot_k_stride)[w] = acc;
+              }
+          }
         }
       }
       if (finish) {

@@ -166,6 +166,7 @@ extern "C" sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
     }
   }
   std::vector<WorkItem> items;
+  const std::vector<JobParams> job_list{jp};
   std::vector<size_t> start(n_chunks), count(n_chunks);
   std::vector<int32_t> splits(n_chunks);
   int32_t max_splits = 0;
@@ -173,7 +174,7 @@ extern "C" sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
     start[c] = items.size();
     for (int64_t t : bucket[c])
       items.push_back(WorkItem{t, 0, 0, static_cast<int16_t>(jp.n_kmers), -1, 1});
-    split_tail(items, start[c], grid, &splits[c]);
+    split_tail(items, start[c], grid, &splits[c], &job_list);
     count[c] = items.size() - start[c];
     max_splits = std::max(max_splits, splits[c]);
   }
@@ -187,7 +188,8 @@ extern "C" sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
     ctrl_at[c] = meta_bytes;
     meta_bytes += (8 + static_cast<size_t>(splits[c]) * cfg->threads * 4 + 255) & ~static_cast<size_t>(255);
   }
-  const size_t slot = count_slot_bytes(*cfg, job_slots(jp));
+  const int32_t k_slots = items_slots(items, job_slots(jp));
+  const size_t slot = count_slot_bytes(*cfg, k_slots);
   const int64_t wps = static_cast<int64_t>(n_kmers) * sketchsize64 * bbits;   // words per sample
   void *meta = nullptr, *staging = nullptr, *cta[2] = {}, *split[2] = {};
   const size_t split_bytes = std::max<size_t>(static_cast<size_t>(max_splits) * slot, 16);
@@ -210,7 +212,7 @@ extern "C" sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
   if (e != cudaSuccess) return cuda_fail(ctx, e, "work list upload");
   LaunchParams base{};
   base.jobs = reinterpret_cast<const JobParams *>(m);
-  base.k_slots = job_slots(jp);
+  base.k_slots = k_slots;
   base.wide = needs_wide(jp) ? 1 : 0;
   base.status = ctx->status_dev;
   base.cancel = ctx->cancel_dev;

@@ -39,8 +39,9 @@
 //   * rows left free in a slice's last query tile are filled with queries of
 //     larger requests: the kernel computes whole tiles anyway.
 //
-// Per slice: pinned staging copy of the query words, cluster ids and
-// lengths, H2D, pack, the distance kernel (core or accessory column vs all
+// Per slice: the query words uploaded straight from a request's page-locked
+// buffer, or staged through the slot's pinned buffer when the caller's is
+// pageable; cluster ids and lengths; H2D, pack, the distance kernel (core or accessory column vs all
 // references, optionally the full core/accessory rows), per-query top-kNN,
 // D2H of the kNN lists (and rows).
 #include <cuda_runtime.h>
@@ -68,6 +69,7 @@ using Clock = std::chrono::steady_clock;
 struct Request {
   int64_t id = 0;
   const uint64_t *words = nullptr;   // caller's host buffer, kept alive until done
+  bool pinned = false;               // page-locked: uploaded directly, not staged
   int64_t n = 0;
   std::vector<uint16_t> cluster;     // [n] random-match cluster per query
   std::vector<uint64_t> seq_len;     // [n] sequence length per query
@@ -200,10 +202,12 @@ sk_status reserve_slice_scratch(sk_server *sv, Slot &s, int64_t *bytes) {
     if (grid < 1) continue;
     const int64_t tiles = ((sq + c->tile_rows - 1) / c->tile_rows) *
                           ((ref->n + c->tile_cols - 1) / c->tile_cols);
-    // the tail tiles (fewer than the grid) may each be cut into K parts
-    const int64_t items = tiles + static_cast<int64_t>(grid) * ref->K;
+    // the tail tiles (fewer than the grid) may each be cut into K parts and
+    // each part into block ranges, every range its own count slot
+    const int32_t q = tail_block_parts(jp);
+    const int64_t items = tiles + static_cast<int64_t>(grid) * ref->K * q;
     meta = std::max(meta, meta_layout(1, static_cast<size_t>(items), grid, c->threads).bytes);
-    const size_t slot = count_slot_bytes(*c, job_slots(jp));
+    const size_t slot = count_slot_bytes(*c, std::max(job_slots(jp), ref->K * q));
     cta = std::max(cta, static_cast<size_t>(grid) * slot);
     split = std::max(split, static_cast<size_t>(grid) * slot);
   }
@@ -230,20 +234,40 @@ sk_status start_slice(sk_server *sv, Slot &s) {
   s.qdb.n = s.nq;
   s.qdb.jv_rc = -1;   // equal-base factors depend on the samples
   s.qdb.seq_len.resize(s.nq);
+  cudaError_t e = cudaSuccess;
+  bool staged = false;
   for (const Segment &seg : s.segs) {
     const Request &r = *seg.req;
-    std::memcpy(s.h_words + seg.row0 * wps, r.words + seg.q0 * wps,
-                static_cast<size_t>(seg.nq) * wps * 8);
+    const size_t bytes = static_cast<size_t>(seg.nq) * wps * 8;
+    if (r.pinned) {   // straight from the caller's page-locked buffer
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s.d_words + seg.row0 * wps, r.words + seg.q0 * wps, bytes,
+                            cudaMemcpyHostToDevice, ctx->stream);
+    } else {
+      std::memcpy(s.h_words + seg.row0 * wps, r.words + seg.q0 * wps, bytes);
+      staged = true;
+    }
     std::copy(r.cluster.begin() + seg.q0, r.cluster.begin() + seg.q0 + seg.nq,
               s.h_cluster + seg.row0);
     std::copy(r.seq_len.begin() + seg.q0, r.seq_len.begin() + seg.q0 + seg.nq,
               s.qdb.seq_len.begin() + seg.row0);
   }
-  cudaError_t e = cudaMemcpyAsync(s.qdb.cluster, s.h_cluster, s.nq * 2, cudaMemcpyHostToDevice,
-                                  ctx->stream);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(s.d_words, s.h_words, static_cast<size_t>(s.nq) * wps * 8,
-                        cudaMemcpyHostToDevice, ctx->stream);
+    e = cudaMemcpyAsync(s.qdb.cluster, s.h_cluster, s.nq * 2, cudaMemcpyHostToDevice, ctx->stream);
+  // staged segments go up in one copy per contiguous run of rows
+  for (size_t a = 0; staged && e == cudaSuccess && a < s.segs.size();) {
+    if (s.segs[a].req->pinned) {
+      ++a;
+      continue;
+    }
+    size_t b = a + 1;
+    while (b < s.segs.size() && !s.segs[b].req->pinned) ++b;
+    const int64_t r0 = s.segs[a].row0, r1 = s.segs[b - 1].row0 + s.segs[b - 1].nq;
+    e = cudaMemcpyAsync(s.d_words + r0 * wps, s.h_words + r0 * wps,
+                        static_cast<size_t>(r1 - r0) * wps * 8, cudaMemcpyHostToDevice,
+                        ctx->stream);
+    a = b;
+  }
   if (e == cudaSuccess)
     e = launch_pack(s.d_words, s.nq, ref->K, ref->s64, s.qdb.ng, s.qdb.packed, ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "query upload");
@@ -576,6 +600,13 @@ sk_status sk_server_submit(sk_server *sv, const uint64_t *query_words, int64_t n
   auto r = std::make_shared<Request>();
   r->words = query_words;
   r->n = n_queries;
+  {
+    DeviceGuard g(sv->ctx->device);   // the query runs on the server's device, not device 0
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, query_words) == cudaSuccess)
+      r->pinned = attr.type == cudaMemoryTypeHost;
+    cudaGetLastError();   // a pageable pointer is not an error worth keeping
+  }
   if (cluster) {
     r->cluster.assign(cluster, cluster + n_queries);
   } else {

@@ -109,6 +109,9 @@ struct WorkItem {
   int16_t k0, k1;
   int32_t split;    // split slot, -1 for a whole tile
   int32_t nparts;   // items sharing the split slot
+  int32_t b0, b1;   // 32-bin blocks [b0, b1) of each k; b1 == 0: all of them
+  int16_t bpart, nbpart;  // block range index, ranges per k (0: one)
+  int32_t pad;
 };
 
 // Everything one launch needs: the job table, the work list and the scratch.

@@ -155,7 +155,10 @@ sk_status build_job(sk_ctx *ctx, const sk_db *ref, const sk_db *query, const sk_
                     JobParams *jp);
 sk_status launch_job(sk_ctx *ctx, const JobParams &jp, const TileConfig &cfg);
 void plan_items(const std::vector<JobParams> &jobs, int grid, Plan &plan);
-void split_tail(std::vector<WorkItem> &items, size_t begin, int grid, int32_t *n_splits);
+void split_tail(std::vector<WorkItem> &items, size_t begin, int grid, int32_t *n_splits,
+                const std::vector<JobParams> *jobs = nullptr);
+int32_t items_slots(const std::vector<WorkItem> &items, int32_t base);
+int32_t tail_block_parts(const JobParams &jp);
 sk_status db_alloc(sk_ctx *ctx, int64_t n, const int32_t *kmers, int32_t K, int32_t s64,
                    int32_t bbits, sk_db **out, int packed_slot = -1);
 void db_free(sk_db *db);

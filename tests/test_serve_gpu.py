@@ -309,3 +309,31 @@ def test_priority_slicing_with_equal_base(setup):
         server.close()
         rnd.close()
         ref.close()
+
+
+def test_pinned_and_pageable_requests_agree(setup):
+    """A request in page-locked memory is uploaded straight from it, a
+    pageable one is staged; both give the same results, also when they share
+    a slice."""
+    import torch
+    ctx, ref, ref_words, queries, kmers = setup
+    q = queries[:90]
+    pinned = torch.empty(q.size, dtype=torch.int64).pin_memory()
+    pinned.numpy().view(np.uint64)[:] = q.reshape(-1)
+    qp = pinned.numpy().view(np.uint64).reshape(q.shape)
+    server = capi.Server(ctx, ref, slots=1, slice_queries=256, kNN=5, keep_rows=True)
+    try:
+        busy = server.submit(queries[200:456])       # occupies the one slot
+        ts = [server.submit(qp[:40]), server.submit(q[40:90]), server.submit(qp[40:90])]
+        server.wait(busy)
+        server.result(busy)
+        got = []
+        for t in ts:
+            server.wait(t)
+            got.append(server.result(t)[:3])
+        assert server.info()["slices_shared"] >= 1
+        for a, b in zip(got[1], got[2]):
+            np.testing.assert_array_equal(a, b)
+        check(got[0], oracle_expected(ref_words, q[:40], kmers, 5))
+    finally:
+        server.close()
