@@ -850,7 +850,7 @@ def run_dropin(device, words, steps):
                     "result)"}
 
 
-def rounded(x, digits=4):
+def rounded(x, digits=6):
     """Floats rounded to `digits` significant digits, recursively (the bench
     line stays one short line)."""
     if isinstance(x, float):

@@ -663,14 +663,17 @@ void not_in_path(const char *what) {
 }
 
 py::dict load_sketch_db(const std::string &db_name, std::vector<std::string> names,
-                        std::vector<size_t> kmer_lengths) {
+                        std::vector<size_t> kmer_lengths, int threads) {
   if (names.empty()) names = skhost::list_samples(db_name);
-  skhost::SketchSet s = skhost::load_sketches(db_name, names, to_kmers(kmer_lengths));
+  if (names.empty()) throw std::runtime_error("Database " + db_name + " holds no sketches");
+  const std::vector<int32_t> kmers = to_kmers(kmer_lengths);
+  skhost::SketchSet s;
+  const py::ssize_t W = static_cast<py::ssize_t>(skhost::sketch_words_per_k(db_name, names[0]));
+  py::array_t<uint64_t> words({static_cast<py::ssize_t>(names.size()),
+                               static_cast<py::ssize_t>(kmers.size()), W});
+  // the same multi-threaded read queryDatabase uses, into the numpy array
+  skhost::load_sketches_into(db_name, names, kmers, s, words.mutable_data(), threads);
   py::dict d;
-  const py::ssize_t W = static_cast<py::ssize_t>(s.sketchsize64) * s.bbits;
-  py::array_t<uint64_t> words({static_cast<py::ssize_t>(s.size()),
-                               static_cast<py::ssize_t>(s.kmers.size()), W});
-  std::copy(s.words.begin(), s.words.end(), words.mutable_data());
   d["names"] = s.names;
   d["kmers"] = s.kmers;
   d["sketchsize64"] = s.sketchsize64;
@@ -749,7 +752,7 @@ PYBIND11_MODULE(_pp_sketchlib, m) {
 
   // not in the reference module: reads a database's sketches (tests, tools)
   m.def("_load_sketch_db", &load_sketch_db, py::arg("db_name"),
-        py::arg("names") = std::vector<std::string>{}, py::arg("klist"));
+        py::arg("names") = std::vector<std::string>{}, py::arg("klist"), py::arg("threads") = 1);
 
   m.def("_load_random", &load_random_model, py::arg("db_name"));
 

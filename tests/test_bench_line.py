@@ -66,5 +66,5 @@ def test_compact_line_is_short_and_complete():
     assert line["e2e"]["h2d_bytes_per_step"] == 1
     assert line["serving"]["q100"]["p99_under_50ms"] is True
     assert line["parity"]["genomes"]["acc_above_1e-5_f32"] == 1
-    assert line["roofline"]["frac"] == 0.7635 and line["ms_per_step"] == 20.79
+    assert line["roofline"]["frac"] == 0.763457 and line["ms_per_step"] == 20.7891
     assert line["config"] == bench.workload_config()

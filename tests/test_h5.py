@@ -46,6 +46,20 @@ def test_sketches_roundtrip(tmp_path):
     np.testing.assert_array_equal(sub["words"][:, 1], words[[7, 3, 250], 0])
 
 
+def test_threaded_read_matches(tmp_path):
+    """The multi-threaded read (what queryDatabase uses, straight from the
+    mapped file into the caller's buffer) gives the single-threaded result,
+    errors included."""
+    path, names, words, kmers, lengths, bases = _db(tmp_path, n=257)
+    one = pp_sketchlib._load_sketch_db(path, names, kmers, threads=1)
+    many = pp_sketchlib._load_sketch_db(path, names, kmers, threads=8)
+    np.testing.assert_array_equal(one["words"], words)
+    np.testing.assert_array_equal(many["words"], words)
+    assert many["length"] == one["length"] and many["base_freq"] == one["base_freq"]
+    with pytest.raises(pp_sketchlib.HDF5Exception, match="Missing sketch"):
+        pp_sketchlib._load_sketch_db(path, names[:100] + ["nope"] + names[100:], kmers, threads=8)
+
+
 def test_missing_sample_and_kmer(tmp_path):
     path, names, *_ = _db(tmp_path, n=4)
     with pytest.raises(pp_sketchlib.HDF5Exception, match="Missing sketch"):
