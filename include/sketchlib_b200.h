@@ -358,7 +358,7 @@ typedef struct sk_server_params {
   int32_t slots;          /* slices on the device at once (one stream each), 1..16 */
   int32_t slice_queries;  /* largest number of queries per slice; a request of at
                              most this many runs as one slice at high priority */
-  int32_t kNN;            /* nearest references returned per query, 0..800 */
+  int32_t kNN;            /* nearest references returned per query, 0..n_refs */
   int32_t dist_col;       /* distance the kNN ranks by: 0 core, 1 accessory */
   int32_t keep_rows;      /* 1: also return each query's core/accessory row */
   int32_t large_slice_queries;  /* slice size for larger requests, 1..slice_queries

@@ -265,6 +265,166 @@ __global__ void knn_rows_kernel(const float *__restrict__ vals, int64_t n_rows, 
   }
 }
 
+// Row kNN for any kNN up to the row length (the kernels above keep kNN lists
+// per lane in shared memory, up to kKnnListMax entries).  One CTA per row, in four steps:
+//  1. radix select over the 32-bit order-preserving image of the key (four
+//     8-bit digits, most significant first; a 256-bin shared histogram per
+//     pass over the row) finds the bucket [lo, hi] of keys that holds the
+//     kNN-th smallest, and how many of its entries (need) are taken;
+//  2. one more pass gathers every entry below lo, and the first `need`
+//     entries of the bucket in column order (a CTA-wide ordered scan), as
+//     64-bit (key image << 32 | column) words: unique, so their order is the
+//     (key, column) order of the per-lane lists above;
+//  3. a bitonic network with every comparator ascending sorts the kNN words;
+//     positions past kNN act as +inf and are never touched, so the list
+//     needs no padding.  It sorts in shared memory, or in the row's own
+//     output slots (j_out, 8 bytes per entry) when the list is larger than
+//     kKnnSmemList;
+//  4. the words become (column, key) outputs.
+// Keys are the distances (1 - J for Jaccard), the row's own column (diag0 >=
+// 0) +inf, -0 read as +0.
+constexpr int kKnnSelectThreads = 512;
+constexpr int kKnnSmemList = 12288;   // 96 KiB of 64-bit words
+
+__device__ __forceinline__ uint32_t key_image(float f) {
+  if (f == 0.0f) f = 0.0f;
+  const uint32_t b = __float_as_uint(f);
+  return b ^ ((b >> 31) ? 0xFFFFFFFFu : 0x80000000u);
+}
+
+__device__ __forceinline__ float image_key(uint32_t u) {
+  return __uint_as_float(u ^ ((u >> 31) ? 0x80000000u : 0xFFFFFFFFu));
+}
+
+__global__ void __launch_bounds__(kKnnSelectThreads)
+knn_select_kernel(const float *__restrict__ vals, int64_t n_rows, int64_t n_cols, int knn,
+                  int64_t diag0, int jaccard, int64_t *__restrict__ j_out,
+                  float *__restrict__ d_out) {
+  extern __shared__ unsigned long long sel_list[];
+  __shared__ unsigned int hist[256];
+  __shared__ unsigned int warp_tot[kKnnSelectThreads / 32];
+  __shared__ unsigned int s_digit, s_before, s_bucket, s_less;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int NW = kKnnSelectThreads / 32;
+  for (int64_t row = blockIdx.x; row < n_rows; row += gridDim.x) {
+    const float *v = vals + row * n_cols;
+    const int64_t own = diag0 >= 0 ? diag0 + row : -1;
+    auto image = [&](int64_t c) -> uint32_t {
+      float d = c == own ? INFINITY : v[c];
+      if (jaccard && c != own) d = 1.0f - d;
+      return key_image(d);
+    };
+
+    // 1. the bucket of the kNN-th smallest key
+    uint32_t prefix = 0, mask = 0;
+    unsigned int rank = static_cast<unsigned int>(knn);
+    for (int shift = 24; shift >= 0; shift -= 8) {
+      for (int i = tid; i < 256; i += kKnnSelectThreads) hist[i] = 0;
+      __syncthreads();
+      for (int64_t c = tid; c < n_cols; c += kKnnSelectThreads) {
+        const uint32_t u = image(c);
+        if ((u & mask) == prefix) atomicAdd(&hist[(u >> shift) & 255u], 1u);
+      }
+      __syncthreads();
+      if (warp == 0) {
+        unsigned int h[8], sum = 0;
+#pragma unroll
+        for (int b = 0; b < 8; ++b) sum += (h[b] = hist[8 * lane + b]);
+        unsigned int incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const unsigned int t = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += t;
+        }
+        const unsigned int hit = __ballot_sync(0xffffffffu, incl >= rank);
+        if (lane == __ffs(hit) - 1) {
+          unsigned int cum = incl - sum;
+          for (int b = 0; b < 8; ++b) {
+            if (cum + h[b] >= rank) {
+              s_digit = 8 * lane + b;
+              s_before = cum;
+              s_bucket = h[b];
+              break;
+            }
+            cum += h[b];
+          }
+        }
+      }
+      __syncthreads();
+      prefix |= s_digit << shift;
+      mask |= 255u << shift;
+      rank -= s_before;
+      const bool whole = s_bucket == rank;   // every entry of the bucket is taken
+      __syncthreads();
+      if (whole) break;
+    }
+    const uint32_t lo = prefix, hi = prefix | ~mask;
+    const unsigned int need = rank;
+
+    // 2. gather: below the bucket in any order, the bucket in column order
+    unsigned long long *list =
+        knn <= kKnnSmemList ? sel_list : reinterpret_cast<unsigned long long *>(j_out + row * knn);
+    if (tid == 0) s_less = 0;
+    __syncthreads();
+    const unsigned int n_less = static_cast<unsigned int>(knn) - need;
+    unsigned int taken = 0;   // bucket entries taken so far (CTA-uniform)
+    unsigned int less = 0;    // entries below the bucket gathered so far (CTA-uniform)
+    for (int64_t c0 = 0; c0 < n_cols && (taken < need || less < n_less); c0 += kKnnSelectThreads) {
+      const int64_t c = c0 + tid;
+      const uint32_t u = c < n_cols ? image(c) : 0xFFFFFFFFu;
+      const bool in = c < n_cols && u >= lo && u <= hi;
+      if (c < n_cols && u < lo) {
+        const unsigned int slot = atomicAdd(&s_less, 1u);
+        list[slot] = (static_cast<unsigned long long>(u) << 32) | static_cast<uint32_t>(c);
+      }
+      const unsigned int bal = __ballot_sync(0xffffffffu, in);
+      if (lane == 0) warp_tot[warp] = __popc(bal);
+      __syncthreads();
+      unsigned int before = 0, total = 0;
+      for (int w = 0; w < NW; ++w) {
+        const unsigned int t = warp_tot[w];
+        if (w < warp) before += t;
+        total += t;
+      }
+      const unsigned int r = taken + before + __popc(bal & ((1u << lane) - 1u));
+      if (in && r < need)
+        list[n_less + r] = (static_cast<unsigned long long>(u) << 32) | static_cast<uint32_t>(c);
+      taken += total;
+      less = s_less;   // read between the two barriers: no thread adds to it here
+      __syncthreads();
+    }
+
+    // 3. sort the kNN words ascending (positions >= knn are +inf)
+    int P = 1;
+    while (P < knn) P <<= 1;
+    for (int k = 2; k <= P; k <<= 1) {
+      for (int h = k >> 1; h >= 1; h >>= 1) {
+        for (int t = tid; t < P / 2; t += kKnnSelectThreads) {
+          const int i = (t / h) * 2 * h + (t % h);
+          const int j = h == (k >> 1) ? (i ^ (k - 1)) : i + h;   // mirror, then half-cleaners
+          if (j < knn) {
+            const unsigned long long a = list[i], b = list[j];
+            if (b < a) {
+              list[i] = b;
+              list[j] = a;
+            }
+          }
+        }
+        __syncthreads();
+      }
+    }
+
+    // 4. outputs
+    for (int e = tid; e < knn; e += kKnnSelectThreads) {
+      const unsigned long long w = list[e];
+      const float key = image_key(static_cast<uint32_t>(w >> 32));
+      j_out[row * knn + e] = static_cast<int64_t>(w & 0xFFFFFFFFull);
+      d_out[row * knn + e] = jaccard ? 1.0f - key : key;
+    }
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------- threshold sparse
 
 // Row i of the square form above the diagonal is condensed entries
@@ -385,6 +545,7 @@ cudaError_t launch_synth(const int32_t *parent, const uint32_t *thresh, int64_t 
 
 cudaError_t launch_knn_self(const float *col_vals, int64_t n, int32_t knn, int32_t jaccard,
                             int64_t *j_out, float *d_out, cudaStream_t stream) {
+  if (knn > kKnnListMax || knn > n) return cudaErrorInvalidValue;
   const int smem = 32 * knn * 8;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(knn_self_kernel,
@@ -399,6 +560,19 @@ cudaError_t launch_knn_self(const float *col_vals, int64_t n, int32_t knn, int32
 cudaError_t launch_knn_rows(const float *vals, int64_t n_rows, int64_t n_cols, int32_t knn,
                             int64_t diag0, int32_t jaccard, int64_t *j_out, float *d_out,
                             cudaStream_t stream) {
+  if (knn > n_cols) return cudaErrorInvalidValue;
+  if (knn > kKnnListMax) {
+    const int smem = knn <= kKnnSmemList ? knn * 8 : 0;
+    if (smem > 48 * 1024) {
+      const cudaError_t attr = cudaFuncSetAttribute(
+          knn_select_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kKnnSmemList * 8);
+      if (attr != cudaSuccess) return attr;
+    }
+    const int blocks = static_cast<int>(n_rows < 148 * 4 ? n_rows : 148 * 4);
+    knn_select_kernel<<<blocks > 0 ? blocks : 1, kKnnSelectThreads, smem, stream>>>(
+        vals, n_rows, n_cols, knn, diag0, jaccard, j_out, d_out);
+    return cudaGetLastError();
+  }
   const int smem = 32 * knn * 8;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(knn_rows_kernel,

@@ -1224,7 +1224,6 @@ sk_status sk_dists_knn(sk_ctx *ctx, const sk_db *db, const sk_random *random, in
   if ((jaccard && dist_col >= db->K) || (dist_col != 0 && dist_col != 1))
     return fail(ctx, SK_EINVAL, "dist_col out of range");
   if (kNN < 0 || kNN > db->n) return fail(ctx, SK_EINVAL, "kNN must be between 0 and the number of samples");
-  if (kNN > 800) return fail(ctx, SK_ENOTSUP, "kNN above 800 is not supported");
   if (kNN == 0) return SK_OK;
   const int64_t n = db->n, pairs = n_pairs(db, nullptr);
   void *d_vals = nullptr, *d_res = nullptr;
@@ -1236,7 +1235,8 @@ sk_status sk_dists_knn(sk_ctx *ctx, const sk_db *db, const sk_random *random, in
   const int out_col = jaccard ? 2 + dist_col : dist_col;
   const size_t budget = dense_budget(ctx);
   cudaError_t e = cudaSuccess;
-  if (static_cast<size_t>(pairs) * 4 > budget) {
+  if (static_cast<size_t>(pairs) * 4 > budget || kNN > kKnnListMax) {
+    // longer lists are selected over dense rows: rows in blocks against every column
     st = knn_blocked(ctx, db, db, true, random, kNN, out_col, jaccard, d_j, d_d, budget);
     if (st != SK_OK) return st;
   } else {
@@ -1266,7 +1266,6 @@ sk_status sk_query_knn(sk_ctx *ctx, const sk_db *ref, const sk_db *query, const 
     return fail(ctx, SK_EINVAL, "Query with empty ref or query list!");
   if (dist_col != 0 && dist_col != 1) return fail(ctx, SK_EINVAL, "dist_col out of range");
   if (kNN < 0 || kNN > ref->n) return fail(ctx, SK_EINVAL, "kNN must be between 0 and the number of references");
-  if (kNN > 800) return fail(ctx, SK_ENOTSUP, "kNN above 800 is not supported");
   if (kNN == 0) return SK_OK;
   const int64_t pairs = n_pairs(ref, query);
   void *d_vals = nullptr, *d_res = nullptr;

@@ -544,7 +544,7 @@ sk_status sk_server_create(sk_ctx *ctx, const sk_db *ref, const sk_random *rando
   const sk_server_params &p = *params;
   if (p.slots < 1 || p.slots > 16 || p.slice_queries < 1 || p.slice_queries > 65536 ||
       p.large_slice_queries < 0 || p.large_slice_queries > p.slice_queries ||
-      p.kNN < 0 || p.kNN > 800 || p.kNN > ref->n || (p.dist_col != 0 && p.dist_col != 1) ||
+      p.kNN < 0 || p.kNN > ref->n || (p.dist_col != 0 && p.dist_col != 1) ||
       p.device_bytes < 0)
     return fail(ctx, SK_EINVAL, "bad server parameters");
   if (random && random->kmers != ref->kmers)

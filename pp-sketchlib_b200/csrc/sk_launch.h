@@ -46,6 +46,10 @@ cudaError_t launch_unpack(const uint32_t *packed, int64_t n, int32_t n_kmers, in
 cudaError_t launch_synth(const int32_t *parent, const uint32_t *thresh, int64_t n,
                          int32_t n_kmers, int32_t s64, uint64_t seed, uint64_t *words,
                          cudaStream_t stream);
+// kNN lists of at most kKnnListMax entries are kept per lane in shared memory
+// (the condensed self column and dense rows); longer ones only over dense
+// rows, by radix select and a bitonic sort per row.
+constexpr int kKnnListMax = 800;
 cudaError_t launch_knn_self(const float *col_vals, int64_t n, int32_t knn, int32_t jaccard,
                             int64_t *j_out, float *d_out, cudaStream_t stream);
 cudaError_t launch_knn_rows(const float *vals, int64_t n_rows, int64_t n_cols, int32_t knn,

@@ -337,3 +337,23 @@ def test_pinned_and_pageable_requests_agree(setup):
         check(got[0], oracle_expected(ref_words, q[:40], kmers, 5))
     finally:
         server.close()
+
+
+def test_long_knn_lists(setup):
+    """kNN above the per-lane list length (radix select per row) through the
+    server equals query_knn on the same queries."""
+    ctx, ref, ref_words, queries, kmers = setup
+    q = queries[:70]
+    server = capi.Server(ctx, ref, slots=2, slice_queries=64, kNN=1000, keep_rows=True)
+    try:
+        t = server.submit(q)
+        server.wait(t)
+        idx, dist, rows, _ = server.result(t)
+    finally:
+        server.close()
+    qry = capi.Database(ctx, q, kmers, S64)
+    r, d = capi.query_knn(ctx, ref, qry, 1000, dist_col=0)
+    qry.close()
+    np.testing.assert_array_equal(idx, r)
+    np.testing.assert_array_equal(dist, d)
+    check((idx, dist, rows), oracle_expected(ref_words, q, kmers, 1000))
