@@ -10,6 +10,7 @@
 #include <cstdint>
 
 #include "sk_common.h"
+#include "sk_device.cuh"
 #include "sk_launch.h"
 
 namespace sk {
@@ -425,6 +426,21 @@ knn_select_kernel(const float *__restrict__ vals, int64_t n_rows, int64_t n_cols
   }
 }
 
+// ------------------------------------------------------------ count tables
+
+// Jaccard (no random-match correction) and its logarithm for every count
+// 0 .. n-1 of a union of `union_bits` bins, by the epilogue's own functions,
+// so a table entry is bit-identical to the per-pair computation it replaces.
+__global__ void count_table_kernel(double union_bits, int64_t n, float *__restrict__ jtab,
+                                   double *__restrict__ ltab) {
+  for (int64_t c = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; c < n;
+       c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const float j = corrected_jaccard(static_cast<uint32_t>(c), union_bits, 0.0);
+    jtab[c] = j;
+    ltab[c] = log(static_cast<double>(j));
+  }
+}
+
 // ---------------------------------------------------------- threshold sparse
 
 // Row i of the square form above the diagonal is condensed entries
@@ -582,6 +598,12 @@ cudaError_t launch_knn_rows(const float *vals, int64_t n_rows, int64_t n_cols, i
   const int blocks = static_cast<int>(n_rows < 148 * 64 ? n_rows : 148 * 64);
   knn_rows_kernel<<<blocks > 0 ? blocks : 1, 32, smem, stream>>>(vals, n_rows, n_cols, knn, diag0,
                                                                  jaccard, j_out, d_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_count_tables(double union_bits, int64_t n, float *jtab, double *ltab,
+                                cudaStream_t stream) {
+  count_table_kernel<<<grid_for(n, kThreads), kThreads, 0, stream>>>(union_bits, n, jtab, ltab);
   return cudaGetLastError();
 }
 

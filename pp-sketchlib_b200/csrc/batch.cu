@@ -73,6 +73,7 @@ sk_status build_jobs(sk_ctx *ctx, const sk_job *in, int n, const TileConfig &cfg
     sk_status st = build_job(ctx, in[j].ref, in[j].query, in[j].random, in[j].out_mode, 0,
                              in[j].out, &used, &jobs[j]);
     ctx->tile_cfg = saved;
+    if (st == SK_OK) st = attach_count_tables(ctx, &jobs[j]);
     if (st != SK_OK) return st;
     *pairs += n_pairs(in[j].ref, in[j].query);
   }

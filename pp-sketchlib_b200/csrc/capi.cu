@@ -50,12 +50,43 @@ sk_status cuda_fail(sk_ctx *ctx, cudaError_t e, const char *what) {
 
 static std::mutex g_ctx_refs_mu;
 
+sk_status attach_count_tables(sk_ctx *ctx, JobParams *jp, bool alloc) {
+  if (jp->rmode != kRandNone || jp->semantics == kSemRefGpu || jp->out_mode == kOutCounts ||
+      jp->nchunk != 1)
+    return SK_OK;
+  const int64_t bins = static_cast<int64_t>(jp->union_bits);
+  std::lock_guard<std::mutex> lock(ctx->count_tables_mu);
+  auto it = ctx->count_tables.find(bins);
+  if (it == ctx->count_tables.end()) {
+    if (!alloc) return SK_OK;
+    float *jt = nullptr;
+    double *lt = nullptr;
+    cudaError_t e = cudaMalloc(&jt, (bins + 1) * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&lt, (bins + 1) * sizeof(double));
+    if (e == cudaSuccess) e = launch_count_tables(jp->union_bits, bins + 1, jt, lt, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+      if (jt) cudaFree(jt);
+      if (lt) cudaFree(lt);
+      return cuda_fail(ctx, e, "count tables");
+    }
+    it = ctx->count_tables.emplace(bins, std::make_pair(jt, lt)).first;
+  }
+  jp->jtab = it->second.first;
+  jp->ltab = it->second.second;
+  return SK_OK;
+}
+
 static void ctx_free(sk_ctx *ctx) {
   {
     DeviceGuard g(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (auto &s : ctx->scratch)
       if (s.ptr) cudaFree(s.ptr);
+    for (auto &t : ctx->count_tables) {
+      cudaFree(t.second.first);
+      cudaFree(t.second.second);
+    }
     if (ctx->status_dev) cudaFree(ctx->status_dev);
     if (ctx->cancel_host) cudaFreeHost(ctx->cancel_host);
     if (ctx->stream && ctx->own_stream) cudaStreamDestroy(ctx->stream);
@@ -554,6 +585,7 @@ sk_status dense_to_device(sk_ctx *ctx, const sk_db *ref, const sk_db *query,
   JobParams jp;
   const TileConfig *cfg = nullptr;
   sk_status st = build_job(ctx, ref, query, random, out_mode, out_col, d_out, &cfg, &jp);
+  if (st == SK_OK) st = attach_count_tables(ctx, &jp);
   if (st != SK_OK) return st;
   return launch_job(ctx, jp, *cfg);
 }
@@ -594,6 +626,7 @@ sk_status dense_blocked_to_host(sk_ctx *ctx, const sk_db *ref, const sk_db *quer
   JobParams base;
   const TileConfig *cfg = nullptr;
   sk_status st = build_job(ctx, ref, query, random, out_mode, 0, nullptr, &cfg, &base);
+  if (st == SK_OK) st = attach_count_tables(ctx, &base);
   if (st != SK_OK) return st;
   st = ensure_copy_stream(ctx);
   if (st != SK_OK) return st;
@@ -743,6 +776,7 @@ sk_status knn_blocked(sk_ctx *ctx, const sk_db *cols, const sk_db *rows, bool se
     JobParams jp;
     const TileConfig *cfg = nullptr;
     st = build_job(ctx, cols, &view, random, kOutColumn, out_col, d_vals, &cfg, &jp);
+    if (st == SK_OK) st = attach_count_tables(ctx, &jp);
     if (st != SK_OK) return st;
     if (self) {
       jp.self_view = 1;

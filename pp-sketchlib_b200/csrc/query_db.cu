@@ -136,6 +136,7 @@ extern "C" sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
   JobParams jp;
   const TileConfig *cfg = nullptr;
   st = build_job(ctx, dbs.ref, dbs.query, random, out_mode, 0, d_out, &cfg, &jp);
+  if (st == SK_OK) st = attach_count_tables(ctx, &jp);
   if (st != SK_OK) return st;
   const int grid = resident_grid(ctx, *cfg);
   if (grid < 1) return fail(ctx, SK_ECUDA, "Tile configuration %d does not fit the device", cfg->id);

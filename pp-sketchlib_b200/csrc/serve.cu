@@ -194,6 +194,8 @@ sk_status reserve_slice_scratch(sk_server *sv, Slot &s, int64_t *bytes) {
   const TileConfig *cfg = nullptr;
   sk_status st = build_job(ctx, ref, &s.qdb, sv->random, kOutColumn, sv->params.dist_col,
                            s.d_col, &cfg, &jp);
+  // the slices' Jaccard tables are built now, not on the first request
+  if (st == SK_OK) st = attach_count_tables(ctx, &jp);
   if (st != SK_OK) return st;
   size_t meta = 0, cta = 16, split = 16;
   for (const TileConfig *c : {choose_config(ctx, ref->K, ref->s64), tile_config(kSmallQueryConfig)}) {

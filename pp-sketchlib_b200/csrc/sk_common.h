@@ -69,6 +69,11 @@ struct JobParams {
   int64_t out_row0;            // long-form row held by out[0] (0 unless the output is blocked)
   double tol;                  // 5 / (64 * s64) (src/dist/linear_regression.cpp:22)
   double union_bits;           // 64 * s64 (src/reference.cpp:91)
+  // Jobs without random-match correction: the Jaccard and its logarithm by
+  // intersection count 0 .. union_bits, shared by every pair of the sketch
+  // width (null: the epilogue computes them per pair)
+  const float *jtab;
+  const double *ltab;
   // random-match correction
   int32_t rmode;
   const float *rtable;         // kRandTable: [K][C][C]

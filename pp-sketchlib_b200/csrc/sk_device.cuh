@@ -185,8 +185,9 @@ __device__ __forceinline__ float corrected_jaccard(uint32_t count, double union_
 //   xm = sum x / n, ym = sum y / n,
 //   slope = sum (x - xm) y / sum (x - xm)^2, intercept = ym - slope xm,
 // without fused multiply-adds, in the same operation order as the oracle.
-template <int KMAX>
-__device__ __forceinline__ float2 fit_core_acc(const float (&jf)[KMAX], const JobParams &p) {
+template <int KMAX, bool CHUNKED>
+__device__ __forceinline__ float2 fit_core_acc(const float (&jf)[KMAX], const JobParams &p,
+                                               const uint16_t *counts, int stride) {
   int first = -1, last = -1;
 #pragma unroll
   for (int k = 0; k < k_bound<KMAX>(p); ++k) {
@@ -214,7 +215,8 @@ __device__ __forceinline__ float2 fit_core_acc(const float (&jf)[KMAX], const Jo
 #pragma unroll
   for (int k = 0; k < k_bound<KMAX>(p); ++k) {
     if (k >= first && k <= last) {
-      const double y = log(static_cast<double>(jf[k]));
+      const double y = p.ltab ? p.ltab[pair_count<CHUNKED>(p, counts, stride, k)]
+                              : log(static_cast<double>(jf[k]));
       const double dx = __dsub_rn(static_cast<double>(p.kmers[k]), xm);
       sy = __dadd_rn(sy, y);
       sxx = __dadd_rn(sxx, __dmul_rn(dx, dx));
@@ -318,8 +320,10 @@ __device__ __forceinline__ void finish_pair(const JobParams &p, int64_t gi, int6
 #pragma unroll
   for (int k = 0; k < k_bound<KMAX>(p); ++k) {
     jf[k] = 0.0f;
-    if (k < K) jf[k] = corrected_jaccard(pair_count<CHUNKED>(p, counts, stride, k), p.union_bits,
-                                         random_match(p, k, gi, gj));
+    if (k < K) {
+      const uint32_t c = pair_count<CHUNKED>(p, counts, stride, k);
+      jf[k] = p.jtab ? p.jtab[c] : corrected_jaccard(c, p.union_bits, random_match(p, k, gi, gj));
+    }
   }
   if (p.out_mode == kOutJaccard) {
     float *o = static_cast<float *>(p.out) + row * K;
@@ -336,7 +340,7 @@ __device__ __forceinline__ void finish_pair(const JobParams &p, int64_t gi, int6
     static_cast<float *>(p.out)[row] = v;
     return;
   }
-  const float2 ca = fit_core_acc<KMAX>(jf, p);
+  const float2 ca = fit_core_acc<KMAX, CHUNKED>(jf, p, counts, stride);
   if (p.out_mode == kOutCoreAcc) {
     static_cast<float2 *>(p.out)[row] = ca;
   } else {

@@ -55,6 +55,10 @@ cudaError_t launch_knn_self(const float *col_vals, int64_t n, int32_t knn, int32
 cudaError_t launch_knn_rows(const float *vals, int64_t n_rows, int64_t n_cols, int32_t knn,
                             int64_t diag0, int32_t jaccard, int64_t *j_out, float *d_out,
                             cudaStream_t stream);
+// Jaccard / log-Jaccard by intersection count 0 .. n-1 for jobs without
+// random-match correction (JobParams::jtab / ltab).
+cudaError_t launch_count_tables(double union_bits, int64_t n, float *jtab, double *ltab,
+                                cudaStream_t stream);
 cudaError_t launch_threshold_count(const float *vals, int64_t n, int32_t stride, int32_t col,
                                    float cutoff, int64_t *row_counts, cudaStream_t stream);
 cudaError_t launch_threshold_fill(const float *vals, int64_t n, int32_t stride, int32_t col,

@@ -67,6 +67,10 @@ struct sk_ctx {
   std::map<std::pair<int, int>, int> tuning;      // (K, s64) -> shape id
   Scratch scratch[kSlotCount];                    // reusable device buffers
   void *noalloc_scratch = nullptr;                // device address of the static no-alloc buffer
+  // Jaccard / log-Jaccard tables by count of uncorrected jobs, per union size
+  // (64 * sketchsize64); allocated on first use, freed with the context
+  std::map<int64_t, std::pair<float *, double *>> count_tables;
+  std::mutex count_tables_mu;
   std::recursive_mutex mu;
   // Databases and random models keep their context alive: sk_ctx_destroy only
   // marks it, the last dependent handle to go frees it.
@@ -154,6 +158,13 @@ sk_status build_job(sk_ctx *ctx, const sk_db *ref, const sk_db *query, const sk_
                     int out_mode, int out_col, void *d_out, const TileConfig **cfg_out,
                     JobParams *jp);
 sk_status launch_job(sk_ctx *ctx, const JobParams &jp, const TileConfig &cfg);
+// Points an uncorrected job at the context's Jaccard / log-Jaccard tables for
+// its union size, building them on first use (one allocation and a small
+// kernel, then a wait on the context stream).  alloc false: only tables that
+// already exist are used.  Jobs with random-match correction, the reference
+// GPU semantics, count output or sketches counted in chunks are left as they
+// are (their epilogue computes per pair).
+sk_status attach_count_tables(sk_ctx *ctx, JobParams *jp, bool alloc = true);
 void plan_items(const std::vector<JobParams> &jobs, int grid, Plan &plan);
 void split_tail(std::vector<WorkItem> &items, size_t begin, int grid, int32_t *n_splits,
                 const std::vector<JobParams> *jobs = nullptr);
