@@ -254,6 +254,23 @@ sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
                       int32_t n_kmers, int32_t sketchsize64, int32_t bbits,
                       const sk_random *random, int32_t out_mode, void *out);
 
+/* sk_query_db for a caller still filling the sketch words (reading them from
+ * a file, say) while the call runs: before the call copies samples
+ * [s0, s0 + n) of one side (side 0 = ref, 1 = query) it calls
+ * ready(user, side, s0, n) on the calling thread, which returns 0 once those
+ * words are in place, or nonzero to abandon the call (SK_ETIMEDOUT).  The
+ * sample counts, cluster ids and sequence lengths must be complete when the
+ * call starts.  Chunks are requested in upload order: an all-vs-all whose
+ * output fits the device from the last samples down, otherwise the queries
+ * first, then the references from the first up.  No reference counterpart: query_db_cuda
+ * starts after every sketch is loaded (src/api.cpp:140-291). */
+typedef int (*sk_words_ready_fn)(void *user, int32_t side, int64_t s0, int64_t n);
+sk_status sk_query_db_ready(sk_ctx *ctx, const sk_host_sketches *ref,
+                            const sk_host_sketches *query, const int32_t *kmers,
+                            int32_t n_kmers, int32_t sketchsize64, int32_t bbits,
+                            const sk_random *random, int32_t out_mode, void *out,
+                            sk_words_ready_fn ready, void *user);
+
 /* Page-locked host memory (cudaHostAlloc, portable) for the sketch words a
  * host program hands to sk_query_db, and its release.  No reference
  * counterpart: query_db_cuda copies from pageable vectors

@@ -47,14 +47,24 @@ int64_t sketch_words_per_k(const std::string &db_name, const std::string &first_
   return f.attr_ints(g, "sketchsize64").at(0) * f.attr_ints(g, "bbits").at(0);
 }
 
-void load_sketches_into(const std::string &db_name, const std::vector<std::string> &names,
-                        const std::vector<int32_t> &kmers, SketchSet &out, uint64_t *dst,
-                        int threads) {
-  h5::File f(h5_path(db_name));
+struct SketchReader::Impl {
+  h5::File f;
+  std::vector<h5::Object> ds;   // [n][K] the samples' datasets
+  size_t K = 0, W = 0;
+  explicit Impl(const std::string &path) : f(path) {}
+};
+
+SketchReader::SketchReader(const std::string &db_name, const std::vector<std::string> &names,
+                           const std::vector<int32_t> &kmers, SketchSet &out, int threads)
+    : impl_(new Impl(h5_path(db_name))) {
+  h5::File &f = impl_->f;
   out.names = names;
   out.kmers = kmers;
   out.words.clear();
   const size_t n = names.size();
+  const size_t K = kmers.size();
+  impl_->K = K;
+  impl_->ds.resize(n * K);
   out.seq_len.assign(n, 0);
   out.bases.assign(n, {});
   std::vector<uint8_t> reads(n, 0);
@@ -99,16 +109,16 @@ void load_sketches_into(const std::string &db_name, const std::vector<std::strin
                                                       : std::vector<double>{0.25, 0.25, 0.25, 0.25};
     if (h5::File::has_attr(g, "reads")) reads[i] = f.attr_ints(g, "reads").at(0) != 0;
     const auto ks = f.members(g);
-    for (size_t ki = 0; ki < kmers.size(); ++ki) {
+    for (size_t ki = 0; ki < K; ++ki) {
       const auto kt = ks.find(std::to_string(kmers[ki]));
       if (kt == ks.end())
         throw h5::Error("Object /sketches/" + names[i] + "/" + std::to_string(kmers[ki]) +
                         " does not exist in " + f.path());
-      const h5::Object ds = f.object_at(kt->second);
+      h5::Object ds = f.object_at(kt->second);
       if (ds.space.count() != W)
         throw std::runtime_error("Sketch " + names[i] + " at k = " + std::to_string(kmers[ki]) +
                                  " has the wrong number of words");
-      f.read_u64(ds, dst + (i * kmers.size() + ki) * W);
+      impl_->ds[i * K + ki] = std::move(ds);
     }
   };
   if (n == 0) return;
@@ -128,9 +138,44 @@ void load_sketches_into(const std::string &db_name, const std::vector<std::strin
   for (auto &th : pool) th.join();
   for (auto &e : errs)
     if (e) std::rethrow_exception(e);
+  impl_->W = W;
   out.sketchsize64 = s64_0;
   out.bbits = bbits_0;
   out.reads = std::any_of(reads.begin(), reads.end(), [](uint8_t r) { return r != 0; });
+}
+
+SketchReader::~SketchReader() = default;
+
+size_t SketchReader::words_per_sample() const { return impl_->K * impl_->W; }
+
+void SketchReader::copy(size_t s0, size_t s1, uint64_t *dst) const {
+  const size_t K = impl_->K, W = impl_->W;
+  for (size_t i = s0; i < s1; ++i)
+    for (size_t ki = 0; ki < K; ++ki)
+      impl_->f.read_u64(impl_->ds[i * K + ki], dst + (i * K + ki) * W);
+}
+
+void load_sketches_into(const std::string &db_name, const std::vector<std::string> &names,
+                        const std::vector<int32_t> &kmers, SketchSet &out, uint64_t *dst,
+                        int threads) {
+  const SketchReader reader(db_name, names, kmers, out, threads);
+  const size_t n = names.size();
+  if (n == 0) return;
+  const int nt = std::max(1, std::min<int>(threads, static_cast<int>(n)));
+  std::vector<std::exception_ptr> errs(nt);
+  auto work = [&](int t) {
+    try {
+      for (size_t i = t; i < n; i += nt) reader.copy(i, i + 1, dst);
+    } catch (...) {
+      errs[t] = std::current_exception();
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nt; ++t) pool.emplace_back(work, t);
+  work(0);
+  for (auto &th : pool) th.join();
+  for (auto &e : errs)
+    if (e) std::rethrow_exception(e);
 }
 
 SketchSet load_sketches(const std::string &db_name, const std::vector<std::string> &names,

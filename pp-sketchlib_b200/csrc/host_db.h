@@ -14,6 +14,7 @@
 
 #include <cstdint>
 #include <map>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -38,6 +39,28 @@ struct SketchSet {
 // before the buffer is sized): out.words stays empty.  Samples are read on up
 // to `threads` threads straight from the mapped file.
 int64_t sketch_words_per_k(const std::string &db_name, const std::string &first_name);
+
+// The same read in two passes.  The constructor reads every sample's
+// attributes and finds its datasets (all of the checks above, on up to
+// `threads` threads) and fills everything of `out` but the words; copy()
+// then moves the words of samples [s0, s1) into dst ([n][K][W], the layout
+// of load_sketches_into), straight from the mapped file, from any thread and
+// in any order -- so a caller can hand the words to the device while later
+// samples are still being read.
+class SketchReader {
+ public:
+  SketchReader(const std::string &db_name, const std::vector<std::string> &names,
+               const std::vector<int32_t> &kmers, SketchSet &out, int threads);
+  ~SketchReader();
+  SketchReader(const SketchReader &) = delete;
+  SketchReader &operator=(const SketchReader &) = delete;
+  void copy(size_t s0, size_t s1, uint64_t *dst) const;
+  size_t words_per_sample() const;   // K * W
+
+ private:
+  struct Impl;
+  std::unique_ptr<Impl> impl_;
+};
 void load_sketches_into(const std::string &db_name, const std::vector<std::string> &names,
                         const std::vector<int32_t> &kmers, SketchSet &out, uint64_t *dst,
                         int threads);

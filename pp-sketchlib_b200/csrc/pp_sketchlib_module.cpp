@@ -26,7 +26,10 @@
 #include <atomic>
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
+#include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -76,19 +79,29 @@ void check(sk_ctx *ctx, sk_status st) {
 // Runs a library call with the GIL released, polling for Ctrl-C like the
 // reference's progress loop (src/gpu/dist.cu:351-370): an interrupt cancels
 // the running kernels (sk_cancel) and raises KeyboardInterrupt here.
+// The wait wakes as soon as the call returns (a 20 ms sleep between polls
+// added 10 ms to a call on average).
 template <class F>
 void run_gpu(sk_ctx *ctx, F &&fn) {
-  std::atomic<bool> done{false};
+  std::mutex mu;
+  std::condition_variable cv;
+  bool done = false;
   sk_status st = SK_OK;
   {
     py::gil_scoped_release release;
     std::thread worker([&] {
-      st = fn();
+      const sk_status s = fn();
+      std::lock_guard<std::mutex> lock(mu);
+      st = s;
       done = true;
+      cv.notify_all();
     });
     bool interrupted = false;
-    while (!done) {
-      std::this_thread::sleep_for(std::chrono::milliseconds(20));
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> lock(mu);
+        if (cv.wait_for(lock, std::chrono::milliseconds(20), [&] { return done; })) break;
+      }
       if (!interrupted) {
         py::gil_scoped_acquire acquire;
         if (PyErr_CheckSignals() != 0) {
@@ -145,7 +158,115 @@ struct PinnedStage {
     return static_cast<uint64_t *>(ptr);
   }
 };
-PinnedStage g_stage;
+PinnedStage g_stage;       // sketch words
+PinnedStage g_out_stage;   // distances (their rows come back while later rows compute)
+
+// Copies a call's sketch words into the page-locked stage on background
+// threads while sk_query_db_ready runs, in blocks of kBlock samples and in
+// the order the upload asks for them (all-vs-all from the last samples down;
+// otherwise the queries, then the references from the first up); the call's
+// ready callback waits for the blocks of the chunk it is about to copy.
+class Prefetch {
+ public:
+  struct Side {
+    const skhost::SketchReader *reader = nullptr;
+    uint64_t *dst = nullptr;
+    size_t n = 0;
+  };
+
+  Prefetch(Side ref, Side query, bool self, int threads) {
+    sides_[0] = ref;
+    sides_[1] = query;
+    for (int s = 0; s < 2; ++s) {
+      const size_t blocks = (sides_[s].n + kBlock - 1) / kBlock;
+      done_[s].reset(new std::atomic<uint8_t>[blocks == 0 ? 1 : blocks]);
+      for (size_t b = 0; b < blocks; ++b) done_[s][b] = 0;
+    }
+    const size_t rb = (ref.n + kBlock - 1) / kBlock, qb = (query.n + kBlock - 1) / kBlock;
+    if (self) {
+      for (size_t b = rb; b-- > 0;) order_.emplace_back(0, b);
+    } else {
+      for (size_t b = 0; b < qb; ++b) order_.emplace_back(1, b);
+      for (size_t b = 0; b < rb; ++b) order_.emplace_back(0, b);
+    }
+    const int nt = std::max(1, std::min<int>(threads, static_cast<int>(order_.size())));
+    for (int t = 0; t < nt; ++t) pool_.emplace_back([this] { work(); });
+  }
+
+  ~Prefetch() { join(); }
+
+  // sk_words_ready_fn: 0 once samples [s0, s0 + n) of `side` are copied
+  static int ready(void *user, int32_t side, int64_t s0, int64_t n) {
+    Prefetch *p = static_cast<Prefetch *>(user);
+    if (side < 0 || side > 1 || n <= 0) return 1;
+    const size_t b0 = static_cast<size_t>(s0) / kBlock, b1 = static_cast<size_t>(s0 + n - 1) / kBlock;
+    std::unique_lock<std::mutex> lock(p->mu_);
+    const bool ok = p->cv_.wait_for(lock, std::chrono::seconds(300), [&] {
+      if (p->failed_) return true;
+      for (size_t b = b0; b <= b1; ++b)
+        if (!p->done_[side][b]) return false;
+      return true;
+    });
+    return ok && !p->failed_ ? 0 : 1;
+  }
+
+  // waits for the copies; rethrows the first error of a copy thread
+  void finish() {
+    join();
+    if (err_) std::rethrow_exception(err_);
+  }
+
+ private:
+  static constexpr size_t kBlock = 32;
+
+  void work() {
+    for (;;) {
+      const size_t i = next_.fetch_add(1);
+      if (i >= order_.size() || failed_) return;
+      const int s = order_[i].first;
+      const size_t b = order_[i].second;
+      try {
+        const size_t s0 = b * kBlock, s1 = std::min(sides_[s].n, s0 + kBlock);
+        sides_[s].reader->copy(s0, s1, sides_[s].dst);
+      } catch (...) {
+        std::lock_guard<std::mutex> lock(mu_);
+        if (!err_) err_ = std::current_exception();
+        failed_ = true;
+        cv_.notify_all();
+        return;
+      }
+      std::lock_guard<std::mutex> lock(mu_);
+      done_[s][b] = 1;
+      cv_.notify_all();
+    }
+  }
+
+  void join() {
+    for (auto &t : pool_)
+      if (t.joinable()) t.join();
+  }
+
+  Side sides_[2];
+  std::vector<std::pair<int, size_t>> order_;
+  std::unique_ptr<std::atomic<uint8_t>[]> done_[2];
+  std::atomic<size_t> next_{0};
+  std::atomic<bool> failed_{false};
+  std::mutex mu_;
+  std::condition_variable cv_;
+  std::exception_ptr err_;
+  std::vector<std::thread> pool_;
+};
+
+// Copies n floats on up to `threads` threads (the result rows from the
+// page-locked stage into the numpy array, whose pages fault in on first touch).
+void parallel_copy(float *dst, const float *src, size_t n, int threads) {
+  const size_t per = std::max<size_t>(1 << 20, (n + threads - 1) / threads);
+  std::vector<std::thread> pool;
+  for (size_t s0 = per; s0 < n; s0 += per)
+    pool.emplace_back([=] { std::memcpy(dst + s0, src + s0, std::min(per, n - s0) * sizeof(float)); });
+  std::memcpy(dst, src, std::min(per, n) * sizeof(float));
+  for (auto &t : pool) t.join();
+}
 
 int loader_threads() {
   const unsigned hw = std::thread::hardware_concurrency();
@@ -228,17 +349,21 @@ py::array_t<float> queryDatabase(const std::string &ref_db_name, const std::stri
   const bool self = ref_db_name == query_db_name && ref_names == query_names;
   // the sketch words go straight from the mapped files into pinned staging
   std::lock_guard<std::mutex> stage_lock(g_stage.mu);
+  std::lock_guard<std::mutex> out_lock(g_out_stage.mu);
   const size_t w_ref = static_cast<size_t>(skhost::sketch_words_per_k(ref_db_name, ref_names[0]));
   const size_t w_query =
       self ? 0 : static_cast<size_t>(skhost::sketch_words_per_k(query_db_name, query_names[0]));
   const size_t ref_words = ref_names.size() * kmers.size() * w_ref;
   const size_t query_words = self ? 0 : query_names.size() * kmers.size() * w_query;
   uint64_t *stage = g_stage.words(ref_words + query_words);
+  // attributes and checks of every sample first; the words follow on
+  // background threads while the upload runs (Prefetch below)
   skhost::SketchSet ref, query;
-  skhost::load_sketches_into(ref_db_name, ref_names, kmers, ref, stage, loader_threads());
+  const skhost::SketchReader ref_reader(ref_db_name, ref_names, kmers, ref, loader_threads());
+  std::unique_ptr<skhost::SketchReader> query_reader;
   if (!self) {
-    skhost::load_sketches_into(query_db_name, query_names, kmers, query, stage + ref_words,
-                               loader_threads());
+    query_reader.reset(
+        new skhost::SketchReader(query_db_name, query_names, kmers, query, loader_threads()));
     // checkSketchParamsMatch (src/gpu/gpu_api.cpp:170-185)
     if (query.bbits != ref.bbits) throw std::runtime_error("Mismatching bbits in sketches");
     if (query.sketchsize64 != ref.sketchsize64)
@@ -263,12 +388,26 @@ py::array_t<float> queryDatabase(const std::string &ref_db_name, const std::stri
   const int64_t rows = self ? n_ref * (n_ref - 1) / 2 : static_cast<int64_t>(query.size()) * n_ref;
   const int64_t cols = jaccard ? static_cast<int64_t>(kmers.size()) : 2;
   py::array_t<float> out({rows, cols});
-  float *dst = out.mutable_data();
-  run_gpu(ctx, [&] {
-    return sk_query_db(ctx, &r, self ? nullptr : &q, kmers.data(),
-                       static_cast<int32_t>(kmers.size()), ref.sketchsize64, ref.bbits, rnd.h,
-                       jaccard ? SK_OUT_JACCARD : SK_OUT_CORE_ACC, dst);
-  });
+  const size_t n_out = static_cast<size_t>(rows) * static_cast<size_t>(cols);
+  float *staged = reinterpret_cast<float *>(g_out_stage.words((n_out + 1) / 2));
+  {
+    Prefetch prefetch({&ref_reader, stage, ref.size()},
+                      {query_reader.get(), stage + ref_words, self ? 0 : query.size()}, self,
+                      loader_threads());
+    try {
+      run_gpu(ctx, [&] {
+        return sk_query_db_ready(ctx, &r, self ? nullptr : &q, kmers.data(),
+                                 static_cast<int32_t>(kmers.size()), ref.sketchsize64, ref.bbits,
+                                 rnd.h, jaccard ? SK_OUT_JACCARD : SK_OUT_CORE_ACC, staged,
+                                 &Prefetch::ready, &prefetch);
+      });
+    } catch (...) {
+      prefetch.finish();   // a failed read explains a failed call best
+      throw;
+    }
+    prefetch.finish();
+  }
+  parallel_copy(out.mutable_data(), staged, n_out, loader_threads());
   return out;
 }
 

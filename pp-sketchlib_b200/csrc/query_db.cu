@@ -100,6 +100,15 @@ extern "C" sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
                                  const sk_host_sketches *query, const int32_t *kmers,
                                  int32_t n_kmers, int32_t sketchsize64, int32_t bbits,
                                  const sk_random *random, int32_t out_mode, void *out) {
+  return sk_query_db_ready(ctx, ref, query, kmers, n_kmers, sketchsize64, bbits, random, out_mode,
+                           out, nullptr, nullptr);
+}
+
+extern "C" sk_status sk_query_db_ready(sk_ctx *ctx, const sk_host_sketches *ref,
+                                       const sk_host_sketches *query, const int32_t *kmers,
+                                       int32_t n_kmers, int32_t sketchsize64, int32_t bbits,
+                                       const sk_random *random, int32_t out_mode, void *out,
+                                       sk_words_ready_fn ready, void *user) {
   if (!ctx) return SK_EINVAL;
   std::lock_guard<std::recursive_mutex> lock(ctx->mu);
   DeviceGuard dev(ctx->device);
@@ -256,6 +265,9 @@ extern "C" sk_status sk_query_db(sk_ctx *ctx, const sk_host_sketches *ref,
   for (size_t i = 0; i < units.size() && e == cudaSuccess; ++i) {
     const Unit &u = units[i];
     const int b = static_cast<int>(i & 1);
+    if (ready && ready(user, u.db == dbs.query ? 1 : 0, u.s0, u.n) != 0)
+      return fail(ctx, SK_ETIMEDOUT, "sketch words of samples %lld..%lld never became ready",
+                  static_cast<long long>(u.s0), static_cast<long long>(u.s0 + u.n - 1));
     if (i >= 2) e = cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_free[b], 0);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(stage[b], u.host, static_cast<size_t>(u.n * wps) * 8, cudaMemcpyHostToDevice,

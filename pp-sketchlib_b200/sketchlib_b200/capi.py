@@ -59,6 +59,7 @@ _SIGNATURES = {
     "sk_dists_rows": (_i64, [_p, _p]),
     "sk_dists_dense": (_i32, [_p, _p, _p, _p, _i32, _p, _i32]),
     "sk_query_db": (_i32, [_p, _p, _p, _p, _i32, _i32, _i32, _p, _i32, _p]),
+    "sk_query_db_ready": (_i32, [_p, _p, _p, _p, _i32, _i32, _i32, _p, _i32, _p, _p, _p]),
     "sk_dists_knn": (_i32, [_p, _p, _p, _i32, _i32, _i32, _p, _p, _p]),
     "sk_query_knn": (_i32, [_p, _p, _p, _p, _i32, _i32, _p, _p]),
     "sk_sparse_threshold": (_i32, [_p, _p, _i64, _i32, _i32, _f32, C.POINTER(_p)]),
@@ -511,11 +512,14 @@ def dists_dense(ctx: Context, ref: Database, query: Database | None = None,
 def query_db(ctx: Context, ref_words, kmers, sketchsize64: int, query_words=None,
              ref_cluster=None, ref_seq_len=None, query_cluster=None, query_seq_len=None,
              random: Random | None = None, out_mode: int = OUT_CORE_ACC, out=None,
-             bbits: int = 14) -> np.ndarray:
+             bbits: int = 14, ready=None) -> np.ndarray:
     """Host sketches in, host distances out (sk_query_db): the upload is
     chunked and overlapped with the distance kernel.  `ref_words` /
     `query_words`: uint64 [n][K][sketchsize64 * bbits]; query_words None =
-    all-vs-all.  Pinned arrays (e.g. from torch's pin_memory) copy fastest."""
+    all-vs-all.  Pinned arrays (e.g. from torch's pin_memory) copy fastest.
+    ready(side, s0, n) -> bool, if given, is asked before each chunk of
+    samples is copied (side 0 ref, 1 query) and returns once its words are in
+    place (sk_query_db_ready); False abandons the call."""
     keep = []
 
     def side(words, cluster, seq_len):
@@ -538,10 +542,20 @@ def query_db(ctx: Context, ref_words, kmers, sketchsize64: int, query_words=None
         else:
             out = np.empty((rows, K), dtype=np.uint32)
     km = np.ascontiguousarray(kmers, np.int32)
-    _check(lib.sk_query_db(ctx.handle, C.byref(r), None if q is None else C.byref(q),
-                           km.ctypes.data, K, sketchsize64, bbits, _h(random), out_mode,
-                           out.ctypes.data), ctx)
+    if ready is None:
+        _check(lib.sk_query_db(ctx.handle, C.byref(r), None if q is None else C.byref(q),
+                               km.ctypes.data, K, sketchsize64, bbits, _h(random), out_mode,
+                               out.ctypes.data), ctx)
+        return out
+    cb = _READY_FN(lambda user, side, s0, n: 0 if ready(side, s0, n) else 1)
+    _check(lib.sk_query_db_ready(ctx.handle, C.byref(r), None if q is None else C.byref(q),
+                                 km.ctypes.data, K, sketchsize64, bbits, _h(random), out_mode,
+                                 out.ctypes.data, C.cast(cb, C.c_void_p), None), ctx)
     return out
+
+
+# sk_words_ready_fn
+_READY_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.c_int64, C.c_int64)
 
 
 def pack_sequences(samples):

@@ -236,3 +236,36 @@ def test_semantics_gpu_matches_reference_kernel(tmp_path):
     with pytest.raises(ValueError):
         pp_sketchlib.queryDatabase(str(tmp_path / "r"), str(tmp_path / "r"), r, r, list(kmers),
                                    semantics="fast")
+
+
+def test_many_samples_read_while_computing(tmp_path):
+    """Databases of several upload chunks: the words are read on background
+    threads while the call runs (all-vs-all from the last samples down, query
+    mode queries first), the rows return through the page-locked stage; the
+    result equals the oracle's, in the caller's sample order, and a repeat
+    call (reused stages) gives the same array."""
+    n, nq, K, s64 = 1300, 150, 4, 16
+    words, kmers = random_sketches(n + nq, K, s64, seed=95)
+    names = [f"s{i:05d}" for i in range(n + nq)]
+    rng = np.random.default_rng(9)
+    lengths = rng.integers(1_000_000, 5_000_000, n + nq)
+    h5write.write_sketch_db(str(tmp_path / "r.h5"), names[:n], words[:n], kmers, s64,
+                            lengths=lengths[:n])
+    h5write.write_sketch_db(str(tmp_path / "q.h5"), names[n:], words[n:], kmers, s64,
+                            lengths=lengths[n:])
+    order = list(rng.permutation(n))                  # not the file's order
+    r = [names[i] for i in order]
+    got = pp_sketchlib.queryDatabase(str(tmp_path / "r"), str(tmp_path / "r"), r, r, list(kmers))
+    L = lengths[order].astype(np.uint64)
+    want = oracle.dists(words[order], kmers, s64, random=_equal_base(L, L))
+    np.testing.assert_allclose(got, want, atol=TOL, rtol=0)
+    again = pp_sketchlib.queryDatabase(str(tmp_path / "r"), str(tmp_path / "r"), r, r, list(kmers))
+    np.testing.assert_array_equal(again, got)
+    q = names[n:]
+    gq = pp_sketchlib.queryDatabase(str(tmp_path / "r"), str(tmp_path / "q"), r, q, list(kmers),
+                                    random_correct=False)
+    wq = oracle.dists(words[order], kmers, s64, query_words=words[n:])
+    np.testing.assert_allclose(gq, wq, atol=TOL, rtol=0)
+    with pytest.raises(pp_sketchlib.HDF5Exception, match="Missing sketch"):
+        pp_sketchlib.queryDatabase(str(tmp_path / "r"), str(tmp_path / "r"), r + ["nope"],
+                                   r + ["nope"], list(kmers))

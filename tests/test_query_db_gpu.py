@@ -95,3 +95,48 @@ def test_empty_and_single_sample(gpu_ctx):
             capi.query_db(gpu_ctx, kmers=kmers, sketchsize64=4, **bad)
     with pytest.raises(capi.SketchlibError):
         capi.query_db(gpu_ctx, words, kmers, 4, bbits=13)
+
+
+@pytest.mark.parametrize("self_", [True, False])
+def test_words_filled_while_the_call_runs(gpu_ctx, self_):
+    """sk_query_db_ready: the words start as zeros and a thread copies them in,
+    chunk by chunk in the order the call asks for them, only when asked; the
+    result equals the call on complete words, and every sample was asked for
+    exactly once before its words were read."""
+    import threading
+    words, kmers = random_sketches(2600, 4, 16, seed=77)
+    qwords = None if self_ else words[:300].copy()
+    rwords = words if self_ else words[300:].copy()
+    want = capi.query_db(gpu_ctx, rwords, kmers, 16, query_words=qwords)
+    sides = [np.zeros_like(rwords), None if self_ else np.zeros_like(qwords)]
+    srcs = [rwords, qwords]
+    asked = [np.zeros(len(rwords), np.int32), None if self_ else np.zeros(len(qwords), np.int32)]
+    order = []
+
+    def ready(side, s0, n):
+        order.append((side, s0, n))
+        asked[side][s0:s0 + n] += 1
+        done = threading.Event()
+
+        def fill():
+            sides[side][s0:s0 + n] = srcs[side][s0:s0 + n]
+            done.set()
+        threading.Thread(target=fill).start()
+        return done.wait(30)
+
+    got = capi.query_db(gpu_ctx, sides[0], kmers, 16, query_words=sides[1], ready=ready)
+    np.testing.assert_array_equal(got, want)
+    assert all((a == 1).all() for a in asked if a is not None)
+    if self_:      # all-vs-all: from the last samples down
+        assert [s0 for _, s0, _ in order] == sorted((s0 for _, s0, _ in order), reverse=True)
+    else:          # the queries first, then the references from the first up
+        assert [side for side, _, _ in order][:1] == [1] and order[-1][0] == 0
+
+
+def test_words_never_ready_abandons_the_call(gpu_ctx):
+    words, kmers = random_sketches(1300, 4, 16, seed=78)
+    with pytest.raises(capi.SketchlibError, match="never became ready"):
+        capi.query_db(gpu_ctx, words, kmers, 16, ready=lambda side, s0, n: s0 > 600)
+    # the context still serves calls
+    np.testing.assert_array_equal(capi.query_db(gpu_ctx, words, kmers, 16),
+                                  capi.query_db(gpu_ctx, words, kmers, 16))
