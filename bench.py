@@ -311,6 +311,17 @@ SKETCH_GENOMES, SKETCH_LEN, SKETCH_SEED = 64, 2_500_000, 0x5EED0001
 SKETCH_PROFILE = ROOT / "profiles" / "sketch_kernel_64_genomes.md"
 
 
+# ALU-pipe instructions one canonical k-mer step of the sketch kernel needs, on
+# 32-bit lanes, counted from its source (csrc/sketch.cu, roll_chunk and the
+# emitter): forward split rotation and table XOR 7, reverse 7, canonical
+# minimum (64-bit compare, two selects) 4, table-index and base-code
+# extraction 2, run-length and window tests 7, reduction mod 2^61 - 1 10,
+# exact bin (64-bit remainder test and increment; its multiplies run on the
+# FMA pipe) 5, bin-minimum test 2.  The ALU utilisation ncu reports (70%)
+# implies about 42 executed per k-mer.
+SKETCH_ALU_OPS_PER_KMER = 44
+
+
 def profiled_alu_pct():
     """ALU-pipe utilisation of the sketch kernel from the committed ncu
     summary (line `alu_pipe_pct: N`), or None."""
@@ -321,7 +332,7 @@ def profiled_alu_pct():
         return None
 
 
-def run_sketch(ctx, dev, steps, warmup, cpu=True):
+def run_sketch(ctx, dev, steps, warmup, cpu=True, alu_peak=None):
     """Sketching of 64 genomes of 2.5 Mb at k = 15..29 odd, sketchsize64 156
     (the CPU parity case's shape): device-resident bases through
     sk_sketch_device (`value`), pinned host bases through sk_sketch (`e2e`),
@@ -375,7 +386,12 @@ def run_sketch(ctx, dev, steps, warmup, cpu=True):
                 "call": "sk_sketch from pinned host bases to pinned host sketches (upload in "
                         "sample chunks overlapped with hashing)",
                 "matches_device_result": bool(np.array_equal(host_words, words_dev))},
-        "roofline": {"bound": "alu", "alu_pipe_pct_ncu": profiled_alu_pct(),
+        "roofline": {"bound": "alu", "alu_ops_per_kmer": SKETCH_ALU_OPS_PER_KMER,
+                     "achieved": kmers_step / sec * SKETCH_ALU_OPS_PER_KMER / 1e12,
+                     "peak": None if not alu_peak else alu_peak / 1e12, "unit": "T ALU op/s",
+                     "frac": None if not alu_peak else
+                     kmers_step / sec * SKETCH_ALU_OPS_PER_KMER / alu_peak,
+                     "alu_pipe_pct_ncu": profiled_alu_pct(),
                      "source": str(SKETCH_PROFILE.relative_to(ROOT))},
     }
     if cpu:
@@ -976,7 +992,8 @@ def run_ours(args, rank, world, local):
         extra["large"] = run_large(ctx, dev, lop3_peak)
     if not args.skip_sketch:
         extra["sketch"] = run_sketch(ctx, dev, max(3, min(args.steps, 10)), max(1, args.warmup),
-                                     cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)
+                                     cpu=rank == 0 and world == 1 and not args.no_cpu_baseline,
+                                     alu_peak=lop3_peak)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -1086,6 +1103,8 @@ def compact_line(line):
     if "sketch" in line:
         sk = line["sketch"]
         out["sketch"] = {"value": sk["value"], "unit": sk["unit"], "e2e": sk["e2e"]["value"]}
+        if sk.get("roofline", {}).get("frac") is not None:
+            out["sketch"]["alu_frac"] = sk["roofline"]["frac"]
         if "cpu_baseline" in sk:
             out["sketch"]["cpu_baseline"] = sk["cpu_baseline"]["value"]
         rd = sk.get("reads", {})
