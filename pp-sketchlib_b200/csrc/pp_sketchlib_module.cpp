@@ -260,6 +260,7 @@ class Prefetch {
 // Copies n floats on up to `threads` threads (the result rows from the
 // page-locked stage into the numpy array, whose pages fault in on first touch).
 void parallel_copy(float *dst, const float *src, size_t n, int threads) {
+  if (n == 0) return;
   const size_t per = std::max<size_t>(1 << 20, (n + threads - 1) / threads);
   std::vector<std::thread> pool;
   for (size_t s0 = per; s0 < n; s0 += per)
