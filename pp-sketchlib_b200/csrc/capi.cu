@@ -309,6 +309,9 @@ sk_status build_job(sk_ctx *ctx, const sk_db *ref, const sk_db *query, const sk_
   jp->rmode = random ? random->mode : kRandNone;
   if (jp->rmode == kRandTable) {
     const int C = random->n_clusters;
+    if ((ref->cluster && ref->max_cluster >= C) || (query && query->cluster && query->max_cluster >= C))
+      return fail(ctx, SK_EINVAL, "Cluster id %d beyond the %d clusters of the random match table",
+                  std::max(ref->max_cluster, query ? query->max_cluster : 0), C);
     jp->rtable = random->table;
     jp->rs_k = C * C;
     // CPU path, self: [k][cluster(i = row)][cluster(j = col)]  (random_match(r1=i, r2=j))
@@ -1079,6 +1082,7 @@ sk_status sk_db_set_sample_info(sk_db *db, const uint16_t *cluster, const uint64
   if (cluster) {
     std::vector<uint16_t> cl(npad, 0);
     std::copy(cluster, cluster + db->n, cl.begin());
+    db->max_cluster = db->n > 0 ? *std::max_element(cluster, cluster + db->n) : 0;
     if (!db->cluster) {
       cudaError_t e = cudaMalloc(&db->cluster, npad * sizeof(uint16_t));
       if (e != cudaSuccess) return cuda_fail(ctx, e, "cluster ids");

@@ -611,6 +611,11 @@ sk_status sk_server_submit(sk_server *sv, const uint64_t *query_words, int64_t n
   }
   if (cluster) {
     r->cluster.assign(cluster, cluster + n_queries);
+    // an id beyond the random-match table would index past it on the device
+    const sk_random *rnd = sv->random;
+    if (rnd && rnd->mode == kRandTable &&
+        *std::max_element(r->cluster.begin(), r->cluster.end()) >= rnd->n_clusters)
+      return SK_EINVAL;
   } else {
     r->cluster.assign(n_queries, 0);
     const sk_random *rnd = sv->random;

@@ -141,19 +141,23 @@ __device__ __forceinline__ int k_bound(const JobParams &p) {
   return KMAX <= kNarrowKmers ? KMAX : p.n_kmers;
 }
 
+// Entry of the Monte Carlo table for (row gi, col gj) at k-mer index k.
+__device__ __forceinline__ int64_t random_table_index(const JobParams &p, int k, int64_t gi,
+                                                      int64_t gj) {
+  int cr = p.cl_rows ? p.cl_rows[gi] : 0;
+  int cc = p.cl_cols ? p.cl_cols[gj] : 0;
+  if (p.self_view && p.row_base + gi > gj) {   // the all-vs-all path sees (gj, row)
+    const int t = cr;
+    cr = cc;
+    cc = t;
+  }
+  return static_cast<int64_t>(k) * p.rs_k + cr * p.rs_row + cc * p.rs_col;
+}
+
 // Random match chance for (row gi, col gj) at k-mer index k
 // (RandomMC::random_match, src/random/random_match.cpp:185-206; csrs :318-336).
 __device__ __forceinline__ double random_match(const JobParams &p, int k, int64_t gi, int64_t gj) {
-  if (p.rmode == kRandTable) {
-    int cr = p.cl_rows ? p.cl_rows[gi] : 0;
-    int cc = p.cl_cols ? p.cl_cols[gj] : 0;
-    if (p.self_view && p.row_base + gi > gj) {   // the all-vs-all path sees (gj, row)
-      const int t = cr;
-      cr = cc;
-      cc = t;
-    }
-    return static_cast<double>(p.rtable[k * p.rs_k + cr * p.rs_row + cc * p.rs_col]);
-  }
+  if (p.rmode == kRandTable) return static_cast<double>(p.rtable[random_table_index(p, k, gi, gj)]);
   if (p.rmode == kRandEqualBase) {
     const double j1 = p.jv_rows[k * p.jv_rows_ld + gi];
     const double j2 = p.jv_cols[k * p.jv_cols_ld + gj];

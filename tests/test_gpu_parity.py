@@ -108,6 +108,22 @@ def test_jaccard_and_coreacc(gpu_ctx, mode, self_):
     assert np.mean(ca == want64) > 0.99
 
 
+def test_cluster_ids_beyond_the_random_table_are_refused(gpu_ctx):
+    """A cluster id >= the table's cluster count would index past the table
+    (and its count tables) on the device: refused before any launch."""
+    K, s64 = 4, 16
+    words, kmers = random_sketches(100, K, s64, seed=23)
+    table = np.full((K, 3, 3), 0.001, np.float32)
+    rnd = capi.Random(gpu_ctx, capi.RANDOM_TABLE, kmers, table=table)
+    ok = _db(gpu_ctx, words, kmers, s64, cluster=np.full(100, 2, np.uint16))
+    capi.dists_dense(gpu_ctx, ok, None, rnd)
+    bad = _db(gpu_ctx, words, kmers, s64, cluster=np.r_[np.zeros(99), 3].astype(np.uint16))
+    with pytest.raises(capi.SketchlibError, match="beyond the 3 clusters"):
+        capi.dists_dense(gpu_ctx, bad, None, rnd)
+    with pytest.raises(capi.SketchlibError, match="beyond the 3 clusters"):
+        capi.dists_dense(gpu_ctx, ok, bad, rnd)
+
+
 @pytest.mark.parametrize("cfg", [c["id"] for c in capi.tile_configs()])
 def test_every_tile_shape_agrees(gpu_ctx, cfg):
     info = {c["id"]: c for c in capi.tile_configs()}[cfg]
