@@ -1,6 +1,6 @@
 // ref_gpu_dists.cu -- launches the reference's own GPU distance kernel.
 //
-// BASELINE / TEST INFRASTRUCTURE ONLY.  oracle/Makefile compiles the
+// Same-GPU comparison and test infrastructure only.  oracle/Makefile compiles the
 // reference's src/gpu/dist.cu for sm_100a from its own tree (with the
 // stand-in header in oracle/ref_gpu_stub/) and links it with this file into
 // oracle/_ref/libref_gpu.so.  This file reproduces what the reference's host
